@@ -1,0 +1,308 @@
+"""ctypes binding of the C ABI in include/genesis_gpu.h.
+
+The shared library is loaded from this package directory.  There is no
+fallback: if ``libgenesis_gpu.so`` is missing or a call fails, an exception
+is raised.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from . import elements as E
+
+LIB_PATH = Path(__file__).resolve().parent / "libgenesis_gpu.so"
+
+GX_FP64, GX_MIXED = 0, 1
+_PRECISION = {"fp64": GX_FP64, "mixed": GX_MIXED}
+
+_D = C.c_double
+_D10 = C.c_double * 10
+
+
+class GxParams(C.Structure):
+    _fields_ = [
+        ("box", C.c_double * 3), ("dt", _D), ("thermal_constant", _D),
+        ("sigma", _D10), ("epsilon_k", _D10), ("charge", _D10),
+        ("lj_cutoff_factor", _D), ("coulomb_constant", _D), ("coulomb_cutoff", _D),
+        ("gravity_constant", _D), ("gravity_cutoff", _D), ("bond_k_bind", _D),
+        ("thermostat_temperature", _D), ("thermostat_tau", _D),
+        ("enable_electrostatics", C.c_int32), ("enable_gravity", C.c_int32),
+        ("enable_bond_interaction", C.c_int32), ("enable_thermostat", C.c_int32),
+        ("enable_boundaries", C.c_int32), ("precision", C.c_int32), ("device", C.c_int32),
+        ("reserved", C.c_int32 * 3),
+    ]
+
+
+class GxTickStats(C.Structure):
+    _fields_ = [("kinetic", _D), ("speed_sum", _D), ("potential", _D), ("bond_energy", _D),
+                ("lambda_", _D), ("pairs", C.c_uint64)]
+
+
+TICK_DTYPE = np.dtype([("kinetic", "f8"), ("speed_sum", "f8"), ("potential", "f8"),
+                       ("bond_energy", "f8"), ("lambda", "f8"), ("pairs", "u8")])
+
+EXPORTS = (
+    "gx_create", "gx_destroy", "gx_last_error", "gx_status_string", "gx_set_precision",
+    "gx_set_state", "gx_get_state", "gx_num_atoms", "gx_set_bonds", "gx_half_kick",
+    "gx_drift", "gx_wrap", "gx_forces", "gx_thermostat", "gx_stats", "gx_step",
+    "gx_cell_assign", "gx_neighbors", "gx_radial_distribution",
+    "gx_radial_distribution_between", "gx_clusters", "gx_bound_pairs",
+    "gx_synchronize", "gx_profile_enable", "gx_profile_read",
+)
+
+_lib = None
+
+
+def load(path: str | Path | None = None) -> C.CDLL:
+    """Loads the library (once) and declares every prototype."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise ImportError(f"{p} is missing: build it with `python -m genesis_b200.build`")
+    lib = C.CDLL(str(p))
+    vp, sz, u32p, u64p, dp, u8p = C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), \
+        C.POINTER(C.c_double), C.POINTER(C.c_uint8)
+    proto = {
+        "gx_create": (C.c_int, [C.POINTER(GxParams), C.POINTER(vp)]),
+        "gx_destroy": (None, [vp]),
+        "gx_last_error": (C.c_char_p, [vp]),
+        "gx_status_string": (C.c_char_p, [C.c_int]),
+        "gx_set_precision": (C.c_int, [vp, C.c_int]),
+        "gx_set_state": (C.c_int, [vp, sz, dp, dp, dp, u8p, dp, dp, u32p]),
+        "gx_get_state": (C.c_int, [vp, dp, dp, dp]),
+        "gx_num_atoms": (sz, [vp]),
+        "gx_set_bonds": (C.c_int, [vp, sz, u32p]),
+        "gx_half_kick": (C.c_int, [vp]),
+        "gx_drift": (C.c_int, [vp]),
+        "gx_wrap": (C.c_int, [vp]),
+        "gx_forces": (C.c_int, [vp, dp, dp, u64p]),
+        "gx_thermostat": (C.c_int, [vp, dp, dp]),
+        "gx_stats": (C.c_int, [vp, dp, dp]),
+        "gx_step": (C.c_int, [vp, C.c_int, C.POINTER(GxTickStats), C.c_int]),
+        "gx_cell_assign": (C.c_int, [vp, _D, u32p]),
+        "gx_neighbors": (C.c_int, [vp, _D, _D, u32p, sz, C.POINTER(sz)]),
+        "gx_radial_distribution": (C.c_int, [vp, _D, sz, sz, u64p, dp, dp, dp]),
+        "gx_radial_distribution_between": (C.c_int, [vp, C.c_uint8, C.c_uint8, _D, sz, sz, u64p, dp, dp, dp]),
+        "gx_clusters": (C.c_int, [vp, _D, u32p, u64p, dp]),
+        "gx_bound_pairs": (C.c_int, [vp, _D, u32p, sz, C.POINTER(sz)]),
+        "gx_synchronize": (C.c_int, [vp]),
+        "gx_profile_enable": (C.c_int, [vp, C.c_int]),
+        "gx_profile_read": (C.c_int, [vp, C.POINTER(C.c_char_p), u64p, dp, C.c_int, C.c_int]),
+    }
+    for name, (res, args) in proto.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+class GxError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{msg} (status {status})")
+        self.status = status
+
+
+def _ptr(a: np.ndarray | None, ctype):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def params(cfg, precision: str | int = "fp64", device: int = 0) -> GxParams:
+    """gx_params from a :class:`genesis_b200.config.Config`."""
+    p = GxParams()
+    p.box[:] = list(cfg.size)
+    p.dt = cfg.dt
+    p.thermal_constant = cfg.thermal_constant
+    p.sigma[:] = list(cfg.sigma)
+    p.epsilon_k[:] = list(cfg.epsilon_k)
+    p.charge[:] = list(cfg.charge)
+    p.lj_cutoff_factor = E.LJ_CUTOFF_FACTOR
+    p.coulomb_constant = cfg.coulomb_constant
+    p.coulomb_cutoff = cfg.coulomb_cutoff
+    p.gravity_constant = cfg.gravity_constant
+    p.gravity_cutoff = cfg.gravity_cutoff
+    p.bond_k_bind = cfg.bond_k_bind
+    p.thermostat_temperature = cfg.thermostat_temperature
+    p.thermostat_tau = cfg.thermostat_tau
+    p.enable_electrostatics = int(cfg.enable_electrostatics)
+    p.enable_gravity = int(cfg.enable_gravity)
+    p.enable_bond_interaction = int(cfg.enable_bond_interaction)
+    p.enable_thermostat = int(cfg.enable_thermostat)
+    p.enable_boundaries = int(cfg.enable_boundaries)
+    p.precision = _PRECISION[precision] if isinstance(precision, str) else int(precision)
+    p.device = device
+    return p
+
+
+class Handle:
+    """One resident universe on one GPU (a ``gx_handle``)."""
+
+    def __init__(self, cfg, precision: str | int = "fp64", device: int = 0):
+        self.lib = load()
+        self.cfg = cfg
+        self._p = params(cfg, precision, device)
+        h = C.c_void_p()
+        rc = self.lib.gx_create(C.byref(self._p), C.byref(h))
+        self.h = h
+        self._check(rc)
+
+    def _check(self, rc: int):
+        if rc != 0:
+            msg = self.lib.gx_last_error(self.h).decode() if self.h else "gx_create failed"
+            raise GxError(rc, msg)
+
+    def close(self):
+        if self.h:
+            self.lib.gx_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- state --------------------------------------------------------------
+    def set_state(self, pos, vel, elem, acc=None, charge=None, mass=None, entity=None):
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        vel = np.ascontiguousarray(vel, dtype=np.float64)
+        elem = np.ascontiguousarray(elem, dtype=np.uint8)
+        n = len(elem)
+        acc = None if acc is None else np.ascontiguousarray(acc, dtype=np.float64)
+        charge = None if charge is None else np.ascontiguousarray(charge, dtype=np.float64)
+        mass = None if mass is None else np.ascontiguousarray(mass, dtype=np.float64)
+        entity = None if entity is None else np.ascontiguousarray(entity, dtype=np.uint32)
+        self._check(self.lib.gx_set_state(self.h, n, _ptr(pos, C.c_double), _ptr(vel, C.c_double),
+                                          _ptr(acc, C.c_double), _ptr(elem, C.c_uint8),
+                                          _ptr(charge, C.c_double), _ptr(mass, C.c_double),
+                                          _ptr(entity, C.c_uint32)))
+
+    def set_universe(self, u, acc=None):
+        self.set_state(u.pos, u.vel, u.elem, acc=acc, charge=u.charge, mass=u.mass, entity=u.entity)
+
+    @property
+    def n(self) -> int:
+        return int(self.lib.gx_num_atoms(self.h))
+
+    def get_state(self):
+        n = self.n
+        pos, vel, acc = (np.empty((n, 3)) for _ in range(3))
+        self._check(self.lib.gx_get_state(self.h, _ptr(pos, C.c_double), _ptr(vel, C.c_double),
+                                          _ptr(acc, C.c_double)))
+        return pos, vel, acc
+
+    def set_bonds(self, pairs):
+        pairs = np.ascontiguousarray(np.asarray(pairs, dtype=np.uint32).reshape(-1, 2))
+        self._check(self.lib.gx_set_bonds(self.h, len(pairs), _ptr(pairs, C.c_uint32)))
+
+    def set_precision(self, precision):
+        self._check(self.lib.gx_set_precision(self.h, _PRECISION.get(precision, precision)))
+
+    # -- systems ------------------------------------------------------------
+    def half_kick(self):
+        self._check(self.lib.gx_half_kick(self.h))
+
+    def drift(self):
+        self._check(self.lib.gx_drift(self.h))
+
+    def wrap(self):
+        self._check(self.lib.gx_wrap(self.h))
+
+    def forces(self):
+        V, Vb, npairs = C.c_double(), C.c_double(), C.c_uint64()
+        self._check(self.lib.gx_forces(self.h, C.byref(V), C.byref(Vb), C.byref(npairs)))
+        return V.value, Vb.value, npairs.value
+
+    def thermostat(self):
+        K, lam = C.c_double(), C.c_double()
+        self._check(self.lib.gx_thermostat(self.h, C.byref(K), C.byref(lam)))
+        return K.value, lam.value
+
+    def stats(self):
+        K, sp = C.c_double(), C.c_double()
+        self._check(self.lib.gx_stats(self.h, C.byref(K), C.byref(sp)))
+        return K.value, sp.value
+
+    def step(self, nsteps: int, stats: bool = True, graph: bool = False):
+        rec = (GxTickStats * max(nsteps, 1))() if stats else None
+        self._check(self.lib.gx_step(self.h, nsteps, rec, int(graph)))
+        if not stats:
+            return None
+        return np.frombuffer(rec, dtype=TICK_DTYPE, count=nsteps).copy()
+
+    def synchronize(self):
+        self._check(self.lib.gx_synchronize(self.h))
+
+    # -- probes and lenses --------------------------------------------------
+    def cell_assign(self, min_cell: float) -> np.ndarray:
+        out = np.empty(self.n, dtype=np.uint32)
+        self._check(self.lib.gx_cell_assign(self.h, min_cell, _ptr(out, C.c_uint32)))
+        return out
+
+    def neighbors(self, min_cell: float, cutoff: float, cap: int | None = None) -> np.ndarray:
+        cap = cap if cap is not None else max(64, self.n * 64)
+        out = np.empty((cap, 2), dtype=np.uint32)
+        total = C.c_size_t()
+        self._check(self.lib.gx_neighbors(self.h, min_cell, cutoff, _ptr(out, C.c_uint32), cap,
+                                          C.byref(total)))
+        return out[: total.value].copy()
+
+    def radial_distribution(self, r_max: float, nbins: int, sample_cap: int = E.G_SAMPLE_CAP,
+                            between: tuple[int, int] | None = None):
+        nb = min(max(nbins, 1), 1 << 16)
+        counts = np.empty(nb, dtype=np.uint64)
+        bins = np.empty(nb, dtype=np.float64)
+        rmo, dro = C.c_double(), C.c_double()
+        if between is None:
+            rc = self.lib.gx_radial_distribution(self.h, r_max, nbins, sample_cap, _ptr(counts, C.c_uint64),
+                                                 _ptr(bins, C.c_double), C.byref(rmo), C.byref(dro))
+        else:
+            rc = self.lib.gx_radial_distribution_between(self.h, between[0], between[1], r_max, nbins,
+                                                         sample_cap, _ptr(counts, C.c_uint64),
+                                                         _ptr(bins, C.c_double), C.byref(rmo), C.byref(dro))
+        self._check(rc)
+        return counts, bins, rmo.value, dro.value
+
+    def clusters(self, bond_factor: float = E.BOND_FACTOR):
+        labels = np.empty(self.n, dtype=np.uint32)
+        st = np.zeros(4, dtype=np.uint64)
+        mean = C.c_double()
+        self._check(self.lib.gx_clusters(self.h, bond_factor, _ptr(labels, C.c_uint32), _ptr(st, C.c_uint64),
+                                         C.byref(mean)))
+        return labels, {"monomers": int(st[0]), "aggregates": int(st[1]), "largest": int(st[2]),
+                        "bound_pairs": int(st[3]), "mean_size": mean.value}
+
+    def bound_pairs(self, k_bind: float, cap: int | None = None) -> np.ndarray:
+        cap = cap if cap is not None else max(64, self.n * 16)
+        out = np.empty((cap, 2), dtype=np.uint32)
+        total = C.c_size_t()
+        self._check(self.lib.gx_bound_pairs(self.h, k_bind, _ptr(out, C.c_uint32), cap, C.byref(total)))
+        return out[: total.value].copy()
+
+    # -- profiling ----------------------------------------------------------
+    def profile(self, on: bool = True):
+        self._check(self.lib.gx_profile_enable(self.h, int(on)))
+
+    def profile_read(self, reset: bool = True) -> dict:
+        cap = 64
+        names = (C.c_char_p * cap)()
+        launches = np.zeros(cap, dtype=np.uint64)
+        ms = np.zeros(cap, dtype=np.float64)
+        k = self.lib.gx_profile_read(self.h, names, _ptr(launches, C.c_uint64), _ptr(ms, C.c_double), cap,
+                                     int(reset))
+        if k < 0:
+            self._check(k)
+        return {names[i].decode(): (int(launches[i]), float(ms[i])) for i in range(min(k, cap))}

@@ -1,0 +1,713 @@
+// gx_api.cu -- C ABI: handle lifecycle, state transfer, the force-schedule
+// systems and the fused tick.  Declarations and the reference interface each
+// entry point replaces are in include/genesis_gpu.h.
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "gx_internal.cuh"
+
+namespace gx {
+int upload_pair_table_f64(gx_handle* h);
+size_t red_doubles(size_t cap);
+}  // namespace gx
+
+namespace gx {
+
+int set_err(gx_handle* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    return code;
+}
+int cuda_err(gx_handle* h, cudaError_t e, const char* what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    return set_err(h, GX_ERR_CUDA, m);
+}
+
+static const int kAllOffsets[27][3] = {  // src/physics/grid.rs:37-47
+    {-1, -1, -1}, {-1, -1, 0}, {-1, -1, 1}, {-1, 0, -1}, {-1, 0, 0}, {-1, 0, 1}, {-1, 1, -1}, {-1, 1, 0}, {-1, 1, 1},
+    {0, -1, -1},  {0, -1, 0},  {0, -1, 1},  {0, 0, -1},  {0, 0, 0},  {0, 0, 1},  {0, 1, -1},  {0, 1, 0},  {0, 1, 1},
+    {1, -1, -1},  {1, -1, 0},  {1, -1, 1},  {1, 0, -1},  {1, 0, 0},  {1, 0, 1},  {1, 1, -1},  {1, 1, 0},  {1, 1, 1}};
+
+GridGeom make_grid(const double box[3], double min_cell, int* ok) {
+    GridGeom g;
+    std::memset(&g, 0, sizeof g);
+    *ok = 0;
+    if (!(min_cell > 0.0) || !std::isfinite(min_cell)) return g;
+    double total = 1.0;
+    for (int k = 0; k < 3; ++k) {
+        if (!(box[k] > 0.0) || !std::isfinite(box[k])) return g;
+        double c = std::floor(box[k] / min_cell);  // grid.rs:68
+        if (c < 1.0) c = 1.0;
+        if (c > 1048576.0) return g;
+        g.n[k] = (uint32_t)c;
+        total *= c;
+    }
+    if (total > 268435456.0) return g;
+    g.ncell = g.n[0] * g.n[1] * g.n[2];
+    for (int k = 0; k < 3; ++k) {
+        g.L[k] = box[k];
+        g.cell[k] = box[k] / (double)g.n[k];
+        g.cellf[k] = (float)g.cell[k];
+        g.Lf[k] = (float)box[k];
+        g.invLf[k] = (float)(1.0 / box[k]);
+        if (g.n[k] < 3) g.minimg_mask |= 1 << k;
+    }
+    // Canonical offsets (grid.rs:275-296): zero on degenerate axes, first
+    // nonzero component +1.  Kept in ALL_OFFSETS order.
+    g.nhalf = 0;
+    for (const auto& o : kAllOffsets) {
+        if (o[0] == 0 && o[1] == 0 && o[2] == 0) continue;
+        bool degen_nonzero = false;
+        for (int k = 0; k < 3; ++k)
+            if (g.n[k] <= 1 && o[k] != 0) degen_nonzero = true;
+        if (degen_nonzero) continue;
+        int first = o[0] != 0 ? o[0] : (o[1] != 0 ? o[1] : o[2]);
+        if (first != 1) continue;
+        for (int k = 0; k < 3; ++k) g.half[g.nhalf][k] = (int8_t)o[k];
+        ++g.nhalf;
+    }
+    g.nfull = 2 * g.nhalf;
+    for (int q = 0; q < g.nhalf; ++q)
+        for (int k = 0; k < 3; ++k) {
+            g.full[q][k] = g.half[q][k];
+            g.full[g.nhalf + q][k] = (int8_t)-g.half[q][k];
+        }
+    *ok = 1;
+    return g;
+}
+
+void prof_begin(gx_handle* h, const char* name) {
+    if (!h->prof_on) return;
+    ProfSlot* s = nullptr;
+    for (auto& p : h->prof)
+        if (p.name == name || std::strcmp(p.name, name) == 0) s = &p;
+    if (!s) {
+        h->prof.push_back(ProfSlot{name, 0, 0.0, {}});
+        s = &h->prof.back();
+    }
+    cudaEvent_t a, b;
+    if (h->ev_pool.size() >= 2) {
+        a = h->ev_pool.back();
+        h->ev_pool.pop_back();
+        b = h->ev_pool.back();
+        h->ev_pool.pop_back();
+    } else {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+    }
+    cudaEventRecord(a, h->stream);
+    s->ev.push_back(a);
+    s->ev.push_back(b);
+}
+void prof_end(gx_handle* h, const char* name) {
+    if (!h->prof_on) return;
+    for (auto& p : h->prof)
+        if (p.name == name || std::strcmp(p.name, name) == 0) {
+            cudaEventRecord(p.ev.back(), h->stream);
+            p.launches += 1;
+            return;
+        }
+}
+
+}  // namespace gx
+
+using namespace gx;
+
+namespace {
+
+const double kElementMass[kNElem] = {1.008, 4.0026, 12.011, 14.007, 15.999,
+                                     22.99, 28.085, 30.974, 32.06,  55.845};  // atom_type.rs:80-93
+
+void free_buf(StateBuf& b) {
+    cudaFree(b.x);
+    cudaFree(b.vx);
+    cudaFree(b.ax);
+    cudaFree(b.charge);
+    cudaFree(b.elem);
+    cudaFree(b.slot);
+    std::memset(&b, 0, sizeof b);
+}
+
+int alloc_buf(gx_handle* h, StateBuf& b, size_t cap) {
+    free_buf(b);
+    GX_CUDA(h, cudaMalloc(&b.x, 3 * cap * sizeof(double)));
+    GX_CUDA(h, cudaMalloc(&b.vx, 3 * cap * sizeof(double)));
+    GX_CUDA(h, cudaMalloc(&b.ax, 3 * cap * sizeof(double)));
+    GX_CUDA(h, cudaMalloc(&b.charge, 3 * cap * sizeof(double)));
+    GX_CUDA(h, cudaMalloc(&b.elem, 2 * cap));
+    GX_CUDA(h, cudaMalloc(&b.slot, cap * sizeof(uint32_t)));
+    b.y = b.x + cap;
+    b.z = b.x + 2 * cap;
+    b.vy = b.vx + cap;
+    b.vz = b.vx + 2 * cap;
+    b.ay = b.ax + cap;
+    b.az = b.ax + 2 * cap;
+    b.mass = b.charge + cap;
+    b.inv_mass = b.charge + 2 * cap;
+    b.kind = b.elem + cap;
+    return GX_OK;
+}
+
+int ensure_capacity(gx_handle* h, size_t n) {
+    if (n <= h->cap && h->cap) return GX_OK;
+    size_t cap = n < 1024 ? 1024 : n;
+    for (int k = 0; k < 2; ++k) {
+        int rc = alloc_buf(h, h->buf[k], cap);
+        if (rc) return rc;
+    }
+    cudaFree(h->key);
+    cudaFree(h->pos4);
+    cudaFree(h->F);
+    cudaFree(h->host_stage);
+    cudaFree(h->red);
+    GX_CUDA(h, cudaMalloc(&h->key, 5 * cap * sizeof(uint32_t)));
+    h->key_sorted = h->key + cap;
+    h->perm = h->key + 2 * cap;
+    h->pos_of_slot = h->key + 3 * cap;
+    h->entity = h->key + 4 * cap;
+    GX_CUDA(h, cudaMalloc(&h->pos4, cap * sizeof(float4)));
+    GX_CUDA(h, cudaMalloc(&h->F, 3 * cap * sizeof(long long)));
+    GX_CUDA(h, cudaMalloc(&h->host_stage, 3 * cap * sizeof(double) + cap * sizeof(uint32_t)));
+    h->u8_stage = (uint8_t*)(h->host_stage + 3 * cap);
+    GX_CUDA(h, cudaMalloc(&h->red, red_doubles(cap) * sizeof(double)));
+    h->cap = cap;
+    int rc = upload_pair_table_f64(h);
+    if (rc) return rc;
+    return GX_OK;
+}
+
+__global__ void k_aos_to_soa(const double* __restrict__ aos, double* x, double* y, double* z, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    x[i] = aos[3 * i];
+    y[i] = aos[3 * i + 1];
+    z[i] = aos[3 * i + 2];
+}
+// sorted SoA -> slot-ordered AoS
+__global__ void k_soa_to_aos(const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
+                             const uint32_t* __restrict__ slot, double* __restrict__ aos, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t s = slot[i];
+    aos[3 * s] = x[i];
+    aos[3 * s + 1] = y[i];
+    aos[3 * s + 2] = z[i];
+}
+__global__ void k_init_slots(StateBuf b, uint32_t* pos_of_slot, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    b.slot[i] = i;
+    pos_of_slot[i] = i;
+    b.inv_mass[i] = xdiv(1.0, b.mass[i]);  // the 1.0 / mass of systems/forces.rs:339
+}
+__global__ void k_fill_d(double* p, uint32_t n, double v) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+__global__ void k_record(gx_tick_stats* rec, const double* dscal, const unsigned long long* dcount, int thermo) {
+    rec->kinetic = dscal[1];
+    rec->speed_sum = dscal[4];
+    rec->potential = dscal[2];
+    rec->bond_energy = dscal[3];
+    rec->lambda = thermo ? dscal[0] : 1.0;
+    rec->pairs = dcount[0];
+}
+
+inline unsigned nblk(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+// The pending Berendsen scale is folded into the next kernel that reads v;
+// anything else that reads v first commits it.
+int commit_lambda(gx_handle* h) {
+    if (!h->lambda_pending) return GX_OK;
+    launch_apply_lambda(h, h->buf[h->cur], (uint32_t)h->n, h->dscal + 0);
+    h->lambda_pending = false;
+    return GX_OK;
+}
+
+int require_state(gx_handle* h) {
+    if (!h) return GX_ERR_ARG;
+    if (!h->cap) return set_err(h, GX_ERR_STATE, "no state uploaded (call gx_set_state first)");
+    return GX_OK;
+}
+
+// Cell list of the force grid: keys, counting sort, reorder (double buffer).
+int rebuild_cells(gx_handle* h) {
+    uint32_t n = (uint32_t)h->n;
+    StateBuf& src = h->buf[h->cur];
+    launch_cell_keys(h, h->fgrid, src, n, h->key);
+    int rc = counting_sort(h, h->cl, h->fgrid.ncell, h->key, n, h->perm);
+    if (rc) return rc;
+    launch_gather(h, src, h->buf[h->cur ^ 1], h->perm, h->key, h->key_sorted, n, h->pos_of_slot);
+    h->cur ^= 1;
+    h->sorted = true;
+    if (h->precision == GX_MIXED) launch_build_pos4(h, h->fgrid, h->buf[h->cur], h->key_sorted, n, h->pos4);
+    return GX_OK;
+}
+
+int check_kinds(gx_handle* h) {
+    if (h->precision == GX_MIXED && h->nkinds > kMaxKinds)
+        return set_err(h, GX_ERR_UNSUPPORTED, "mixed precision supports at most 16 distinct (element, charge) kinds");
+    return GX_OK;
+}
+
+int upload_pairf(gx_handle* h) {
+    if (!h->d_pairf) GX_CUDA(h, cudaMalloc(&h->d_pairf, kMaxKinds * kMaxKinds * sizeof(PairF)));
+    PairF tab[kMaxKinds * kMaxKinds];
+    std::memset(tab, 0, sizeof tab);
+    int nk = h->nkinds < kMaxKinds ? h->nkinds : kMaxKinds;
+    for (int a = 0; a < nk; ++a)
+        for (int b = 0; b < nk; ++b) {
+            int ea = h->kind_elem[a], eb = h->kind_elem[b];
+            double sg = h->fs.pair_sigma[ea * kNElem + eb], ep = h->fs.pair_eps[ea * kNElem + eb];
+            PairF& t = tab[a * nk + b];
+            t.sigma = (float)sg;
+            t.half_sigma = (float)(0.5 * sg);
+            t.inv_half_sigma = (float)(2.0 / sg);
+            t.eps4 = (float)(4.0 * ep);
+            t.eps24 = (float)(24.0 * ep);
+            t.qq = (float)(h->p.coulomb_constant * h->kind_charge[a] * h->kind_charge[b]);
+        }
+    GX_CUDA(h, cudaMemcpy(h->d_pairf, tab, sizeof tab, cudaMemcpyHostToDevice));
+    return GX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* gx_status_string(int s) {
+    switch (s) {
+        case GX_OK: return "ok";
+        case GX_ERR_ARG: return "invalid argument";
+        case GX_ERR_OOM: return "device allocation failed";
+        case GX_ERR_CUDA: return "CUDA error";
+        case GX_ERR_CAPACITY: return "capacity exceeded";
+        case GX_ERR_SATURATION: return "fixed-point saturation";
+        case GX_ERR_NONFINITE: return "non-finite value";
+        case GX_ERR_TIMEOUT: return "device wait timed out";
+        case GX_ERR_UNSUPPORTED: return "unsupported configuration";
+        case GX_ERR_STATE: return "call out of order";
+        default: return "unknown status";
+    }
+}
+
+const char* gx_last_error(const gx_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int gx_create(const gx_params* p, gx_handle** out) {
+    if (!p || !out) return GX_ERR_ARG;
+    *out = nullptr;
+    if (p->precision != GX_FP64 && p->precision != GX_MIXED) return GX_ERR_ARG;
+    if (!(p->dt == p->dt) || !(p->thermal_constant == p->thermal_constant)) return GX_ERR_ARG;
+    gx_handle* h = new gx_handle();
+    h->p = *p;
+    h->precision = p->precision;
+    // ForceSystem::new (systems/forces.rs:100-142) and LjTable::new (physics/forces.rs:223-237).
+    ForceSetup& fs = h->fs;
+    double max_pair = 0.0, max_sigma = 0.0;
+    for (int i = 0; i < kNElem; ++i) {
+        max_sigma = std::fmax(max_sigma, p->sigma[i]);
+        for (int j = 0; j < kNElem; ++j) {
+            double s = 0.5 * (p->sigma[i] + p->sigma[j]);
+            double e = p->thermal_constant * std::sqrt(p->epsilon_k[i] * p->epsilon_k[j]);
+            max_pair = std::fmax(max_pair, s);
+            fs.pair_sigma[i * kNElem + j] = s;
+            fs.pair_eps[i * kNElem + j] = e;
+        }
+    }
+    fs.lj_rc = std::fmax(p->lj_cutoff_factor, 1.0) * max_pair;
+    fs.lj_ron = 0.9 * fs.lj_rc;
+    fs.coul_rc = p->enable_electrostatics ? std::fmax(p->coulomb_cutoff, 1.0) * max_sigma : 0.0;
+    fs.grav_rc = p->enable_gravity ? std::fmax(p->gravity_cutoff, 1.0) * max_sigma : 0.0;
+    fs.rc = std::fmax(std::fmax(fs.lj_rc, fs.coul_rc), fs.grav_rc);
+    fs.coul_ron = 0.9 * fs.coul_rc;
+    fs.grav_ron = 0.9 * fs.grav_rc;
+    fs.bond_k_bind = p->bond_k_bind;
+    fs.max_sigma = max_sigma;
+    fs.r_eq_factor = std::pow(2.0, 1.0 / 6.0);
+    fs.curv_factor = 72.0 * std::pow(2.0, -1.0 / 3.0);
+    int ok = 0;
+    h->fgrid = make_grid(p->box, fs.rc, &ok);
+    if (!ok) {
+        int rc = set_err(h, GX_ERR_ARG, "invalid box or cutoff (grid would be empty or too large)");
+        *out = h;
+        return rc;
+    }
+    cudaError_t e = cudaSetDevice(p->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&h->dscal, 16 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&h->dcount, 8 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&h->derr, sizeof(uint32_t));
+    if (e != cudaSuccess) {
+        int rc = cuda_err(h, e, "gx_create");
+        *out = h;
+        return rc;
+    }
+    double init[16] = {1.0, 0, 0, 0, 0, 1.0};
+    cudaMemcpy(h->dscal, init, sizeof init, cudaMemcpyHostToDevice);
+    cudaMemset(h->dcount, 0, 8 * sizeof(unsigned long long));
+    cudaMemset(h->derr, 0, sizeof(uint32_t));
+    *out = h;
+    return GX_OK;
+}
+
+void gx_destroy(gx_handle* h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    free_buf(h->buf[0]);
+    free_buf(h->buf[1]);
+    cudaFree(h->key);
+    cudaFree(h->pos4);
+    cudaFree(h->F);
+    cudaFree(h->host_stage);
+    cudaFree(h->red);
+    cudaFree(h->dscal);
+    cudaFree(h->dcount);
+    cudaFree(h->derr);
+    cudaFree(h->d_pairf);
+    cudaFree(h->bonds);
+    cudaFree(h->cl.count);
+    cudaFree(h->cl.start);
+    cudaFree(h->cl.fill);
+    for (auto q : h->cl.scan_levels) cudaFree(q);
+    for (auto& s : h->prof)
+        for (auto ev : s.ev) cudaEventDestroy(ev);
+    for (auto ev : h->ev_pool) cudaEventDestroy(ev);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+int gx_set_precision(gx_handle* h, int precision) {
+    if (!h || (precision != GX_FP64 && precision != GX_MIXED)) return GX_ERR_ARG;
+    if (precision == GX_MIXED && h->p.enable_gravity)
+        return set_err(h, GX_ERR_UNSUPPORTED, "gravity is only implemented in the FP64 path");
+    h->precision = precision;
+    h->sorted = false;
+    if (h->graph_exec) {
+        cudaGraphExecDestroy(h->graph_exec);
+        h->graph_exec = nullptr;
+    }
+    return check_kinds(h);
+}
+
+size_t gx_num_atoms(const gx_handle* h) { return h ? h->n : 0; }
+
+int gx_set_state(gx_handle* h, size_t n, const double* pos, const double* vel, const double* acc,
+                 const uint8_t* elem, const double* charge, const double* mass, const uint32_t* entity) {
+    if (!h || (n && (!pos || !vel || !elem))) return GX_ERR_ARG;
+    if (n > 0x7FFFFFFFu) return set_err(h, GX_ERR_ARG, "too many atoms");
+    for (size_t i = 0; i < n; ++i)
+        if (elem[i] >= kNElem) return set_err(h, GX_ERR_ARG, "element index out of range (0..9)");
+    GX_CUDA(h, cudaSetDevice(h->p.device));
+    int rc = ensure_capacity(h, n);
+    if (rc) return rc;
+    h->n = n;
+    h->cur = 0;
+    h->sorted = false;
+    h->lambda_pending = false;
+    if (h->graph_exec) {
+        cudaGraphExecDestroy(h->graph_exec);
+        h->graph_exec = nullptr;
+    }
+    StateBuf& b = h->buf[0];
+    uint32_t un = (uint32_t)n;
+    std::vector<double> tmp(n);
+    // kinds: distinct (element, charge) pairs, first-seen order
+    h->nkinds = 0;
+    std::vector<uint8_t> kind(n);
+    for (size_t i = 0; i < n; ++i) {
+        double q = charge ? charge[i] : h->p.charge[elem[i]];
+        int found = -1;
+        for (int k = 0; k < h->nkinds && k < kMaxKinds; ++k)
+            if (h->kind_elem[k] == elem[i] && h->kind_charge[k] == q) found = k;
+        if (found < 0) {
+            if (h->nkinds < kMaxKinds) {
+                h->kind_elem[h->nkinds] = elem[i];
+                h->kind_charge[h->nkinds] = q;
+            }
+            found = h->nkinds++;
+        }
+        kind[i] = (uint8_t)(found < 255 ? found : 255);
+    }
+    rc = upload_pairf(h);
+    if (rc) return rc;
+    if (n) {
+        GX_CUDA(h, cudaMemcpyAsync(h->host_stage, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        k_aos_to_soa<<<nblk(n, 256), 256, 0, h->stream>>>(h->host_stage, b.x, b.y, b.z, un);
+        GX_CUDA(h, cudaStreamSynchronize(h->stream));
+        GX_CUDA(h, cudaMemcpyAsync(h->host_stage, vel, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        k_aos_to_soa<<<nblk(n, 256), 256, 0, h->stream>>>(h->host_stage, b.vx, b.vy, b.vz, un);
+        GX_CUDA(h, cudaStreamSynchronize(h->stream));
+        if (acc) {
+            GX_CUDA(h, cudaMemcpyAsync(h->host_stage, acc, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+            k_aos_to_soa<<<nblk(n, 256), 256, 0, h->stream>>>(h->host_stage, b.ax, b.ay, b.az, un);
+            GX_CUDA(h, cudaStreamSynchronize(h->stream));
+        } else {
+            GX_CUDA(h, cudaMemsetAsync(b.ax, 0, 3 * h->cap * sizeof(double), h->stream));
+        }
+        for (size_t i = 0; i < n; ++i) tmp[i] = charge ? charge[i] : h->p.charge[elem[i]];
+        GX_CUDA(h, cudaMemcpyAsync(b.charge, tmp.data(), n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        GX_CUDA(h, cudaStreamSynchronize(h->stream));
+        for (size_t i = 0; i < n; ++i) tmp[i] = mass ? mass[i] : kElementMass[elem[i]];
+        GX_CUDA(h, cudaMemcpyAsync(b.mass, tmp.data(), n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        GX_CUDA(h, cudaMemcpyAsync(b.elem, elem, n, cudaMemcpyHostToDevice, h->stream));
+        GX_CUDA(h, cudaMemcpyAsync(b.kind, kind.data(), n, cudaMemcpyHostToDevice, h->stream));
+        if (entity)
+            GX_CUDA(h, cudaMemcpyAsync(h->entity, entity, n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+        k_init_slots<<<nblk(n, 256), 256, 0, h->stream>>>(b, h->pos_of_slot, un);
+        GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    }
+    h->has_entity = entity != nullptr;
+    double one = 1.0;
+    GX_CUDA(h, cudaMemcpy(h->dscal, &one, sizeof one, cudaMemcpyHostToDevice));
+    GX_CUDA(h, cudaGetLastError());
+    return check_kinds(h);
+}
+
+int gx_get_state(gx_handle* h, double* pos, double* vel, double* acc) {
+    int rc = require_state(h);
+    if (rc) return rc;
+    commit_lambda(h);
+    StateBuf& b = h->buf[h->cur];
+    uint32_t n = (uint32_t)h->n;
+    double* outs[3] = {pos, vel, acc};
+    double* srcs[3][3] = {{b.x, b.y, b.z}, {b.vx, b.vy, b.vz}, {b.ax, b.ay, b.az}};
+    for (int k = 0; k < 3; ++k) {
+        if (!outs[k] || !n) continue;
+        k_soa_to_aos<<<nblk(n, 256), 256, 0, h->stream>>>(srcs[k][0], srcs[k][1], srcs[k][2], b.slot, h->host_stage, n);
+        GX_CUDA(h, cudaMemcpyAsync(outs[k], h->host_stage, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost,
+                                   h->stream));
+        GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    }
+    GX_CUDA(h, cudaGetLastError());
+    return GX_OK;
+}
+
+int gx_set_bonds(gx_handle* h, size_t nbonds, const uint32_t* pairs) {
+    int rc = require_state(h);
+    if (rc) return rc;
+    if (nbonds && !pairs) return GX_ERR_ARG;
+    for (size_t k = 0; k < 2 * nbonds; ++k)
+        if (pairs[k] >= h->n) return set_err(h, GX_ERR_ARG, "bond slot out of range");
+    if (nbonds > 2 * h->cap + (size_t)kRedCap * 64) return set_err(h, GX_ERR_CAPACITY, "too many bonds");
+    if (nbonds > h->bonds_cap) {
+        cudaFree(h->bonds);
+        h->bonds = nullptr;
+        GX_CUDA(h, cudaMalloc(&h->bonds, 2 * nbonds * sizeof(uint32_t)));
+        h->bonds_cap = nbonds;
+    }
+    if (nbonds) GX_CUDA(h, cudaMemcpy(h->bonds, pairs, 2 * nbonds * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    h->nbonds = nbonds;
+    return GX_OK;
+}
+
+int gx_half_kick(gx_handle* h) {
+    int rc = require_state(h);
+    if (rc) return rc;
+    const double* lam = h->lambda_pending ? h->dscal + 0 : nullptr;
+    launch_kick(h, h->buf[h->cur], (uint32_t)h->n, 0.5 * h->p.dt, lam);
+    if (h->lambda_pending) {
+        double one = 1.0;
+        GX_CUDA(h, cudaMemcpyAsync(h->dscal, &one, sizeof one, cudaMemcpyHostToDevice, h->stream));
+        h->lambda_pending = false;
+    }
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    GX_CUDA(h, cudaGetLastError());
+    return GX_OK;
+}
+
+int gx_drift(gx_handle* h) {
+    int rc = require_state(h);
+    if (rc) return rc;
+    commit_lambda(h);
+    launch_drift(h, h->buf[h->cur], (uint32_t)h->n, h->p.dt);
+    h->sorted = false;
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    GX_CUDA(h, cudaGetLastError());
+    return GX_OK;
+}
+
+int gx_wrap(gx_handle* h) {
+    int rc = require_state(h);
+    if (rc) return rc;
+    launch_wrap(h, h->buf[h->cur], (uint32_t)h->n);
+    h->sorted = false;
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    GX_CUDA(h, cudaGetLastError());
+    return GX_OK;
+}
+
+int gx_forces(gx_handle* h, double* potential, double* bond_energy, uint64_t* pairs) {
+    int rc = require_state(h);
+    if (rc) return rc;
+    if ((rc = check_kinds(h))) return rc;
+    if (h->n == 0) {  // systems/forces.rs:201-203
+        if (potential) *potential = 0.0;
+        if (bond_energy) *bond_energy = 0.0;
+        if (pairs) *pairs = 0;
+        return GX_OK;
+    }
+    if ((rc = rebuild_cells(h))) return rc;
+    if ((rc = force_pass(h, true, potential, bond_energy, pairs, true))) return rc;
+    GX_CUDA(h, cudaGetLastError());
+    return GX_OK;
+}
+
+int gx_thermostat(gx_handle* h, double* kinetic, double* lambda) {
+    int rc = require_state(h);
+    if (rc) return rc;
+    double tau = std::fmax(h->p.thermostat_tau, 1.0);  // thermostat.rs:26
+    if (kinetic) *kinetic = 0.0;
+    if (lambda) *lambda = 1.0;
+    if (h->p.thermostat_temperature <= 0.0) return GX_OK;  // thermostat.rs:48-50
+    commit_lambda(h);
+    size_t rows = h->cap / 64 + kRedCap;
+    double* kpart = h->red + 2 * rows;
+    int nb = 0;
+    launch_kinetic(h, h->buf[h->cur], (uint32_t)h->n, nullptr, kpart, nullptr, &nb);
+    launch_thermostat_lambda(h, kpart, nb, h->p.thermal_constant, h->p.thermostat_temperature, tau,
+                             (uint32_t)h->n, h->dscal + 0, h->dscal + 1);
+    double out[2];
+    GX_CUDA(h, cudaMemcpyAsync(out, h->dscal, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->lambda_pending = true;
+    commit_lambda(h);
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (kinetic) *kinetic = out[1];
+    if (lambda) *lambda = out[0];
+    GX_CUDA(h, cudaGetLastError());
+    return GX_OK;
+}
+
+int gx_stats(gx_handle* h, double* kinetic, double* speed_sum) {
+    int rc = require_state(h);
+    if (rc) return rc;
+    size_t rows = h->cap / 64 + kRedCap;
+    double* kpart = h->red + 2 * rows;
+    double* spart = h->red + 3 * rows;
+    int nb = 0;
+    launch_kinetic(h, h->buf[h->cur], (uint32_t)h->n, h->lambda_pending ? h->dscal + 0 : nullptr, kpart, spart, &nb);
+    launch_finalize_sum(h, kpart, nb, h->dscal + 1);
+    launch_finalize_sum(h, spart, nb, h->dscal + 4);
+    double out[5];
+    GX_CUDA(h, cudaMemcpyAsync(out, h->dscal, 5 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (kinetic) *kinetic = out[1];
+    if (speed_sum) *speed_sum = out[4];
+    GX_CUDA(h, cudaGetLastError());
+    return GX_OK;
+}
+
+int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
+    int rc = require_state(h);
+    if (rc) return rc;
+    if (nsteps < 0) return GX_ERR_ARG;
+    if ((rc = check_kinds(h))) return rc;
+    (void)use_graph;
+    uint32_t n = (uint32_t)h->n;
+    bool thermo = h->p.enable_thermostat && h->p.thermostat_temperature > 0.0;
+    double tau = std::fmax(h->p.thermostat_tau, 1.0);
+    size_t rows = h->cap / 64 + kRedCap;
+    double* kpart = h->red + 2 * rows;
+    double* spart = h->red + 3 * rows;
+    gx_tick_stats* drec = nullptr;
+    if (stats && nsteps) {
+        // per-tick records live in the tail of the reduction buffer
+        drec = (gx_tick_stats*)(h->red + 4 * rows);
+        if ((size_t)nsteps * sizeof(gx_tick_stats) > 2 * rows * sizeof(double)) {
+            // record in chunks
+            int done = 0;
+            int chunk = (int)(2 * rows * sizeof(double) / sizeof(gx_tick_stats));
+            while (done < nsteps) {
+                int k = nsteps - done < chunk ? nsteps - done : chunk;
+                if ((rc = gx_step(h, k, stats + done, use_graph))) return rc;
+                done += k;
+            }
+            return GX_OK;
+        }
+    }
+    for (int s = 0; s < nsteps; ++s) {
+        // VelocityHalfKick (with the previous tick's pending thermostat scale)
+        const double* lam = h->lambda_pending ? h->dscal + 0 : nullptr;
+        launch_kick(h, h->buf[h->cur], n, 0.5 * h->p.dt, lam);
+        if (h->lambda_pending) {
+            k_fill_d<<<1, 32, 0, h->stream>>>(h->dscal, 1, 1.0);
+            h->lambda_pending = false;
+        }
+        launch_drift(h, h->buf[h->cur], n, h->p.dt);                // PositionDrift
+        if (h->p.enable_boundaries) launch_wrap(h, h->buf[h->cur], n);  // BoundarySystem
+        if (n) {                                                   // ForceSystem
+            if ((rc = rebuild_cells(h))) return rc;
+            if ((rc = force_pass(h, true, nullptr, nullptr, nullptr, false))) return rc;
+        }
+        launch_kick(h, h->buf[h->cur], n, 0.5 * h->p.dt, nullptr);  // VelocityHalfKick
+        if (thermo) {                                              // ThermostatSystem
+            int nb = 0;
+            launch_kinetic(h, h->buf[h->cur], n, nullptr, kpart, nullptr, &nb);
+            launch_thermostat_lambda(h, kpart, nb, h->p.thermal_constant, h->p.thermostat_temperature, tau, n,
+                                     h->dscal + 0, nullptr);
+            h->lambda_pending = true;
+        }
+        if (drec) {
+            int nb = 0;
+            launch_kinetic(h, h->buf[h->cur], n, h->lambda_pending ? h->dscal + 0 : nullptr, kpart, spart, &nb);
+            launch_finalize_sum(h, kpart, nb, h->dscal + 1);
+            launch_finalize_sum(h, spart, nb, h->dscal + 4);
+            k_record<<<1, 1, 0, h->stream>>>(drec + s, h->dscal, h->dcount, thermo ? 1 : 0);
+        }
+    }
+    if (drec) {
+        GX_CUDA(h, cudaMemcpyAsync(stats, drec, (size_t)nsteps * sizeof(gx_tick_stats), cudaMemcpyDeviceToHost,
+                                   h->stream));
+    }
+    uint32_t e = 0;
+    GX_CUDA(h, cudaMemcpyAsync(&e, h->derr, sizeof e, cudaMemcpyDeviceToHost, h->stream));
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    GX_CUDA(h, cudaGetLastError());
+    if (e) {
+        cudaMemset(h->derr, 0, sizeof(uint32_t));
+        if (e & kErrNonFinite) return set_err(h, GX_ERR_NONFINITE, "non-finite force in the pair pass");
+        if (e & kErrSaturation) return set_err(h, GX_ERR_SATURATION, "fixed-point force saturated");
+    }
+    return GX_OK;
+}
+
+int gx_synchronize(gx_handle* h) {
+    if (!h) return GX_ERR_ARG;
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    return GX_OK;
+}
+
+int gx_profile_enable(gx_handle* h, int on) {
+    if (!h) return GX_ERR_ARG;
+    h->prof_on = on != 0;
+    return GX_OK;
+}
+
+int gx_profile_read(gx_handle* h, const char** names, uint64_t* launches, double* ms, int cap, int reset) {
+    if (!h) return GX_ERR_ARG;
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    int k = 0;
+    for (auto& s : h->prof) {
+        for (size_t q = 0; q + 1 < s.ev.size(); q += 2) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, s.ev[q], s.ev[q + 1]) == cudaSuccess) s.ms += t;
+            h->ev_pool.push_back(s.ev[q]);
+            h->ev_pool.push_back(s.ev[q + 1]);
+        }
+        s.ev.clear();
+        if (k < cap) {
+            if (names) names[k] = s.name;
+            if (launches) launches[k] = s.launches;
+            if (ms) ms[k] = s.ms;
+        }
+        ++k;
+        if (reset) {
+            s.launches = 0;
+            s.ms = 0.0;
+        }
+    }
+    return k;
+}
+
+}  // extern "C"

@@ -1,0 +1,522 @@
+// gx_force.cu -- the pair-force pass (ForceSystem::run, src/systems/forces.rs:163-353).
+//
+// Two precisions share the cell list built by gx_cells.cu:
+//
+//  * GX_FP64 ("plain"): every pair is evaluated with the reference's FP64
+//    operation order (exact intrinsics, no FMA), so each pair's force and
+//    energy are bit-identical to the reference; only the order in which an
+//    atom's contributions are summed differs.  Each thread gathers the full
+//    neighbourhood of its atom (every pair visited from both ends), so the
+//    accumulation needs no atomics and is deterministic.
+//
+//  * GX_MIXED: pair arithmetic in FP32 on cell-local coordinates; every pair
+//    force is quantised to 64-bit fixed point (2^-32 units) before any sum,
+//    and sums are integer atomics, so the result does not depend on launch
+//    configuration or scheduling.  Each pair is evaluated once (canonical
+//    half shell) and contributes +F / -F to its two ends.
+#include "gx_internal.cuh"
+
+namespace gx {
+
+namespace {
+
+struct LawF64 {
+    double lj_rc, lj_ron, coul_rc, coul_ron, grav_rc, grav_ron;
+    double rc2;
+    double k_e, G;
+    double box[3];
+    int coul, grav;
+};
+
+struct LawF32 {
+    float rc2, lj_rc, lj_ron, inv_lj_w, coul_rc, coul_ron, inv_coul_w;
+    int coul, nkinds;
+};
+
+// smooth_cutoff, src/physics/forces.rs:302-318 (exact FP64).
+__device__ __forceinline__ void smooth_f64(double r, double ron, double rc, double& sw, double& dsw) {
+    if (r <= ron) { sw = 1.0; dsw = 0.0; return; }
+    if (r >= rc) { sw = 0.0; dsw = 0.0; return; }
+    double w = xsub(rc, ron);
+    double u = xdiv(xsub(r, ron), w);
+    double u2 = xmul(u, u);
+    double u3 = xmul(u2, u);
+    double u4 = xmul(u3, u);
+    double u5 = xmul(u4, u);
+    sw = xsub(xadd(xsub(1.0, xmul(10.0, u3)), xmul(15.0, u4)), xmul(6.0, u5));
+    double omu = xsub(1.0, u);
+    dsw = xdiv(xmul(xmul(xmul(-30.0, u2), omu), omu), w);
+}
+
+// One pair's LJ + Coulomb + gravity scalar (systems/forces.rs:270-299), exact.
+__device__ __forceinline__ void pair_f64(const LawF64& L, double d, double sg, double ep, double qa, double qb,
+                                         double ma, double mb, double& fmag, double& V) {
+    fmag = 0.0;
+    double sw, dsw;
+    if (d < L.lj_rc) {  // force_switched_scalar, forces.rs:270-275; lj_raw :346-353
+        double r = fmax(d, xmul(0.5, sg));
+        double s = xdiv(sg, r);
+        double s6 = xmul(xmul(xmul(xmul(xmul(s, s), s), s), s), s);
+        double s12 = xmul(s6, s6);
+        double v = xmul(xmul(4.0, ep), xsub(s12, s6));
+        double m = xmul(xmul(xdiv(xmul(24.0, ep), sg), s), xsub(xmul(2.0, s12), s6));
+        smooth_f64(r, L.lj_ron, L.lj_rc, sw, dsw);
+        fmag = xadd(fmag, xsub(xmul(m, sw), xmul(v, dsw)));
+        V = xadd(V, xmul(v, sw));
+    }
+    if (L.coul && d < L.coul_rc) {  // :282-289, coulomb_raw :330-333
+        double r = fmax(d, 0.5);
+        double q = xmul(xmul(L.k_e, qa), qb);
+        double m = xdiv(q, xmul(r, r));
+        double v = xdiv(q, r);
+        smooth_f64(d, L.coul_ron, L.coul_rc, sw, dsw);
+        fmag = xadd(fmag, xsub(xmul(m, sw), xmul(v, dsw)));
+        V = xadd(V, xmul(v, sw));
+    }
+    if (L.grav && d < L.grav_rc) {  // :292-299, gravity_raw :338-341
+        double r = fmax(d, 0.5);
+        double mm = xmul(xmul(L.G, ma), mb);
+        double m = xdiv(-mm, xmul(r, r));
+        double v = xdiv(-mm, r);
+        smooth_f64(d, L.grav_ron, L.grav_rc, sw, dsw);
+        fmag = xadd(fmag, xsub(xmul(m, sw), xmul(v, dsw)));
+        V = xadd(V, xmul(v, sw));
+    }
+}
+
+constexpr int kForceThreads = 128;
+
+template <int BS>
+__device__ __forceinline__ double block_sum_d(double v, double* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    v = (threadIdx.x < BS / 32) ? sh[threadIdx.x] : 0.0;
+    if (wid == 0) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    __syncthreads();
+    return v;
+}
+template <int BS>
+__device__ __forceinline__ unsigned long long block_sum_u(unsigned long long v, unsigned long long* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    v = (threadIdx.x < BS / 32) ? sh[threadIdx.x] : 0ull;
+    if (wid == 0) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    __syncthreads();
+    return v;
+}
+
+// FP64 gather pass.  Each thread owns one atom i and visits every j of its
+// cell and of the cells at all offsets; V and the pair count are taken only
+// on visits through the canonical half shell (or j > i in the same cell), so
+// each reference pair-list entry is counted once.
+__global__ void __launch_bounds__(kForceThreads) k_force_f64(GridGeom g, StateBuf b, const uint32_t* __restrict__ key,
+                                                              const uint32_t* __restrict__ start, uint32_t n, LawF64 L,
+                                                              const double* __restrict__ psig,
+                                                              const double* __restrict__ peps, double* __restrict__ vpart,
+                                                              unsigned long long* __restrict__ npairs) {
+    __shared__ double shd[kForceThreads / 32];
+    __shared__ unsigned long long shu[kForceThreads / 32];
+    uint32_t i = blockIdx.x * kForceThreads + threadIdx.x;
+    double V = 0.0;
+    unsigned long long np = 0;
+    if (i < n) {
+        uint32_t c = key[i];
+        uint32_t cx, cy, cz;
+        decode(g, c, cx, cy, cz);
+        double xi = b.x[i], yi = b.y[i], zi = b.z[i];
+        int ti = b.elem[i];
+        double qi = b.charge[i], mi = b.mass[i], inv_mi = b.inv_mass[i];
+        double ax = 0.0, ay = 0.0, az = 0.0;
+        for (int k = -1; k < g.nfull; ++k) {
+            uint32_t B;
+            bool half;
+            if (k < 0) {
+                B = c;
+                half = true;
+            } else {
+                B = encode(g, wrap_add(cx, g.full[k][0], g.n[0]), wrap_add(cy, g.full[k][1], g.n[1]),
+                           wrap_add(cz, g.full[k][2], g.n[2]));
+                half = k < g.nhalf;
+            }
+            uint32_t lo = start[B], hi = start[B + 1];
+            for (uint32_t j = lo; j < hi; ++j) {
+                if (j == i) continue;
+                double dx = min_image1(xsub(xi, b.x[j]), L.box[0]);
+                double dy = min_image1(xsub(yi, b.y[j]), L.box[1]);
+                double dz = min_image1(xsub(zi, b.z[j]), L.box[2]);
+                double d2 = xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
+                if (d2 >= L.rc2) continue;
+                double d = xsqrt(d2);
+                if (d <= kEpsF64) continue;
+                bool count = (k < 0) ? (j > i) : half;
+                int tj = b.elem[j];
+                double fmag, Vij = 0.0;
+                pair_f64(L, d, psig[ti * kNElem + tj], peps[ti * kNElem + tj], qi, b.charge[j], mi, b.mass[j], fmag,
+                         Vij);
+                if (count) {
+                    V = xadd(V, Vij);
+                    ++np;
+                }
+                if (fmag != 0.0) {
+                    double inv = xdiv(1.0, d);
+                    ax = xadd(ax, xmul(xmul(xmul(dx, inv), fmag), inv_mi));
+                    ay = xadd(ay, xmul(xmul(xmul(dy, inv), fmag), inv_mi));
+                    az = xadd(az, xmul(xmul(xmul(dz, inv), fmag), inv_mi));
+                }
+            }
+        }
+        b.ax[i] = ax;
+        b.ay[i] = ay;
+        b.az[i] = az;
+    }
+    V = block_sum_d<kForceThreads>(V, shd);
+    np = block_sum_u<kForceThreads>(np, shu);
+    if (threadIdx.x == 0) {
+        vpart[blockIdx.x] = V;
+        if (np) atomicAdd(npairs, np);
+    }
+}
+
+// Quantise one FP32 value to 2^-32 fixed point, flagging saturation.
+__device__ __forceinline__ long long quant(float v, uint32_t* err) {
+    float s = v * kFixScaleF;
+    if (!(fabsf(s) < 9.0e18f)) {
+        atomicOr(err, isfinite(v) ? kErrSaturation : kErrNonFinite);
+        return 0;
+    }
+    return __float2ll_rn(s);
+}
+
+// Mixed pass: one thread per atom, canonical half shell, FP32 pair math,
+// fixed-point +F/-F via integer atomics.
+__global__ void __launch_bounds__(kForceThreads) k_force_mixed(GridGeom g, const float4* __restrict__ pos4,
+                                                                const uint32_t* __restrict__ key,
+                                                                const uint32_t* __restrict__ start, uint32_t n,
+                                                                LawF32 L, const PairF* __restrict__ tab,
+                                                                long long* __restrict__ F, size_t fstride,
+                                                                unsigned long long* __restrict__ vacc,
+                                                                unsigned long long* __restrict__ npairs,
+                                                                uint32_t* __restrict__ err) {
+    __shared__ PairF st[kMaxKinds * kMaxKinds];
+    __shared__ unsigned long long shu[kForceThreads / 32];
+    int nk2 = L.nkinds * L.nkinds;
+    for (int t = threadIdx.x; t < nk2; t += kForceThreads) st[t] = tab[t];
+    __syncthreads();
+    uint32_t i = blockIdx.x * kForceThreads + threadIdx.x;
+    long long vq = 0;
+    unsigned long long np = 0;
+    if (i < n) {
+        float4 pi = pos4[i];
+        int ki = __float_as_int(pi.w);
+        uint32_t c = key[i];
+        uint32_t cx, cy, cz;
+        decode(g, c, cx, cy, cz);
+        long long fx = 0, fy = 0, fz = 0;
+        for (int k = -1; k < g.nhalf; ++k) {
+            uint32_t B, lo, hi;
+            float sx = 0.f, sy = 0.f, sz = 0.f;
+            if (k < 0) {
+                B = c;
+                lo = i + 1;
+            } else {
+                int ox = g.half[k][0], oy = g.half[k][1], oz = g.half[k][2];
+                B = encode(g, wrap_add(cx, ox, g.n[0]), wrap_add(cy, oy, g.n[1]), wrap_add(cz, oz, g.n[2]));
+                lo = start[B];
+                sx = -(float)ox * g.cellf[0];
+                sy = -(float)oy * g.cellf[1];
+                sz = -(float)oz * g.cellf[2];
+            }
+            hi = start[B + 1];
+            float bx = pi.x + sx, by = pi.y + sy, bz = pi.z + sz;
+            for (uint32_t j = lo; j < hi; ++j) {
+                float4 pj = pos4[j];
+                float dx = bx - pj.x, dy = by - pj.y, dz = bz - pj.z;
+                if (g.minimg_mask) {
+                    if (g.minimg_mask & 1) dx -= g.Lf[0] * rintf(dx * g.invLf[0]);
+                    if (g.minimg_mask & 2) dy -= g.Lf[1] * rintf(dy * g.invLf[1]);
+                    if (g.minimg_mask & 4) dz -= g.Lf[2] * rintf(dz * g.invLf[2]);
+                }
+                float d2 = dx * dx + dy * dy + dz * dz;
+                if (!(d2 < L.rc2) || d2 == 0.f) continue;
+                ++np;
+                const PairF t = st[ki * L.nkinds + __float_as_int(pj.w)];
+                float inv_d = rsqrtf(d2);
+                float d = d2 * inv_d;
+                float f = 0.f, v = 0.f;
+                if (d < L.lj_rc) {
+                    bool core = d < t.half_sigma;
+                    float r = core ? t.half_sigma : d;
+                    float inv_r = core ? t.inv_half_sigma : inv_d;
+                    float s = t.sigma * inv_r;
+                    float s2 = s * s;
+                    float s6 = s2 * s2 * s2;
+                    float s12 = s6 * s6;
+                    float vl = t.eps4 * (s12 - s6);
+                    float ml = t.eps24 * inv_r * (2.f * s12 - s6);
+                    float u = (r - L.lj_ron) * L.inv_lj_w;
+                    if (u <= 0.f) {
+                        f = ml;
+                        v = vl;
+                    } else if (u < 1.f) {
+                        float u2 = u * u;
+                        float sw = 1.f + u2 * u * (-10.f + u * (15.f - 6.f * u));
+                        float omu = 1.f - u;
+                        float dsw = -30.f * u2 * omu * omu * L.inv_lj_w;
+                        f = ml * sw - vl * dsw;
+                        v = vl * sw;
+                    }
+                }
+                if (L.coul && d < L.coul_rc) {
+                    float inv_r = d < 0.5f ? 2.f : inv_d;
+                    float vc = t.qq * inv_r;
+                    float mc = vc * inv_r;
+                    float u = (d - L.coul_ron) * L.inv_coul_w;
+                    if (u <= 0.f) {
+                        f += mc;
+                        v += vc;
+                    } else if (u < 1.f) {
+                        float u2 = u * u;
+                        float sw = 1.f + u2 * u * (-10.f + u * (15.f - 6.f * u));
+                        float omu = 1.f - u;
+                        float dsw = -30.f * u2 * omu * omu * L.inv_coul_w;
+                        f += mc * sw - vc * dsw;
+                        v += vc * sw;
+                    }
+                }
+                float fs = f * inv_d;
+                long long qx = quant(dx * fs, err), qy = quant(dy * fs, err), qz = quant(dz * fs, err);
+                fx += qx;
+                fy += qy;
+                fz += qz;
+                atomicAdd((unsigned long long*)&F[j], (unsigned long long)(-qx));
+                atomicAdd((unsigned long long*)&F[fstride + j], (unsigned long long)(-qy));
+                atomicAdd((unsigned long long*)&F[2 * fstride + j], (unsigned long long)(-qz));
+                vq += quant(v, err);
+            }
+        }
+        atomicAdd((unsigned long long*)&F[i], (unsigned long long)fx);
+        atomicAdd((unsigned long long*)&F[fstride + i], (unsigned long long)fy);
+        atomicAdd((unsigned long long*)&F[2 * fstride + i], (unsigned long long)fz);
+    }
+    unsigned long long s = block_sum_u<kForceThreads>((unsigned long long)vq, shu);
+    np = block_sum_u<kForceThreads>(np, shu);
+    if (threadIdx.x == 0) {
+        if (s) atomicAdd(vacc, s);
+        if (np) atomicAdd(npairs, np);
+    }
+}
+
+// a = F * 2^-32 * (1/m) for the mixed path.
+__global__ void k_fix_to_acc(StateBuf b, const long long* __restrict__ F, size_t fstride, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double im = b.inv_mass[i];
+    b.ax[i] = xmul(xmul(__ll2double_rn(F[i]), kFixInv), im);
+    b.ay[i] = xmul(xmul(__ll2double_rn(F[fstride + i]), kFixInv), im);
+    b.az[i] = xmul(xmul(__ll2double_rn(F[2 * fstride + i]), kFixInv), im);
+}
+
+// Observed-bond spring (src/systems/forces.rs:305-317, bond_harmonic_raw
+// forces.rs:290-293) for each bond in the list, applied as many times as the
+// reference's pair list holds the pair.  FP64 in both precisions; the mixed
+// path quantises the result into the fixed-point accumulators.
+__global__ void k_bonds(GridGeom g, StateBuf b, const uint32_t* __restrict__ key,
+                        const uint32_t* __restrict__ pos_of_slot, const uint32_t* __restrict__ bonds, size_t nbonds,
+                        LawF64 L, const double* __restrict__ psig, const double* __restrict__ peps, double k_bind,
+                        double r_eq_factor, double curv_factor, int mixed, long long* __restrict__ F, size_t fstride,
+                        double* __restrict__ vbpart, unsigned long long* __restrict__ vbfix, uint32_t* __restrict__ err) {
+    __shared__ double shd[kForceThreads / 32];
+    size_t t = (size_t)blockIdx.x * kForceThreads + threadIdx.x;
+    double vb = 0.0;
+    if (t < nbonds) {
+        uint32_t ia = pos_of_slot[bonds[2 * t]], ib = pos_of_slot[bonds[2 * t + 1]];
+        double dx = min_image1(xsub(b.x[ia], b.x[ib]), L.box[0]);
+        double dy = min_image1(xsub(b.y[ia], b.y[ib]), L.box[1]);
+        double dz = min_image1(xsub(b.z[ia], b.z[ib]), L.box[2]);
+        double d2 = xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
+        double d = xsqrt(d2);
+        if (d2 < L.rc2 && d > kEpsF64) {
+            int ta = b.elem[ia], tb = b.elem[ib];
+            double sg = psig[ta * kNElem + tb], ep = peps[ta * kNElem + tb];
+            double r_eq = xmul(sg, r_eq_factor);
+            double rc_bond = xmul(k_bind, sg);
+            if (d < rc_bond) {
+                double kk = xdiv(xmul(curv_factor, ep), xmul(sg, sg));
+                double dr = xsub(d, r_eq);
+                double m = xmul(-kk, dr);
+                double v = xmul(xmul(xmul(0.5, kk), dr), dr);
+                double sw, dsw;
+                smooth_f64(d, r_eq, rc_bond, sw, dsw);
+                double fm = xsub(xmul(m, sw), xmul(v, dsw));
+                double vv = xmul(v, sw);
+                int mult = pair_multiplicity(g, key[ia], key[ib]);
+                double inv = xdiv(1.0, d);
+                double nx = xmul(dx, inv), ny = xmul(dy, inv), nz = xmul(dz, inv);
+                for (int r = 0; r < mult; ++r) {
+                    vb = xadd(vb, vv);
+                    if (fm == 0.0) continue;
+                    if (mixed) {
+                        long long qx = __double2ll_rn(xmul(xmul(nx, fm), kFixScale));
+                        long long qy = __double2ll_rn(xmul(xmul(ny, fm), kFixScale));
+                        long long qz = __double2ll_rn(xmul(xmul(nz, fm), kFixScale));
+                        atomicAdd((unsigned long long*)&F[ia], (unsigned long long)qx);
+                        atomicAdd((unsigned long long*)&F[fstride + ia], (unsigned long long)qy);
+                        atomicAdd((unsigned long long*)&F[2 * fstride + ia], (unsigned long long)qz);
+                        atomicAdd((unsigned long long*)&F[ib], (unsigned long long)(-qx));
+                        atomicAdd((unsigned long long*)&F[fstride + ib], (unsigned long long)(-qy));
+                        atomicAdd((unsigned long long*)&F[2 * fstride + ib], (unsigned long long)(-qz));
+                    } else {
+                        atomicAdd(&b.ax[ia], xmul(xmul(nx, fm), b.inv_mass[ia]));
+                        atomicAdd(&b.ay[ia], xmul(xmul(ny, fm), b.inv_mass[ia]));
+                        atomicAdd(&b.az[ia], xmul(xmul(nz, fm), b.inv_mass[ia]));
+                        atomicAdd(&b.ax[ib], xmul(xmul(nx, -fm), b.inv_mass[ib]));
+                        atomicAdd(&b.ay[ib], xmul(xmul(ny, -fm), b.inv_mass[ib]));
+                        atomicAdd(&b.az[ib], xmul(xmul(nz, -fm), b.inv_mass[ib]));
+                    }
+                }
+            }
+        }
+    }
+    if (mixed) {
+        long long q = __double2ll_rn(xmul(vb, kFixScale));
+        if (q) atomicAdd(vbfix, (unsigned long long)q);
+        (void)err;
+    } else {
+        vb = block_sum_d<kForceThreads>(vb, shd);
+        if (threadIdx.x == 0) vbpart[blockIdx.x] = vb;
+    }
+}
+
+__global__ void k_fix_to_double(const unsigned long long* __restrict__ v, double* out) {
+    *out = xmul(__ll2double_rn((long long)*v), kFixInv);
+}
+
+__global__ void __launch_bounds__(256) k_sum_rows(const double* __restrict__ part, int nb, double* out) {
+    __shared__ double sh[8];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < nb; i += 256) s = xadd(s, part[i]);
+    s = block_sum_d<256>(s, sh);
+    if (threadIdx.x == 0) *out = s;
+}
+
+inline unsigned nblk(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+LawF64 make_law64(const gx_handle* h) {
+    LawF64 L;
+    L.lj_rc = h->fs.lj_rc;
+    L.lj_ron = h->fs.lj_ron;
+    L.coul_rc = h->fs.coul_rc;
+    L.coul_ron = h->fs.coul_ron;
+    L.grav_rc = h->fs.grav_rc;
+    L.grav_ron = h->fs.grav_ron;
+    L.rc2 = h->fs.rc * h->fs.rc;
+    L.k_e = h->p.coulomb_constant;
+    L.G = h->p.gravity_constant;
+    for (int k = 0; k < 3; ++k) L.box[k] = h->p.box[k];
+    L.coul = h->p.enable_electrostatics ? 1 : 0;
+    L.grav = h->p.enable_gravity ? 1 : 0;
+    return L;
+}
+
+}  // namespace
+
+// Device copies of the FP64 pair table (the mixed table is built in gx_api.cu).
+static double* d_psig(gx_handle* h) { return h->red + 6 * (size_t)h->cap / 64 + 6 * kRedCap; }
+
+int force_pass(gx_handle* h, bool finalize_acc, double* V, double* Vb, uint64_t* npairs_out, bool sync_out) {
+    uint32_t n = (uint32_t)h->n;
+    const GridGeom& g = h->fgrid;
+    StateBuf& b = h->buf[h->cur];
+    size_t rows = (size_t)h->cap / 64 + kRedCap;
+    double* vpart = h->red + 0 * rows;
+    double* vbpart = h->red + 1 * rows;
+    double* psig = d_psig(h);
+    double* peps = psig + kNElem * kNElem;
+    GX_CUDA(h, cudaMemsetAsync(h->dcount, 0, 4 * sizeof(unsigned long long), h->stream));
+    bool mixed = h->precision == GX_MIXED;
+    LawF64 L64 = make_law64(h);
+    unsigned fb = nblk(n, kForceThreads);
+    if (!mixed) {
+        prof_begin(h, "force_f64");
+        if (n) k_force_f64<<<fb, kForceThreads, 0, h->stream>>>(g, b, h->key_sorted, h->cl.start, n, L64, psig, peps,
+                                                                vpart, h->dcount + 0);
+        prof_end(h, "force_f64");
+    } else {
+        LawF32 L;
+        L.rc2 = (float)(h->fs.rc * h->fs.rc);
+        L.lj_rc = (float)h->fs.lj_rc;
+        L.lj_ron = (float)h->fs.lj_ron;
+        L.inv_lj_w = (float)(1.0 / (h->fs.lj_rc - h->fs.lj_ron));
+        L.coul = h->p.enable_electrostatics ? 1 : 0;
+        L.coul_rc = (float)h->fs.coul_rc;
+        L.coul_ron = (float)h->fs.coul_ron;
+        L.inv_coul_w = L.coul ? (float)(1.0 / (h->fs.coul_rc - h->fs.coul_ron)) : 0.f;
+        L.nkinds = h->nkinds;
+        if (h->p.enable_gravity) return set_err(h, GX_ERR_UNSUPPORTED, "gravity is only implemented in the FP64 path");
+        GX_CUDA(h, cudaMemsetAsync(h->F, 0, 3 * h->cap * sizeof(long long), h->stream));
+        prof_begin(h, "force_mixed");
+        if (n) k_force_mixed<<<fb, kForceThreads, 0, h->stream>>>(g, h->pos4, h->key_sorted, h->cl.start, n, L,
+                                                                  h->d_pairf, h->F, h->cap, h->dcount + 1,
+                                                                  h->dcount + 0, h->derr);
+        prof_end(h, "force_mixed");
+    }
+    bool bonds_on = h->p.enable_bond_interaction && h->nbonds > 0;
+    if (bonds_on) {
+        prof_begin(h, "bonds");
+        k_bonds<<<nblk(h->nbonds, kForceThreads), kForceThreads, 0, h->stream>>>(
+            g, b, h->key_sorted, h->pos_of_slot, h->bonds, h->nbonds, L64, psig, peps, h->fs.bond_k_bind,
+            h->fs.r_eq_factor, h->fs.curv_factor, mixed ? 1 : 0, h->F, h->cap, vbpart, h->dcount + 2, h->derr);
+        prof_end(h, "bonds");
+    }
+    if (mixed) {
+        if (finalize_acc && n) k_fix_to_acc<<<nblk(n, 256), 256, 0, h->stream>>>(b, h->F, h->cap, n);
+        k_fix_to_double<<<1, 1, 0, h->stream>>>(h->dcount + 1, h->dscal + 2);
+        if (bonds_on) k_fix_to_double<<<1, 1, 0, h->stream>>>(h->dcount + 2, h->dscal + 3);
+        else GX_CUDA(h, cudaMemsetAsync(h->dscal + 3, 0, sizeof(double), h->stream));
+    } else {
+        k_sum_rows<<<1, 256, 0, h->stream>>>(vpart, (int)fb, h->dscal + 2);
+        if (bonds_on) k_sum_rows<<<1, 256, 0, h->stream>>>(vbpart, (int)nblk(h->nbonds, kForceThreads), h->dscal + 3);
+        else GX_CUDA(h, cudaMemsetAsync(h->dscal + 3, 0, sizeof(double), h->stream));
+    }
+    if (sync_out) {
+        double vv[2];
+        unsigned long long cnt;
+        GX_CUDA(h, cudaMemcpyAsync(vv, h->dscal + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        GX_CUDA(h, cudaMemcpyAsync(&cnt, h->dcount, sizeof(cnt), cudaMemcpyDeviceToHost, h->stream));
+        uint32_t e = 0;
+        GX_CUDA(h, cudaMemcpyAsync(&e, h->derr, sizeof(e), cudaMemcpyDeviceToHost, h->stream));
+        GX_CUDA(h, cudaStreamSynchronize(h->stream));
+        if (V) *V = vv[0];
+        if (Vb) *Vb = vv[1];
+        if (npairs_out) *npairs_out = cnt;
+        if (e) {
+            GX_CUDA(h, cudaMemsetAsync(h->derr, 0, sizeof(uint32_t), h->stream));
+            if (e & kErrNonFinite) return set_err(h, GX_ERR_NONFINITE, "non-finite force in the pair pass");
+            if (e & kErrSaturation) return set_err(h, GX_ERR_SATURATION, "fixed-point force saturated");
+        }
+    }
+    return GX_OK;
+}
+
+int upload_pair_table_f64(gx_handle* h) {
+    double* psig = d_psig(h);
+    GX_CUDA(h, cudaMemcpy(psig, h->fs.pair_sigma, sizeof(h->fs.pair_sigma), cudaMemcpyHostToDevice));
+    GX_CUDA(h, cudaMemcpy(psig + kNElem * kNElem, h->fs.pair_eps, sizeof(h->fs.pair_eps), cudaMemcpyHostToDevice));
+    return GX_OK;
+}
+
+size_t red_doubles(size_t cap) { return 6 * (cap / 64) + 6 * kRedCap + 2 * kNElem * kNElem + 64; }
+
+}  // namespace gx

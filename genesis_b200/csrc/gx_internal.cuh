@@ -1,0 +1,255 @@
+// gx_internal.cuh -- shared definitions of the sm_100a hot-path library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "genesis_gpu.h"
+
+namespace gx {
+
+constexpr int kNElem = GX_NELEM;
+constexpr int kMaxKinds = 16;          // distinct (element, charge) kinds in the mixed path
+constexpr double kFixScale = 4294967296.0;  // 2^32 fixed-point units per force/energy unit
+constexpr double kFixInv = 1.0 / 4294967296.0;
+constexpr float kFixScaleF = 4294967296.0f;
+constexpr double kEpsF64 = 2.220446049250313e-16;  // f64::EPSILON (grid.rs:217)
+
+// Device error word bits (read back by the host after a call).
+enum : uint32_t {
+    kErrSaturation = 1u,
+    kErrNonFinite = 2u,
+    kErrCapacity = 4u,
+    kErrBinRange = 8u,
+};
+
+// ---------------------------------------------------------------------------
+// Exact FP64: the intrinsics below are never contracted into FMAs, so a chain
+// of them rounds exactly like the reference's Rust arithmetic.
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double xsqrt(double a) { return __dsqrt_rn(a); }
+
+// f64::rem_euclid: r = a % b (fmod, exact); r < 0 ? r + |b| : r.
+__device__ __forceinline__ double rem_euclid(double a, double b) {
+    double r = fmod(a, b);
+    return r < 0.0 ? xadd(r, fabs(b)) : r;
+}
+// min_image, src/physics/grid.rs:300-306 (round = half away from zero).
+__device__ __forceinline__ double min_image1(double d, double L) {
+    return xsub(d, xmul(L, round(xdiv(d, L))));
+}
+
+// Geometry of one SpatialGrid (src/physics/grid.rs:67-86).
+struct GridGeom {
+    uint32_t n[3];      // cells per axis
+    double cell[3];     // cell edge per axis = L / n
+    double L[3];        // world size
+    float cellf[3];
+    float Lf[3];
+    float invLf[3];
+    uint32_t ncell;
+    int minimg_mask;    // bit k set when axis k has < 3 cells (FP32 min-image needed)
+    // Canonical half-shell offsets (grid.rs:275-296): first nonzero +1,
+    // zero on degenerate axes.  Up to 13.
+    int nhalf;
+    int8_t half[13][3];
+    // All distinct offsets on non-degenerate axes, excluding 0 (for gather passes).
+    int nfull;
+    int8_t full[26][3];
+};
+
+GridGeom make_grid(const double box[3], double min_cell, int* ok);
+
+__device__ __forceinline__ uint32_t axis_cell(double v, double L, double c, uint32_t n) {
+    double u = rem_euclid(xadd(v, xmul(0.5, L)), L);  // grid.rs:230
+    double f = floor(xdiv(u, c));                     // grid.rs:231
+    uint32_t i = f <= 0.0 ? 0u : (f >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)f);
+    return i < n - 1 ? i : n - 1;
+}
+__device__ __forceinline__ uint32_t encode(const GridGeom& g, uint32_t ix, uint32_t iy, uint32_t iz) {
+    return ix + g.n[0] * (iy + g.n[1] * iz);
+}
+__device__ __forceinline__ void decode(const GridGeom& g, uint32_t idx, uint32_t& ix, uint32_t& iy,
+                                       uint32_t& iz) {
+    uint32_t nxny = g.n[0] * g.n[1];
+    iz = idx / nxny;
+    uint32_t rem = idx - iz * nxny;
+    iy = rem / g.n[0];
+    ix = rem - iy * g.n[0];
+}
+__device__ __forceinline__ uint32_t wrap_add(uint32_t c, int d, uint32_t n) {
+    int v = (int)c + d;
+    if (v < 0) v += (int)n;
+    if (v >= (int)n) v -= (int)n;
+    return (uint32_t)v;
+}
+__device__ __forceinline__ uint32_t cell_of(const GridGeom& g, double x, double y, double z) {
+    return encode(g, axis_cell(x, g.L[0], g.cell[0], g.n[0]), axis_cell(y, g.L[1], g.cell[1], g.n[1]),
+                  axis_cell(z, g.L[2], g.cell[2], g.n[2]));
+}
+// Number of times the reference's neighbors() reports a pair whose members
+// sit in cells A != B: the count of offsets o (zero on degenerate axes, o != 0)
+// with A + o == B (mod n).  It is > 1 only on axes with exactly two cells.
+__device__ __forceinline__ int pair_multiplicity(const GridGeom& g, uint32_t A, uint32_t B) {
+    if (A == B) return 1;
+    uint32_t a[3], b[3];
+    decode(g, A, a[0], a[1], a[2]);
+    decode(g, B, b[0], b[1], b[2]);
+    int cnt = 0;
+    for (int k = 0; k < g.nfull; ++k) {
+        bool hit = true;
+        for (int ax = 0; ax < 3; ++ax)
+            if (wrap_add(a[ax], g.full[k][ax], g.n[ax]) != b[ax]) hit = false;
+        cnt += hit;
+    }
+    return cnt;
+}
+
+// Force-law setup (ForceSystem::new, src/systems/forces.rs:100-142).
+struct ForceSetup {
+    double pair_sigma[kNElem * kNElem];
+    double pair_eps[kNElem * kNElem];
+    double lj_rc, lj_ron;
+    double rc;  // largest enabled cutoff = grid cell
+    double coul_rc, coul_ron, grav_rc, grav_ron;
+    double bond_k_bind;
+    double max_sigma;
+    double r_eq_factor;   // 2^(1/6)   (equilibrium_distance, forces.rs:281-283)
+    double curv_factor;   // 72 * 2^(-1/3) (well_curvature, forces.rs:194-196)
+};
+
+// Mixed-path pair table entry, one per (kind_i, kind_j).
+struct PairF {
+    float sigma, half_sigma, inv_half_sigma, eps4;
+    float eps24, qq, pad0, pad1;
+};
+
+// Device buffers of one atom set in cell-sorted order.
+struct StateBuf {
+    double *x, *y, *z, *vx, *vy, *vz, *ax, *ay, *az;
+    double *charge, *mass, *inv_mass;
+    uint8_t* elem;
+    uint8_t* kind;
+    uint32_t* slot;  // ECS slot of the atom stored at this position
+};
+
+// Scratch of one counting sort (cell list).
+struct CellList {
+    uint32_t* count = nullptr;   // ncell
+    uint32_t* start = nullptr;   // ncell + 1
+    uint32_t* fill = nullptr;    // ncell
+    size_t cap_cells = 0;
+    std::vector<uint32_t*> scan_levels;  // block sums per scan level
+    std::vector<size_t> scan_sizes;
+};
+
+struct ProfSlot {
+    const char* name;
+    uint64_t launches;
+    double ms;
+    std::vector<cudaEvent_t> ev;  // pairs (start, stop) not yet read
+};
+
+}  // namespace gx
+
+struct gx_handle {
+    gx_params p;
+    gx::ForceSetup fs;
+    gx::GridGeom fgrid;  // force grid (cell >= rc)
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int precision = GX_FP64;
+
+    size_t n = 0, cap = 0;
+    gx::StateBuf buf[2];
+    int cur = 0;
+    bool sorted = false;  // buf[cur] is sorted by the force grid and keys are valid
+
+    // per-atom scratch
+    uint32_t* key = nullptr;       // cell key per atom (current order)
+    uint32_t* key_sorted = nullptr;
+    uint32_t* perm = nullptr;      // sorted position -> previous position
+    uint32_t* pos_of_slot = nullptr;  // ECS slot -> sorted position
+    uint32_t* entity = nullptr;    // EntityId::index per ECS slot
+    bool has_entity = false;
+    float4* pos4 = nullptr;        // mixed staging: cell-local xyz + kind
+    long long* F = nullptr;        // mixed fixed-point forces, 3 * cap (SoA)
+    double* host_stage = nullptr;  // device AoS staging for host transfers (3 * cap)
+    uint8_t* u8_stage = nullptr;
+    gx::CellList cl;
+
+    // reductions and scalars on device
+    double* red = nullptr;         // block partials (several rows of kRedCap)
+    double* dscal = nullptr;       // [0]=lambda pending, [1]=K, [2]=V, [3]=Vb, [4]=speed, [5]=one
+    unsigned long long* dcount = nullptr;  // [0]=pairs, [1..3]=fixed V, Vb, ...
+    uint32_t* derr = nullptr;      // device error word
+    bool lambda_pending = false;
+
+    // mixed kinds
+    int nkinds = 0;
+    double kind_charge[gx::kMaxKinds];
+    uint8_t kind_elem[gx::kMaxKinds];
+    gx::PairF* d_pairf = nullptr;  // kMaxKinds^2
+
+    // bonds (slot pairs)
+    uint32_t* bonds = nullptr;
+    size_t nbonds = 0, bonds_cap = 0;
+
+    // profiling
+    bool prof_on = false;
+    std::vector<gx::ProfSlot> prof;
+    std::vector<cudaEvent_t> ev_pool;
+
+    // CUDA graph of one tick
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_flags = -1;
+};
+
+namespace gx {
+
+constexpr int kRedCap = 4096;  // max reduction blocks per row
+
+// Error helpers (host).
+int set_err(gx_handle* h, int code, const std::string& msg);
+int cuda_err(gx_handle* h, cudaError_t e, const char* what);
+#define GX_CUDA(h, call)                                        \
+    do {                                                        \
+        cudaError_t e_ = (call);                                \
+        if (e_ != cudaSuccess) return gx::cuda_err(h, e_, #call); \
+    } while (0)
+
+// Profiling wrappers around kernel launches.
+void prof_begin(gx_handle* h, const char* name);
+void prof_end(gx_handle* h, const char* name);
+
+// Launchers implemented in the .cu files.
+int ensure_cells(gx_handle* h, CellList& cl, uint32_t ncell);
+// Counting sort of atoms [0,n) by key into perm (sorted pos -> source index),
+// deterministic (ties keep ascending source index).  cl.start gets cell starts.
+int counting_sort(gx_handle* h, CellList& cl, uint32_t ncell, const uint32_t* key, uint32_t n,
+                  uint32_t* perm);
+void launch_cell_keys(gx_handle* h, const GridGeom& g, const StateBuf& b, uint32_t n, uint32_t* key);
+void launch_gather(gx_handle* h, const StateBuf& src, const StateBuf& dst, const uint32_t* perm,
+                   const uint32_t* key_in, uint32_t* key_out, uint32_t n, uint32_t* pos_of_slot);
+void launch_build_pos4(gx_handle* h, const GridGeom& g, const StateBuf& b, const uint32_t* key,
+                       uint32_t n, float4* pos4);
+
+int force_pass(gx_handle* h, bool finalize_acc, double* V, double* Vb, uint64_t* npairs, bool sync_out);
+
+void launch_kick(gx_handle* h, const StateBuf& b, uint32_t n, double half_dt, const double* lambda);
+void launch_drift(gx_handle* h, const StateBuf& b, uint32_t n, double dt);
+void launch_wrap(gx_handle* h, const StateBuf& b, uint32_t n);
+void launch_apply_lambda(gx_handle* h, const StateBuf& b, uint32_t n, double* lambda);
+void launch_kinetic(gx_handle* h, const StateBuf& b, uint32_t n, const double* lambda, double* partials,
+                    double* speed_partials, int* nblocks);
+void launch_finalize_sum(gx_handle* h, const double* partials, int nblocks, double* out);
+void launch_thermostat_lambda(gx_handle* h, const double* partials, int nblocks, double k, double target,
+                              double tau, uint32_t n, double* lambda_out, double* K_out);
+
+}  // namespace gx

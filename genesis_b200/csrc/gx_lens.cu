@@ -1,0 +1,564 @@
+// gx_lens.cu -- the observation lenses and the grid parity probes:
+//   cell assignment           SpatialGrid::cell_of      src/physics/grid.rs:228-246
+//   neighbour pairs           SpatialGrid::neighbors    src/physics/grid.rs:119-153
+//   g(r), partial g(r)        radial_distribution(_between) src/analysis/mod.rs:87-201
+//   friends-of-friends        clusters                  src/analysis/mod.rs:221-307
+//   bound pairs               bound_pairs_with_grid     src/analysis/pairs.rs:132-174
+//
+// Each lens builds its own grid (cell = the lens cutoff) over the selected
+// atoms with the same counting sort as the force pass, then enumerates the
+// canonical half shell.  Distance tests use the reference's FP64 operation
+// order, so the pair multiset (including the repeats the reference produces
+// on axes with exactly two cells) is identical to the reference's.
+#include <cmath>
+#include <cstring>
+
+#include "gx_internal.cuh"
+
+namespace gx {
+
+struct AuxSet {
+    double *x, *y, *z;
+    uint8_t* elem;
+    uint32_t* slot;
+    uint32_t* key;  // aux-grid cell of each sorted aux atom
+    const uint32_t* start;
+    uint32_t m;
+};
+
+}  // namespace gx
+
+using namespace gx;
+
+namespace {
+
+struct AuxPool {
+    double* xyz = nullptr;  // 6 * cap: staging xyz + sorted xyz
+    uint8_t* elem = nullptr;  // 2 * cap
+    uint32_t* u32 = nullptr;  // 6 * cap: slot, slot_sorted, key, key_sorted, perm, sel
+    size_t cap = 0;
+    CellList cl;
+    uint32_t* parent = nullptr;
+    uint32_t* size = nullptr;
+    uint32_t* entity = nullptr;
+    size_t ucap = 0;
+    unsigned long long* cnt = nullptr;  // 8 counters
+    uint64_t* counts = nullptr;
+    size_t ncap = 0;
+};
+
+// One pool per handle, keyed by address (handles are few).
+struct PoolEntry {
+    const gx_handle* h;
+    AuxPool pool;
+};
+std::vector<PoolEntry> g_pools;
+
+AuxPool& pool_of(const gx_handle* h) {
+    for (auto& e : g_pools)
+        if (e.h == h) return e.pool;
+    g_pools.push_back(PoolEntry{h, AuxPool{}});
+    return g_pools.back().pool;
+}
+
+inline unsigned nblk(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+int ensure_pool(gx_handle* h, AuxPool& P, size_t m, size_t natoms) {
+    if (m > P.cap) {
+        cudaFree(P.xyz);
+        cudaFree(P.elem);
+        cudaFree(P.u32);
+        size_t cap = m < 1024 ? 1024 : m;
+        GX_CUDA(h, cudaMalloc(&P.xyz, 6 * cap * sizeof(double)));
+        GX_CUDA(h, cudaMalloc(&P.elem, 2 * cap));
+        GX_CUDA(h, cudaMalloc(&P.u32, 6 * cap * sizeof(uint32_t)));
+        P.cap = cap;
+    }
+    if (natoms > P.ucap) {
+        cudaFree(P.parent);
+        size_t cap = natoms < 1024 ? 1024 : natoms;
+        GX_CUDA(h, cudaMalloc(&P.parent, 3 * cap * sizeof(uint32_t)));
+        P.size = P.parent + cap;
+        P.entity = P.parent + 2 * cap;
+        P.ucap = cap;
+    }
+    if (!P.cnt) GX_CUDA(h, cudaMalloc(&P.cnt, 8 * sizeof(unsigned long long)));
+    return GX_OK;
+}
+
+__global__ void k_sample(const uint32_t* __restrict__ pos_of_slot, uint32_t count, uint32_t step,
+                         uint32_t* __restrict__ sel) {
+    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < count) sel[q] = pos_of_slot[q * step];
+}
+
+__global__ void k_select(GridGeom g, StateBuf b, const uint32_t* __restrict__ sel, uint32_t m, double* tx, double* ty,
+                         double* tz, uint8_t* te, uint32_t* tslot, uint32_t* key) {
+    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= m) return;
+    uint32_t p = sel ? sel[q] : q;
+    double x = b.x[p], y = b.y[p], z = b.z[p];
+    tx[q] = x;
+    ty[q] = y;
+    tz[q] = z;
+    te[q] = b.elem[p];
+    tslot[q] = b.slot[p];
+    key[q] = cell_of(g, x, y, z);
+}
+
+__global__ void k_aux_gather(const uint32_t* __restrict__ perm, uint32_t m, const double* tx, const double* ty,
+                             const double* tz, const uint8_t* te, const uint32_t* tslot, const uint32_t* key,
+                             AuxSet a) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= m) return;
+    uint32_t q = perm[p];
+    a.x[p] = tx[q];
+    a.y[p] = ty[q];
+    a.z[p] = tz[q];
+    a.elem[p] = te[q];
+    a.slot[p] = tslot[q];
+    a.key[p] = key[q];
+}
+
+// Canonical half-shell enumeration with the exact check_pair test
+// (src/physics/grid.rs:201-225).  V::operator()(i, j, d) sees aux indices.
+template <class V>
+__global__ void k_pairs(GridGeom g, AuxSet a, double box0, double box1, double box2, double cd2, V visit) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    visit.begin();
+    if (i < a.m) {
+        uint32_t c = a.key[i];
+        uint32_t cx, cy, cz;
+        decode(g, c, cx, cy, cz);
+        double xi = a.x[i], yi = a.y[i], zi = a.z[i];
+        for (int k = -1; k < g.nhalf; ++k) {
+            uint32_t B, lo;
+            if (k < 0) {
+                B = c;
+                lo = i + 1;
+            } else {
+                B = encode(g, wrap_add(cx, g.half[k][0], g.n[0]), wrap_add(cy, g.half[k][1], g.n[1]),
+                           wrap_add(cz, g.half[k][2], g.n[2]));
+                lo = a.start[B];
+            }
+            uint32_t hi = a.start[B + 1];
+            for (uint32_t j = lo; j < hi; ++j) {
+                double dx = min_image1(xsub(xi, a.x[j]), box0);
+                double dy = min_image1(xsub(yi, a.y[j]), box1);
+                double dz = min_image1(xsub(zi, a.z[j]), box2);
+                double d2 = xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
+                if (d2 >= cd2) continue;
+                double d = xsqrt(d2);
+                if (d <= kEpsF64) continue;
+                visit(a, i, j, d);
+            }
+        }
+    }
+    visit.end();
+}
+
+struct NeighborsVisit {
+    uint32_t* out;
+    size_t cap;
+    unsigned long long* cnt;
+    __device__ void begin() const {}
+    __device__ void end() const {}
+    __device__ void operator()(const AuxSet& a, uint32_t i, uint32_t j, double) const {
+        unsigned long long k = atomicAdd(cnt, 1ull);
+        if (k < cap) {
+            out[2 * k] = a.slot[i];
+            out[2 * k + 1] = a.slot[j];
+        }
+    }
+};
+
+struct GrVisit {
+    double r_max, dr;
+    unsigned long long* counts;
+    uint32_t nbins;
+    int ta, tb;
+    uint32_t* err;
+    __device__ void begin() const {}
+    __device__ void end() const {}
+    __device__ void operator()(const AuxSet& a, uint32_t i, uint32_t j, double d) const {
+        if (ta >= 0) {
+            int x = a.elem[i], y = a.elem[j];
+            if (!((x == ta && y == tb) || (x == tb && y == ta))) return;
+        }
+        if (d >= r_max) return;  // analysis/mod.rs:113-115
+        double f = xdiv(d, dr);  // (d / dr) as usize
+        uint32_t bi = f >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)f;
+        if (bi >= nbins) {
+            atomicOr(err, kErrBinRange);
+            return;
+        }
+        atomicAdd(&counts[bi], 1ull);
+    }
+};
+
+__device__ __forceinline__ uint32_t uf_root(uint32_t* par, uint32_t x) {
+    uint32_t cur = par[x];
+    if (cur != x) {
+        uint32_t next, prev = x;
+        while (cur > (next = par[cur])) {
+            par[prev] = next;
+            prev = cur;
+            cur = next;
+        }
+    }
+    return cur;
+}
+__device__ __forceinline__ void uf_unite(uint32_t* par, uint32_t a, uint32_t b) {
+    uint32_t ra = uf_root(par, a), rb = uf_root(par, b);
+    while (ra != rb) {
+        if (ra < rb) {
+            uint32_t t = ra;
+            ra = rb;
+            rb = t;
+        }
+        uint32_t old = atomicCAS(&par[ra], ra, rb);
+        if (old == ra) break;
+        ra = uf_root(par, old);
+        rb = uf_root(par, rb);
+    }
+}
+
+struct FofVisit {
+    double bond_factor;
+    double sig[kNElem];
+    uint32_t* parent;
+    unsigned long long* bound;
+    __device__ void begin() const {}
+    __device__ void end() const {}
+    __device__ void operator()(const AuxSet& a, uint32_t i, uint32_t j, double d) const {
+        // bond = bond_factor * 0.5 * (sigma_a + sigma_b), analysis/mod.rs:250
+        double bond = xmul(xmul(bond_factor, 0.5), xadd(sig[a.elem[i]], sig[a.elem[j]]));
+        if (d < bond) {
+            uf_unite(parent, a.slot[i], a.slot[j]);
+            atomicAdd(bound, 1ull);
+        }
+    }
+};
+
+struct BoundVisit {
+    double k_bind;
+    double sig[kNElem];
+    const uint32_t* entity;
+    uint32_t* out;
+    size_t cap;
+    unsigned long long* cnt;
+    __device__ void begin() const {}
+    __device__ void end() const {}
+    __device__ void operator()(const AuxSet& a, uint32_t i, uint32_t j, double d) const {
+        // threshold = k_bind * mix_sigma, analysis/pairs.rs:163
+        double threshold = xmul(k_bind, xmul(0.5, xadd(sig[a.elem[i]], sig[a.elem[j]])));
+        if (!(d < threshold)) return;
+        uint32_t ea = entity[a.slot[i]], eb = entity[a.slot[j]];
+        if (eb < ea) {
+            uint32_t t = ea;
+            ea = eb;
+            eb = t;
+        }
+        unsigned long long k = atomicAdd(cnt, 1ull);
+        if (k < cap) {
+            out[2 * k] = ea;
+            out[2 * k + 1] = eb;
+        }
+    }
+};
+
+__global__ void k_iota(uint32_t* p, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = i;
+}
+__global__ void k_fof_finish(uint32_t* par, uint32_t* size, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t r = uf_root(par, i);
+    atomicAdd(&size[r], 1u);
+}
+__global__ void k_fof_labels(uint32_t* par, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    par[i] = uf_root(par, i);
+}
+// cnt[0] monomers, [1] aggregates, [2] largest, [3] components
+__global__ void k_fof_stats(const uint32_t* size, const uint32_t* par, uint32_t n, unsigned long long* cnt) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || par[i] != i) return;
+    uint32_t s = size[i];
+    atomicAdd(&cnt[3], 1ull);
+    if (s == 1) atomicAdd(&cnt[0], 1ull);
+    else atomicAdd(&cnt[1], 1ull);
+    atomicMax(&cnt[2], (unsigned long long)s);
+}
+__global__ void k_cell_assign(GridGeom g, StateBuf b, uint32_t n, uint32_t* out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[b.slot[i]] = cell_of(g, b.x[i], b.y[i], b.z[i]);
+}
+
+// Builds the aux grid over m selected atoms (sel = sorted positions, or
+// nullptr for all atoms).
+int build_aux(gx_handle* h, AuxPool& P, const GridGeom& g, const uint32_t* sel, uint32_t m, AuxSet& a) {
+    size_t cap = P.cap;
+    double* tx = P.xyz;
+    double* ty = tx + cap;
+    double* tz = ty + cap;
+    a.x = P.xyz + 3 * cap;
+    a.y = a.x + cap;
+    a.z = a.y + cap;
+    uint8_t* te = P.elem;
+    a.elem = P.elem + cap;
+    uint32_t* tslot = P.u32;
+    a.slot = P.u32 + cap;
+    uint32_t* key = P.u32 + 2 * cap;
+    a.key = P.u32 + 3 * cap;
+    uint32_t* perm = P.u32 + 4 * cap;
+    a.m = m;
+    if (m) k_select<<<nblk(m, 256), 256, 0, h->stream>>>(g, h->buf[h->cur], sel, m, tx, ty, tz, te, tslot, key);
+    int rc = counting_sort(h, P.cl, g.ncell, key, m, perm);
+    if (rc) return rc;
+    if (m) k_aux_gather<<<nblk(m, 256), 256, 0, h->stream>>>(perm, m, tx, ty, tz, te, tslot, key, a);
+    a.start = P.cl.start;
+    return GX_OK;
+}
+
+int require(gx_handle* h) {
+    if (!h) return GX_ERR_ARG;
+    if (!h->cap) return set_err(h, GX_ERR_STATE, "no state uploaded (call gx_set_state first)");
+    return GX_OK;
+}
+
+int gr_common(gx_handle* h, int ta, int tb, double r_max_in, size_t nbins_in, size_t sample_cap, uint64_t* counts,
+              double* bins, double* rmo, double* dro) {
+    int rc = require(h);
+    if (rc) return rc;
+    if (!counts) return GX_ERR_ARG;
+    size_t nbins = nbins_in < 1 ? 1 : (nbins_in > 65536 ? 65536 : nbins_in);
+    const double* box = h->p.box;
+    double half_min = std::fmin(std::fmin(box[0], box[1]), box[2]) * 0.5;
+    double r_max = std::fmin(std::fmax(r_max_in, 1e-9), half_min);
+    double dr = r_max / (double)nbins;
+    double vol = box[0] * box[1] * box[2];
+    size_t n = h->n;
+    // g_subsample (analysis/mod.rs:32-46)
+    size_t step = 1, m = n;
+    if (sample_cap && n > sample_cap) {
+        step = n / sample_cap + 1;
+        m = n / step;
+    }
+    AuxPool& P = pool_of(h);
+    if ((rc = ensure_pool(h, P, m, n))) return rc;
+    if (nbins > P.ncap) {
+        cudaFree(P.counts);
+        GX_CUDA(h, cudaMalloc(&P.counts, nbins * sizeof(uint64_t)));
+        P.ncap = nbins;
+    }
+    uint32_t* sel = nullptr;
+    if (step > 1) {
+        sel = P.u32 + 5 * P.cap;
+        k_sample<<<nblk(m, 256), 256, 0, h->stream>>>(h->pos_of_slot, (uint32_t)m, (uint32_t)step, sel);
+    }
+    int ok = 0;
+    GridGeom g = make_grid(box, r_max, &ok);
+    if (!ok) return set_err(h, GX_ERR_UNSUPPORTED, "g(r) grid too large");
+    AuxSet a;
+    if ((rc = build_aux(h, P, g, sel, (uint32_t)m, a))) return rc;
+    GX_CUDA(h, cudaMemsetAsync(P.counts, 0, nbins * sizeof(uint64_t), h->stream));
+    GX_CUDA(h, cudaMemsetAsync(h->derr, 0, sizeof(uint32_t), h->stream));
+    GrVisit v{r_max, dr, (unsigned long long*)P.counts, (uint32_t)nbins, ta, tb, h->derr};
+    prof_begin(h, "gr_pairs");
+    if (m) k_pairs<<<nblk(m, 128), 128, 0, h->stream>>>(g, a, box[0], box[1], box[2], r_max * r_max, v);
+    prof_end(h, "gr_pairs");
+    uint32_t e = 0;
+    GX_CUDA(h, cudaMemcpyAsync(counts, P.counts, nbins * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+    GX_CUDA(h, cudaMemcpyAsync(&e, h->derr, sizeof e, cudaMemcpyDeviceToHost, h->stream));
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    GX_CUDA(h, cudaGetLastError());
+    if (rmo) *rmo = r_max;
+    if (dro) *dro = dr;
+    // normalisation on the host (analysis/mod.rs:119-132, 184-199)
+    if (bins) {
+        for (size_t i = 0; i < nbins; ++i) bins[i] = 0.0;
+        double pair_count = 0.0;
+        bool partial = ta >= 0;
+        if (partial) {
+            // species counts of the sample come from the counts kernel-free path:
+            // recount on the host from the element column of the sample.
+            std::vector<uint8_t> el(m);
+            GX_CUDA(h, cudaMemcpy(el.data(), a.elem, m, cudaMemcpyDeviceToHost));
+            size_t na = 0, nb = 0;
+            for (uint8_t t : el) {
+                na += t == ta;
+                nb += t == tb;
+            }
+            pair_count = ta == tb ? (double)na * (double)(na == 0 ? 0 : na - 1) * 0.5 : (double)na * (double)nb;
+        }
+        bool skip = partial ? !(pair_count > 0.0) : m < 2;
+        if (!skip) {
+            const double pi = 3.141592653589793;
+            for (size_t i = 0; i < nbins; ++i) {
+                double r_lo = (double)i * dr;
+                double r_hi = r_lo + dr;
+                double shell = 4.0 / 3.0 * pi * (r_hi * r_hi * r_hi - r_lo * r_lo * r_lo);
+                double expected = partial ? pair_count * shell / vol : (double)(m * (m - 1)) * 0.5 * shell / vol;
+                bins[i] = (double)counts[i] / std::fmax(expected, 2.2250738585072014e-308);
+            }
+        }
+    }
+    if (e & kErrBinRange) return set_err(h, GX_ERR_CAPACITY, "a distance rounded into bin nbins (the reference panics here)");
+    return GX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gx_cell_assign(gx_handle* h, double min_cell, uint32_t* cells) {
+    int rc = require(h);
+    if (rc) return rc;
+    if (!cells) return GX_ERR_ARG;
+    int ok = 0;
+    GridGeom g = make_grid(h->p.box, min_cell, &ok);
+    if (!ok) return set_err(h, GX_ERR_ARG, "invalid grid");
+    AuxPool& P = pool_of(h);
+    if ((rc = ensure_pool(h, P, h->n, h->n))) return rc;
+    uint32_t n = (uint32_t)h->n;
+    if (n) k_cell_assign<<<nblk(n, 256), 256, 0, h->stream>>>(g, h->buf[h->cur], n, P.u32);
+    if (n) GX_CUDA(h, cudaMemcpyAsync(cells, P.u32, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    GX_CUDA(h, cudaGetLastError());
+    return GX_OK;
+}
+
+int gx_neighbors(gx_handle* h, double min_cell, double cutoff, uint32_t* pairs, size_t cap, size_t* npairs) {
+    int rc = require(h);
+    if (rc) return rc;
+    if (cap && !pairs) return GX_ERR_ARG;
+    int ok = 0;
+    GridGeom g = make_grid(h->p.box, min_cell, &ok);
+    if (!ok) return set_err(h, GX_ERR_ARG, "invalid grid");
+    AuxPool& P = pool_of(h);
+    uint32_t n = (uint32_t)h->n;
+    if ((rc = ensure_pool(h, P, n, n))) return rc;
+    AuxSet a;
+    if ((rc = build_aux(h, P, g, nullptr, n, a))) return rc;
+    uint32_t* dout = nullptr;
+    if (cap) GX_CUDA(h, cudaMalloc(&dout, 2 * cap * sizeof(uint32_t)));
+    GX_CUDA(h, cudaMemsetAsync(P.cnt, 0, sizeof(unsigned long long), h->stream));
+    NeighborsVisit v{dout, cap, P.cnt};
+    if (n) k_pairs<<<nblk(n, 128), 128, 0, h->stream>>>(g, a, h->p.box[0], h->p.box[1], h->p.box[2], cutoff * cutoff, v);
+    unsigned long long total = 0;
+    GX_CUDA(h, cudaMemcpyAsync(&total, P.cnt, sizeof total, cudaMemcpyDeviceToHost, h->stream));
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    size_t w = total < cap ? (size_t)total : cap;
+    if (w) GX_CUDA(h, cudaMemcpy(pairs, dout, 2 * w * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    cudaFree(dout);
+    if (npairs) *npairs = (size_t)total;
+    GX_CUDA(h, cudaGetLastError());
+    return total > cap ? set_err(h, GX_ERR_CAPACITY, "pair buffer too small") : GX_OK;
+}
+
+int gx_radial_distribution(gx_handle* h, double r_max, size_t nbins, size_t sample_cap, uint64_t* counts,
+                           double* bins, double* r_max_out, double* dr_out) {
+    return gr_common(h, -1, -1, r_max, nbins, sample_cap, counts, bins, r_max_out, dr_out);
+}
+
+int gx_radial_distribution_between(gx_handle* h, uint8_t ta, uint8_t tb, double r_max, size_t nbins,
+                                   size_t sample_cap, uint64_t* counts, double* bins, double* r_max_out,
+                                   double* dr_out) {
+    if (ta >= kNElem || tb >= kNElem) return GX_ERR_ARG;
+    return gr_common(h, ta, tb, r_max, nbins, sample_cap, counts, bins, r_max_out, dr_out);
+}
+
+int gx_clusters(gx_handle* h, double bond_factor, uint32_t* labels, uint64_t stats[4], double* mean_size) {
+    int rc = require(h);
+    if (rc) return rc;
+    if (!stats) return GX_ERR_ARG;
+    stats[0] = stats[1] = stats[2] = stats[3] = 0;
+    if (mean_size) *mean_size = 0.0;
+    uint32_t n = (uint32_t)h->n;
+    if (n == 0) return GX_OK;  // analysis/mod.rs:230-232
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    AuxPool& P = pool_of(h);
+    if ((rc = ensure_pool(h, P, n, n))) return rc;
+    // max sigma over the particles present (analysis/mod.rs:236-238)
+    std::vector<uint8_t> el(n);
+    GX_CUDA(h, cudaMemcpy(el.data(), h->buf[h->cur].elem, n, cudaMemcpyDeviceToHost));
+    double max_sigma = 0.0;
+    for (uint8_t t : el) max_sigma = std::fmax(max_sigma, h->p.sigma[t]);
+    double cutoff = std::fmax(std::fmax(bond_factor, 0.1) * max_sigma, 1e-9);
+    int ok = 0;
+    GridGeom g = make_grid(h->p.box, cutoff, &ok);
+    if (!ok) return set_err(h, GX_ERR_UNSUPPORTED, "FoF grid too large");
+    AuxSet a;
+    if ((rc = build_aux(h, P, g, nullptr, n, a))) return rc;
+    k_iota<<<nblk(n, 256), 256, 0, h->stream>>>(P.parent, n);
+    GX_CUDA(h, cudaMemsetAsync(P.size, 0, n * sizeof(uint32_t), h->stream));
+    GX_CUDA(h, cudaMemsetAsync(P.cnt, 0, 8 * sizeof(unsigned long long), h->stream));
+    FofVisit v;
+    v.bond_factor = bond_factor;
+    for (int k = 0; k < kNElem; ++k) v.sig[k] = h->p.sigma[k];
+    v.parent = P.parent;
+    v.bound = P.cnt + 4;
+    prof_begin(h, "fof_pairs");
+    k_pairs<<<nblk(n, 128), 128, 0, h->stream>>>(g, a, h->p.box[0], h->p.box[1], h->p.box[2], cutoff * cutoff, v);
+    prof_end(h, "fof_pairs");
+    k_fof_finish<<<nblk(n, 256), 256, 0, h->stream>>>(P.parent, P.size, n);
+    k_fof_labels<<<nblk(n, 256), 256, 0, h->stream>>>(P.parent, n);
+    k_fof_stats<<<nblk(n, 256), 256, 0, h->stream>>>(P.size, P.parent, n, P.cnt);
+    unsigned long long c[8];
+    GX_CUDA(h, cudaMemcpyAsync(c, P.cnt, sizeof c, cudaMemcpyDeviceToHost, h->stream));
+    if (labels) GX_CUDA(h, cudaMemcpyAsync(labels, P.parent, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    GX_CUDA(h, cudaGetLastError());
+    stats[0] = c[0];
+    stats[1] = c[1];
+    stats[2] = c[2];
+    stats[3] = c[4];
+    if (mean_size) *mean_size = (double)n / (double)(c[3] > 0 ? c[3] : 1);
+    return GX_OK;
+}
+
+int gx_bound_pairs(gx_handle* h, double k_bind, uint32_t* pairs, size_t cap, size_t* npairs) {
+    int rc = require(h);
+    if (rc) return rc;
+    if (cap && !pairs) return GX_ERR_ARG;
+    uint32_t n = (uint32_t)h->n;
+    AuxPool& P = pool_of(h);
+    if ((rc = ensure_pool(h, P, n, n))) return rc;
+    double ms = 0.0;  // bind_cutoff, analysis/pairs.rs:112-114
+    for (int k = 0; k < kNElem; ++k) ms = std::fmax(ms, h->p.sigma[k]);
+    double cutoff = k_bind * ms;
+    int ok = 0;
+    GridGeom g = make_grid(h->p.box, cutoff, &ok);
+    if (!ok) return set_err(h, GX_ERR_ARG, "invalid bond grid");
+    AuxSet a;
+    if ((rc = build_aux(h, P, g, nullptr, n, a))) return rc;
+    if (h->has_entity) GX_CUDA(h, cudaMemcpyAsync(P.entity, h->entity, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream));
+    else k_iota<<<nblk(n, 256), 256, 0, h->stream>>>(P.entity, n);
+    uint32_t* dout = nullptr;
+    if (cap) GX_CUDA(h, cudaMalloc(&dout, 2 * cap * sizeof(uint32_t)));
+    GX_CUDA(h, cudaMemsetAsync(P.cnt, 0, sizeof(unsigned long long), h->stream));
+    BoundVisit v;
+    v.k_bind = k_bind;
+    for (int k = 0; k < kNElem; ++k) v.sig[k] = h->p.sigma[k];
+    v.entity = P.entity;
+    v.out = dout;
+    v.cap = cap;
+    v.cnt = P.cnt;
+    prof_begin(h, "bound_pairs");
+    if (n) k_pairs<<<nblk(n, 128), 128, 0, h->stream>>>(g, a, h->p.box[0], h->p.box[1], h->p.box[2], cutoff * cutoff, v);
+    prof_end(h, "bound_pairs");
+    unsigned long long total = 0;
+    GX_CUDA(h, cudaMemcpyAsync(&total, P.cnt, sizeof total, cudaMemcpyDeviceToHost, h->stream));
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    size_t w = total < cap ? (size_t)total : cap;
+    if (w) GX_CUDA(h, cudaMemcpy(pairs, dout, 2 * w * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    cudaFree(dout);
+    if (npairs) *npairs = (size_t)total;
+    GX_CUDA(h, cudaGetLastError());
+    return total > cap ? set_err(h, GX_ERR_CAPACITY, "pair buffer too small") : GX_OK;
+}
+
+}  // extern "C"

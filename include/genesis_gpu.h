@@ -1,0 +1,192 @@
+/*
+ * genesis_gpu.h -- C ABI of the B200 (sm_100a) per-tick particle hot path.
+ *
+ * One gx_handle is one universe held resident on one GPU (or, for the
+ * gx_batch_* calls, many small universes advanced together).  The caller
+ * owns every host array; the library owns all device memory.  A handle is
+ * not re-entrant: one host thread drives it at a time (the reference's
+ * Scheduler::run calls systems sequentially on one thread,
+ * src/scheduler/mod.rs:83-89).  Every call returns a gx_status; on error
+ * gx_last_error() gives the text.
+ *
+ * Slot order.  Per-atom host arrays are in the order the reference's
+ * World::for_each3::<Position, Mass, AtomType> visits entities
+ * (src/ecs/world.rs:345-383) -- the "slot" order of ForceSystem
+ * (src/systems/forces.rs:179-203).  `entity` carries EntityId::index per
+ * slot (src/ecs/entity.rs:28-30).  Internally atoms are kept sorted by cell;
+ * the library converts on the way in and out.
+ *
+ * Each entry point below names the reference interface it replaces.
+ */
+#ifndef GENESIS_GPU_H
+#define GENESIS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GX_NELEM 10 /* AtomType::COUNT, src/components/atom_type.rs:34 */
+
+typedef enum {
+    GX_OK = 0,
+    GX_ERR_ARG = -1,          /* invalid argument (null pointer, bad size) */
+    GX_ERR_OOM = -2,          /* device allocation failed */
+    GX_ERR_CUDA = -3,         /* a CUDA runtime call failed */
+    GX_ERR_CAPACITY = -4,     /* an output buffer or a per-cell capacity was too small */
+    GX_ERR_SATURATION = -5,   /* a fixed-point force/energy left the int64 range */
+    GX_ERR_NONFINITE = -6,    /* non-finite position or velocity seen on device */
+    GX_ERR_TIMEOUT = -7,      /* a bounded device wait gave up */
+    GX_ERR_UNSUPPORTED = -8,  /* configuration not supported by this path */
+    GX_ERR_STATE = -9         /* call out of order (e.g. no state uploaded) */
+} gx_status;
+
+typedef enum {
+    GX_FP64 = 0,  /* plain path: FP64 throughout, per-pair arithmetic bit-exact to the reference */
+    GX_MIXED = 1  /* FP32 pair arithmetic, 64-bit fixed-point force/energy accumulation */
+} gx_precision;
+
+/* Parameters: the Config fields the force, integrator, boundary and
+ * thermostat systems read (src/config/mod.rs:15-229), with the affinity
+ * table already resolved (ElementTable::apply_overrides,
+ * src/physics/forces.rs:90-109).  Element order: H He C N O Na Si P S Fe
+ * (element_index, src/physics/forces.rs:176-189). */
+typedef struct {
+    double box[3];                 /* universe.size */
+    double dt;                     /* universe.dt */
+    double thermal_constant;       /* physics.thermal_constant */
+    double sigma[GX_NELEM];        /* LjElement::sigma */
+    double epsilon_k[GX_NELEM];    /* LjElement::epsilon_k (kelvin) */
+    double charge[GX_NELEM];       /* LjElement::charge */
+    double lj_cutoff_factor;       /* LJ_CUTOFF_FACTOR = 2.5 */
+    double coulomb_constant;       /* physics.coulomb_constant */
+    double coulomb_cutoff;         /* physics.coulomb_cutoff (x max sigma) */
+    double gravity_constant;       /* physics.gravity_constant */
+    double gravity_cutoff;         /* physics.gravity_cutoff (x max sigma) */
+    double bond_k_bind;            /* stats.bond_k_bind */
+    double thermostat_temperature; /* physics.thermostat_temperature */
+    double thermostat_tau;         /* physics.thermostat_tau (ticks) */
+    int32_t enable_electrostatics; /* systems.enable_electrostatics */
+    int32_t enable_gravity;        /* systems.enable_gravity */
+    int32_t enable_bond_interaction; /* systems.enable_bond_interaction */
+    int32_t enable_thermostat;     /* systems.enable_thermostat */
+    int32_t enable_boundaries;     /* systems.enable_boundaries */
+    int32_t precision;             /* gx_precision */
+    int32_t device;                /* CUDA device ordinal */
+    int32_t reserved[3];           /* must be zero */
+} gx_params;
+
+/* Per-tick observables, what StatsSystem reads after the force schedule
+ * (src/systems/aggregate.rs:86-143) plus the force-pass counters. */
+typedef struct {
+    double kinetic;         /* sum 0.5*m*|v|^2 after the thermostat */
+    double speed_sum;       /* sum |v| */
+    double potential;       /* PotentialEnergy (LJ + Coulomb + gravity) */
+    double bond_energy;     /* BondEnergy */
+    double lambda;          /* Berendsen scale applied this tick (1 when off) */
+    uint64_t pairs;         /* pair-list entries within the cutoff this tick */
+} gx_tick_stats;
+
+typedef struct gx_handle gx_handle;
+
+/* ---- lifecycle ------------------------------------------------------- */
+
+/* ForceSystem::new (src/systems/forces.rs:100-142) + ThermostatSystem::new
+ * (src/systems/thermostat.rs:26-32): builds the LJ table
+ * (LjTable::new, src/physics/forces.rs:223-237), the cutoffs and the grid
+ * geometry, and creates the CUDA stream the handle uses. */
+int gx_create(const gx_params* params, gx_handle** out);
+void gx_destroy(gx_handle* h);
+const char* gx_last_error(const gx_handle* h);
+const char* gx_status_string(int status);
+int gx_set_precision(gx_handle* h, int precision);
+
+/* ---- state ----------------------------------------------------------- */
+
+/* Upload the ECS columns the hot path reads: Position, Velocity,
+ * Acceleration (Vec3 AoS f64), AtomType as element index 0..9, Charge,
+ * Mass, and EntityId::index per slot (src/systems/forces.rs:185-200;
+ * src/components/*.rs).  acc may be NULL (zero, as spawn_atom writes,
+ * src/universe/mod.rs:272); entity may be NULL (slot number). */
+int gx_set_state(gx_handle* h, size_t n, const double* pos, const double* vel,
+                 const double* acc, const uint8_t* elem, const double* charge,
+                 const double* mass, const uint32_t* entity);
+/* Download Position, Velocity, Acceleration in slot order (the write-backs
+ * of src/systems/integrate.rs:40-43,63-66, boundary.rs:28-34,
+ * forces.rs:343-345, thermostat.rs:68-70).  Any NULL pointer is skipped. */
+int gx_get_state(gx_handle* h, double* pos, double* vel, double* acc);
+size_t gx_num_atoms(const gx_handle* h);
+/* Observed bonds as slot pairs, one entry per bond: the adjacency that
+ * ForceSystem builds from the Bonds component (src/systems/forces.rs:208-226). */
+int gx_set_bonds(gx_handle* h, size_t nbonds, const uint32_t* slot_pairs);
+
+/* ---- systems of the force schedule (src/universe/mod.rs:356-369) ------ */
+
+int gx_half_kick(gx_handle* h);  /* VelocityHalfKick::run, src/systems/integrate.rs:38-45 */
+int gx_drift(gx_handle* h);      /* PositionDrift::run, src/systems/integrate.rs:61-67 */
+int gx_wrap(gx_handle* h);       /* BoundarySystem::run, src/systems/boundary.rs:22-35 */
+/* ForceSystem::run, src/systems/forces.rs:163-353: rebuilds the cell list
+ * (counting sort by cell) and runs the pair pass; outputs PotentialEnergy,
+ * BondEnergy and the number of pairs within the cutoff.  Any output may be NULL. */
+int gx_forces(gx_handle* h, double* potential, double* bond_energy, uint64_t* pairs);
+/* ThermostatSystem::run, src/systems/thermostat.rs:47-71. */
+int gx_thermostat(gx_handle* h, double* kinetic, double* lambda);
+/* StatsSystem reductions, src/systems/aggregate.rs:86-93. */
+int gx_stats(gx_handle* h, double* kinetic, double* speed_sum);
+/* nsteps ticks of the whole chain: kick, drift, [wrap], forces, kick,
+ * [thermostat] -- Universe::tick with the force schedule
+ * (src/universe/mod.rs:141-159, 356-369).  stats may be NULL, else it
+ * receives nsteps entries.  Runs as one captured CUDA graph per tick
+ * shape when use_graph != 0. */
+int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph);
+
+/* ---- parity probes and lenses ---------------------------------------- */
+
+/* SpatialGrid::new + cell_of + encode (src/physics/grid.rs:67-86,228-246):
+ * cell index of every atom, slot order, for a grid of cells >= min_cell. */
+int gx_cell_assign(gx_handle* h, double min_cell, uint32_t* cells);
+/* SpatialGrid::build + neighbors (src/physics/grid.rs:99-153): every pair
+ * (slot a, slot b) with distance < cutoff on a grid of cells >= min_cell,
+ * with the reference's multiplicity (a pair is repeated when an axis has
+ * exactly two cells).  Order is unspecified.  Writes min(total, cap) pairs;
+ * *npairs receives the total. */
+int gx_neighbors(gx_handle* h, double min_cell, double cutoff, uint32_t* pairs,
+                 size_t cap, size_t* npairs);
+/* radial_distribution (src/analysis/mod.rs:87-133).  sample_cap is
+ * G_SAMPLE_CAP (8192) for the reference's evenly spaced subsample, 0 for
+ * every atom.  counts: nbins u64; bins: nbins f64 (may be NULL). */
+int gx_radial_distribution(gx_handle* h, double r_max, size_t nbins, size_t sample_cap,
+                           uint64_t* counts, double* bins, double* r_max_out,
+                           double* dr_out);
+/* radial_distribution_between (src/analysis/mod.rs:143-201). */
+int gx_radial_distribution_between(gx_handle* h, uint8_t ta, uint8_t tb, double r_max,
+                                   size_t nbins, size_t sample_cap, uint64_t* counts,
+                                   double* bins, double* r_max_out, double* dr_out);
+/* clusters (src/analysis/mod.rs:221-284): friends-of-friends with
+ * r < bond_factor * sigma_ij.  labels[slot] = smallest slot of its
+ * component; stats = {monomers, aggregates, largest, bound_pairs}. */
+int gx_clusters(gx_handle* h, double bond_factor, uint32_t* labels, uint64_t stats[4],
+                double* mean_size);
+/* bound_pairs_with_grid (src/analysis/pairs.rs:132-174): entity-index pairs
+ * (a < b) with r < k_bind * sigma_ij, reference multiplicity, unspecified
+ * order. */
+int gx_bound_pairs(gx_handle* h, double k_bind, uint32_t* pairs, size_t cap, size_t* npairs);
+
+/* ---- timing ---------------------------------------------------------- */
+
+/* Waits for the handle's stream. */
+int gx_synchronize(gx_handle* h);
+/* Per-kernel CUDA-event timing of gx_step/gx_forces launches (on the
+ * handle's stream).  When enabled, each launch is bracketed by events. */
+int gx_profile_enable(gx_handle* h, int on);
+/* Names, launch counts and summed milliseconds since the last reset;
+ * returns the number of kernels (up to cap entries written). */
+int gx_profile_read(gx_handle* h, const char** names, uint64_t* launches, double* ms,
+                    int cap, int reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GENESIS_GPU_H */
