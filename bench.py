@@ -1,0 +1,417 @@
+#!/usr/bin/env python
+"""Headline benchmark of the per-tick particle hot path on B200.
+
+Workload: the 2,097,152-atom condensation quench (128^3 lattice, spacing
+1.2 x max sigma, 10-element mixture with the element charges, LJ + Coulomb,
+velocities at 300 K, Berendsen to 20 K, g(r) every 100 ticks with 256 bins
+and r_max = 3 r_c), one tick = kick, drift, wrap, cell sort, pair pass, kick,
+thermostat.  Synthetic seeded inputs; the state (~300 MB) is larger than L2,
+so no flush is needed between ticks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line (rank 0).  Under torchrun each rank advances its own
+replica of the workload on its own GPU (the single-universe path has no
+inter-GPU exchange in this build), so scaling is weak.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "atom-steps/s/GPU mixed vs plain FP64 at ≤1e-5 force err; replica-steps/s"
+UNIT = "atom-steps/s"
+FLOP_PER_PAIR_LJ = 67      # algorithmic FLOPs per in-cutoff pair (LJ), FMA = 2
+FLOP_PER_PAIR_LJC = 75     # with Coulomb sharing the switch
+# Algorithmic bytes per atom of each memory-bound kernel (reads + writes of
+# the arrays the kernel must touch; FP64 state, u8 element/kind, u32 ids).
+BYTES_PER_ATOM = {
+    "kick": 72, "drift": 72, "wrap": 48, "cell_keys": 28, "cell_count": 4, "cell_scan": 0,
+    "cell_scatter": 16, "reorder": 220, "stage_pos4": 45, "kinetic": 32,
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c3")
+    ap.add_argument("--n-side", type=int, default=0, help="override the lattice edge (testing only)")
+    ap.add_argument("--no-extras", action="store_true", help="skip fp64/e2e/cpu legs (testing only)")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- distributed
+
+
+class Dist:
+    def __init__(self, n_gpus: int):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", self.local))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{self.local}")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------- clocks
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9 and f[1].replace(".", "").isdigit():
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows]
+        reasons = set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            for k, nm in enumerate(names):
+                if r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit()) if rows else None,
+                "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------- helpers
+
+
+def workload(args):
+    from genesis_b200 import workloads as W
+
+    wl = W.WORKLOADS[args.workload]
+    if args.n_side:
+        wl = wl.scaled(args.n_side)
+    return wl
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except Exception:
+            pass
+    return {}
+
+
+def ncu_traffic(kernel: str) -> float | None:
+    """DRAM bytes per launch from the committed ncu summary, if present."""
+    for f in (ROOT / "profiles").glob("*.txt"):
+        for line in f.read_text().splitlines():
+            if line.startswith(f"traffic_bytes_per_launch[{kernel}]"):
+                try:
+                    return float(line.split(":", 1)[1].split()[0])
+                except Exception:
+                    return None
+    return None
+
+
+def run_ticks(h, wl, cfg, steps: int, start_tick: int) -> int:
+    """steps ticks through gx_step, with the workload's g(r) every gr_every ticks."""
+    from genesis_b200 import elements as E
+
+    t = start_tick
+    done = 0
+    rc = E.LJ_CUTOFF_FACTOR * max(cfg.sigma)
+    while done < steps:
+        k = steps - done
+        if wl.gr_every:
+            k = min(k, wl.gr_every - (t % wl.gr_every))
+        h.step(k, stats=False)
+        done += k
+        t += k
+        if wl.gr_every and t % wl.gr_every == 0:
+            h.radial_distribution(wl.gr_rmax_factor * rc, wl.gr_bins, E.G_SAMPLE_CAP)
+    return t
+
+
+def cpu_reference(wl, cfg, u, budget_s: float, threads: int) -> dict:
+    """The oracle's threaded restatement of the reference's rayon tick."""
+    from oracle import oracle
+
+    pos, vel, acc = u.pos, u.vel, None
+    oracle.ticks(cfg, pos[:1], vel[:1], None, u.elem[:1], u.charge[:1], u.mass[:1], 1, nthreads=1)
+    ticks, elapsed = 0, 0.0
+    while elapsed < budget_s or ticks == 0:
+        t0 = time.perf_counter()
+        pos, vel, acc, _ = oracle.ticks(cfg, pos, vel, acc, u.elem, u.charge, u.mass, 1, nthreads=threads)
+        elapsed += time.perf_counter() - t0
+        ticks += 1
+        if elapsed > 3 * budget_s:
+            break
+    return {"value": u.n * ticks / elapsed, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{ticks} full ticks of the {u.n}-atom workload ({elapsed:.1f} s), C++ restatement of the "
+                      f"reference rayon tick on {threads} host threads"}
+
+
+# ---------------------------------------------------------------- arms
+
+
+def reference_arm(args, dist):
+    if dist.rank != 0:
+        return
+    wl = workload(args)
+    cfg = wl.config()
+    u = wl.generate()
+    threads = os.cpu_count() or 1
+    budget = float(os.environ.get("GENESIS_REF_BUDGET_S", "60"))
+    cb = cpu_reference(wl, cfg, u, budget, threads)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": wl.name, "atoms": u.n, "host_threads": threads},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def ours_arm(args, dist):
+    import numpy as np
+
+    from genesis_b200 import _lib
+    from genesis_b200._lib import Handle
+
+    wl = workload(args)
+    cfg = wl.config()
+    u = wl.generate(salt=dist.rank)
+    dev = dist.local
+    K, Wm = args.steps, max(args.warmup, 0)
+    extras = {}
+
+    h = Handle(cfg, "mixed", dev)
+    h.set_universe(u)
+    tick = run_ticks(h, wl, cfg, Wm, 0)
+    h.synchronize()
+    dist.barrier()
+    h.synchronize()
+    clocks = Clocks(dev)
+    clocks.start()
+    l0 = h.launches
+    h.mark(0)
+    tick = run_ticks(h, wl, cfg, K, tick)
+    h.mark(1)
+    ms = h.elapsed_ms(0, 1)
+    launches = h.launches - l0
+    clk = clocks.stop()
+    h.synchronize()
+    dist.barrier()
+    ms_max = dist.max(ms)
+    value = dist.world * u.n * K / (ms_max * 1e-3)
+
+    # per-kernel device times over a profiled pass of the same ticks
+    h.profile(True)
+    st = h.step(min(K, 50), stats=True)
+    prof = h.profile_read(reset=True)
+    h.profile(False)
+    pairs = float(np.mean(st["pairs"]))
+    force_k = "force_mixed"
+    f_launch, f_ms = prof.get(force_k, (1, float("nan")))
+    force_ms = f_ms / max(f_launch, 1)
+    tot_ms = sum(v[1] for v in prof.values())
+    flop_pp = FLOP_PER_PAIR_LJC if cfg.enable_electrostatics else FLOP_PER_PAIR_LJ
+    achieved = pairs * flop_pp / (force_ms * 1e-3) / 1e12
+    try:
+        peak = _lib.measure_fp32_peak(dev)
+        peak_src = "measured: FP32 FMA loop on all SMs (gx_measure_fp32_peak)"
+    except Exception as e:  # noqa: BLE001
+        peak, peak_src = 74.4, f"nominal 148 SM x 128 lanes x 2 x 1.965 GHz ({e})"
+    traffic = ncu_traffic(force_k)
+    roof = {"kernel": force_k, "bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
+            "flop_per_launch": pairs * flop_pp, "pairs_per_launch": pairs, "launch_ms": force_ms,
+            "share_of_step": f_ms / tot_ms if tot_ms else None}
+    hbm = measured_peaks().get("hbm_gbs")
+    mem = {}
+    for k, (nl, kms) in prof.items():
+        if k in BYTES_PER_ATOM and nl and BYTES_PER_ATOM[k]:
+            gbs = BYTES_PER_ATOM[k] * u.n / (kms / nl * 1e-3) / 1e9
+            mem[k] = {"launch_ms": kms / nl, "GB/s": gbs, "frac": gbs / hbm if hbm else None,
+                      "share": kms / tot_ms if tot_ms else None}
+    top_mem = max(mem.items(), key=lambda kv: kv[1]["launch_ms"] * prof[kv[0]][0]) if mem else None
+    roof_hbm = None
+    if top_mem:
+        roof_hbm = {"kernel": top_mem[0], "bound": "hbm", "achieved": top_mem[1]["GB/s"], "peak": hbm,
+                    "unit": "GB/s", "frac": top_mem[1]["frac"], "peak_source": "MEASURED_PEAKS.json hbm_gbs"
+                    if hbm else "fallback 6650 GB/s", "traffic": ncu_traffic(top_mem[0])}
+    kernels = {k: {"launches": v[0], "ms": v[1], "share": v[1] / tot_ms if tot_ms else None}
+               for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}
+
+    if not args.no_extras:
+        # plain FP64 GPU path on the same state
+        try:
+            pos, vel, acc = h.get_state()
+            h64 = Handle(cfg, "fp64", dev)
+            h64.set_state(pos, vel, u.elem, acc=acc, charge=u.charge, mass=u.mass, entity=u.entity)
+            K64 = max(10, min(K, 60))
+            run_ticks(h64, wl, cfg, 3, tick)
+            h64.synchronize()
+            h64.mark(0)
+            run_ticks(h64, wl, cfg, K64, tick + 3)
+            h64.mark(1)
+            ms64 = dist.max(h64.elapsed_ms(0, 1))
+            v64 = dist.world * u.n * K64 / (ms64 * 1e-3)
+            # force accuracy of the mixed pass against the FP64 pass (which
+            # matches the oracle to 1e-12) on one state
+            hm = Handle(cfg, "mixed", dev)
+            pos, vel, acc = h64.get_state()
+            hm.set_state(pos, vel, u.elem, charge=u.charge, mass=u.mass, entity=u.entity)
+            h64.set_state(pos, vel, u.elem, charge=u.charge, mass=u.mass, entity=u.entity)
+            Vm, _, _ = hm.forces()
+            V64, _, _ = h64.forces()
+            am = hm.get_state()[2]
+            a64 = h64.get_state()[2]
+            rel = float(np.linalg.norm(am - a64) / np.linalg.norm(a64))
+            extras["fp64"] = {"value": v64, "ms_per_step": ms64 / K64, "steps": K64,
+                              "mixed_over_fp64": value / v64}
+            extras["force_rel_rms_vs_fp64"] = rel
+            extras["potential_rel_err_vs_fp64"] = abs(Vm - V64) / abs(V64)
+            hm.close()
+            h64.close()
+        except Exception as e:  # noqa: BLE001
+            extras["fp64_error"] = repr(e)
+
+        # end to end through the C ABI: host ECS columns synced every tick
+        try:
+            import torch
+
+            n = u.n
+            pin = [torch.empty((n, 3), dtype=torch.float64, pin_memory=True) for _ in range(3)]
+            arr = [p.numpy() for p in pin]
+            pos, vel, acc = h.get_state()
+            arr[0][:] = pos
+            arr[1][:] = vel
+            arr[2][:] = acc
+            Ke = max(5, min(K, 20))
+            he = Handle(cfg, "mixed", dev)
+            he.set_state(arr[0], arr[1], u.elem, acc=arr[2], charge=u.charge, mass=u.mass, entity=u.entity)
+            he.step(2)
+            he.synchronize()
+            dist.barrier()
+            t0 = time.perf_counter()
+            for _ in range(Ke):
+                he.set_dynamic(arr[0], arr[1], arr[2])
+                stt = he.step(1, stats=True)
+                he.get_state_into(arr[0], arr[1], arr[2])
+            he.synchronize()
+            te = time.perf_counter() - t0
+            te = dist.max(te)
+            extras["e2e"] = {"value": dist.world * n * Ke / te, "unit": UNIT,
+                             "h2d_bytes_per_step": 3 * n * 24, "d2h_bytes_per_step": 3 * n * 24 + stt.nbytes,
+                             "steps": Ke, "timing": "host wall clock, pinned host buffers, "
+                             "gx_set_dynamic + gx_step(1) + gx_get_state every tick"}
+            he.close()
+        except Exception as e:  # noqa: BLE001
+            extras["e2e_error"] = repr(e)
+
+        if dist.rank == 0 and dist.world == 1:
+            try:
+                threads = os.cpu_count() or 1
+                extras["cpu_baseline"] = cpu_reference(wl, cfg, u, 12.0, threads)
+            except Exception as e:  # noqa: BLE001
+                extras["cpu_baseline_error"] = repr(e)
+
+    h.close()
+    if dist.rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": K, "warmup": Wm,
+                "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 pair arithmetic, i64 fixed-point accumulation, f64 state",
+                "data": "synthetic",
+                "config": {"workload": wl.name, "atoms": u.n, "precision": "mixed", "thermostat_target_K":
+                           cfg.thermostat_temperature, "electrostatics": cfg.enable_electrostatics,
+                           "gr_every": wl.gr_every, "l2": "inputs larger than L2 (state ~300 MB > 126 MB); no flush",
+                           "parallelism": f"{dist.world} independent replicas (one per GPU)"},
+                "gpu_launches": launches, "clocks": clk, "roofline": roof, "roofline_hbm": roof_hbm,
+                "kernels": kernels, "memory_kernels": mem, "pairs_per_tick": pairs}
+        line.update(extras)
+        if "e2e" not in line:
+            line["e2e"] = None
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    dist = Dist(args.gpus)
+    try:
+        if args.impl == "reference":
+            reference_arm(args, dist)
+        else:
+            ours_arm(args, dist)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -50,7 +50,8 @@ EXPORTS = (
     "gx_drift", "gx_wrap", "gx_forces", "gx_thermostat", "gx_stats", "gx_step",
     "gx_cell_assign", "gx_neighbors", "gx_radial_distribution",
     "gx_radial_distribution_between", "gx_clusters", "gx_bound_pairs",
-    "gx_synchronize", "gx_profile_enable", "gx_profile_read",
+    "gx_synchronize", "gx_profile_enable", "gx_profile_read", "gx_set_dynamic",
+    "gx_timer_mark", "gx_timer_elapsed", "gx_launch_count", "gx_measure_fp32_peak",
 )
 
 _lib = None
@@ -93,6 +94,11 @@ def load(path: str | Path | None = None) -> C.CDLL:
         "gx_synchronize": (C.c_int, [vp]),
         "gx_profile_enable": (C.c_int, [vp, C.c_int]),
         "gx_profile_read": (C.c_int, [vp, C.POINTER(C.c_char_p), u64p, dp, C.c_int, C.c_int]),
+        "gx_set_dynamic": (C.c_int, [vp, dp, dp, dp]),
+        "gx_timer_mark": (C.c_int, [vp, C.c_int]),
+        "gx_timer_elapsed": (C.c_int, [vp, C.c_int, C.c_int, dp]),
+        "gx_launch_count": (C.c_uint64, [vp]),
+        "gx_measure_fp32_peak": (C.c_int, [C.c_int, dp]),
     }
     for name, (res, args) in proto.items():
         f = getattr(lib, name)
@@ -246,6 +252,28 @@ class Handle:
     def synchronize(self):
         self._check(self.lib.gx_synchronize(self.h))
 
+    def set_dynamic(self, pos=None, vel=None, acc=None):
+        """Per-tick sync of the dynamic columns from host arrays (slot order)."""
+        a = [None if x is None else np.ascontiguousarray(x, dtype=np.float64) for x in (pos, vel, acc)]
+        self._check(self.lib.gx_set_dynamic(self.h, *(_ptr(x, C.c_double) for x in a)))
+
+    def get_state_into(self, pos=None, vel=None, acc=None):
+        """gx_get_state into caller-owned (e.g. pinned) float64 (n, 3) arrays."""
+        self._check(self.lib.gx_get_state(self.h, _ptr(pos, C.c_double), _ptr(vel, C.c_double),
+                                          _ptr(acc, C.c_double)))
+
+    def mark(self, slot: int):
+        self._check(self.lib.gx_timer_mark(self.h, slot))
+
+    def elapsed_ms(self, a: int, b: int) -> float:
+        ms = C.c_double()
+        self._check(self.lib.gx_timer_elapsed(self.h, a, b, C.byref(ms)))
+        return ms.value
+
+    @property
+    def launches(self) -> int:
+        return int(self.lib.gx_launch_count(self.h))
+
     # -- probes and lenses --------------------------------------------------
     def cell_assign(self, min_cell: float) -> np.ndarray:
         out = np.empty(self.n, dtype=np.uint32)
@@ -306,3 +334,13 @@ class Handle:
         if k < 0:
             self._check(k)
         return {names[i].decode(): (int(launches[i]), float(ms[i])) for i in range(min(k, cap))}
+
+
+def measure_fp32_peak(device: int = 0) -> float:
+    """Measured FP32 FMA throughput (TFLOP/s) of the device."""
+    lib = load()
+    t = C.c_double()
+    rc = lib.gx_measure_fp32_peak(device, C.byref(t))
+    if rc != 0:
+        raise GxError(rc, "gx_measure_fp32_peak failed")
+    return t.value

@@ -193,6 +193,31 @@ __global__ void k_soa_to_aos(const double* __restrict__ x, const double* __restr
     aos[3 * s + 1] = y[i];
     aos[3 * s + 2] = z[i];
 }
+// slot-ordered AoS -> sorted SoA (per-tick host column sync)
+__global__ void k_aos_to_sorted(const double* __restrict__ aos, const uint32_t* __restrict__ pos_of_slot, double* x,
+                                double* y, double* z, uint32_t n) {
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    uint32_t p = pos_of_slot[s];
+    x[p] = aos[3 * s];
+    y[p] = aos[3 * s + 1];
+    z[p] = aos[3 * s + 2];
+}
+// Eight independent FMA chains per thread (diagnostic FP32 peak probe).
+__global__ void k_fma_peak(float* out, int iters, float seed) {
+    float a[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = seed + 1e-3f * (threadIdx.x + k);
+    const float m = 0.9999999f, c = 1e-7f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a[k] = fmaf(a[k], m, c);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += a[k];
+    if (s == 12345.678f) out[threadIdx.x] = s;  // keeps the chains live
+}
 __global__ void k_init_slots(StateBuf b, uint32_t* pos_of_slot, uint32_t n) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -433,14 +458,14 @@ int gx_set_state(gx_handle* h, size_t n, const double* pos, const double* vel, c
     if (rc) return rc;
     if (n) {
         GX_CUDA(h, cudaMemcpyAsync(h->host_stage, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-        k_aos_to_soa<<<nblk(n, 256), 256, 0, h->stream>>>(h->host_stage, b.x, b.y, b.z, un);
+        GX_LAUNCH(h, k_aos_to_soa, nblk(n, 256), 256, h->host_stage, b.x, b.y, b.z, un);
         GX_CUDA(h, cudaStreamSynchronize(h->stream));
         GX_CUDA(h, cudaMemcpyAsync(h->host_stage, vel, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-        k_aos_to_soa<<<nblk(n, 256), 256, 0, h->stream>>>(h->host_stage, b.vx, b.vy, b.vz, un);
+        GX_LAUNCH(h, k_aos_to_soa, nblk(n, 256), 256, h->host_stage, b.vx, b.vy, b.vz, un);
         GX_CUDA(h, cudaStreamSynchronize(h->stream));
         if (acc) {
             GX_CUDA(h, cudaMemcpyAsync(h->host_stage, acc, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-            k_aos_to_soa<<<nblk(n, 256), 256, 0, h->stream>>>(h->host_stage, b.ax, b.ay, b.az, un);
+            GX_LAUNCH(h, k_aos_to_soa, nblk(n, 256), 256, h->host_stage, b.ax, b.ay, b.az, un);
             GX_CUDA(h, cudaStreamSynchronize(h->stream));
         } else {
             GX_CUDA(h, cudaMemsetAsync(b.ax, 0, 3 * h->cap * sizeof(double), h->stream));
@@ -454,7 +479,7 @@ int gx_set_state(gx_handle* h, size_t n, const double* pos, const double* vel, c
         GX_CUDA(h, cudaMemcpyAsync(b.kind, kind.data(), n, cudaMemcpyHostToDevice, h->stream));
         if (entity)
             GX_CUDA(h, cudaMemcpyAsync(h->entity, entity, n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
-        k_init_slots<<<nblk(n, 256), 256, 0, h->stream>>>(b, h->pos_of_slot, un);
+        GX_LAUNCH(h, k_init_slots, nblk(n, 256), 256, b, h->pos_of_slot, un);
         GX_CUDA(h, cudaStreamSynchronize(h->stream));
     }
     h->has_entity = entity != nullptr;
@@ -474,7 +499,7 @@ int gx_get_state(gx_handle* h, double* pos, double* vel, double* acc) {
     double* srcs[3][3] = {{b.x, b.y, b.z}, {b.vx, b.vy, b.vz}, {b.ax, b.ay, b.az}};
     for (int k = 0; k < 3; ++k) {
         if (!outs[k] || !n) continue;
-        k_soa_to_aos<<<nblk(n, 256), 256, 0, h->stream>>>(srcs[k][0], srcs[k][1], srcs[k][2], b.slot, h->host_stage, n);
+        GX_LAUNCH(h, k_soa_to_aos, nblk(n, 256), 256, srcs[k][0], srcs[k][1], srcs[k][2], b.slot, h->host_stage, n);
         GX_CUDA(h, cudaMemcpyAsync(outs[k], h->host_stage, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost,
                                    h->stream));
         GX_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -631,7 +656,7 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
         const double* lam = h->lambda_pending ? h->dscal + 0 : nullptr;
         launch_kick(h, h->buf[h->cur], n, 0.5 * h->p.dt, lam);
         if (h->lambda_pending) {
-            k_fill_d<<<1, 32, 0, h->stream>>>(h->dscal, 1, 1.0);
+            GX_LAUNCH(h, k_fill_d, 1, 32, h->dscal, 1, 1.0);
             h->lambda_pending = false;
         }
         launch_drift(h, h->buf[h->cur], n, h->p.dt);                // PositionDrift
@@ -653,7 +678,7 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
             launch_kinetic(h, h->buf[h->cur], n, h->lambda_pending ? h->dscal + 0 : nullptr, kpart, spart, &nb);
             launch_finalize_sum(h, kpart, nb, h->dscal + 1);
             launch_finalize_sum(h, spart, nb, h->dscal + 4);
-            k_record<<<1, 1, 0, h->stream>>>(drec + s, h->dscal, h->dcount, thermo ? 1 : 0);
+            GX_LAUNCH(h, k_record, 1, 1, drec + s, h->dscal, h->dcount, thermo ? 1 : 0);
         }
     }
     if (drec) {
@@ -672,9 +697,84 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
     return GX_OK;
 }
 
+int gx_set_dynamic(gx_handle* h, const double* pos, const double* vel, const double* acc) {
+    int rc = require_state(h);
+    if (rc) return rc;
+    if (h->lambda_pending) {  // the host columns replace v: the pending scale is void
+        GX_LAUNCH(h, k_fill_d, 1, 32, h->dscal, 1, 1.0);
+        h->lambda_pending = false;
+    }
+    StateBuf& b = h->buf[h->cur];
+    uint32_t n = (uint32_t)h->n;
+    const double* ins[3] = {pos, vel, acc};
+    double* dsts[3][3] = {{b.x, b.y, b.z}, {b.vx, b.vy, b.vz}, {b.ax, b.ay, b.az}};
+    for (int k = 0; k < 3; ++k) {
+        if (!ins[k] || !n) continue;
+        double* stage = h->host_stage;
+        GX_CUDA(h, cudaMemcpyAsync(stage, ins[k], 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        GX_LAUNCH(h, k_aos_to_sorted, nblk(n, 256), 256, stage, h->pos_of_slot, dsts[k][0], dsts[k][1], dsts[k][2], n);
+    }
+    if (pos) h->sorted = false;
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    GX_CUDA(h, cudaGetLastError());
+    return GX_OK;
+}
+
 int gx_synchronize(gx_handle* h) {
     if (!h) return GX_ERR_ARG;
     GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    return GX_OK;
+}
+
+int gx_timer_mark(gx_handle* h, int slot) {
+    if (!h || slot < 0 || slot >= 16) return GX_ERR_ARG;
+    if (!h->timers[slot]) GX_CUDA(h, cudaEventCreate(&h->timers[slot]));
+    GX_CUDA(h, cudaEventRecord(h->timers[slot], h->stream));
+    return GX_OK;
+}
+
+int gx_timer_elapsed(gx_handle* h, int a, int b, double* ms) {
+    if (!h || !ms || a < 0 || b < 0 || a >= 16 || b >= 16 || !h->timers[a] || !h->timers[b]) return GX_ERR_ARG;
+    GX_CUDA(h, cudaEventSynchronize(h->timers[b]));
+    float t = 0.f;
+    GX_CUDA(h, cudaEventElapsedTime(&t, h->timers[a], h->timers[b]));
+    *ms = (double)t;
+    return GX_OK;
+}
+
+uint64_t gx_launch_count(const gx_handle* h) { return h ? h->launches : 0; }
+
+int gx_measure_fp32_peak(int device, double* tflops) {
+    if (!tflops) return GX_ERR_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return GX_ERR_CUDA;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    float* out = nullptr;
+    if (cudaMalloc(&out, 1024 * 1024 * sizeof(float)) != cudaSuccess) return GX_ERR_OOM;
+    const int iters = 4096, threads = 512, blocks = sms * 8;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    k_fma_peak<<<blocks, threads>>>(out, iters, 1.0f);  // warm-up
+    double best = 0.0;
+    for (int rep = 0; rep < 5; ++rep) {
+        cudaEventRecord(a);
+        k_fma_peak<<<blocks, threads>>>(out, iters, 1.0f + rep * 1e-7f);
+        cudaEventRecord(b);
+        cudaEventSynchronize(b);
+        float t = 0.f;
+        cudaEventElapsedTime(&t, a, b);
+        // 8 independent FMA chains x iters per thread, 2 FLOP per FMA
+        double flop = 2.0 * 8.0 * iters * (double)threads * blocks;
+        double tf = flop / (t * 1e-3) / 1e12;
+        if (tf > best) best = tf;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaError_t e = cudaGetLastError();
+    cudaFree(out);
+    if (e != cudaSuccess) return GX_ERR_CUDA;
+    *tflops = best;
     return GX_OK;
 }
 

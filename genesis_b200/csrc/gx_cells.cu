@@ -295,13 +295,13 @@ int ensure_cells(gx_handle* h, CellList& cl, uint32_t ncell) {
 static void scan_rec(gx_handle* h, CellList& cl, const uint32_t* in, uint32_t* out, uint32_t n, int level) {
     unsigned nb = (n + kScanTile - 1) / kScanTile;
     if (nb <= 1) {
-        k_scan_tile<<<1, kScanThreads, 0, h->stream>>>(in, out, n, nullptr);
+        GX_LAUNCH(h, k_scan_tile, 1, kScanThreads, in, out, n, nullptr);
         return;
     }
     uint32_t* sums = cl.scan_levels[level];
-    k_scan_tile<<<nb, kScanThreads, 0, h->stream>>>(in, out, n, sums);
+    GX_LAUNCH(h, k_scan_tile, nb, kScanThreads, in, out, n, sums);
     scan_rec(h, cl, sums, sums, nb, level + 1);
-    k_scan_add<<<nblk(n, 256), 256, 0, h->stream>>>(out, n, sums);
+    GX_LAUNCH(h, k_scan_add, nblk(n, 256), 256, out, n, sums);
 }
 
 int counting_sort(gx_handle* h, CellList& cl, uint32_t ncell, const uint32_t* key, uint32_t n, uint32_t* perm) {
@@ -310,14 +310,14 @@ int counting_sort(gx_handle* h, CellList& cl, uint32_t ncell, const uint32_t* ke
     prof_begin(h, "cell_count");
     GX_CUDA(h, cudaMemsetAsync(cl.count, 0, ((size_t)ncell + 1) * sizeof(uint32_t), h->stream));
     GX_CUDA(h, cudaMemsetAsync(cl.fill, 0, (size_t)ncell * sizeof(uint32_t), h->stream));
-    if (n) k_count<<<nblk(n, 256), 256, 0, h->stream>>>(key, n, cl.count);
+    if (n) GX_LAUNCH(h, k_count, nblk(n, 256), 256, key, n, cl.count);
     prof_end(h, "cell_count");
     prof_begin(h, "cell_scan");
     scan_rec(h, cl, cl.count, cl.start, ncell + 1, 0);
     prof_end(h, "cell_scan");
     prof_begin(h, "cell_scatter");
-    if (n) k_scatter<<<nblk(n, 256), 256, 0, h->stream>>>(key, n, cl.start, cl.fill, perm);
-    k_segsort<<<nblk(ncell, 128), 128, 0, h->stream>>>(cl.start, ncell, perm);
+    if (n) GX_LAUNCH(h, k_scatter, nblk(n, 256), 256, key, n, cl.start, cl.fill, perm);
+    GX_LAUNCH(h, k_segsort, nblk(ncell, 128), 128, cl.start, ncell, perm);
     prof_end(h, "cell_scatter");
     return GX_OK;
 }
@@ -325,7 +325,7 @@ int counting_sort(gx_handle* h, CellList& cl, uint32_t ncell, const uint32_t* ke
 void launch_cell_keys(gx_handle* h, const GridGeom& g, const StateBuf& b, uint32_t n, uint32_t* key) {
     if (!n) return;
     prof_begin(h, "cell_keys");
-    k_cell_keys<<<nblk(n, 256), 256, 0, h->stream>>>(g, b.x, b.y, b.z, n, key, h->derr);
+    GX_LAUNCH(h, k_cell_keys, nblk(n, 256), 256, g, b.x, b.y, b.z, n, key, h->derr);
     prof_end(h, "cell_keys");
 }
 
@@ -333,7 +333,7 @@ void launch_gather(gx_handle* h, const StateBuf& src, const StateBuf& dst, const
                    const uint32_t* key_in, uint32_t* key_out, uint32_t n, uint32_t* pos_of_slot) {
     if (!n) return;
     prof_begin(h, "reorder");
-    k_gather<<<nblk(n, 256), 256, 0, h->stream>>>(src, dst, perm, key_in, key_out, n, pos_of_slot);
+    GX_LAUNCH(h, k_gather, nblk(n, 256), 256, src, dst, perm, key_in, key_out, n, pos_of_slot);
     prof_end(h, "reorder");
 }
 
@@ -341,31 +341,31 @@ void launch_build_pos4(gx_handle* h, const GridGeom& g, const StateBuf& b, const
                        float4* pos4) {
     if (!n) return;
     prof_begin(h, "stage_pos4");
-    k_build_pos4<<<nblk(n, 256), 256, 0, h->stream>>>(g, b, key, n, pos4);
+    GX_LAUNCH(h, k_build_pos4, nblk(n, 256), 256, g, b, key, n, pos4);
     prof_end(h, "stage_pos4");
 }
 
 void launch_kick(gx_handle* h, const StateBuf& b, uint32_t n, double half_dt, const double* lambda) {
     if (!n) return;
     prof_begin(h, "kick");
-    k_kick<<<nblk(n, 256), 256, 0, h->stream>>>(b, n, half_dt, lambda);
+    GX_LAUNCH(h, k_kick, nblk(n, 256), 256, b, n, half_dt, lambda);
     prof_end(h, "kick");
 }
 void launch_drift(gx_handle* h, const StateBuf& b, uint32_t n, double dt) {
     if (!n) return;
     prof_begin(h, "drift");
-    k_drift<<<nblk(n, 256), 256, 0, h->stream>>>(b, n, dt);
+    GX_LAUNCH(h, k_drift, nblk(n, 256), 256, b, n, dt);
     prof_end(h, "drift");
 }
 void launch_wrap(gx_handle* h, const StateBuf& b, uint32_t n) {
     if (!n) return;
     prof_begin(h, "wrap");
-    k_wrap<<<nblk(n, 256), 256, 0, h->stream>>>(b, n, 0.5 * h->p.box[0], 0.5 * h->p.box[1], 0.5 * h->p.box[2]);
+    GX_LAUNCH(h, k_wrap, nblk(n, 256), 256, b, n, 0.5 * h->p.box[0], 0.5 * h->p.box[1], 0.5 * h->p.box[2]);
     prof_end(h, "wrap");
 }
 void launch_apply_lambda(gx_handle* h, const StateBuf& b, uint32_t n, double* lambda) {
-    if (n) k_apply_lambda<<<nblk(n, 256), 256, 0, h->stream>>>(b, n, lambda);
-    k_set_one<<<1, 1, 0, h->stream>>>(lambda);
+    if (n) GX_LAUNCH(h, k_apply_lambda, nblk(n, 256), 256, b, n, lambda);
+    GX_LAUNCH(h, k_set_one, 1, 1, lambda);
 }
 void launch_kinetic(gx_handle* h, const StateBuf& b, uint32_t n, const double* lambda, double* kpart,
                     double* spart, int* nblocks) {
@@ -373,16 +373,16 @@ void launch_kinetic(gx_handle* h, const StateBuf& b, uint32_t n, const double* l
     if (nb > 1184) nb = 1184;  // 8 x 148 SMs; fixed for a given n
     if (nb < 1) nb = 1;
     prof_begin(h, "kinetic");
-    k_kinetic<<<nb, kRedThreads, 0, h->stream>>>(b, n, lambda, kpart, spart);
+    GX_LAUNCH(h, k_kinetic, nb, kRedThreads, b, n, lambda, kpart, spart);
     prof_end(h, "kinetic");
     *nblocks = nb;
 }
 void launch_finalize_sum(gx_handle* h, const double* partials, int nblocks, double* out) {
-    k_finalize_sum<<<1, kRedThreads, 0, h->stream>>>(partials, nblocks, out);
+    GX_LAUNCH(h, k_finalize_sum, 1, kRedThreads, partials, nblocks, out);
 }
 void launch_thermostat_lambda(gx_handle* h, const double* partials, int nblocks, double k, double target,
                               double tau, uint32_t n, double* lambda_out, double* K_out) {
-    k_thermostat_lambda<<<1, kRedThreads, 0, h->stream>>>(partials, nblocks, k, target, tau, n, lambda_out, K_out);
+    GX_LAUNCH(h, k_thermostat_lambda, 1, kRedThreads, partials, nblocks, k, target, tau, n, lambda_out, K_out);
 }
 
 }  // namespace gx

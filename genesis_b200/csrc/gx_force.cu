@@ -450,7 +450,7 @@ int force_pass(gx_handle* h, bool finalize_acc, double* V, double* Vb, uint64_t*
     unsigned fb = nblk(n, kForceThreads);
     if (!mixed) {
         prof_begin(h, "force_f64");
-        if (n) k_force_f64<<<fb, kForceThreads, 0, h->stream>>>(g, b, h->key_sorted, h->cl.start, n, L64, psig, peps,
+        if (n) GX_LAUNCH(h, k_force_f64, fb, kForceThreads, g, b, h->key_sorted, h->cl.start, n, L64, psig, peps,
                                                                 vpart, h->dcount + 0);
         prof_end(h, "force_f64");
     } else {
@@ -467,7 +467,7 @@ int force_pass(gx_handle* h, bool finalize_acc, double* V, double* Vb, uint64_t*
         if (h->p.enable_gravity) return set_err(h, GX_ERR_UNSUPPORTED, "gravity is only implemented in the FP64 path");
         GX_CUDA(h, cudaMemsetAsync(h->F, 0, 3 * h->cap * sizeof(long long), h->stream));
         prof_begin(h, "force_mixed");
-        if (n) k_force_mixed<<<fb, kForceThreads, 0, h->stream>>>(g, h->pos4, h->key_sorted, h->cl.start, n, L,
+        if (n) GX_LAUNCH(h, k_force_mixed, fb, kForceThreads, g, h->pos4, h->key_sorted, h->cl.start, n, L,
                                                                   h->d_pairf, h->F, h->cap, h->dcount + 1,
                                                                   h->dcount + 0, h->derr);
         prof_end(h, "force_mixed");
@@ -475,19 +475,19 @@ int force_pass(gx_handle* h, bool finalize_acc, double* V, double* Vb, uint64_t*
     bool bonds_on = h->p.enable_bond_interaction && h->nbonds > 0;
     if (bonds_on) {
         prof_begin(h, "bonds");
-        k_bonds<<<nblk(h->nbonds, kForceThreads), kForceThreads, 0, h->stream>>>(
+        GX_LAUNCH(h, k_bonds, nblk(h->nbonds, kForceThreads), kForceThreads, 
             g, b, h->key_sorted, h->pos_of_slot, h->bonds, h->nbonds, L64, psig, peps, h->fs.bond_k_bind,
             h->fs.r_eq_factor, h->fs.curv_factor, mixed ? 1 : 0, h->F, h->cap, vbpart, h->dcount + 2, h->derr);
         prof_end(h, "bonds");
     }
     if (mixed) {
-        if (finalize_acc && n) k_fix_to_acc<<<nblk(n, 256), 256, 0, h->stream>>>(b, h->F, h->cap, n);
-        k_fix_to_double<<<1, 1, 0, h->stream>>>(h->dcount + 1, h->dscal + 2);
-        if (bonds_on) k_fix_to_double<<<1, 1, 0, h->stream>>>(h->dcount + 2, h->dscal + 3);
+        if (finalize_acc && n) GX_LAUNCH(h, k_fix_to_acc, nblk(n, 256), 256, b, h->F, h->cap, n);
+        GX_LAUNCH(h, k_fix_to_double, 1, 1, h->dcount + 1, h->dscal + 2);
+        if (bonds_on) GX_LAUNCH(h, k_fix_to_double, 1, 1, h->dcount + 2, h->dscal + 3);
         else GX_CUDA(h, cudaMemsetAsync(h->dscal + 3, 0, sizeof(double), h->stream));
     } else {
-        k_sum_rows<<<1, 256, 0, h->stream>>>(vpart, (int)fb, h->dscal + 2);
-        if (bonds_on) k_sum_rows<<<1, 256, 0, h->stream>>>(vbpart, (int)nblk(h->nbonds, kForceThreads), h->dscal + 3);
+        GX_LAUNCH(h, k_sum_rows, 1, 256, vpart, (int)fb, h->dscal + 2);
+        if (bonds_on) GX_LAUNCH(h, k_sum_rows, 1, 256, vbpart, (int)nblk(h->nbonds, kForceThreads), h->dscal + 3);
         else GX_CUDA(h, cudaMemsetAsync(h->dscal + 3, 0, sizeof(double), h->stream));
     }
     if (sync_out) {

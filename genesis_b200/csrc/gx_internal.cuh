@@ -209,7 +209,19 @@ struct gx_handle {
     // CUDA graph of one tick
     cudaGraphExec_t graph_exec = nullptr;
     int graph_flags = -1;
+
+    // stream-ordered timers and the launch counter
+    cudaEvent_t timers[16] = {};
+    uint64_t launches = 0;
 };
+
+// Every kernel launch of the library goes through this macro so the
+// handle's launch counter is exact.
+#define GX_LAUNCH(h, kern, grid, block, ...)                          \
+    do {                                                              \
+        kern<<<(grid), (block), 0, (h)->stream>>>(__VA_ARGS__);       \
+        ++(h)->launches;                                              \
+    } while (0)
 
 namespace gx {
 

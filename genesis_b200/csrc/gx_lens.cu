@@ -315,10 +315,10 @@ int build_aux(gx_handle* h, AuxPool& P, const GridGeom& g, const uint32_t* sel, 
     a.key = P.u32 + 3 * cap;
     uint32_t* perm = P.u32 + 4 * cap;
     a.m = m;
-    if (m) k_select<<<nblk(m, 256), 256, 0, h->stream>>>(g, h->buf[h->cur], sel, m, tx, ty, tz, te, tslot, key);
+    if (m) GX_LAUNCH(h, k_select, nblk(m, 256), 256, g, h->buf[h->cur], sel, m, tx, ty, tz, te, tslot, key);
     int rc = counting_sort(h, P.cl, g.ncell, key, m, perm);
     if (rc) return rc;
-    if (m) k_aux_gather<<<nblk(m, 256), 256, 0, h->stream>>>(perm, m, tx, ty, tz, te, tslot, key, a);
+    if (m) GX_LAUNCH(h, k_aux_gather, nblk(m, 256), 256, perm, m, tx, ty, tz, te, tslot, key, a);
     a.start = P.cl.start;
     return GX_OK;
 }
@@ -357,7 +357,7 @@ int gr_common(gx_handle* h, int ta, int tb, double r_max_in, size_t nbins_in, si
     uint32_t* sel = nullptr;
     if (step > 1) {
         sel = P.u32 + 5 * P.cap;
-        k_sample<<<nblk(m, 256), 256, 0, h->stream>>>(h->pos_of_slot, (uint32_t)m, (uint32_t)step, sel);
+        GX_LAUNCH(h, k_sample, nblk(m, 256), 256, h->pos_of_slot, (uint32_t)m, (uint32_t)step, sel);
     }
     int ok = 0;
     GridGeom g = make_grid(box, r_max, &ok);
@@ -368,7 +368,7 @@ int gr_common(gx_handle* h, int ta, int tb, double r_max_in, size_t nbins_in, si
     GX_CUDA(h, cudaMemsetAsync(h->derr, 0, sizeof(uint32_t), h->stream));
     GrVisit v{r_max, dr, (unsigned long long*)P.counts, (uint32_t)nbins, ta, tb, h->derr};
     prof_begin(h, "gr_pairs");
-    if (m) k_pairs<<<nblk(m, 128), 128, 0, h->stream>>>(g, a, box[0], box[1], box[2], r_max * r_max, v);
+    if (m) GX_LAUNCH(h, k_pairs, nblk(m, 128), 128, g, a, box[0], box[1], box[2], r_max * r_max, v);
     prof_end(h, "gr_pairs");
     uint32_t e = 0;
     GX_CUDA(h, cudaMemcpyAsync(counts, P.counts, nbins * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
@@ -424,7 +424,7 @@ int gx_cell_assign(gx_handle* h, double min_cell, uint32_t* cells) {
     AuxPool& P = pool_of(h);
     if ((rc = ensure_pool(h, P, h->n, h->n))) return rc;
     uint32_t n = (uint32_t)h->n;
-    if (n) k_cell_assign<<<nblk(n, 256), 256, 0, h->stream>>>(g, h->buf[h->cur], n, P.u32);
+    if (n) GX_LAUNCH(h, k_cell_assign, nblk(n, 256), 256, g, h->buf[h->cur], n, P.u32);
     if (n) GX_CUDA(h, cudaMemcpyAsync(cells, P.u32, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
     GX_CUDA(h, cudaStreamSynchronize(h->stream));
     GX_CUDA(h, cudaGetLastError());
@@ -447,7 +447,7 @@ int gx_neighbors(gx_handle* h, double min_cell, double cutoff, uint32_t* pairs, 
     if (cap) GX_CUDA(h, cudaMalloc(&dout, 2 * cap * sizeof(uint32_t)));
     GX_CUDA(h, cudaMemsetAsync(P.cnt, 0, sizeof(unsigned long long), h->stream));
     NeighborsVisit v{dout, cap, P.cnt};
-    if (n) k_pairs<<<nblk(n, 128), 128, 0, h->stream>>>(g, a, h->p.box[0], h->p.box[1], h->p.box[2], cutoff * cutoff, v);
+    if (n) GX_LAUNCH(h, k_pairs, nblk(n, 128), 128, g, a, h->p.box[0], h->p.box[1], h->p.box[2], cutoff * cutoff, v);
     unsigned long long total = 0;
     GX_CUDA(h, cudaMemcpyAsync(&total, P.cnt, sizeof total, cudaMemcpyDeviceToHost, h->stream));
     GX_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -493,7 +493,7 @@ int gx_clusters(gx_handle* h, double bond_factor, uint32_t* labels, uint64_t sta
     if (!ok) return set_err(h, GX_ERR_UNSUPPORTED, "FoF grid too large");
     AuxSet a;
     if ((rc = build_aux(h, P, g, nullptr, n, a))) return rc;
-    k_iota<<<nblk(n, 256), 256, 0, h->stream>>>(P.parent, n);
+    GX_LAUNCH(h, k_iota, nblk(n, 256), 256, P.parent, n);
     GX_CUDA(h, cudaMemsetAsync(P.size, 0, n * sizeof(uint32_t), h->stream));
     GX_CUDA(h, cudaMemsetAsync(P.cnt, 0, 8 * sizeof(unsigned long long), h->stream));
     FofVisit v;
@@ -502,11 +502,11 @@ int gx_clusters(gx_handle* h, double bond_factor, uint32_t* labels, uint64_t sta
     v.parent = P.parent;
     v.bound = P.cnt + 4;
     prof_begin(h, "fof_pairs");
-    k_pairs<<<nblk(n, 128), 128, 0, h->stream>>>(g, a, h->p.box[0], h->p.box[1], h->p.box[2], cutoff * cutoff, v);
+    GX_LAUNCH(h, k_pairs, nblk(n, 128), 128, g, a, h->p.box[0], h->p.box[1], h->p.box[2], cutoff * cutoff, v);
     prof_end(h, "fof_pairs");
-    k_fof_finish<<<nblk(n, 256), 256, 0, h->stream>>>(P.parent, P.size, n);
-    k_fof_labels<<<nblk(n, 256), 256, 0, h->stream>>>(P.parent, n);
-    k_fof_stats<<<nblk(n, 256), 256, 0, h->stream>>>(P.size, P.parent, n, P.cnt);
+    GX_LAUNCH(h, k_fof_finish, nblk(n, 256), 256, P.parent, P.size, n);
+    GX_LAUNCH(h, k_fof_labels, nblk(n, 256), 256, P.parent, n);
+    GX_LAUNCH(h, k_fof_stats, nblk(n, 256), 256, P.size, P.parent, n, P.cnt);
     unsigned long long c[8];
     GX_CUDA(h, cudaMemcpyAsync(c, P.cnt, sizeof c, cudaMemcpyDeviceToHost, h->stream));
     if (labels) GX_CUDA(h, cudaMemcpyAsync(labels, P.parent, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
@@ -536,7 +536,7 @@ int gx_bound_pairs(gx_handle* h, double k_bind, uint32_t* pairs, size_t cap, siz
     AuxSet a;
     if ((rc = build_aux(h, P, g, nullptr, n, a))) return rc;
     if (h->has_entity) GX_CUDA(h, cudaMemcpyAsync(P.entity, h->entity, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream));
-    else k_iota<<<nblk(n, 256), 256, 0, h->stream>>>(P.entity, n);
+    else GX_LAUNCH(h, k_iota, nblk(n, 256), 256, P.entity, n);
     uint32_t* dout = nullptr;
     if (cap) GX_CUDA(h, cudaMalloc(&dout, 2 * cap * sizeof(uint32_t)));
     GX_CUDA(h, cudaMemsetAsync(P.cnt, 0, sizeof(unsigned long long), h->stream));
@@ -548,7 +548,7 @@ int gx_bound_pairs(gx_handle* h, double k_bind, uint32_t* pairs, size_t cap, siz
     v.cap = cap;
     v.cnt = P.cnt;
     prof_begin(h, "bound_pairs");
-    if (n) k_pairs<<<nblk(n, 128), 128, 0, h->stream>>>(g, a, h->p.box[0], h->p.box[1], h->p.box[2], cutoff * cutoff, v);
+    if (n) GX_LAUNCH(h, k_pairs, nblk(n, 128), 128, g, a, h->p.box[0], h->p.box[1], h->p.box[2], cutoff * cutoff, v);
     prof_end(h, "bound_pairs");
     unsigned long long total = 0;
     GX_CUDA(h, cudaMemcpyAsync(&total, P.cnt, sizeof total, cudaMemcpyDeviceToHost, h->stream));

@@ -174,10 +174,25 @@ int gx_clusters(gx_handle* h, double bond_factor, uint32_t* labels, uint64_t sta
  * order. */
 int gx_bound_pairs(gx_handle* h, double k_bind, uint32_t* pairs, size_t cap, size_t* npairs);
 
+/* Per-tick column sync of a drop-in system whose ECS lives on the host:
+ * overwrite Position, Velocity and Acceleration (slot order, AoS f64) of the
+ * resident atoms without touching the static columns (AtomType, Mass,
+ * Charge, EntityId).  Any pointer may be NULL (column unchanged). */
+int gx_set_dynamic(gx_handle* h, const double* pos, const double* vel, const double* acc);
+
 /* ---- timing ---------------------------------------------------------- */
 
 /* Waits for the handle's stream. */
 int gx_synchronize(gx_handle* h);
+/* Records CUDA event `slot` (0..15) on the handle's stream. */
+int gx_timer_mark(gx_handle* h, int slot);
+/* Milliseconds between two recorded events (waits for the second). */
+int gx_timer_elapsed(gx_handle* h, int from_slot, int to_slot, double* ms);
+/* Number of kernels this handle has launched since creation. */
+uint64_t gx_launch_count(const gx_handle* h);
+/* Diagnostic: measured FP32 FMA throughput of this GPU in TFLOP/s (a
+ * dependent-FMA loop on every SM; roofline denominator for the pair pass). */
+int gx_measure_fp32_peak(int device, double* tflops);
 /* Per-kernel CUDA-event timing of gx_step/gx_forces launches (on the
  * handle's stream).  When enabled, each launch is bracketed by events. */
 int gx_profile_enable(gx_handle* h, int on);
