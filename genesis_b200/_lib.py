@@ -99,6 +99,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
         "gx_timer_elapsed": (C.c_int, [vp, C.c_int, C.c_int, dp]),
         "gx_launch_count": (C.c_uint64, [vp]),
         "gx_measure_fp32_peak": (C.c_int, [C.c_int, dp]),
+        "gx_radial_distribution_noalloc": (C.c_int, [sz, dp, dp, _D, sz, u64p, dp, dp, dp]),
     }
     for name, (res, args) in proto.items():
         f = getattr(lib, name)
@@ -344,3 +345,22 @@ def measure_fp32_peak(device: int = 0) -> float:
     if rc != 0:
         raise GxError(rc, "gx_measure_fp32_peak failed")
     return t.value
+
+
+def radial_distribution_noalloc(pos, box, r_max: float, nbins: int):
+    """gx_radial_distribution_noalloc: g(r) of host positions on the current
+    device without any device allocation (fixed scratch, 8192-atom sample,
+    at most 65536 grid cells).  Returns (counts, bins, r_max, dr)."""
+    lib = load()
+    pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+    b = np.ascontiguousarray(box, dtype=np.float64)
+    nb = min(max(nbins, 1), 1 << 16)
+    counts = np.empty(nb, dtype=np.uint64)
+    bins = np.empty(nb, dtype=np.float64)
+    rmo, dro = C.c_double(), C.c_double()
+    rc = lib.gx_radial_distribution_noalloc(len(pos), _ptr(pos, C.c_double), _ptr(b, C.c_double), r_max, nbins,
+                                            _ptr(counts, C.c_uint64), _ptr(bins, C.c_double), C.byref(rmo),
+                                            C.byref(dro))
+    if rc != 0:
+        raise GxError(rc, "gx_radial_distribution_noalloc: " + lib.gx_status_string(rc).decode())
+    return counts, bins, rmo.value, dro.value

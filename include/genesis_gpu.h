@@ -164,6 +164,22 @@ int gx_radial_distribution(gx_handle* h, double r_max, size_t nbins, size_t samp
 int gx_radial_distribution_between(gx_handle* h, uint8_t ta, uint8_t tb, double r_max,
                                    size_t nbins, size_t sample_cap, uint64_t* counts,
                                    double* bins, double* r_max_out, double* dr_out);
+/* No counterpart in the reference.  g(r) for callers that cannot allocate
+ * device memory: code held to a fixed device-memory budget, or code that must
+ * not call cudaMalloc/cudaFree because those can synchronise the whole
+ * device.  Same result as gx_radial_distribution with sample_cap = 8192, but
+ * computed from host positions (pos: n x 3 f64, slot order) on the current
+ * CUDA device, with every intermediate in one fixed file-scope device array
+ * (about 1.9 MB per GPU that loads the library, held until exit); the call
+ * allocates nothing.  Limits: the g(r) grid, floor(L/r_max) cells per axis,
+ * may hold at most 65536 cells (GX_ERR_CAPACITY otherwise); nbins is clamped
+ * to [1, 65536] like the reference; the sample never exceeds 8192 atoms.
+ * The first call on a device looks up the array's address and should come
+ * before any stream capture.  Calls share the array: calls that overlap on
+ * the GPU race. */
+int gx_radial_distribution_noalloc(size_t n, const double* pos, const double box[3], double r_max,
+                                   size_t nbins, uint64_t* counts, double* bins, double* r_max_out,
+                                   double* dr_out);
 /* clusters (src/analysis/mod.rs:221-284): friends-of-friends with
  * r < bond_factor * sigma_ij.  labels[slot] = smallest slot of its
  * component; stats = {monomers, aggregates, largest, bound_pairs}. */
