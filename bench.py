@@ -63,15 +63,19 @@ class Dist:
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.backend = os.environ.get("GENESIS_DIST_BACKEND", "nccl")
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
 
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                    device_id=torch.device("cuda", self.local))
+            if self.backend == "nccl":
+                torch.cuda.set_device(self.local)
+                dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                        device_id=torch.device("cuda", self.local))
+            else:
+                dist.init_process_group(self.backend, timeout=datetime.timedelta(seconds=60))
             self.pg = dist
 
     def barrier(self):
@@ -83,7 +87,8 @@ class Dist:
             return x
         import torch
 
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{self.local}")
+        dev = f"cuda:{self.local}" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 

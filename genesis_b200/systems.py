@@ -1,0 +1,444 @@
+"""Host-side mirror of the reference's plugin interface, driving the GPU path.
+
+The reference composes a tick from systems: ``trait System { name, access,
+run(&mut SystemContext) }`` (src/scheduler/system.rs:86-97), registered in
+order by ``build_schedule`` (src/universe/mod.rs:355-392) and run
+sequentially by ``Scheduler::run`` (src/scheduler/mod.rs:83-89).  This
+module restates that interface in Python over the C ABI: the same system
+names, the same Access declarations and the same order.  The ECS columns
+live in a :class:`World` on the host; the GPU systems share one
+:class:`GpuWorld` (one device handle) and sync columns lazily, so a tick of
+GPU systems never crosses PCIe unless a host system touches the columns.
+
+Host-only logic that is part of the path stays here: the pair tracker and the
+persistence threshold of the bond observation (src/analysis/pairs.rs:43-109,
+src/systems/bonds.rs:73-185).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import elements as E
+from ._lib import Handle
+
+
+# ---------------------------------------------------------------- scheduler
+
+
+@dataclass
+class Access:
+    """Declared reads/writes (src/scheduler/system.rs:16-69)."""
+
+    reads: list = field(default_factory=list)
+    writes: list = field(default_factory=list)
+    resources_read: list = field(default_factory=list)
+    resources_write: list = field(default_factory=list)
+
+    def conflicts_with(self, o: "Access") -> bool:  # system.rs:47-69
+        comp = any(c in o.reads or c in o.writes for c in self.writes) or \
+            any(c in self.reads or c in self.writes for c in o.writes)
+        res = any(c in o.resources_read or c in o.resources_write for c in self.resources_write) or \
+            any(c in self.resources_read or c in self.resources_write for c in o.resources_write)
+        return comp or res
+
+
+@dataclass
+class Time:
+    dt: float
+    t: float = 0.0
+    tick: int = 0
+
+    def advance(self):  # src/universe/time.rs:25-28
+        self.t += self.dt
+        self.tick += 1
+
+
+@dataclass
+class World:
+    """ECS columns in slot order (Position, Velocity, Acceleration, AtomType,
+    Mass, Charge, EntityId::index, Bonds)."""
+
+    pos: np.ndarray
+    vel: np.ndarray
+    acc: np.ndarray
+    elem: np.ndarray
+    mass: np.ndarray
+    charge: np.ndarray
+    entity: np.ndarray
+    bonds: dict = field(default_factory=dict)  # entity -> list of bonded entities
+
+    @classmethod
+    def from_universe(cls, u) -> "World":
+        return cls(pos=u.pos.copy(), vel=u.vel.copy(), acc=np.zeros_like(u.pos), elem=u.elem.copy(),
+                   mass=u.mass.copy(), charge=u.charge.copy(), entity=u.entity.copy())
+
+    def __len__(self):
+        return len(self.elem)
+
+
+@dataclass
+class SystemContext:
+    world: World
+    resources: dict
+    time: Time
+    dt: float
+
+
+class System:
+    def name(self) -> str:
+        raise NotImplementedError
+
+    def access(self) -> Access:
+        return Access()
+
+    def run(self, ctx: SystemContext) -> None:
+        raise NotImplementedError
+
+
+class Scheduler:
+    """Sequential run in registration order (src/scheduler/mod.rs:59-89)."""
+
+    def __init__(self):
+        self.systems: list[System] = []
+
+    def add_system(self, s: System):
+        self.systems.append(s)
+
+    def run(self, ctx: SystemContext):
+        for s in self.systems:
+            s.run(ctx)
+
+    def names(self) -> list[str]:
+        return [s.name() for s in self.systems]
+
+
+# ---------------------------------------------------------------- device world
+
+
+class GpuWorld:
+    """One device handle shared by every GPU system, with lazy column sync.
+
+    ``host_dirty``: a host system wrote the columns, upload before the next
+    GPU system.  ``device_dirty``: the device copy is newer, download before a
+    host system reads.
+    """
+
+    def __init__(self, cfg, world: World, precision: str = "mixed", device: int = 0):
+        self.h = Handle(cfg, precision, device)
+        self.world = world
+        self.h.set_state(world.pos, world.vel, world.elem, acc=world.acc, charge=world.charge, mass=world.mass,
+                         entity=world.entity)
+        self.host_dirty = False
+        self.device_dirty = False
+        self.slot_of_entity = {int(e): i for i, e in enumerate(world.entity)}
+
+    def to_device(self):
+        if self.host_dirty:
+            self.h.set_dynamic(self.world.pos, self.world.vel, self.world.acc)
+            self.host_dirty = False
+
+    def to_host(self):
+        if self.device_dirty:
+            self.world.pos, self.world.vel, self.world.acc = self.h.get_state()
+            self.device_dirty = False
+
+    def set_bonds_from_world(self):
+        """Bonds component -> slot pairs, once per bond (systems/forces.rs:208-226):
+        from entity e's list, only neighbours with a larger index are taken."""
+        pairs = []
+        for e, lst in self.world.bonds.items():
+            si = self.slot_of_entity.get(int(e))
+            if si is None:
+                continue
+            for nb in lst:
+                if int(e) >= int(nb):
+                    continue
+                sj = self.slot_of_entity.get(int(nb))
+                if sj is not None:
+                    pairs.append((si, sj))
+        self.h.set_bonds(np.asarray(pairs, dtype=np.uint32).reshape(-1, 2))
+
+
+class _GpuSystem(System):
+    def __init__(self, gpu: GpuWorld):
+        self.gpu = gpu
+
+    def _enter(self):
+        self.gpu.to_device()
+
+    def _leave(self):
+        self.gpu.device_dirty = True
+
+
+class GpuVelocityHalfKick(_GpuSystem):
+    """VelocityHalfKick (src/systems/integrate.rs:25-45)."""
+
+    def name(self):
+        return "velocity_half_kick"
+
+    def access(self):
+        return Access(reads=["Acceleration"], writes=["Velocity"])
+
+    def run(self, ctx):
+        self._enter()
+        self.gpu.h.half_kick()
+        self._leave()
+
+
+class GpuPositionDrift(_GpuSystem):
+    """PositionDrift (src/systems/integrate.rs:48-68)."""
+
+    def name(self):
+        return "position_drift"
+
+    def access(self):
+        return Access(reads=["Velocity"], writes=["Position"])
+
+    def run(self, ctx):
+        self._enter()
+        self.gpu.h.drift()
+        self._leave()
+
+
+class GpuBoundary(_GpuSystem):
+    """BoundarySystem (src/systems/boundary.rs:22-35)."""
+
+    def name(self):
+        return "boundary"
+
+    def access(self):
+        return Access(writes=["Position"], resources_read=["Config"])
+
+    def run(self, ctx):
+        self._enter()
+        self.gpu.h.wrap()
+        self._leave()
+
+
+class GpuForceSystem(_GpuSystem):
+    """ForceSystem (src/systems/forces.rs:145-353)."""
+
+    def __init__(self, gpu: GpuWorld, bonds_on: bool):
+        super().__init__(gpu)
+        self.bonds_on = bonds_on
+
+    def name(self):
+        return "forces"
+
+    def access(self):
+        return Access(reads=["Position", "Mass", "AtomType", "Charge", "Bonds"], writes=["Acceleration"],
+                      resources_read=["Config"], resources_write=["PotentialEnergy", "BondEnergy"])
+
+    def run(self, ctx):
+        self._enter()
+        if self.bonds_on:
+            self.gpu.set_bonds_from_world()
+        V, Vb, _ = self.gpu.h.forces()
+        ctx.resources["PotentialEnergy"] = V
+        ctx.resources["BondEnergy"] = Vb
+        self._leave()
+
+
+class GpuThermostat(_GpuSystem):
+    """ThermostatSystem (src/systems/thermostat.rs:19-71)."""
+
+    def name(self):
+        return "thermostat"
+
+    def access(self):
+        return Access(reads=["Mass"], writes=["Velocity"])
+
+    def run(self, ctx):
+        self._enter()
+        self.gpu.h.thermostat()
+        self._leave()
+
+
+class GpuStructure(_GpuSystem):
+    """StructureSystem (src/systems/structure.rs:44-84): FoF every interval ticks."""
+
+    def __init__(self, gpu: GpuWorld, interval: int):
+        super().__init__(gpu)
+        self.interval = max(int(interval), 1)
+
+    def name(self):
+        return "structure"
+
+    def access(self):
+        return Access(reads=["Position", "AtomType"], resources_read=["Config"],
+                      resources_write=["StructureStats"])
+
+    def run(self, ctx):
+        if ctx.time.tick % self.interval != 0:
+            return
+        self._enter()
+        _, st = self.gpu.h.clusters(E.BOND_FACTOR)
+        st["tick"] = ctx.time.tick
+        ctx.resources["StructureStats"] = st
+
+
+class PairTracker:
+    """Episode tracking with debounce (src/analysis/pairs.rs:43-109).
+    Pairs are (a, b) entity tuples with a < b."""
+
+    def __init__(self, debounce: int):
+        self.debounce = max(int(debounce), 1)
+        self.open: dict = {}
+        self.missing: dict = {}
+        self.completed: list = []
+
+    def track_tick(self, bound):
+        current = set(bound)
+        for p in current:
+            self.missing.pop(p, None)
+            self.open[p] = self.open.get(p, 0) + 1
+        for p in [p for p in self.open if p not in current]:
+            self.missing[p] = self.missing.get(p, 0) + 1
+            if self.missing[p] >= self.debounce:
+                ticks = self.open.pop(p)
+                del self.missing[p]
+                self.completed.append((p, ticks))
+
+    def close_all(self):
+        for p, t in self.open.items():
+            self.completed.append((p, t))
+        self.open.clear()
+        self.missing.clear()
+
+    def open_count(self) -> int:
+        return len(self.open)
+
+
+def well_curvature(eps: float, sigma: float) -> float:  # physics/forces.rs:194-196
+    return 72.0 * 2.0 ** (-1.0 / 3.0) * eps / (sigma * sigma)
+
+
+def vib_period(eps: float, sigma: float, mu: float) -> float:  # physics/forces.rs:201-203
+    return 2.0 * math.pi * math.sqrt(mu / well_curvature(eps, sigma))
+
+
+def persistence_ticks(cfg, ea: int, eb: int) -> int:
+    """ceil(min_periods * vib_period / dt) for a species pair (src/systems/bonds.rs:94-99)."""
+    ma, mb = E.MASS[ea], E.MASS[eb]
+    mu = ma * mb / (ma + mb)
+    eps = cfg.thermal_constant * math.sqrt(cfg.epsilon_k[ea] * cfg.epsilon_k[eb])
+    sig = 0.5 * (cfg.sigma[ea] + cfg.sigma[eb])
+    return math.ceil(max(cfg.bond_min_periods, 0.1) * vib_period(eps, sig, mu) / cfg.dt)
+
+
+class GpuBondObservation(_GpuSystem):
+    """BondObservationSystem (src/systems/bonds.rs:58-185): bound pairs on the
+    device (gx_bound_pairs), episodes and persistence on the host, the result
+    written to the Bonds column that the next force pass reads."""
+
+    def __init__(self, gpu: GpuWorld, cfg):
+        super().__init__(gpu)
+        self.cfg = cfg
+        self.tracker = PairTracker(E.DEBOUNCE)
+        self.active_since: dict = {}
+        self.elem_of_entity = {int(e): int(t) for e, t in zip(gpu.world.entity, gpu.world.elem)}
+
+    def name(self):
+        return "bond-observation"
+
+    def access(self):
+        return Access(reads=["Position", "AtomType"], writes=["Bonds"], resources_read=["Config"],
+                      resources_write=["BondObservation"])
+
+    def run(self, ctx):
+        self._enter()
+        bp = self.gpu.h.bound_pairs(self.cfg.bond_k_bind)
+        self.tracker.track_tick([(int(a), int(b)) for a, b in bp])
+        persistent: dict = {}
+        for (a, b), ticks in self.tracker.open.items():
+            if ticks < persistence_ticks(self.cfg, self.elem_of_entity[a], self.elem_of_entity[b]):
+                continue
+            persistent.setdefault(a, []).append(b)
+            persistent.setdefault(b, []).append(a)
+        ctx.world.bonds = persistent
+        current = {(min(a, b), max(a, b)) for a, lst in persistent.items() for b in lst}
+        bo = ctx.resources.setdefault("BondObservation", {"bonds_formed": 0, "lifetime_sum_ticks": 0.0})
+        now = ctx.time.tick
+        for p in [p for p in self.active_since if p not in current]:
+            bo["bonds_formed"] += 1
+            bo["lifetime_sum_ticks"] += now - self.active_since.pop(p)
+        for p in current:
+            self.active_since.setdefault(p, now)
+        matrix = np.zeros((E.COUNT, E.COUNT), dtype=np.uint64)
+        for a, b in current:
+            ia, ib = self.elem_of_entity[a], self.elem_of_entity[b]
+            matrix[ia, ib] += 1
+            matrix[ib, ia] += 1
+        bo.update(tick=now, bonded_pairs=len(current), bonded_entities=len(persistent), species_matrix=matrix)
+
+
+class GpuStats(_GpuSystem):
+    """StatsSystem (src/systems/aggregate.rs:36-144): K, T, E = K + V + E_bond."""
+
+    def __init__(self, gpu: GpuWorld, cfg):
+        super().__init__(gpu)
+        self.cfg = cfg
+
+    def name(self):
+        return "stats"
+
+    def access(self):
+        return Access(reads=["Velocity", "Mass"], resources_read=["Config", "PotentialEnergy", "BondEnergy"])
+
+    def run(self, ctx):
+        self._enter()
+        K, speed = self.gpu.h.stats()
+        n = len(ctx.world)
+        V = ctx.resources.get("PotentialEnergy", 0.0)
+        Vb = ctx.resources.get("BondEnergy", 0.0)
+        e_avg = K / n if n else 0.0
+        T = (2.0 / 3.0) * e_avg / self.cfg.thermal_constant if self.cfg.thermal_constant > 0 else 0.0
+        ctx.resources["StatsSnapshot"] = {"tick": ctx.time.tick, "energy_total": K + V + Vb, "kinetic": K,
+                                          "energy_potential": V, "bond_energy": Vb, "temperature_avg": T,
+                                          "mean_speed": speed / n if n else 0.0}
+
+
+def build_schedule(cfg, gpu: GpuWorld) -> Scheduler:
+    """The force schedule of build_schedule (src/universe/mod.rs:355-392)."""
+    s = Scheduler()
+    s.add_system(GpuVelocityHalfKick(gpu))
+    s.add_system(GpuPositionDrift(gpu))
+    if cfg.enable_boundaries:
+        s.add_system(GpuBoundary(gpu))
+    s.add_system(GpuForceSystem(gpu, cfg.enable_bond_interaction))
+    s.add_system(GpuVelocityHalfKick(gpu))
+    if cfg.enable_thermostat:
+        s.add_system(GpuThermostat(gpu))
+    if cfg.enable_bond_observation:
+        s.add_system(GpuBondObservation(gpu, cfg))
+    s.add_system(GpuStructure(gpu, cfg.structure_interval))
+    s.add_system(GpuStats(gpu, cfg))
+    return s
+
+
+class GpuUniverse:
+    """Universe::tick over the GPU schedule (src/universe/mod.rs:141-159)."""
+
+    def __init__(self, cfg, u, precision: str = "mixed", device: int = 0):
+        self.cfg = cfg
+        self.world = World.from_universe(u)
+        self.gpu = GpuWorld(cfg, self.world, precision, device)
+        self.time = Time(cfg.dt)
+        self.resources: dict = {"Config": cfg}
+        self.scheduler = build_schedule(cfg, self.gpu)
+
+    def tick(self):
+        self.time.advance()
+        ctx = SystemContext(self.world, self.resources, self.time, self.time.dt)
+        self.scheduler.run(ctx)
+
+    def run_ticks(self, n: int):
+        for _ in range(n):
+            self.tick()
+
+    def sync(self) -> World:
+        self.gpu.to_host()
+        return self.world
