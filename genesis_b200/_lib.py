@@ -100,6 +100,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
         "gx_launch_count": (C.c_uint64, [vp]),
         "gx_measure_fp32_peak": (C.c_int, [C.c_int, dp]),
         "gx_radial_distribution_noalloc": (C.c_int, [sz, dp, dp, _D, sz, u64p, dp, dp, dp]),
+        "gx_set_kernel_variant": (C.c_int, [vp, C.c_int]),
     }
     for name, (res, args) in proto.items():
         f = getattr(lib, name)
@@ -217,6 +218,10 @@ class Handle:
 
     def set_precision(self, precision):
         self._check(self.lib.gx_set_precision(self.h, _PRECISION.get(precision, precision)))
+
+    def set_kernel_variant(self, variant: int):
+        """Mixed pair pass: 0 automatic, 1 thread per atom, 2 tiled."""
+        self._check(self.lib.gx_set_kernel_variant(self.h, variant))
 
     # -- systems ------------------------------------------------------------
     def half_kick(self):

@@ -290,7 +290,9 @@ int upload_pairf(gx_handle* h) {
             t.inv_half_sigma = (float)(2.0 / sg);
             t.eps4 = (float)(4.0 * ep);
             t.eps24 = (float)(24.0 * ep);
-            t.qq = (float)(h->p.coulomb_constant * h->kind_charge[a] * h->kind_charge[b]);
+            // symmetric by construction: (i, j) and (j, i) must round identically
+            int lo = a < b ? a : b, hi = a < b ? b : a;
+            t.qq = (float)(h->p.coulomb_constant * h->kind_charge[lo] * h->kind_charge[hi]);
         }
     GX_CUDA(h, cudaMemcpy(h->d_pairf, tab, sizeof tab, cudaMemcpyHostToDevice));
     return GX_OK;
@@ -693,7 +695,14 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
         cudaMemset(h->derr, 0, sizeof(uint32_t));
         if (e & kErrNonFinite) return set_err(h, GX_ERR_NONFINITE, "non-finite force in the pair pass");
         if (e & kErrSaturation) return set_err(h, GX_ERR_SATURATION, "fixed-point force saturated");
+        if (e & kErrTimeout) return set_err(h, GX_ERR_TIMEOUT, "shared-memory staging wait timed out");
     }
+    return GX_OK;
+}
+
+int gx_set_kernel_variant(gx_handle* h, int variant) {
+    if (!h || variant < 0 || variant > 4) return GX_ERR_ARG;
+    h->kernel_variant = variant;
     return GX_OK;
 }
 

@@ -14,7 +14,7 @@
 //    and sums are integer atomics, so the result does not depend on launch
 //    configuration or scheduling.  Each pair is evaluated once (canonical
 //    half shell) and contributes +F / -F to its two ends.
-#include "gx_internal.cuh"
+#include "gx_pair_f32.cuh"
 
 namespace gx {
 
@@ -26,11 +26,6 @@ struct LawF64 {
     double k_e, G;
     double box[3];
     int coul, grav;
-};
-
-struct LawF32 {
-    float rc2, lj_rc, lj_ron, inv_lj_w, coul_rc, coul_ron, inv_coul_w;
-    int coul, nkinds;
 };
 
 // smooth_cutoff, src/physics/forces.rs:302-318 (exact FP64).
@@ -189,16 +184,6 @@ __global__ void __launch_bounds__(kForceThreads) k_force_f64(GridGeom g, StateBu
     }
 }
 
-// Quantise one FP32 value to 2^-32 fixed point, flagging saturation.
-__device__ __forceinline__ long long quant(float v, uint32_t* err) {
-    float s = v * kFixScaleF;
-    if (!(fabsf(s) < 9.0e18f)) {
-        atomicOr(err, isfinite(v) ? kErrSaturation : kErrNonFinite);
-        return 0;
-    }
-    return __float2ll_rn(s);
-}
-
 // Mixed pass: one thread per atom, canonical half shell, FP32 pair math,
 // fixed-point +F/-F via integer atomics.
 __global__ void __launch_bounds__(kForceThreads) k_force_mixed(GridGeom g, const float4* __restrict__ pos4,
@@ -239,64 +224,20 @@ __global__ void __launch_bounds__(kForceThreads) k_force_mixed(GridGeom g, const
                 sz = -(float)oz * g.cellf[2];
             }
             hi = start[B + 1];
-            float bx = pi.x + sx, by = pi.y + sy, bz = pi.z + sz;
             for (uint32_t j = lo; j < hi; ++j) {
                 float4 pj = pos4[j];
-                float dx = bx - pj.x, dy = by - pj.y, dz = bz - pj.z;
+                float dx = delta1(pi.x, pj.x, sx), dy = delta1(pi.y, pj.y, sy), dz = delta1(pi.z, pj.z, sz);
                 if (g.minimg_mask) {
-                    if (g.minimg_mask & 1) dx -= g.Lf[0] * rintf(dx * g.invLf[0]);
-                    if (g.minimg_mask & 2) dy -= g.Lf[1] * rintf(dy * g.invLf[1]);
-                    if (g.minimg_mask & 4) dz -= g.Lf[2] * rintf(dz * g.invLf[2]);
+                    if (g.minimg_mask & 1) dx = fsub(dx, fmul(g.Lf[0], rintf(fmul(dx, g.invLf[0]))));
+                    if (g.minimg_mask & 2) dy = fsub(dy, fmul(g.Lf[1], rintf(fmul(dy, g.invLf[1]))));
+                    if (g.minimg_mask & 4) dz = fsub(dz, fmul(g.Lf[2], rintf(fmul(dz, g.invLf[2]))));
                 }
-                float d2 = dx * dx + dy * dy + dz * dz;
+                float d2 = dist2(dx, dy, dz);
                 if (!(d2 < L.rc2) || d2 == 0.f) continue;
                 ++np;
-                const PairF t = st[ki * L.nkinds + __float_as_int(pj.w)];
-                float inv_d = rsqrtf(d2);
-                float d = d2 * inv_d;
-                float f = 0.f, v = 0.f;
-                if (d < L.lj_rc) {
-                    bool core = d < t.half_sigma;
-                    float r = core ? t.half_sigma : d;
-                    float inv_r = core ? t.inv_half_sigma : inv_d;
-                    float s = t.sigma * inv_r;
-                    float s2 = s * s;
-                    float s6 = s2 * s2 * s2;
-                    float s12 = s6 * s6;
-                    float vl = t.eps4 * (s12 - s6);
-                    float ml = t.eps24 * inv_r * (2.f * s12 - s6);
-                    float u = (r - L.lj_ron) * L.inv_lj_w;
-                    if (u <= 0.f) {
-                        f = ml;
-                        v = vl;
-                    } else if (u < 1.f) {
-                        float u2 = u * u;
-                        float sw = 1.f + u2 * u * (-10.f + u * (15.f - 6.f * u));
-                        float omu = 1.f - u;
-                        float dsw = -30.f * u2 * omu * omu * L.inv_lj_w;
-                        f = ml * sw - vl * dsw;
-                        v = vl * sw;
-                    }
-                }
-                if (L.coul && d < L.coul_rc) {
-                    float inv_r = d < 0.5f ? 2.f : inv_d;
-                    float vc = t.qq * inv_r;
-                    float mc = vc * inv_r;
-                    float u = (d - L.coul_ron) * L.inv_coul_w;
-                    if (u <= 0.f) {
-                        f += mc;
-                        v += vc;
-                    } else if (u < 1.f) {
-                        float u2 = u * u;
-                        float sw = 1.f + u2 * u * (-10.f + u * (15.f - 6.f * u));
-                        float omu = 1.f - u;
-                        float dsw = -30.f * u2 * omu * omu * L.inv_coul_w;
-                        f += mc * sw - vc * dsw;
-                        v += vc * sw;
-                    }
-                }
-                float fs = f * inv_d;
-                long long qx = quant(dx * fs, err), qy = quant(dy * fs, err), qz = quant(dz * fs, err);
+                float fs, v;
+                pair_f32(L, st[ki * L.nkinds + __float_as_int(pj.w)], d2, fs, v);
+                long long qx = quant(fmul(dx, fs), err), qy = quant(fmul(dy, fs), err), qz = quant(fmul(dz, fs), err);
                 fx += qx;
                 fy += qy;
                 fz += qz;
@@ -454,22 +395,24 @@ int force_pass(gx_handle* h, bool finalize_acc, double* V, double* Vb, uint64_t*
                                                                 vpart, h->dcount + 0);
         prof_end(h, "force_f64");
     } else {
-        LawF32 L;
-        L.rc2 = (float)(h->fs.rc * h->fs.rc);
-        L.lj_rc = (float)h->fs.lj_rc;
-        L.lj_ron = (float)h->fs.lj_ron;
-        L.inv_lj_w = (float)(1.0 / (h->fs.lj_rc - h->fs.lj_ron));
-        L.coul = h->p.enable_electrostatics ? 1 : 0;
-        L.coul_rc = (float)h->fs.coul_rc;
-        L.coul_ron = (float)h->fs.coul_ron;
-        L.inv_coul_w = L.coul ? (float)(1.0 / (h->fs.coul_rc - h->fs.coul_ron)) : 0.f;
-        L.nkinds = h->nkinds;
+        LawF32 L = make_law32(h);
         if (h->p.enable_gravity) return set_err(h, GX_ERR_UNSUPPORTED, "gravity is only implemented in the FP64 path");
         GX_CUDA(h, cudaMemsetAsync(h->F, 0, 3 * h->cap * sizeof(long long), h->stream));
+        // staged kernels pack atom indices in 27 bits and need >= 3 cells per axis
+        const int var = h->kernel_variant;
+        bool small_ids = n < (1u << 27);
+        bool tiled = g.n[0] >= 3 && g.n[1] >= 3 && g.n[2] >= 3 && (var == 2 || var == 3) && small_ids;
+        bool lists = (var == 0 || var == 4) && small_ids;
         prof_begin(h, "force_mixed");
-        if (n) GX_LAUNCH(h, k_force_mixed, fb, kForceThreads, g, h->pos4, h->key_sorted, h->cl.start, n, L,
-                                                                  h->d_pairf, h->F, h->cap, h->dcount + 1,
-                                                                  h->dcount + 0, h->derr);
+        if (n && lists)
+            launch_force_mixed_lists(h, g, h->pos4, h->key_sorted, h->cl.start, n, L, h->d_pairf, h->F, h->cap,
+                                     h->dcount + 1, h->dcount + 0, h->derr);
+        else if (n && tiled)
+            launch_force_mixed_tiled(h, g, h->pos4, h->cl.start, L, h->d_pairf, h->F, h->cap, h->dcount + 1,
+                                     h->dcount + 0, h->derr);
+        else if (n)
+            GX_LAUNCH(h, k_force_mixed, fb, kForceThreads, g, h->pos4, h->key_sorted, h->cl.start, n, L, h->d_pairf,
+                      h->F, h->cap, h->dcount + 1, h->dcount + 0, h->derr);
         prof_end(h, "force_mixed");
     }
     bool bonds_on = h->p.enable_bond_interaction && h->nbonds > 0;
@@ -505,9 +448,24 @@ int force_pass(gx_handle* h, bool finalize_acc, double* V, double* Vb, uint64_t*
             GX_CUDA(h, cudaMemsetAsync(h->derr, 0, sizeof(uint32_t), h->stream));
             if (e & kErrNonFinite) return set_err(h, GX_ERR_NONFINITE, "non-finite force in the pair pass");
             if (e & kErrSaturation) return set_err(h, GX_ERR_SATURATION, "fixed-point force saturated");
+            if (e & kErrTimeout) return set_err(h, GX_ERR_TIMEOUT, "shared-memory staging wait timed out");
         }
     }
     return GX_OK;
+}
+
+LawF32 make_law32(const gx_handle* h) {
+    LawF32 L;
+    L.rc2 = (float)(h->fs.rc * h->fs.rc);
+    L.lj_rc = (float)h->fs.lj_rc;
+    L.lj_ron = (float)h->fs.lj_ron;
+    L.inv_lj_w = (float)(1.0 / (h->fs.lj_rc - h->fs.lj_ron));
+    L.coul = h->p.enable_electrostatics ? 1 : 0;
+    L.coul_rc = (float)h->fs.coul_rc;
+    L.coul_ron = (float)h->fs.coul_ron;
+    L.inv_coul_w = L.coul ? (float)(1.0 / (h->fs.coul_rc - h->fs.coul_ron)) : 0.f;
+    L.nkinds = h->nkinds;
+    return L;
 }
 
 int upload_pair_table_f64(gx_handle* h) {

@@ -24,6 +24,7 @@ enum : uint32_t {
     kErrNonFinite = 2u,
     kErrCapacity = 4u,
     kErrBinRange = 8u,
+    kErrTimeout = 16u,
 };
 
 // ---------------------------------------------------------------------------
@@ -213,6 +214,9 @@ struct gx_handle {
     // stream-ordered timers and the launch counter
     cudaEvent_t timers[16] = {};
     uint64_t launches = 0;
+
+    // mixed pair-pass variant: 0 = automatic, 1 = thread per atom, 2 = tiled
+    int kernel_variant = 0;
 };
 
 // Every kernel launch of the library goes through this macro so the

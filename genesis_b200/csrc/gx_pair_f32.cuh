@@ -1,0 +1,114 @@
+// gx_pair_f32.cuh -- the mixed path's FP32 pair law, shared by its kernels.
+//
+// One in-cutoff pair: Lennard-Jones with the hardened core r = max(d, σ/2)
+// and the quintic switch on [r_on, r_c] (force_switched_scalar, lj_raw,
+// smooth_cutoff, switched: src/physics/forces.rs:270-353), plus Coulomb with
+// the absolute core max(d, 0.5) and its own switch on d
+// (src/systems/forces.rs:282-289).  Returns the force magnitude divided by d
+// (so F_vec = delta * fs) and the switched potential.
+//
+// Every operation is an explicit round-to-nearest intrinsic or fmaf, so the
+// compiler has no contraction choices left: all pair kernels produce the same
+// bits for the same pair, which keeps the fixed-point sums identical across
+// kernel variants and launch shapes.
+#pragma once
+
+#include "gx_internal.cuh"
+
+namespace gx {
+
+struct LawF32 {
+    float rc2, lj_rc, lj_ron, inv_lj_w, coul_rc, coul_ron, inv_coul_w;
+    int coul, nkinds;
+};
+
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+
+// (pi - pj) + shift: exactly antisymmetric under swapping the pair's ends.
+__device__ __forceinline__ float delta1(float a, float b, float s) { return fadd(fsub(a, b), s); }
+__device__ __forceinline__ float dist2(float dx, float dy, float dz) {
+    return fmaf(dz, dz, fmaf(dy, dy, fmul(dx, dx)));
+}
+
+// quintic switch 1 - 10u^3 + 15u^4 - 6u^5 and its derivative (per unit u)
+__device__ __forceinline__ void switch5(float u, float& sw, float& dsw_du) {
+    float u2 = fmul(u, u);
+    float p = fmaf(-6.f, u, 15.f);       // 15 - 6u
+    p = fmaf(p, u, -10.f);               // -10 + u(15 - 6u)
+    sw = fmaf(fmul(u2, u), p, 1.f);
+    float omu = fsub(1.f, u);
+    dsw_du = fmul(fmul(fmul(-30.f, u2), omu), omu);
+}
+
+__device__ __forceinline__ void pair_f32(const LawF32& L, const PairF& t, float d2, float& fs, float& v) {
+    float inv_d = rsqrtf(d2);
+    float d = fmul(d2, inv_d);
+    float f = 0.f;
+    v = 0.f;
+    if (d < L.lj_rc) {
+        bool core = d < t.half_sigma;
+        float r = core ? t.half_sigma : d;
+        float inv_r = core ? t.inv_half_sigma : inv_d;
+        float s = fmul(t.sigma, inv_r);
+        float s2 = fmul(s, s);
+        float s6 = fmul(fmul(s2, s2), s2);
+        float s12 = fmul(s6, s6);
+        float vl = fmul(t.eps4, fsub(s12, s6));
+        float ml = fmul(fmul(t.eps24, inv_r), fmaf(2.f, s12, -s6));
+        float u = fmul(fsub(r, L.lj_ron), L.inv_lj_w);
+        if (u <= 0.f) {
+            f = ml;
+            v = vl;
+        } else if (u < 1.f) {
+            float sw, dsdu;
+            switch5(u, sw, dsdu);
+            float dsw = fmul(dsdu, L.inv_lj_w);
+            f = fmaf(ml, sw, -fmul(vl, dsw));
+            v = fmul(vl, sw);
+        }
+    }
+    if (L.coul && d < L.coul_rc) {
+        float inv_r = d < 0.5f ? 2.f : inv_d;
+        float vc = fmul(t.qq, inv_r);
+        float mc = fmul(vc, inv_r);
+        float u = fmul(fsub(d, L.coul_ron), L.inv_coul_w);
+        if (u <= 0.f) {
+            f = fadd(f, mc);
+            v = fadd(v, vc);
+        } else if (u < 1.f) {
+            float sw, dsdu;
+            switch5(u, sw, dsdu);
+            float dsw = fmul(dsdu, L.inv_coul_w);
+            f = fadd(f, fmaf(mc, sw, -fmul(vc, dsw)));
+            v = fadd(v, fmul(vc, sw));
+        }
+    }
+    fs = fmul(f, inv_d);
+}
+
+// One FP32 value to 2^-32 fixed point; flags saturation / non-finite.
+__device__ __forceinline__ long long quant(float v, uint32_t* err) {
+    float s = fmul(v, kFixScaleF);
+    if (!(fabsf(s) < 9.0e18f)) {
+        atomicOr(err, isfinite(v) ? kErrSaturation : kErrNonFinite);
+        return 0;
+    }
+    return __float2ll_rn(s);
+}
+
+LawF32 make_law32(const gx_handle* h);
+
+// Thread-per-atom pair pass with per-thread candidate lists (gx_force_tiled.cu);
+// any grid, atom indices below 2^27.
+void launch_force_mixed_lists(gx_handle* h, const GridGeom& g, const float4* pos4, const uint32_t* key,
+                              const uint32_t* start, uint32_t n, const LawF32& L, const PairF* tab, long long* F,
+                              size_t fstride, unsigned long long* vacc, unsigned long long* npairs, uint32_t* err);
+
+// Tiled mixed pair pass (gx_force_tiled.cu); needs >= 3 cells on every axis.
+void launch_force_mixed_tiled(gx_handle* h, const GridGeom& g, const float4* pos4, const uint32_t* start,
+                              const LawF32& L, const PairF* tab, long long* F, size_t fstride,
+                              unsigned long long* vacc, unsigned long long* npairs, uint32_t* err);
+
+}  // namespace gx

@@ -102,6 +102,12 @@ void gx_destroy(gx_handle* h);
 const char* gx_last_error(const gx_handle* h);
 const char* gx_status_string(int status);
 int gx_set_precision(gx_handle* h, int precision);
+/* Tuning knob of the mixed pair pass: 0 = automatic (tiled when every axis
+ * has >= 3 force-grid cells), 1 = one thread per atom, 2 = warp-tiled with
+ * ballot compaction, 3 = thread per atom with staged rows and per-thread
+ * candidate lists (the automatic choice).  Results
+ * are bit-identical across variants (fixed-point sums). */
+int gx_set_kernel_variant(gx_handle* h, int variant);
 
 /* ---- state ----------------------------------------------------------- */
 

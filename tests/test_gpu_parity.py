@@ -247,6 +247,26 @@ def test_mixed_force_accuracy(gpu, orc, ionic):
     assert abs(int(npairs) - np_ref) <= max(2, np_ref // 100000)
 
 
+@pytest.mark.parametrize("ionic", [False, True])
+def test_mixed_kernel_variants_bit_identical(gpu, ionic):
+    # thread-per-atom (reference half shell) and tiled (row half shell,
+    # shared-memory staging, compaction) must give the same fixed-point sums
+    wl, cfg, u = _small_ionic(16) if ionic else _c1(n_side=20)
+    out = []
+    for variant in (1, 2, 3, 4):
+        h = _handle(cfg, "mixed")
+        h.set_kernel_variant(variant)
+        h.set_universe(u)
+        V, _, npairs = h.forces()
+        st = h.step(4)
+        out.append((V, npairs, h.get_state(), st))
+    for o in out[1:]:
+        assert out[0][0] == o[0] and out[0][1] == o[1]
+        for x, y in zip(out[0][2], o[2]):
+            assert np.array_equal(x, y)
+        assert np.array_equal(out[0][3], o[3])
+
+
 def test_mixed_is_deterministic(gpu):
     wl, cfg, u = _c1(n_side=14)
     cfg.enable_electrostatics = True
