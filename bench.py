@@ -195,7 +195,7 @@ def run_ticks(h, wl, cfg, steps: int, start_tick: int) -> int:
         k = steps - done
         if wl.gr_every:
             k = min(k, wl.gr_every - (t % wl.gr_every))
-        h.step(k, stats=False)
+        h.step(k, stats=False, graph=True)
         done += k
         t += k
         if wl.gr_every and t % wl.gr_every == 0:
@@ -258,6 +258,7 @@ def ours_arm(args, dist):
 
     h = Handle(cfg, "mixed", dev)
     h.set_universe(u)
+    variant, tune_ms = h.autotune(reps=3)  # picks the pair-pass work shape; state unchanged
     tick = run_ticks(h, wl, cfg, Wm, 0)
     h.synchronize()
     dist.barrier()
@@ -397,7 +398,9 @@ def ours_arm(args, dist):
                 "config": {"workload": wl.name, "atoms": u.n, "precision": "mixed", "thermostat_target_K":
                            cfg.thermostat_temperature, "electrostatics": cfg.enable_electrostatics,
                            "gr_every": wl.gr_every, "l2": "inputs larger than L2 (state ~300 MB > 126 MB); no flush",
-                           "parallelism": f"{dist.world} independent replicas (one per GPU)"},
+                           "parallelism": f"{dist.world} independent replicas (one per GPU)",
+                           "pair_pass_variant": variant, "autotune_ms_per_pass": tune_ms,
+                           "cuda_graph": True},
                 "gpu_launches": launches, "clocks": clk, "roofline": roof, "roofline_hbm": roof_hbm,
                 "kernels": kernels, "memory_kernels": mem, "pairs_per_tick": pairs}
         line.update(extras)

@@ -101,6 +101,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
         "gx_measure_fp32_peak": (C.c_int, [C.c_int, dp]),
         "gx_radial_distribution_noalloc": (C.c_int, [sz, dp, dp, _D, sz, u64p, dp, dp, dp]),
         "gx_set_kernel_variant": (C.c_int, [vp, C.c_int]),
+        "gx_autotune": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), dp]),
     }
     for name, (res, args) in proto.items():
         f = getattr(lib, name)
@@ -220,8 +221,17 @@ class Handle:
         self._check(self.lib.gx_set_precision(self.h, _PRECISION.get(precision, precision)))
 
     def set_kernel_variant(self, variant: int):
-        """Mixed pair pass: 0 automatic, 1 thread per atom, 2 tiled."""
+        """Mixed pair pass: 0 automatic, 1 thread per atom, 2 warp-tiled,
+        3 staged rows, 4 per-thread candidate lists."""
         self._check(self.lib.gx_set_kernel_variant(self.h, variant))
+
+    def autotune(self, reps: int = 5):
+        """Times every applicable pair-pass variant and keeps the fastest;
+        returns (variant, {variant: ms per pass})."""
+        best = C.c_int()
+        ms = np.full(5, -1.0)
+        self._check(self.lib.gx_autotune(self.h, reps, C.byref(best), _ptr(ms, C.c_double)))
+        return best.value, {v: float(t) for v, t in enumerate(ms) if t >= 0}
 
     # -- systems ------------------------------------------------------------
     def half_kick(self):

@@ -229,16 +229,29 @@ __global__ void k_fill_d(double* p, uint32_t n, double v) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) p[i] = v;
 }
-__global__ void k_record(gx_tick_stats* rec, const double* dscal, const unsigned long long* dcount, int thermo) {
-    rec->kinetic = dscal[1];
-    rec->speed_sum = dscal[4];
-    rec->potential = dscal[2];
-    rec->bond_energy = dscal[3];
-    rec->lambda = thermo ? dscal[0] : 1.0;
-    rec->pairs = dcount[0];
+// Appends this tick's observables at record index dcount[5] (a device-side
+// cursor, so the same launch sequence can be replayed from a CUDA graph).
+__global__ void k_record(gx_tick_stats* rec, const double* dscal, unsigned long long* dcount, int thermo) {
+    unsigned long long k = dcount[5];
+    rec[k].kinetic = dscal[1];
+    rec[k].speed_sum = dscal[4];
+    rec[k].potential = dscal[2];
+    rec[k].bond_energy = dscal[3];
+    rec[k].lambda = thermo ? dscal[0] : 1.0;
+    rec[k].pairs = dcount[0];
+    dcount[5] = k + 1;
 }
 
 inline unsigned nblk(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+void invalidate_graphs(gx_handle* h) {
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+            if (h->graph_exec[a][b]) cudaGraphExecDestroy(h->graph_exec[a][b]);
+            h->graph_exec[a][b] = nullptr;
+            h->graph_key[a][b] = 0;
+        }
+}
 
 // The pending Berendsen scale is folded into the next kernel that reads v;
 // anything else that reads v first commits it.
@@ -380,7 +393,7 @@ int gx_create(const gx_params* p, gx_handle** out) {
 void gx_destroy(gx_handle* h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
-    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    invalidate_graphs(h);
     free_buf(h->buf[0]);
     free_buf(h->buf[1]);
     cudaFree(h->key);
@@ -410,10 +423,7 @@ int gx_set_precision(gx_handle* h, int precision) {
         return set_err(h, GX_ERR_UNSUPPORTED, "gravity is only implemented in the FP64 path");
     h->precision = precision;
     h->sorted = false;
-    if (h->graph_exec) {
-        cudaGraphExecDestroy(h->graph_exec);
-        h->graph_exec = nullptr;
-    }
+    invalidate_graphs(h);
     return check_kinds(h);
 }
 
@@ -432,10 +442,7 @@ int gx_set_state(gx_handle* h, size_t n, const double* pos, const double* vel, c
     h->cur = 0;
     h->sorted = false;
     h->lambda_pending = false;
-    if (h->graph_exec) {
-        cudaGraphExecDestroy(h->graph_exec);
-        h->graph_exec = nullptr;
-    }
+    invalidate_graphs(h);
     StateBuf& b = h->buf[0];
     uint32_t un = (uint32_t)n;
     std::vector<double> tmp(n);
@@ -524,6 +531,7 @@ int gx_set_bonds(gx_handle* h, size_t nbonds, const uint32_t* pairs) {
         h->bonds_cap = nbonds;
     }
     if (nbonds) GX_CUDA(h, cudaMemcpy(h->bonds, pairs, 2 * nbonds * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    if (nbonds != h->nbonds) invalidate_graphs(h);
     h->nbonds = nbonds;
     return GX_OK;
 }
@@ -653,19 +661,21 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
             return GX_OK;
         }
     }
-    for (int s = 0; s < nsteps; ++s) {
-        // VelocityHalfKick (with the previous tick's pending thermostat scale)
-        const double* lam = h->lambda_pending ? h->dscal + 0 : nullptr;
-        launch_kick(h, h->buf[h->cur], n, 0.5 * h->p.dt, lam);
-        if (h->lambda_pending) {
-            GX_LAUNCH(h, k_fill_d, 1, 32, h->dscal, 1, 1.0);
-            h->lambda_pending = false;
-        }
-        launch_drift(h, h->buf[h->cur], n, h->p.dt);                // PositionDrift
+    // One tick.  With `uniform` the launch sequence does not depend on host
+    // state, so it can be captured: the first kick always applies the lambda
+    // slot (1.0 unless a Berendsen scale is pending; v * 1.0 == v) and resets it.
+    auto tick = [&](bool uniform) -> int {
+        const bool pend = uniform || h->lambda_pending;
+        // VelocityHalfKick, with the previous tick's pending thermostat scale
+        launch_kick(h, h->buf[h->cur], n, 0.5 * h->p.dt, pend ? h->dscal + 0 : nullptr);
+        if (pend) GX_LAUNCH(h, k_fill_d, 1, 32, h->dscal, 1, 1.0);
+        h->lambda_pending = false;
+        launch_drift(h, h->buf[h->cur], n, h->p.dt);                    // PositionDrift
         if (h->p.enable_boundaries) launch_wrap(h, h->buf[h->cur], n);  // BoundarySystem
-        if (n) {                                                   // ForceSystem
-            if ((rc = rebuild_cells(h))) return rc;
-            if ((rc = force_pass(h, true, nullptr, nullptr, nullptr, false))) return rc;
+        if (n) {                                                        // ForceSystem
+            int r = rebuild_cells(h);
+            if (!r) r = force_pass(h, true, nullptr, nullptr, nullptr, false);
+            if (r) return r;
         }
         launch_kick(h, h->buf[h->cur], n, 0.5 * h->p.dt, nullptr);  // VelocityHalfKick
         if (thermo) {                                              // ThermostatSystem
@@ -680,8 +690,54 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
             launch_kinetic(h, h->buf[h->cur], n, h->lambda_pending ? h->dscal + 0 : nullptr, kpart, spart, &nb);
             launch_finalize_sum(h, kpart, nb, h->dscal + 1);
             launch_finalize_sum(h, spart, nb, h->dscal + 4);
-            GX_LAUNCH(h, k_record, 1, 1, drec + s, h->dscal, h->dcount, thermo ? 1 : 0);
+            GX_LAUNCH(h, k_record, 1, 1, drec, h->dscal, h->dcount, thermo ? 1 : 0);
         }
+        return GX_OK;
+    };
+    if (drec) GX_CUDA(h, cudaMemsetAsync(h->dcount + 5, 0, sizeof(unsigned long long), h->stream));
+    const bool graph = use_graph && n && !h->prof_on;
+    const uint64_t key = ((uint64_t)n << 20) ^ ((uint64_t)h->precision << 1) ^ ((uint64_t)h->kernel_variant << 3) ^
+                         ((uint64_t)(h->nbonds > 0) << 6) ^ ((uint64_t)thermo << 7) ^ ((uint64_t)h->cap << 8) ^ 1u;
+    for (int s = 0; s < nsteps; ++s) {
+        if (!graph) {
+            if ((rc = tick(false))) return rc;
+            continue;
+        }
+        const int par = h->cur, rs = drec ? 1 : 0;
+        if (h->graph_exec[par][rs] && h->graph_key[par][rs] == key) {
+            GX_CUDA(h, cudaGraphLaunch(h->graph_exec[par][rs], h->stream));
+            h->launches += h->graph_kernels[par][rs];
+            h->cur ^= 1;  // the captured tick rebuilt the cell list into the other buffer
+            h->sorted = true;
+            h->lambda_pending = thermo;
+            continue;
+        }
+        if (!h->sorted) {  // first tick runs eagerly: every buffer it needs gets allocated
+            if ((rc = tick(true))) return rc;
+            continue;
+        }
+        if (h->graph_exec[par][rs]) cudaGraphExecDestroy(h->graph_exec[par][rs]);
+        h->graph_exec[par][rs] = nullptr;
+        const uint64_t l0 = h->launches;
+        const bool pend0 = h->lambda_pending;
+        GX_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        int trc = tick(true);
+        cudaGraph_t gr = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(h->stream, &gr);
+        if (trc || ce != cudaSuccess) {
+            if (gr) cudaGraphDestroy(gr);
+            h->cur ^= 1;  // capture did not execute: undo the host-side effects
+            h->lambda_pending = pend0;
+            return trc ? trc : cuda_err(h, ce, "cudaStreamEndCapture");
+        }
+        cudaGraphExec_t ex = nullptr;
+        ce = cudaGraphInstantiate(&ex, gr, 0);
+        cudaGraphDestroy(gr);
+        if (ce != cudaSuccess) return cuda_err(h, ce, "cudaGraphInstantiate");
+        h->graph_exec[par][rs] = ex;
+        h->graph_key[par][rs] = key;
+        h->graph_kernels[par][rs] = h->launches - l0;
+        GX_CUDA(h, cudaGraphLaunch(ex, h->stream));  // the captured tick has not run yet: run it now
     }
     if (drec) {
         GX_CUDA(h, cudaMemcpyAsync(stats, drec, (size_t)nsteps * sizeof(gx_tick_stats), cudaMemcpyDeviceToHost,
@@ -703,7 +759,47 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
 int gx_set_kernel_variant(gx_handle* h, int variant) {
     if (!h || variant < 0 || variant > 4) return GX_ERR_ARG;
     h->kernel_variant = variant;
+    invalidate_graphs(h);
     return GX_OK;
+}
+
+int gx_autotune(gx_handle* h, int reps, int* best, double* ms) {
+    int rc = require_state(h);
+    if (rc) return rc;
+    if (reps < 1) reps = 1;
+    for (int v = 0; v < 5; ++v)
+        if (ms) ms[v] = -1.0;
+    if (h->precision != GX_MIXED || h->n == 0) {
+        if (best) *best = h->kernel_variant;
+        return GX_OK;
+    }
+    // Each variant produces the same fixed-point sums, so repeated force
+    // passes leave the state bit-identical whichever variant runs.
+    const int cand[4] = {4, 1, 3, 2};
+    int pick = 4;
+    double best_ms = 1e300;
+    const int saved = h->kernel_variant;
+    for (int v : cand) {
+        const GridGeom& g = h->fgrid;
+        if ((v == 2 || v == 3) && (g.n[0] < 3 || g.n[1] < 3 || g.n[2] < 3)) continue;
+        h->kernel_variant = v;
+        if ((rc = gx_forces(h, nullptr, nullptr, nullptr))) break;  // warm-up
+        if ((rc = gx_timer_mark(h, 14))) break;
+        for (int r = 0; r < reps && !rc; ++r) rc = force_pass(h, true, nullptr, nullptr, nullptr, false);
+        if (rc || (rc = gx_timer_mark(h, 15))) break;
+        double t = 0.0;
+        if ((rc = gx_timer_elapsed(h, 14, 15, &t))) break;
+        t /= reps;
+        if (ms) ms[v] = t;
+        if (t < best_ms) {
+            best_ms = t;
+            pick = v;
+        }
+    }
+    h->kernel_variant = rc ? saved : pick;
+    invalidate_graphs(h);
+    if (best) *best = h->kernel_variant;
+    return rc;
 }
 
 int gx_set_dynamic(gx_handle* h, const double* pos, const double* vel, const double* acc) {

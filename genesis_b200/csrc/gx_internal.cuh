@@ -207,9 +207,10 @@ struct gx_handle {
     std::vector<gx::ProfSlot> prof;
     std::vector<cudaEvent_t> ev_pool;
 
-    // CUDA graph of one tick
-    cudaGraphExec_t graph_exec = nullptr;
-    int graph_flags = -1;
+    // CUDA graphs of one tick, per buffer parity and with/without records
+    cudaGraphExec_t graph_exec[2][2] = {};
+    uint64_t graph_key[2][2] = {};
+    uint64_t graph_kernels[2][2] = {};
 
     // stream-ordered timers and the launch counter
     cudaEvent_t timers[16] = {};

@@ -108,6 +108,11 @@ int gx_set_precision(gx_handle* h, int precision);
  * candidate lists (the automatic choice).  Results
  * are bit-identical across variants (fixed-point sums). */
 int gx_set_kernel_variant(gx_handle* h, int variant);
+/* Autotuner: times `reps` mixed pair passes of every applicable variant on
+ * the resident state (the state is left bit-identical: every variant gives
+ * the same fixed-point sums), selects the fastest and returns it in *best;
+ * ms[0..4], when given, receives the per-pass milliseconds (-1 = not run). */
+int gx_autotune(gx_handle* h, int reps, int* best, double* ms);
 
 /* ---- state ----------------------------------------------------------- */
 

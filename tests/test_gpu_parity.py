@@ -267,6 +267,39 @@ def test_mixed_kernel_variants_bit_identical(gpu, ionic):
         assert np.array_equal(out[0][3], o[3])
 
 
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_graph_replay_matches_eager_ticks(gpu, prec):
+    wl, cfg, u = _c1(n_side=12)
+    cfg.enable_thermostat = True
+    cfg.thermostat_temperature = 30.0
+    cfg.enable_electrostatics = True
+    res = []
+    for graph in (False, True):
+        h = _handle(cfg, prec)
+        h.set_universe(u)
+        parts = [h.step(3, graph=graph), h.step(6, graph=graph)]
+        h.step(1, stats=False, graph=graph)
+        parts.append(h.step(4, graph=graph))
+        st = np.concatenate(parts)
+        res.append((h.get_state(), st))
+    for x, y in zip(res[0][0], res[1][0]):
+        assert np.array_equal(x, y)
+    assert np.array_equal(res[0][1], res[1][1])
+
+
+def test_autotune_leaves_state_unchanged(gpu):
+    wl, cfg, u = _c1(n_side=14)
+    a = _handle(cfg, "mixed")
+    a.set_universe(u)
+    a.step(2)
+    before = a.get_state()
+    best, ms = a.autotune(reps=2)
+    assert best in ms and best in (1, 2, 3, 4)
+    after = a.get_state()
+    for x, y in zip(before, after):
+        assert np.array_equal(x, y)
+
+
 def test_mixed_is_deterministic(gpu):
     wl, cfg, u = _c1(n_side=14)
     cfg.enable_electrostatics = True
