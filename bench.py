@@ -382,6 +382,26 @@ def ours_arm(args, dist):
         except Exception as e:  # noqa: BLE001
             extras["e2e_error"] = repr(e)
 
+        # batched temperature sweep: replica-steps/s in one persistent launch vs
+        # the same replicas one after another through gx_step
+        try:
+            from genesis_b200 import sweep
+
+            wls = sweep.make_replicas(256, seed=dist.rank)
+            sweep_steps = 2000
+            vb, _, msb = sweep.run_batched(wls, sweep_steps, dev)
+            seq_steps = 50
+            vs, mss = sweep.run_sequential(wls, seq_steps, dev)
+            extras["replica_sweep"] = {
+                "metric": "replica-steps/s", "replicas": len(wls), "atoms": sweep.atoms(wls),
+                "batched": {"value": dist.world * vb, "steps": sweep_steps, "ms": msb},
+                "sequential": {"value": dist.world * vs, "steps_per_replica": seq_steps, "ms": mss},
+                "batched_over_sequential": vb / vs,
+                "workload": "256 replicas, n^3 atoms with n = round(N^(1/3)) in [8, 25], N log-uniform in "
+                            "[512, 16384], 10-element LJ mixture, Berendsen T uniform in [20, 120] K"}
+        except Exception as e:  # noqa: BLE001
+            extras["replica_sweep_error"] = repr(e)
+
         if dist.rank == 0 and dist.world == 1:
             try:
                 threads = os.cpu_count() or 1

@@ -379,3 +379,84 @@ def radial_distribution_noalloc(pos, box, r_max: float, nbins: int):
     if rc != 0:
         raise GxError(rc, "gx_radial_distribution_noalloc: " + lib.gx_status_string(rc).decode())
     return counts, bins, rmo.value, dro.value
+
+
+class Batch:
+    """Many independent universes advanced together in one persistent launch
+    (a ``gx_batch``): the temperature-sweep replicas."""
+
+    def __init__(self, base_cfg, boxes, targets=None, device: int = 0):
+        self.lib = load()
+        _declare_batch(self.lib)
+        self._p = params(base_cfg, "mixed", device)
+        boxes = np.ascontiguousarray(np.asarray(boxes, dtype=np.float64).reshape(-1, 3))
+        self.nrep = len(boxes)
+        tg = None if targets is None else np.ascontiguousarray(targets, dtype=np.float64)
+        b = C.c_void_p()
+        rc = self.lib.gx_batch_create(C.byref(self._p), self.nrep, _ptr(boxes, C.c_double), _ptr(tg, C.c_double),
+                                      C.byref(b))
+        self.b = b
+        self._check(rc)
+        self.natoms = None
+
+    def _check(self, rc):
+        if rc != 0:
+            msg = self.lib.gx_batch_last_error(self.b).decode() if self.b else "gx_batch_create failed"
+            raise GxError(rc, msg)
+
+    def close(self):
+        if self.b:
+            self.lib.gx_batch_destroy(self.b)
+            self.b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_universes(self, universes):
+        self.natoms = np.array([u.n for u in universes], dtype=np.uint32)
+        cat = lambda f: np.ascontiguousarray(np.concatenate([getattr(u, f) for u in universes]))  # noqa: E731
+        pos, vel, elem, q, m = cat("pos"), cat("vel"), cat("elem").astype(np.uint8), cat("charge"), cat("mass")
+        self._check(self.lib.gx_batch_set_state(self.b, _ptr(self.natoms, C.c_uint32), _ptr(pos, C.c_double),
+                                                _ptr(vel, C.c_double), None, _ptr(elem, C.c_uint8),
+                                                _ptr(q, C.c_double), _ptr(m, C.c_double)))
+
+    def step(self, nsteps: int):
+        """Returns (stats[nrep, 4] = K, V, lambda, pairs; device milliseconds)."""
+        st = np.zeros((self.nrep, 4))
+        ms = C.c_double()
+        self._check(self.lib.gx_batch_step(self.b, nsteps, _ptr(st, C.c_double), C.byref(ms)))
+        return st, ms.value
+
+    def get_state(self):
+        n = int(self.natoms.sum())
+        pos, vel, acc = (np.empty((n, 3)) for _ in range(3))
+        self._check(self.lib.gx_batch_get_state(self.b, _ptr(pos, C.c_double), _ptr(vel, C.c_double),
+                                                _ptr(acc, C.c_double)))
+        offs = np.concatenate([[0], np.cumsum(self.natoms)]).astype(np.int64)
+        return [(pos[a:b], vel[a:b], acc[a:b]) for a, b in zip(offs[:-1], offs[1:])]
+
+
+_batch_declared = False
+
+
+def _declare_batch(lib):
+    global _batch_declared
+    if _batch_declared:
+        return
+    vp, dp = C.c_void_p, C.POINTER(C.c_double)
+    proto = {
+        "gx_batch_create": (C.c_int, [C.POINTER(GxParams), C.c_int, dp, dp, C.POINTER(vp)]),
+        "gx_batch_destroy": (None, [vp]),
+        "gx_batch_last_error": (C.c_char_p, [vp]),
+        "gx_batch_set_state": (C.c_int, [vp, C.POINTER(C.c_uint32), dp, dp, dp, C.POINTER(C.c_uint8), dp, dp]),
+        "gx_batch_step": (C.c_int, [vp, C.c_int, dp, dp]),
+        "gx_batch_get_state": (C.c_int, [vp, dp, dp, dp]),
+    }
+    for name, (res, args) in proto.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _batch_declared = True

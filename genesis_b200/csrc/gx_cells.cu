@@ -135,9 +135,9 @@ __global__ void k_build_pos4(GridGeom g, StateBuf b, const uint32_t* __restrict_
     if (i >= n) return;
     uint32_t ix, iy, iz;
     decode(g, key[i], ix, iy, iz);
-    double ux = rem_euclid(b.x[i] + 0.5 * g.L[0], g.L[0]) - (double)ix * g.cell[0];
-    double uy = rem_euclid(b.y[i] + 0.5 * g.L[1], g.L[1]) - (double)iy * g.cell[1];
-    double uz = rem_euclid(b.z[i] + 0.5 * g.L[2], g.L[2]) - (double)iz * g.cell[2];
+    double ux = cell_local(b.x[i], g.L[0], g.cell[0], ix);
+    double uy = cell_local(b.y[i], g.L[1], g.cell[1], iy);
+    double uz = cell_local(b.z[i], g.L[2], g.cell[2], iz);
     pos4[i] = make_float4((float)ux, (float)uy, (float)uz, __int_as_float((int)b.kind[i]));
 }
 

@@ -94,6 +94,12 @@ __device__ __forceinline__ uint32_t cell_of(const GridGeom& g, double x, double 
     return encode(g, axis_cell(x, g.L[0], g.cell[0], g.n[0]), axis_cell(y, g.L[1], g.cell[1], g.n[1]),
                   axis_cell(z, g.L[2], g.cell[2], g.n[2]));
 }
+// Offset of a coordinate from the origin of its cell (u - i*cell, u as in
+// cell_of), exact FP64 so every kernel that stages FP32 positions agrees.
+__device__ __forceinline__ double cell_local(double v, double L, double c, uint32_t i) {
+    return xsub(rem_euclid(xadd(v, xmul(0.5, L)), L), xmul((double)i, c));
+}
+
 // Number of times the reference's neighbors() reports a pair whose members
 // sit in cells A != B: the count of offsets o (zero on degenerate axes, o != 0)
 // with A + o == B (mod n).  It is > 1 only on axes with exactly two cells.

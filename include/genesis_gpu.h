@@ -207,6 +207,34 @@ int gx_bound_pairs(gx_handle* h, double k_bind, uint32_t* pairs, size_t cap, siz
  * Charge, EntityId).  Any pointer may be NULL (column unchanged). */
 int gx_set_dynamic(gx_handle* h, const double* pos, const double* vel, const double* acc);
 
+/* ---- batched replicas (temperature sweep) ------------------------------ */
+
+/* The reference sweeps temperatures with one fresh Universe per T, run one
+ * after another (examples/temperature_sweep.rs:70-113).  A gx_batch holds
+ * nrep independent universes of uneven sizes that share the laws in `base`
+ * (mixed precision) and advances all of them in one persistent launch, one
+ * CTA per replica.  box: 3 doubles per replica; target_T: Berendsen target
+ * per replica (<= 0 or base->enable_thermostat == 0: NVE); NULL uses
+ * base->thermostat_temperature.  Each replica's force grid must have >= 1
+ * and <= 4096 cells. */
+typedef struct gx_batch gx_batch;
+int gx_batch_create(const gx_params* base, int nrep, const double* box, const double* target_T,
+                    gx_batch** out);
+void gx_batch_destroy(gx_batch* b);
+const char* gx_batch_last_error(const gx_batch* b);
+/* Replica r owns atoms [sum(natoms[0..r)), +natoms[r]) of the concatenated
+ * AoS/per-atom arrays (same column meaning as gx_set_state).  acc, charge,
+ * mass may be NULL. */
+int gx_batch_set_state(gx_batch* b, const uint32_t* natoms, const double* pos, const double* vel,
+                       const double* acc, const uint8_t* elem, const double* charge,
+                       const double* mass);
+/* nsteps ticks of every replica in one launch.  stats (may be NULL): 4
+ * doubles per replica after the last tick -- kinetic energy after the
+ * thermostat, potential energy, lambda, pairs.  device_ms (may be NULL):
+ * CUDA-event time of the launch. */
+int gx_batch_step(gx_batch* b, int nsteps, double* stats, double* device_ms);
+int gx_batch_get_state(gx_batch* b, double* pos, double* vel, double* acc);
+
 /* ---- timing ---------------------------------------------------------- */
 
 /* Waits for the handle's stream. */
