@@ -41,6 +41,11 @@ class GxTickStats(C.Structure):
                 ("lambda_", _D), ("pairs", C.c_uint64)]
 
 
+class GxAdjointSpec(C.Structure):
+    _fields_ = [("nsteps", C.c_int32), ("checkpoint_every", C.c_int32), ("gr_bins", C.c_int32),
+                ("gr_every", C.c_int32), ("gr_rmax", _D), ("gr_width", _D), ("gr_support", _D)]
+
+
 TICK_DTYPE = np.dtype([("kinetic", "f8"), ("speed_sum", "f8"), ("potential", "f8"),
                        ("bond_energy", "f8"), ("lambda", "f8"), ("pairs", "u8")])
 
@@ -52,6 +57,9 @@ EXPORTS = (
     "gx_radial_distribution_between", "gx_clusters", "gx_bound_pairs",
     "gx_synchronize", "gx_profile_enable", "gx_profile_read", "gx_set_dynamic",
     "gx_timer_mark", "gx_timer_elapsed", "gx_launch_count", "gx_measure_fp32_peak",
+    "gx_radial_distribution_noalloc", "gx_set_kernel_variant", "gx_autotune",
+    "gx_batch_create", "gx_batch_destroy", "gx_batch_last_error", "gx_batch_set_state",
+    "gx_batch_step", "gx_batch_get_state", "gx_adjoint_forward", "gx_adjoint_backward",
 )
 
 _lib = None
@@ -102,6 +110,8 @@ def load(path: str | Path | None = None) -> C.CDLL:
         "gx_radial_distribution_noalloc": (C.c_int, [sz, dp, dp, _D, sz, u64p, dp, dp, dp]),
         "gx_set_kernel_variant": (C.c_int, [vp, C.c_int]),
         "gx_autotune": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), dp]),
+        "gx_adjoint_forward": (C.c_int, [vp, C.POINTER(GxAdjointSpec), dp, dp]),
+        "gx_adjoint_backward": (C.c_int, [vp, dp, dp, dp, dp, dp, dp, dp]),
     }
     for name, (res, args) in proto.items():
         f = getattr(lib, name)
@@ -335,6 +345,39 @@ class Handle:
         total = C.c_size_t()
         self._check(self.lib.gx_bound_pairs(self.h, k_bind, _ptr(out, C.c_uint32), cap, C.byref(total)))
         return out[: total.value].copy()
+
+    # -- adjoint --------------------------------------------------------------
+    def adjoint_forward(self, nsteps: int, checkpoint_every: int = 20, gr_bins: int = 0, gr_every: int = 1,
+                        gr_rmax: float = 1.0, gr_width: float = 0.1, gr_support: float = 6.0):
+        """FP64 trajectory of ``nsteps`` NVE ticks from the current state
+        (left unchanged); returns (V per tick, time-averaged Gaussian-kernel
+        g(r) or None)."""
+        spec = GxAdjointSpec(nsteps, checkpoint_every, gr_bins, gr_every, gr_rmax, gr_width, gr_support)
+        V = np.zeros(nsteps)
+        g = np.zeros(gr_bins) if gr_bins > 0 else None
+        self._check(self.lib.gx_adjoint_forward(self.h, C.byref(spec), _ptr(V, C.c_double), _ptr(g, C.c_double)))
+        self._adj_T, self._adj_bins = nsteps, gr_bins
+        return V, g
+
+    def adjoint_backward(self, dl_dpotential=None, dl_dgr=None, initial_state: bool = False):
+        """Gradients of the loss whose cotangents are given, with respect to
+        (sigma[10], epsilon_k[10]); with ``initial_state`` also with respect
+        to the initial (pos, vel, acc)."""
+        dV = None if dl_dpotential is None else np.ascontiguousarray(dl_dpotential, dtype=np.float64)
+        dg = None if dl_dgr is None else np.ascontiguousarray(dl_dgr, dtype=np.float64)
+        T, bins = getattr(self, "_adj_T", None), getattr(self, "_adj_bins", None)
+        if T is not None and dV is not None and len(dV) != T:
+            raise ValueError("dl_dpotential needs one entry per tick")
+        if bins is not None and dg is not None and len(dg) != bins:
+            raise ValueError("dl_dgr needs one entry per g(r) bin")
+        gs, ge = np.zeros(10), np.zeros(10)
+        st = [np.zeros((self.n, 3)) for _ in range(3)] if initial_state else [None, None, None]
+        self._check(self.lib.gx_adjoint_backward(self.h, _ptr(dV, C.c_double), _ptr(dg, C.c_double),
+                                                 _ptr(gs, C.c_double), _ptr(ge, C.c_double),
+                                                 *(_ptr(a, C.c_double) for a in st)))
+        if initial_state:
+            return gs, ge, tuple(st)
+        return gs, ge
 
     # -- profiling ----------------------------------------------------------
     def profile(self, on: bool = True):

@@ -394,6 +394,7 @@ void gx_destroy(gx_handle* h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
     invalidate_graphs(h);
+    adjoint_free(h);
     free_buf(h->buf[0]);
     free_buf(h->buf[1]);
     cudaFree(h->key);

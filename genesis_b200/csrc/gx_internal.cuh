@@ -224,6 +224,9 @@ struct gx_handle {
 
     // mixed pair-pass variant: 0 = automatic, 1 = thread per atom, 2 = tiled
     int kernel_variant = 0;
+
+    // adjoint (gx_adjoint.cu): checkpoints and work buffers, owned there
+    void* adj = nullptr;
 };
 
 // Every kernel launch of the library goes through this macro so the
@@ -264,6 +267,7 @@ void launch_build_pos4(gx_handle* h, const GridGeom& g, const StateBuf& b, const
                        uint32_t n, float4* pos4);
 
 int force_pass(gx_handle* h, bool finalize_acc, double* V, double* Vb, uint64_t* npairs, bool sync_out);
+void adjoint_free(gx_handle* h);
 
 void launch_kick(gx_handle* h, const StateBuf& b, uint32_t n, double half_dt, const double* lambda);
 void launch_drift(gx_handle* h, const StateBuf& b, uint32_t n, double dt);

@@ -235,6 +235,50 @@ int gx_batch_set_state(gx_batch* b, const uint32_t* natoms, const double* pos, c
 int gx_batch_step(gx_batch* b, int nsteps, double* stats, double* device_ms);
 int gx_batch_get_state(gx_batch* b, double* pos, double* vel, double* acc);
 
+/* ---- adjoint: derivatives of short NVE horizons ----------------------- */
+
+/* No counterpart in the reference, which has no derivatives.  Reverse-mode
+ * gradients with respect to the per-element sigma[10] and epsilon_k[10] of
+ * gx_params, of any loss of two smoothed observables of the trajectory that
+ * starts from the handle's current state (the state is left unchanged):
+ *   V_t  the potential energy (LJ + Coulomb + gravity) after tick t = 1..T;
+ *   g_k  a Gaussian-kernel pair distribution averaged over the ticks
+ *        t = gr_every, 2 gr_every, ... <= T:
+ *          g_k = c_k * sum over pair-list entries with |d - r_k| < gr_support * w
+ *                of exp(-(d - r_k)^2 / (2 w^2)),
+ *          r_k = (k + 1/2) gr_rmax / gr_bins,  w = gr_width,
+ *          c_k = L_x L_y L_z / (N (N - 1) / 2 * 4 pi r_k^2 * sqrt(2 pi) w).
+ * The ticks are the reference's (src/universe/mod.rs:356-369: kick, drift,
+ * wrap, forces, kick) in FP64 with its per-pair arithmetic, whatever the
+ * handle's precision.  gx_adjoint_forward keeps a checkpoint of (x, v, a)
+ * every checkpoint_every ticks; gx_adjoint_backward recomputes each segment
+ * from its checkpoint and runs the adjoint of the velocity-Verlet step and
+ * of the force pass backwards through it.  The cutoffs (LJ, Coulomb,
+ * gravity) are multiples of max sigma: their derivative goes to the
+ * lowest-index element with the largest sigma.  Supported: LJ, Coulomb,
+ * gravity, periodic wrap, every epsilon_k > 0; the thermostat and the bond
+ * spring give GX_ERR_UNSUPPORTED.  gr_rmax + gr_support * gr_width must not
+ * exceed the force cutoff; gr_bins <= 512. */
+typedef struct {
+    int32_t nsteps;           /* horizon T >= 1 */
+    int32_t checkpoint_every; /* K >= 1 */
+    int32_t gr_bins;          /* number of g bin centres; 0 = no g observable */
+    int32_t gr_every;         /* sample g every this many ticks (>= 1) */
+    double gr_rmax;
+    double gr_width;          /* kernel width w */
+    double gr_support;        /* kernel truncated at gr_support * w */
+} gx_adjoint_spec;
+
+/* potential: [nsteps] V_t.  gr: [gr_bins] the time-averaged g_k, or NULL. */
+int gx_adjoint_forward(gx_handle* h, const gx_adjoint_spec* spec, double* potential, double* gr);
+/* dl_dpotential [nsteps] and dl_dgr [gr_bins] are the cotangents dL/dV_t and
+ * dL/dg_k of the caller's loss L (NULL = zero).  Writes dL/dsigma[10] and
+ * dL/depsilon_k[10]; grad_pos0 / grad_vel0 / grad_acc0 (slot-ordered [3n] or
+ * NULL) receive dL/d(initial position, velocity, acceleration).  Uses the
+ * checkpoints of the last gx_adjoint_forward on this handle. */
+int gx_adjoint_backward(gx_handle* h, const double* dl_dpotential, const double* dl_dgr, double* grad_sigma,
+                        double* grad_epsilon_k, double* grad_pos0, double* grad_vel0, double* grad_acc0);
+
 /* ---- timing ---------------------------------------------------------- */
 
 /* Waits for the handle's stream. */

@@ -112,6 +112,24 @@ int orc_ticks(const orc_params* p, size_t n, double* pos, double* vel, double* a
               size_t nbonds, const uint32_t* bonds, int nticks, int nthreads,
               double* out_stats);
 
+/* ---- adjoint reference (oracle_dual.cpp) ----
+ * The NVE tick templated on the scalar type.  Returns per tick V_t and the
+ * time-averaged Gaussian-kernel g_k; when dpotential / dgr are non-null the
+ * run uses dual numbers and also returns dV_t/dtheta [nsteps][20] and
+ * dg_k/dtheta [gr_bins][20], theta = (sigma[0..9], epsilon_k[0..9]).
+ * Returns -1 with bonds or thermostat on, -2 when gr_rmax + gr_support *
+ * gr_width exceeds the force cutoff, -3 on bad arguments. */
+int orc_adjoint_forward(const orc_params* p, size_t n, const double* pos, const double* vel,
+                        const double* acc, const uint8_t* elem, const double* charge,
+                        const double* mass, int nsteps, int gr_bins, int gr_every, double gr_rmax,
+                        double gr_width, double gr_support, int nthreads, double* potential,
+                        double* gr, double* dpotential, double* dgr);
+/* The template's T = double trajectory (in place), for the bit-for-bit
+ * comparison with orc_ticks. */
+int orc_adjoint_trajectory(const orc_params* p, size_t n, double* pos, double* vel, double* acc,
+                           const uint8_t* elem, const double* charge, const double* mass,
+                           int nsteps, int nthreads, double* potential);
+
 /* ---- lenses: src/analysis/mod.rs, src/analysis/pairs.rs ---- */
 int orc_radial_distribution(size_t n, const double* pos, const double box[3],
                             double r_max, size_t nbins, uint64_t* counts,

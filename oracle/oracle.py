@@ -34,7 +34,7 @@ class OrcParams(C.Structure):
 
 
 def build(force: bool = False) -> Path:
-    src = [HERE / "oracle.cpp", HERE / "oracle.h"]
+    src = [HERE / n for n in ("oracle.cpp", "oracle_dual.cpp", "oracle.h", "oracle_grid.h", "Makefile")]
     if force or not LIB.exists() or any(p.stat().st_mtime > LIB.stat().st_mtime for p in src):
         subprocess.run(["make", "-s", "-C", str(HERE), "-B" if force else "liboracle.so"], check=True)
     return LIB
@@ -79,6 +79,9 @@ def load() -> C.CDLL:
                                                           dp, dp]),
             "orc_clusters": (C.c_int, [sz, dp, u8p, dp, _D, dp, u32p, u64p, dp]),
             "orc_bound_pairs": (sz, [sz, dp, u8p, u32p, dp, _D, dp, u32p, sz]),
+            "orc_adjoint_forward": (C.c_int, [pp, sz, dp, dp, dp, u8p, dp, dp, C.c_int, C.c_int, C.c_int, _D, _D,
+                                              _D, C.c_int, dp, dp, dp, dp]),
+            "orc_adjoint_trajectory": (C.c_int, [pp, sz, dp, dp, dp, u8p, dp, dp, C.c_int, C.c_int, dp]),
         }
         for name, (res, args) in proto.items():
             f = getattr(lib, name)
@@ -314,3 +317,44 @@ def bound_pairs(pos, elem, entity, box, k_bind, sigma):
     out = np.empty((total, 2), dtype=np.uint32)
     lib.orc_bound_pairs(*args, _p(out, C.c_uint32), total)
     return out
+
+
+def adjoint_forward(cfg, pos, vel, acc, elem, charge, mass, nsteps, gr_bins=0, gr_every=1, gr_rmax=1.0,
+                    gr_width=0.1, gr_support=6.0, nthreads=1, dual=False):
+    """Potential per tick and time-averaged Gaussian-kernel g(r) of an NVE
+    run (oracle_dual.cpp).  With ``dual`` also their exact derivatives with
+    respect to (sigma[0..9], epsilon_k[0..9]): returns
+    (V[nsteps], g[gr_bins], dV[nsteps, 20], dg[gr_bins, 20])."""
+    lib = load()
+    elem = np.ascontiguousarray(elem, dtype=np.uint8)
+    n = len(elem)
+    V = np.zeros(nsteps)
+    g = np.zeros(max(gr_bins, 0))
+    dV = np.zeros((nsteps, 20)) if dual else None
+    dg = np.zeros((max(gr_bins, 0), 20)) if dual else None
+    if dual and gr_bins <= 0:
+        dg = None
+    rc = lib.orc_adjoint_forward(C.byref(params(cfg)), n, _p(_f64(pos), C.c_double), _p(_f64(vel), C.c_double),
+                                 _p(_f64(acc), C.c_double), _p(elem, C.c_uint8), _p(_f64(charge), C.c_double),
+                                 _p(_f64(mass), C.c_double), nsteps, gr_bins, gr_every, gr_rmax, gr_width,
+                                 gr_support, nthreads, _p(V, C.c_double), _p(g, C.c_double) if gr_bins > 0 else None,
+                                 _p(dV, C.c_double), _p(dg, C.c_double))
+    if rc != 0:
+        raise ValueError(f"orc_adjoint_forward failed ({rc})")
+    if dual and dg is None:
+        dg = np.zeros((0, 20))
+    return V, g, dV, dg
+
+
+def adjoint_trajectory(cfg, pos, vel, acc, elem, charge, mass, nsteps, nthreads=1):
+    """The dual template's T = double trajectory: (pos, vel, acc, V[nsteps])."""
+    lib = load()
+    pos, vel, acc = _f64(pos).copy(), _f64(vel).copy(), _f64(acc).copy()
+    elem = np.ascontiguousarray(elem, dtype=np.uint8)
+    V = np.zeros(nsteps)
+    rc = lib.orc_adjoint_trajectory(C.byref(params(cfg)), len(elem), _p(pos, C.c_double), _p(vel, C.c_double),
+                                    _p(acc, C.c_double), _p(elem, C.c_uint8), _p(_f64(charge), C.c_double),
+                                    _p(_f64(mass), C.c_double), nsteps, nthreads, _p(V, C.c_double))
+    if rc != 0:
+        raise ValueError(f"orc_adjoint_trajectory failed ({rc})")
+    return pos, vel, acc, V

@@ -178,7 +178,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_params_layout_matches_header():
-    from genesis_b200._lib import GxParams, GxTickStats
+    from genesis_b200._lib import GxAdjointSpec, GxParams, GxTickStats
     src = """
 #include <stddef.h>
 #include <stdio.h>
@@ -187,6 +187,8 @@ int main(void) {
   printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(gx_params), offsetof(gx_params, enable_electrostatics),
          offsetof(gx_params, precision), offsetof(gx_params, device), sizeof(gx_tick_stats),
          offsetof(gx_tick_stats, pairs));
+  printf("%zu %zu %zu\\n", sizeof(gx_adjoint_spec), offsetof(gx_adjoint_spec, gr_rmax),
+         offsetof(gx_adjoint_spec, gr_support));
   return 0;
 }
 """
@@ -197,7 +199,8 @@ int main(void) {
         subprocess.run(["gcc", f"-I{ROOT / 'include'}", str(c), "-o", str(exe)], check=True)
         got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     want = [ctypes.sizeof(GxParams), GxParams.enable_electrostatics.offset, GxParams.precision.offset,
-            GxParams.device.offset, ctypes.sizeof(GxTickStats), GxTickStats.pairs.offset]
+            GxParams.device.offset, ctypes.sizeof(GxTickStats), GxTickStats.pairs.offset,
+            ctypes.sizeof(GxAdjointSpec), GxAdjointSpec.gr_rmax.offset, GxAdjointSpec.gr_support.offset]
     assert got == want
 
 
