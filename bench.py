@@ -225,6 +225,55 @@ def cpu_reference(wl, cfg, u, budget_s: float, threads: int) -> dict:
 # ---------------------------------------------------------------- arms
 
 
+def adjoint_leg(dev: int) -> dict:
+    """Wall-clock cost of one adjoint gradient on the C5 workload (8,000
+    atoms, 200 NVE ticks, checkpoint every 20), the cost of the 40 forward
+    runs central differences need, and the largest disagreement."""
+    import numpy as np
+
+    from genesis_b200 import adjoint as adj
+    from genesis_b200._lib import Handle
+
+    _, acfg, au = adj.c5()
+    spec = adj.AdjointSpec()
+    target = adj.gr_target(acfg, au, spec, dev)
+    with Handle(acfg, "fp64", dev) as ha:
+        ha.set_universe(au)
+        ha.adjoint_forward(spec.nsteps, **spec.kwargs())  # warm-up
+        ha.adjoint_backward(np.full(spec.nsteps, 1.0 / spec.nsteps))
+        l0 = ha.launches
+        t0 = time.perf_counter()
+        V, g = ha.adjoint_forward(spec.nsteps, **spec.kwargs())
+        t1 = time.perf_counter()
+        lv, cv = adj.potential_loss(V)
+        gsV, geV = ha.adjoint_backward(dl_dpotential=cv)
+        t2 = time.perf_counter()
+        lg, cg = adj.gr_loss(g, target)
+        gsG, geG = ha.adjoint_backward(dl_dgr=cg)
+        t3 = time.perf_counter()
+        launches = ha.launches - l0
+    tf = time.perf_counter()
+    fd = adj.fd_gradients(acfg, au, spec, target, 1e-5, dev)
+    fd_s = time.perf_counter() - tf
+
+    def err(ad, ref):
+        return float(np.max(np.abs(ad - ref) / (np.abs(ref) + 1e-6 * np.abs(ref).max())))
+
+    grad_ms = (t1 - t0 + t2 - t1) * 1e3
+    return {"workload": "adjoint LJ NVE 20^3: 8000 atoms, 60 K, 200 ticks, checkpoint every 20",
+            "parameters": "10 sigma + 10 epsilon_k", "precision": "fp64",
+            "losses": {"potential": "<V> over the 200 ticks", "gr": "sum_k (gbar_k - target_k)^2, Gaussian kernel "
+                       f"w = {spec.gr_width:.4f} (0.05 max sigma), {spec.gr_bins} centres to {spec.gr_rmax}, "
+                       "target = same run with sigma x 1.02"},
+            "forward_ms": (t1 - t0) * 1e3, "backward_ms": ((t2 - t1) + (t3 - t2)) * 0.5e3,
+            "gradient_ms": grad_ms, "fd_ms": fd_s * 1e3, "fd_runs": 40,
+            "speedup_vs_fd": fd_s * 1e3 / grad_ms, "gpu_launches": launches,
+            "max_rel_err_vs_fd": {"potential": err(np.r_[gsV, geV], fd["potential"]),
+                                  "gr": err(np.r_[gsG, geG], fd["gr"])},
+            "fd_step": "central, 1e-5 x parameter", "loss_values": {"potential": lv, "gr": lg},
+            "timing": "host wall clock around the synchronous C-ABI calls"}
+
+
 def reference_arm(args, dist):
     if dist.rank != 0:
         return
@@ -401,6 +450,13 @@ def ours_arm(args, dist):
                             "[512, 16384], 10-element LJ mixture, Berendsen T uniform in [20, 120] K"}
         except Exception as e:  # noqa: BLE001
             extras["replica_sweep_error"] = repr(e)
+
+        # adjoint (C5): gradients of <V> and of the g(r) fitting loss with
+        # respect to the 10 sigma + 10 epsilon_k, against 40 central differences
+        try:
+            extras["adjoint"] = adjoint_leg(dev)
+        except Exception as e:  # noqa: BLE001
+            extras["adjoint_error"] = repr(e)
 
         if dist.rank == 0 and dist.world == 1:
             try:

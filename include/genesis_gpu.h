@@ -102,11 +102,12 @@ void gx_destroy(gx_handle* h);
 const char* gx_last_error(const gx_handle* h);
 const char* gx_status_string(int status);
 int gx_set_precision(gx_handle* h, int precision);
-/* Tuning knob of the mixed pair pass: 0 = automatic (tiled when every axis
- * has >= 3 force-grid cells), 1 = one thread per atom, 2 = warp-tiled with
- * ballot compaction, 3 = thread per atom with staged rows and per-thread
- * candidate lists (the automatic choice).  Results
- * are bit-identical across variants (fixed-point sums). */
+/* Tuning knob of the mixed pair pass: 0 = automatic (same as 4),
+ * 1 = one thread per atom over the canonical half shell, 2 = warp-tiled
+ * cell pairs with ballot compaction, 3 = thread per atom with staged rows,
+ * 4 = thread per atom with per-thread candidate lists.  Variants 2 and 3
+ * need >= 3 force-grid cells per axis and fall back to 1 otherwise.
+ * Results are bit-identical across variants (fixed-point sums). */
 int gx_set_kernel_variant(gx_handle* h, int variant);
 /* Autotuner: times `reps` mixed pair passes of every applicable variant on
  * the resident state (the state is left bit-identical: every variant gives
