@@ -39,6 +39,11 @@ FLOP_PER_PAIR_LJC = 75     # with Coulomb sharing the switch
 BYTES_PER_ATOM = {
     "kick": 72, "drift": 72, "wrap": 48, "cell_keys": 28, "cell_count": 4, "cell_scan": 0,
     "cell_scatter": 16, "reorder": 220, "stage_pos4": 45, "kinetic": 32,
+    # list path: fused kick + drift + wrap + FP32 staging + displacement test
+    # (read x v a 72, kind 1, home cell 4, reference float4 16; write x v 48,
+    # float4 16), and fused F -> a + kick + K (read F 24, v 24, 1/m 8, m 8;
+    # write a 24, v 24)
+    "nl_advance": 157, "nl_finish": 112,
 }
 
 
@@ -311,7 +316,7 @@ def ours_arm(args, dist):
     tick = run_ticks(h, wl, cfg, Wm, 0)
     h.synchronize()
     dist.barrier()
-    h.synchronize()
+    rb0 = h.list_rebuilds()  # synchronises
     clocks = Clocks(dev)
     clocks.start()
     l0 = h.launches
@@ -322,6 +327,7 @@ def ours_arm(args, dist):
     launches = h.launches - l0
     clk = clocks.stop()
     h.synchronize()
+    rebuilds = h.list_rebuilds() - rb0
     dist.barrier()
     ms_max = dist.max(ms)
     value = dist.world * u.n * K / (ms_max * 1e-3)
@@ -332,7 +338,7 @@ def ours_arm(args, dist):
     prof = h.profile_read(reset=True)
     h.profile(False)
     pairs = float(np.mean(st["pairs"]))
-    force_k = "force_mixed"
+    force_k = "force_nl" if "force_nl" in prof else "force_mixed"
     f_launch, f_ms = prof.get(force_k, (1, float("nan")))
     force_ms = f_ms / max(f_launch, 1)
     tot_ms = sum(v[1] for v in prof.values())
@@ -475,7 +481,8 @@ def ours_arm(args, dist):
                            cfg.thermostat_temperature, "electrostatics": cfg.enable_electrostatics,
                            "gr_every": wl.gr_every, "l2": "inputs larger than L2 (state ~300 MB > 126 MB); no flush",
                            "parallelism": f"{dist.world} independent replicas (one per GPU)",
-                           "pair_pass_variant": variant, "autotune_ms_per_pass": tune_ms,
+                           "pair_pass_variant": variant, "autotune_ms": tune_ms,
+                           "neighbour_list_rebuilds_in_timed_ticks": rebuilds,
                            "cuda_graph": True},
                 "gpu_launches": launches, "clocks": clk, "roofline": roof, "roofline_hbm": roof_hbm,
                 "kernels": kernels, "memory_kernels": mem, "pairs_per_tick": pairs}

@@ -60,6 +60,7 @@ EXPORTS = (
     "gx_radial_distribution_noalloc", "gx_set_kernel_variant", "gx_autotune",
     "gx_batch_create", "gx_batch_destroy", "gx_batch_last_error", "gx_batch_set_state",
     "gx_batch_step", "gx_batch_get_state", "gx_adjoint_forward", "gx_adjoint_backward",
+    "gx_set_list_skin", "gx_list_rebuilds",
 )
 
 _lib = None
@@ -111,6 +112,8 @@ def load(path: str | Path | None = None) -> C.CDLL:
         "gx_set_kernel_variant": (C.c_int, [vp, C.c_int]),
         "gx_autotune": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), dp]),
         "gx_adjoint_forward": (C.c_int, [vp, C.POINTER(GxAdjointSpec), dp, dp]),
+        "gx_set_list_skin": (C.c_int, [vp, _D]),
+        "gx_list_rebuilds": (C.c_int, [vp, u64p]),
         "gx_adjoint_backward": (C.c_int, [vp, dp, dp, dp, dp, dp, dp, dp]),
     }
     for name, (res, args) in proto.items():
@@ -232,16 +235,27 @@ class Handle:
 
     def set_kernel_variant(self, variant: int):
         """Mixed pair pass: 0 automatic, 1 thread per atom, 2 warp-tiled,
-        3 staged rows, 4 per-thread candidate lists."""
+        3 staged rows, 4 per-thread candidate lists, 5 persistent neighbour
+        list."""
         self._check(self.lib.gx_set_kernel_variant(self.h, variant))
 
     def autotune(self, reps: int = 5):
         """Times every applicable pair-pass variant and keeps the fastest;
-        returns (variant, {variant: ms per pass})."""
+        returns (variant, {variant: ms}) -- ms per pass for 1-4, ms per tick
+        for 5 and for 0 (the tick of the best of 1-4)."""
         best = C.c_int()
-        ms = np.full(5, -1.0)
+        ms = np.full(6, -1.0)
         self._check(self.lib.gx_autotune(self.h, reps, C.byref(best), _ptr(ms, C.c_double)))
         return best.value, {v: float(t) for v, t in enumerate(ms) if t >= 0}
+
+    def set_list_skin(self, skin: float):
+        """Skin of the variant-5 neighbour list (default 0.1 r_c)."""
+        self._check(self.lib.gx_set_list_skin(self.h, skin))
+
+    def list_rebuilds(self) -> int:
+        out = C.c_uint64()
+        self._check(self.lib.gx_list_rebuilds(self.h, C.byref(out)))
+        return out.value
 
     # -- systems ------------------------------------------------------------
     def half_kick(self):

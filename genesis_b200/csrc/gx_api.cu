@@ -278,6 +278,7 @@ int rebuild_cells(gx_handle* h) {
     launch_gather(h, src, h->buf[h->cur ^ 1], h->perm, h->key, h->key_sorted, n, h->pos_of_slot);
     h->cur ^= 1;
     h->sorted = true;
+    h->nl_valid = false;
     if (h->precision == GX_MIXED) launch_build_pos4(h, h->fgrid, h->buf[h->cur], h->key_sorted, n, h->pos4);
     return GX_OK;
 }
@@ -395,6 +396,7 @@ void gx_destroy(gx_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     invalidate_graphs(h);
     adjoint_free(h);
+    nl_free(h);
     free_buf(h->buf[0]);
     free_buf(h->buf[1]);
     cudaFree(h->key);
@@ -442,6 +444,7 @@ int gx_set_state(gx_handle* h, size_t n, const double* pos, const double* vel, c
     h->n = n;
     h->cur = 0;
     h->sorted = false;
+    h->nl_valid = false;
     h->lambda_pending = false;
     invalidate_graphs(h);
     StateBuf& b = h->buf[0];
@@ -665,7 +668,35 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
     // One tick.  With `uniform` the launch sequence does not depend on host
     // state, so it can be captured: the first kick always applies the lambda
     // slot (1.0 unless a Berendsen scale is pending; v * 1.0 == v) and resets it.
+    const bool use_nl = n && (h->kernel_variant == 5 || h->kernel_variant == 0) && nl_eligible(h);
+    if (use_nl) {
+        bool stale = false;
+        if ((rc = nl_prepare(h, &stale))) return rc;
+        if (stale) invalidate_graphs(h);
+    }
+    // One tick of the neighbour-list path (gx_nlist.cu): no buffer flip.
+    auto tick_nl = [&](bool uniform) -> int {
+        const bool pend = uniform || h->lambda_pending;
+        int nb = 0;
+        int r = nl_tick(h, pend ? h->dscal + 0 : nullptr, thermo ? kpart : nullptr, &nb);
+        if (r) return r;
+        if (pend) GX_LAUNCH(h, k_fill_d, 1, 32, h->dscal, 1, 1.0);
+        h->lambda_pending = false;
+        if (thermo) {
+            launch_thermostat_lambda(h, kpart, nb, h->p.thermal_constant, h->p.thermostat_temperature, tau, n,
+                                     h->dscal + 0, nullptr);
+            h->lambda_pending = true;
+        }
+        if (drec) {
+            launch_kinetic(h, h->buf[h->cur], n, h->lambda_pending ? h->dscal + 0 : nullptr, kpart, spart, &nb);
+            launch_finalize_sum(h, kpart, nb, h->dscal + 1);
+            launch_finalize_sum(h, spart, nb, h->dscal + 4);
+            GX_LAUNCH(h, k_record, 1, 1, drec, h->dscal, h->dcount, thermo ? 1 : 0);
+        }
+        return GX_OK;
+    };
     auto tick = [&](bool uniform) -> int {
+        if (use_nl) return tick_nl(uniform);
         const bool pend = uniform || h->lambda_pending;
         // VelocityHalfKick, with the previous tick's pending thermostat scale
         launch_kick(h, h->buf[h->cur], n, 0.5 * h->p.dt, pend ? h->dscal + 0 : nullptr);
@@ -698,7 +729,8 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
     if (drec) GX_CUDA(h, cudaMemsetAsync(h->dcount + 5, 0, sizeof(unsigned long long), h->stream));
     const bool graph = use_graph && n && !h->prof_on;
     const uint64_t key = ((uint64_t)n << 20) ^ ((uint64_t)h->precision << 1) ^ ((uint64_t)h->kernel_variant << 3) ^
-                         ((uint64_t)(h->nbonds > 0) << 6) ^ ((uint64_t)thermo << 7) ^ ((uint64_t)h->cap << 8) ^ 1u;
+                         ((uint64_t)(h->nbonds > 0) << 6) ^ ((uint64_t)thermo << 7) ^ ((uint64_t)h->cap << 8) ^
+                         ((uint64_t)use_nl << 62) ^ 1u;
     for (int s = 0; s < nsteps; ++s) {
         if (!graph) {
             if ((rc = tick(false))) return rc;
@@ -708,12 +740,14 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
         if (h->graph_exec[par][rs] && h->graph_key[par][rs] == key) {
             GX_CUDA(h, cudaGraphLaunch(h->graph_exec[par][rs], h->stream));
             h->launches += h->graph_kernels[par][rs];
-            h->cur ^= 1;  // the captured tick rebuilt the cell list into the other buffer
-            h->sorted = true;
+            if (!use_nl) {
+                h->cur ^= 1;  // the captured tick rebuilt the cell list into the other buffer
+                h->sorted = true;
+            }
             h->lambda_pending = thermo;
             continue;
         }
-        if (!h->sorted) {  // first tick runs eagerly: every buffer it needs gets allocated
+        if (!use_nl && !h->sorted) {  // first tick runs eagerly: every buffer it needs gets allocated
             if ((rc = tick(true))) return rc;
             continue;
         }
@@ -727,7 +761,7 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
         cudaError_t ce = cudaStreamEndCapture(h->stream, &gr);
         if (trc || ce != cudaSuccess) {
             if (gr) cudaGraphDestroy(gr);
-            h->cur ^= 1;  // capture did not execute: undo the host-side effects
+            if (!use_nl) h->cur ^= 1;  // capture did not execute: undo the host-side effects
             h->lambda_pending = pend0;
             return trc ? trc : cuda_err(h, ce, "cudaStreamEndCapture");
         }
@@ -740,6 +774,7 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
         h->graph_kernels[par][rs] = h->launches - l0;
         GX_CUDA(h, cudaGraphLaunch(ex, h->stream));  // the captured tick has not run yet: run it now
     }
+    if (use_nl) h->sorted = false;  // buf[cur] is ordered by the list grid, not the force grid
     if (drec) {
         GX_CUDA(h, cudaMemcpyAsync(stats, drec, (size_t)nsteps * sizeof(gx_tick_stats), cudaMemcpyDeviceToHost,
                                    h->stream));
@@ -758,7 +793,7 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
 }
 
 int gx_set_kernel_variant(gx_handle* h, int variant) {
-    if (!h || variant < 0 || variant > 4) return GX_ERR_ARG;
+    if (!h || variant < 0 || variant > 5) return GX_ERR_ARG;
     h->kernel_variant = variant;
     invalidate_graphs(h);
     return GX_OK;
@@ -768,7 +803,7 @@ int gx_autotune(gx_handle* h, int reps, int* best, double* ms) {
     int rc = require_state(h);
     if (rc) return rc;
     if (reps < 1) reps = 1;
-    for (int v = 0; v < 5; ++v)
+    for (int v = 0; v < 6; ++v)
         if (ms) ms[v] = -1.0;
     if (h->precision != GX_MIXED || h->n == 0) {
         if (best) *best = h->kernel_variant;
@@ -797,10 +832,70 @@ int gx_autotune(gx_handle* h, int reps, int* best, double* ms) {
             pick = v;
         }
     }
+    // The neighbour-list path (variant 5) changes the whole tick, so it is
+    // compared with the best single-pass variant over full ticks, each run
+    // from the same snapshot of (x, v, a, pending lambda) restored afterwards.
+    if (!rc && nl_eligible(h)) {
+        const uint32_t n = (uint32_t)h->n;
+        double* snap = nullptr;
+        if (cudaMalloc(&snap, 9 * (size_t)n * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            snap = nullptr;
+        }
+        if (snap) {
+            const bool pend0 = h->lambda_pending;
+            double lam0 = 1.0;
+            StateBuf& b0 = h->buf[h->cur];
+            GX_LAUNCH(h, k_soa_to_aos, nblk(n, 256), 256, b0.x, b0.y, b0.z, b0.slot, snap, n);
+            GX_LAUNCH(h, k_soa_to_aos, nblk(n, 256), 256, b0.vx, b0.vy, b0.vz, b0.slot, snap + 3 * (size_t)n, n);
+            GX_LAUNCH(h, k_soa_to_aos, nblk(n, 256), 256, b0.ax, b0.ay, b0.az, b0.slot, snap + 6 * (size_t)n, n);
+            cudaMemcpyAsync(&lam0, h->dscal, sizeof lam0, cudaMemcpyDeviceToHost, h->stream);
+            cudaStreamSynchronize(h->stream);
+            const int vs[2] = {pick, 5};
+            double tt[2] = {1e300, 1e300};
+            const int ticks = reps < 4 ? 4 : reps;
+            for (int q = 0; q < 2 && !rc; ++q) {
+                h->kernel_variant = vs[q];
+                invalidate_graphs(h);
+                double t = 0.0;
+                if (!(rc = gx_step(h, 2, nullptr, 1)) && !(rc = gx_timer_mark(h, 14)) &&
+                    !(rc = gx_step(h, ticks, nullptr, 1)) && !(rc = gx_timer_mark(h, 15)) &&
+                    !(rc = gx_timer_elapsed(h, 14, 15, &t)))
+                    tt[q] = t / ticks;
+                StateBuf& b = h->buf[h->cur];
+                GX_LAUNCH(h, k_aos_to_sorted, nblk(n, 256), 256, snap, h->pos_of_slot, b.x, b.y, b.z, n);
+                GX_LAUNCH(h, k_aos_to_sorted, nblk(n, 256), 256, snap + 3 * (size_t)n, h->pos_of_slot, b.vx, b.vy,
+                          b.vz, n);
+                GX_LAUNCH(h, k_aos_to_sorted, nblk(n, 256), 256, snap + 6 * (size_t)n, h->pos_of_slot, b.ax, b.ay,
+                          b.az, n);
+                cudaMemcpyAsync(h->dscal, &lam0, sizeof lam0, cudaMemcpyHostToDevice, h->stream);
+                cudaStreamSynchronize(h->stream);
+                h->lambda_pending = pend0;
+                h->sorted = false;
+            }
+            cudaFree(snap);
+            if (ms) {
+                ms[0] = tt[0] < 1e300 ? tt[0] : -1.0;
+                ms[5] = tt[1] < 1e300 ? tt[1] : -1.0;
+            }
+            if (!rc && tt[1] < tt[0]) pick = 5;
+        }
+    }
     h->kernel_variant = rc ? saved : pick;
     invalidate_graphs(h);
     if (best) *best = h->kernel_variant;
     return rc;
+}
+
+int gx_set_list_skin(gx_handle* h, double skin) {
+    if (!h || !(skin >= 0.0) || !std::isfinite(skin)) return GX_ERR_ARG;
+    invalidate_graphs(h);
+    return nl_set_skin(h, skin);
+}
+
+int gx_list_rebuilds(gx_handle* h, uint64_t* rebuilds) {
+    if (!h || !rebuilds) return GX_ERR_ARG;
+    return nl_rebuilds(h, rebuilds);
 }
 
 int gx_set_dynamic(gx_handle* h, const double* pos, const double* vel, const double* acc) {

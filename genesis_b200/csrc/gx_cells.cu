@@ -16,15 +16,22 @@ constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 4;
 constexpr int kScanTile = kScanThreads * kScanItems;
 
-__global__ void k_count(const uint32_t* __restrict__ key, uint32_t n, uint32_t* __restrict__ count) {
+// `gate` (may be null): when it points at 0 the kernel does nothing, so a
+// captured CUDA graph can carry a rebuild that runs only when requested.
+__device__ __forceinline__ bool gated_off(const uint32_t* gate) { return gate && *gate == 0u; }
+
+__global__ void k_count(const uint32_t* __restrict__ key, uint32_t n, uint32_t* __restrict__ count,
+                        const uint32_t* __restrict__ gate) {
+    if (gated_off(gate)) return;
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) atomicAdd(&count[key[i]], 1u);
 }
 
 // Exclusive scan of one tile of kScanTile elements; block total to sums.
 __global__ void __launch_bounds__(kScanThreads) k_scan_tile(const uint32_t* in, uint32_t* out, uint32_t n,
-                                                            uint32_t* sums) {
+                                                            uint32_t* sums, const uint32_t* __restrict__ gate) {
     __shared__ uint32_t warp_tot[kScanThreads / 32];
+    if (gated_off(gate)) return;
     uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
     uint32_t local = 0;
@@ -63,13 +70,16 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tile(const uint32_t* in, 
     }
 }
 
-__global__ void k_scan_add(uint32_t* out, uint32_t n, const uint32_t* offs) {
+__global__ void k_scan_add(uint32_t* out, uint32_t n, const uint32_t* offs, const uint32_t* __restrict__ gate) {
+    if (gated_off(gate)) return;
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] += offs[i / kScanTile];
 }
 
 __global__ void k_scatter(const uint32_t* __restrict__ key, uint32_t n, const uint32_t* __restrict__ start,
-                          uint32_t* __restrict__ fill, uint32_t* __restrict__ perm) {
+                          uint32_t* __restrict__ fill, uint32_t* __restrict__ perm,
+                          const uint32_t* __restrict__ gate) {
+    if (gated_off(gate)) return;
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     uint32_t c = key[i];
@@ -77,7 +87,9 @@ __global__ void k_scatter(const uint32_t* __restrict__ key, uint32_t n, const ui
 }
 
 // Makes the scatter deterministic: each cell's segment sorted by source index.
-__global__ void k_segsort(const uint32_t* __restrict__ start, uint32_t ncell, uint32_t* __restrict__ perm) {
+__global__ void k_segsort(const uint32_t* __restrict__ start, uint32_t ncell, uint32_t* __restrict__ perm,
+                          const uint32_t* __restrict__ gate) {
+    if (gated_off(gate)) return;
     uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncell) return;
     uint32_t lo = start[c], hi = start[c + 1];
@@ -94,7 +106,8 @@ __global__ void k_segsort(const uint32_t* __restrict__ start, uint32_t ncell, ui
 
 __global__ void k_cell_keys(GridGeom g, const double* __restrict__ x, const double* __restrict__ y,
                             const double* __restrict__ z, uint32_t n, uint32_t* __restrict__ key,
-                            uint32_t* __restrict__ err) {
+                            uint32_t* __restrict__ err, const uint32_t* __restrict__ gate) {
+    if (gated_off(gate)) return;
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double px = x[i], py = y[i], pz = z[i];
@@ -104,7 +117,8 @@ __global__ void k_cell_keys(GridGeom g, const double* __restrict__ x, const doub
 
 __global__ void k_gather(StateBuf s, StateBuf d, const uint32_t* __restrict__ perm,
                          const uint32_t* __restrict__ key_in, uint32_t* __restrict__ key_out, uint32_t n,
-                         uint32_t* __restrict__ pos_of_slot) {
+                         uint32_t* __restrict__ pos_of_slot, const uint32_t* __restrict__ gate) {
+    if (gated_off(gate)) return;
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     uint32_t q = perm[p];
@@ -292,48 +306,52 @@ int ensure_cells(gx_handle* h, CellList& cl, uint32_t ncell) {
     return GX_OK;
 }
 
-static void scan_rec(gx_handle* h, CellList& cl, const uint32_t* in, uint32_t* out, uint32_t n, int level) {
+static void scan_rec(gx_handle* h, CellList& cl, const uint32_t* in, uint32_t* out, uint32_t n, int level,
+                     const uint32_t* gate) {
     unsigned nb = (n + kScanTile - 1) / kScanTile;
     if (nb <= 1) {
-        GX_LAUNCH(h, k_scan_tile, 1, kScanThreads, in, out, n, nullptr);
+        GX_LAUNCH(h, k_scan_tile, 1, kScanThreads, in, out, n, nullptr, gate);
         return;
     }
     uint32_t* sums = cl.scan_levels[level];
-    GX_LAUNCH(h, k_scan_tile, nb, kScanThreads, in, out, n, sums);
-    scan_rec(h, cl, sums, sums, nb, level + 1);
-    GX_LAUNCH(h, k_scan_add, nblk(n, 256), 256, out, n, sums);
+    GX_LAUNCH(h, k_scan_tile, nb, kScanThreads, in, out, n, sums, gate);
+    scan_rec(h, cl, sums, sums, nb, level + 1, gate);
+    GX_LAUNCH(h, k_scan_add, nblk(n, 256), 256, out, n, sums, gate);
 }
 
-int counting_sort(gx_handle* h, CellList& cl, uint32_t ncell, const uint32_t* key, uint32_t n, uint32_t* perm) {
+int counting_sort(gx_handle* h, CellList& cl, uint32_t ncell, const uint32_t* key, uint32_t n, uint32_t* perm,
+                  const uint32_t* gate) {
     int rc = ensure_cells(h, cl, ncell);
     if (rc) return rc;
     prof_begin(h, "cell_count");
     GX_CUDA(h, cudaMemsetAsync(cl.count, 0, ((size_t)ncell + 1) * sizeof(uint32_t), h->stream));
     GX_CUDA(h, cudaMemsetAsync(cl.fill, 0, (size_t)ncell * sizeof(uint32_t), h->stream));
-    if (n) GX_LAUNCH(h, k_count, nblk(n, 256), 256, key, n, cl.count);
+    if (n) GX_LAUNCH(h, k_count, nblk(n, 256), 256, key, n, cl.count, gate);
     prof_end(h, "cell_count");
     prof_begin(h, "cell_scan");
-    scan_rec(h, cl, cl.count, cl.start, ncell + 1, 0);
+    scan_rec(h, cl, cl.count, cl.start, ncell + 1, 0, gate);
     prof_end(h, "cell_scan");
     prof_begin(h, "cell_scatter");
-    if (n) GX_LAUNCH(h, k_scatter, nblk(n, 256), 256, key, n, cl.start, cl.fill, perm);
-    GX_LAUNCH(h, k_segsort, nblk(ncell, 128), 128, cl.start, ncell, perm);
+    if (n) GX_LAUNCH(h, k_scatter, nblk(n, 256), 256, key, n, cl.start, cl.fill, perm, gate);
+    GX_LAUNCH(h, k_segsort, nblk(ncell, 128), 128, cl.start, ncell, perm, gate);
     prof_end(h, "cell_scatter");
     return GX_OK;
 }
 
-void launch_cell_keys(gx_handle* h, const GridGeom& g, const StateBuf& b, uint32_t n, uint32_t* key) {
+void launch_cell_keys(gx_handle* h, const GridGeom& g, const StateBuf& b, uint32_t n, uint32_t* key,
+                      const uint32_t* gate) {
     if (!n) return;
     prof_begin(h, "cell_keys");
-    GX_LAUNCH(h, k_cell_keys, nblk(n, 256), 256, g, b.x, b.y, b.z, n, key, h->derr);
+    GX_LAUNCH(h, k_cell_keys, nblk(n, 256), 256, g, b.x, b.y, b.z, n, key, h->derr, gate);
     prof_end(h, "cell_keys");
 }
 
 void launch_gather(gx_handle* h, const StateBuf& src, const StateBuf& dst, const uint32_t* perm,
-                   const uint32_t* key_in, uint32_t* key_out, uint32_t n, uint32_t* pos_of_slot) {
+                   const uint32_t* key_in, uint32_t* key_out, uint32_t n, uint32_t* pos_of_slot,
+                   const uint32_t* gate) {
     if (!n) return;
     prof_begin(h, "reorder");
-    GX_LAUNCH(h, k_gather, nblk(n, 256), 256, src, dst, perm, key_in, key_out, n, pos_of_slot);
+    GX_LAUNCH(h, k_gather, nblk(n, 256), 256, src, dst, perm, key_in, key_out, n, pos_of_slot, gate);
     prof_end(h, "reorder");
 }
 

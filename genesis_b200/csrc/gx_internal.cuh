@@ -227,6 +227,11 @@ struct gx_handle {
 
     // adjoint (gx_adjoint.cu): checkpoints and work buffers, owned there
     void* adj = nullptr;
+
+    // persistent neighbour list of the mixed pass (gx_nlist.cu), owned there;
+    // nl_valid: the list matches buf[cur]'s order and home cells
+    void* nl = nullptr;
+    bool nl_valid = false;
 };
 
 // Every kernel launch of the library goes through this macro so the
@@ -258,16 +263,27 @@ void prof_end(gx_handle* h, const char* name);
 int ensure_cells(gx_handle* h, CellList& cl, uint32_t ncell);
 // Counting sort of atoms [0,n) by key into perm (sorted pos -> source index),
 // deterministic (ties keep ascending source index).  cl.start gets cell starts.
+// `gate` (may be null): a device word; the launches do nothing while it is 0.
 int counting_sort(gx_handle* h, CellList& cl, uint32_t ncell, const uint32_t* key, uint32_t n,
-                  uint32_t* perm);
-void launch_cell_keys(gx_handle* h, const GridGeom& g, const StateBuf& b, uint32_t n, uint32_t* key);
+                  uint32_t* perm, const uint32_t* gate = nullptr);
+void launch_cell_keys(gx_handle* h, const GridGeom& g, const StateBuf& b, uint32_t n, uint32_t* key,
+                      const uint32_t* gate = nullptr);
 void launch_gather(gx_handle* h, const StateBuf& src, const StateBuf& dst, const uint32_t* perm,
-                   const uint32_t* key_in, uint32_t* key_out, uint32_t n, uint32_t* pos_of_slot);
+                   const uint32_t* key_in, uint32_t* key_out, uint32_t n, uint32_t* pos_of_slot,
+                   const uint32_t* gate = nullptr);
 void launch_build_pos4(gx_handle* h, const GridGeom& g, const StateBuf& b, const uint32_t* key,
                        uint32_t n, float4* pos4);
 
 int force_pass(gx_handle* h, bool finalize_acc, double* V, double* Vb, uint64_t* npairs, bool sync_out);
 void adjoint_free(gx_handle* h);
+
+// Neighbour-list path of the mixed pass (gx_nlist.cu).
+bool nl_eligible(gx_handle* h);
+int nl_prepare(gx_handle* h, bool* graphs_stale);
+int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nblocks);
+int nl_rebuilds(gx_handle* h, uint64_t* out);
+int nl_set_skin(gx_handle* h, double skin);
+void nl_free(gx_handle* h);
 
 void launch_kick(gx_handle* h, const StateBuf& b, uint32_t n, double half_dt, const double* lambda);
 void launch_drift(gx_handle* h, const StateBuf& b, uint32_t n, double dt);

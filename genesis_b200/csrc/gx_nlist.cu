@@ -1,0 +1,528 @@
+// gx_nlist.cu -- the mixed pair pass over a persistent neighbour list
+// (kernel variant 5).
+//
+// The reference rebuilds its cell list and pair list every tick
+// (ForceSystem::run, src/systems/forces.rs:228-232).  The pair SET it
+// evaluates is {pairs with d < r_c} at this tick, and the mixed path's sums
+// are order-independent integers, so any enumeration that yields exactly
+// that set gives the same forces.  Here a list of all pairs within
+// r_c + skin is built on a grid whose cells are at least r_c + skin wide and
+// reused while no atom has moved more than skin/2 since the build: then every
+// pair now within r_c was within r_c + skin at the build.  Between rebuilds
+// the atoms keep their sorted positions and their home cell, so the FP32
+// cell-local frame (offsets from the home cell's origin, |offset| below a
+// cell plus skin/2) keeps the same precision as the per-tick frame.
+//
+// The reference's wrap, x <- rem_euclid(x, 2h) - h (boundary.rs:28-34,
+// reproduced bit for bit), translates the whole periodic system by h = L/2
+// on every tick.  The list frame therefore co-moves: a device parity counts
+// those half-box translations since the last rebuild and the staging adds
+// them back, so only physical motion enters the displacement test (a wrong
+// parity reads as an L/2 jump, which forces a rebuild).
+//
+// One tick (all launches captured in one CUDA graph; the rebuild launches
+// read a device flag and do nothing when it is clear):
+//   k_nl_advance   kick (with the pending Berendsen scale), drift, wrap,
+//                  home-frame FP32 staging, displacement check -> flag
+//   [rebuild]      cell keys, counting sort, gather, copy back, staging,
+//                  list build
+//   k_nl_end       rebuild count, frame parity
+//   k_nl_force     one thread per atom over its full list: FP32 pair law,
+//                  fixed-point sums in registers, plain stores (no atomics);
+//                  the potential and pair count take each pair once (q > p)
+//   k_nl_finish    a = F 2^-32 / m, second kick, kinetic-energy partials
+// An atom whose list overflowed scans its 27 home-grid cells directly, so
+// the pair set stays exact whatever the local density.
+#include <cmath>
+#include <cstring>
+
+#include "gx_pair_f32.cuh"
+
+namespace gx {
+
+struct NlState {
+    GridGeom lg{};            // list grid: cells >= r_c + skin
+    double skin = -1.0;       // < 0: default (0.1 r_c)
+    double skin_used = 0.0;
+    int cap_nb = 0;           // list entries per atom
+    size_t cap = 0;           // atoms the buffers hold
+    uint32_t* list = nullptr; // entry e of atom p at list[e * cap + p]
+    uint32_t* cnt = nullptr;  // entries per atom (> cap_nb: overflowed)
+    float4* ref = nullptr;    // home-frame positions at the last rebuild
+    uint32_t* flag = nullptr; // [0] rebuild requested, [1] rebuilds done, [2] half-box translations since (mod 2)
+    CellList cl;
+};
+
+namespace {
+
+constexpr int kNlThreads = 128;
+constexpr int kRedThreads = 256;
+constexpr uint32_t kIdxMask = (1u << 27) - 1u;
+
+inline unsigned nblk(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+__device__ __forceinline__ bool gated_off(const uint32_t* gate) { return gate && *gate == 0u; }
+
+// Offset of a coordinate from its home cell's origin in the frame of the
+// last rebuild (`shift` = the translation to undo, 0 or L/2), unwrapped
+// across the periodic boundary (the atom may have left its home cell).
+__device__ __forceinline__ double home_local(double v, double L, double c, uint32_t i, double shift) {
+    double u = xsub(rem_euclid(xadd(xadd(v, xmul(0.5, L)), shift), L), xmul((double)i, c));
+    if (u > 0.5 * L) u = xsub(u, L);
+    else if (u < -0.5 * L) u = xadd(u, L);
+    return u;
+}
+
+__device__ __forceinline__ float4 stage_one(const GridGeom& g, const StateBuf& b, uint32_t home, uint32_t i,
+                                            double x, double y, double z, bool half) {
+    uint32_t ix, iy, iz;
+    decode(g, home, ix, iy, iz);
+    return make_float4((float)home_local(x, g.L[0], g.cell[0], ix, half ? xmul(0.5, g.L[0]) : 0.0),
+                       (float)home_local(y, g.L[1], g.cell[1], iy, half ? xmul(0.5, g.L[1]) : 0.0),
+                       (float)home_local(z, g.L[2], g.cell[2], iz, half ? xmul(0.5, g.L[2]) : 0.0),
+                       __int_as_float((int)b.kind[i]));
+}
+
+// Neighbour-cell code: (ox+1) + 3(oy+1) + 9(oz+1); 13 is the home cell.
+__device__ __forceinline__ void code_shift(const GridGeom& g, uint32_t code, float& sx, float& sy, float& sz) {
+    int ox = (int)(code % 3u) - 1, oy = (int)((code / 3u) % 3u) - 1, oz = (int)(code / 9u) - 1;
+    sx = -(float)ox * g.cellf[0];
+    sy = -(float)oy * g.cellf[1];
+    sz = -(float)oz * g.cellf[2];
+}
+
+__device__ __forceinline__ uint32_t cell_at(const GridGeom& g, uint32_t cx, uint32_t cy, uint32_t cz, uint32_t code) {
+    int ox = (int)(code % 3u) - 1, oy = (int)((code / 3u) % 3u) - 1, oz = (int)(code / 9u) - 1;
+    return encode(g, wrap_add(cx, ox, g.n[0]), wrap_add(cy, oy, g.n[1]), wrap_add(cz, oz, g.n[2]));
+}
+
+// Kick (integrate.rs:38-45, with the pending scale of thermostat.rs:68-70),
+// drift (integrate.rs:62-66), wrap (boundary.rs:28-34) with the same exact
+// FP64 operations as k_kick/k_drift/k_wrap; then the home-frame staging and
+// the displacement test against the last rebuild.
+__global__ void __launch_bounds__(256) k_nl_advance(StateBuf b, uint32_t n, const double* __restrict__ lambda,
+                                                     double half_dt, double dt, double hx, double hy, double hz,
+                                                     int wrap, GridGeom g, const uint32_t* __restrict__ home,
+                                                     float4* __restrict__ pos4, const float4* __restrict__ ref,
+                                                     float lim2, uint32_t* __restrict__ flag,
+                                                     uint32_t* __restrict__ err) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool over = false;
+    // translations since the rebuild, this tick's wrap included
+    const bool half = ((flag[2] + (wrap ? 1u : 0u)) & 1u) != 0u;
+    if (i < n) {
+        double vx = b.vx[i], vy = b.vy[i], vz = b.vz[i];
+        if (lambda) {
+            double l = *lambda;
+            vx = xmul(vx, l);
+            vy = xmul(vy, l);
+            vz = xmul(vz, l);
+        }
+        vx = xadd(vx, xmul(b.ax[i], half_dt));
+        vy = xadd(vy, xmul(b.ay[i], half_dt));
+        vz = xadd(vz, xmul(b.az[i], half_dt));
+        double x = xadd(b.x[i], xmul(vx, dt)), y = xadd(b.y[i], xmul(vy, dt)), z = xadd(b.z[i], xmul(vz, dt));
+        if (wrap) {
+            x = xsub(rem_euclid(x, xmul(2.0, hx)), hx);
+            y = xsub(rem_euclid(y, xmul(2.0, hy)), hy);
+            z = xsub(rem_euclid(z, xmul(2.0, hz)), hz);
+        }
+        b.vx[i] = vx;
+        b.vy[i] = vy;
+        b.vz[i] = vz;
+        b.x[i] = x;
+        b.y[i] = y;
+        b.z[i] = z;
+        if (!(isfinite(x) && isfinite(y) && isfinite(z))) {
+            atomicOr(err, kErrNonFinite);
+            over = true;
+        } else {
+            float4 p = stage_one(g, b, home[i], i, x, y, z, half);
+            pos4[i] = p;
+            float4 r = ref[i];
+            float dx = p.x - r.x, dy = p.y - r.y, dz = p.z - r.z;
+            over = !(dx * dx + dy * dy + dz * dz <= lim2);
+        }
+    }
+    if (__any_sync(0xffffffffu, over) && (threadIdx.x & 31) == 0) atomicOr(flag, 1u);
+}
+
+// buf[cur ^ 1] (just gathered) back into buf[cur], so the live state never
+// changes buffers and the captured tick does not depend on a parity.
+__global__ void k_nl_copy(StateBuf s, StateBuf d, uint32_t n, const uint32_t* __restrict__ gate) {
+    if (gated_off(gate)) return;
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    d.x[p] = s.x[p];
+    d.y[p] = s.y[p];
+    d.z[p] = s.z[p];
+    d.vx[p] = s.vx[p];
+    d.vy[p] = s.vy[p];
+    d.vz[p] = s.vz[p];
+    d.ax[p] = s.ax[p];
+    d.ay[p] = s.ay[p];
+    d.az[p] = s.az[p];
+    d.charge[p] = s.charge[p];
+    d.mass[p] = s.mass[p];
+    d.inv_mass[p] = s.inv_mass[p];
+    d.elem[p] = s.elem[p];
+    d.kind[p] = s.kind[p];
+    d.slot[p] = s.slot[p];
+}
+
+__global__ void k_nl_stage(GridGeom g, StateBuf b, const uint32_t* __restrict__ home, uint32_t n,
+                           float4* __restrict__ pos4, float4* __restrict__ ref, const uint32_t* __restrict__ gate) {
+    if (gated_off(gate)) return;
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 p = stage_one(g, b, home[i], i, b.x[i], b.y[i], b.z[i], false);
+    pos4[i] = p;
+    ref[i] = p;
+}
+
+// Full list of the pairs within r_l (r_l^2 = rl2) over the 27 home-grid cells.
+__global__ void __launch_bounds__(kNlThreads) k_nl_build(GridGeom g, const float4* __restrict__ pos4,
+                                                          const uint32_t* __restrict__ home,
+                                                          const uint32_t* __restrict__ start, uint32_t n, float rl2,
+                                                          uint32_t* __restrict__ list, size_t stride, int cap_nb,
+                                                          uint32_t* __restrict__ cnt, const uint32_t* __restrict__ gate) {
+    if (gated_off(gate)) return;
+    uint32_t p = blockIdx.x * kNlThreads + threadIdx.x;
+    if (p >= n) return;
+    float4 pi = pos4[p];
+    uint32_t cx, cy, cz;
+    decode(g, home[p], cx, cy, cz);
+    uint32_t m = 0;
+    for (uint32_t code = 0; code < 27; ++code) {
+        uint32_t B = cell_at(g, cx, cy, cz, code);
+        float sx, sy, sz;
+        code_shift(g, code, sx, sy, sz);
+        uint32_t lo = start[B], hi = start[B + 1];
+        for (uint32_t q = lo; q < hi; ++q) {
+            if (q == p) continue;
+            float4 pj = pos4[q];
+            float dx = delta1(pi.x, pj.x, sx), dy = delta1(pi.y, pj.y, sy), dz = delta1(pi.z, pj.z, sz);
+            if (dist2(dx, dy, dz) < rl2) {
+                if (m < (uint32_t)cap_nb) list[(size_t)m * stride + p] = q | (code << 27);
+                ++m;
+            }
+        }
+    }
+    cnt[p] = m;
+}
+
+// End of the list work of a tick: a rebuild starts a fresh frame; otherwise
+// this tick's wrap added one half-box translation.
+__global__ void k_nl_end(uint32_t* flag, int wrap) {
+    if (flag[0]) {
+        flag[1] += 1u;
+        flag[0] = 0u;
+        flag[2] = 0u;
+    } else if (wrap) {
+        flag[2] ^= 1u;
+    }
+}
+
+template <int BS>
+__device__ __forceinline__ unsigned long long block_sum_u(unsigned long long v, unsigned long long* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    v = (threadIdx.x < BS / 32) ? sh[threadIdx.x] : 0ull;
+    if (wid == 0) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    __syncthreads();
+    return v;
+}
+
+struct PairAcc {
+    long long fx = 0, fy = 0, fz = 0, vq = 0;
+    unsigned long long np = 0;
+};
+
+__device__ __forceinline__ void nl_pair(const LawF32& L, const PairF* st, int ki, float4 pi, float4 pj, float sx,
+                                        float sy, float sz, bool once, PairAcc& a, uint32_t* err) {
+    float dx = delta1(pi.x, pj.x, sx), dy = delta1(pi.y, pj.y, sy), dz = delta1(pi.z, pj.z, sz);
+    float d2 = dist2(dx, dy, dz);
+    if (!(d2 < L.rc2) || d2 == 0.f) return;
+    float fs, v;
+    pair_f32(L, st[ki * L.nkinds + __float_as_int(pj.w)], d2, fs, v);
+    a.fx += quant(fmul(dx, fs), err);
+    a.fy += quant(fmul(dy, fs), err);
+    a.fz += quant(fmul(dz, fs), err);
+    if (once) {
+        a.vq += quant(v, err);
+        ++a.np;
+    }
+}
+
+__global__ void __launch_bounds__(kNlThreads) k_nl_force(GridGeom g, const float4* __restrict__ pos4,
+                                                          const uint32_t* __restrict__ home,
+                                                          const uint32_t* __restrict__ start, uint32_t n, LawF32 L,
+                                                          const PairF* __restrict__ tab,
+                                                          const uint32_t* __restrict__ list, size_t stride,
+                                                          int cap_nb, const uint32_t* __restrict__ cnt,
+                                                          long long* __restrict__ F, size_t fstride,
+                                                          unsigned long long* __restrict__ vacc,
+                                                          unsigned long long* __restrict__ npairs,
+                                                          uint32_t* __restrict__ err) {
+    __shared__ PairF st[kMaxKinds * kMaxKinds];
+    __shared__ unsigned long long shu[kNlThreads / 32];
+    int nk2 = L.nkinds * L.nkinds;
+    for (int t = threadIdx.x; t < nk2; t += kNlThreads) st[t] = tab[t];
+    __syncthreads();
+    uint32_t p = blockIdx.x * kNlThreads + threadIdx.x;
+    PairAcc a;
+    if (p < n) {
+        float4 pi = pos4[p];
+        int ki = __float_as_int(pi.w);
+        uint32_t m = cnt[p];
+        if (m <= (uint32_t)cap_nb) {
+            for (uint32_t e = 0; e < m; ++e) {
+                uint32_t w = list[(size_t)e * stride + p];
+                uint32_t q = w & kIdxMask;
+                float sx, sy, sz;
+                code_shift(g, w >> 27, sx, sy, sz);
+                nl_pair(L, st, ki, pi, pos4[q], sx, sy, sz, q > p, a, err);
+            }
+        } else {  // overflowed list: scan the home-grid cells directly
+            uint32_t cx, cy, cz;
+            decode(g, home[p], cx, cy, cz);
+            for (uint32_t code = 0; code < 27; ++code) {
+                uint32_t B = cell_at(g, cx, cy, cz, code);
+                float sx, sy, sz;
+                code_shift(g, code, sx, sy, sz);
+                for (uint32_t q = start[B], hi = start[B + 1]; q < hi; ++q)
+                    if (q != p) nl_pair(L, st, ki, pi, pos4[q], sx, sy, sz, q > p, a, err);
+            }
+        }
+        F[p] = a.fx;
+        F[fstride + p] = a.fy;
+        F[2 * fstride + p] = a.fz;
+    }
+    unsigned long long s = block_sum_u<kNlThreads>((unsigned long long)a.vq, shu);
+    unsigned long long np = block_sum_u<kNlThreads>(a.np, shu);
+    if (threadIdx.x == 0) {
+        if (s) atomicAdd(vacc, s);
+        if (np) atomicAdd(npairs, np);
+    }
+}
+
+__global__ void k_nl_fix_to_double(const unsigned long long* __restrict__ v, double* out, double* zero) {
+    *out = xmul(__ll2double_rn((long long)*v), kFixInv);
+    *zero = 0.0;
+}
+
+template <int BS>
+__device__ __forceinline__ double block_sum_d(double v, double* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    v = (threadIdx.x < BS / 32) ? sh[threadIdx.x] : 0.0;
+    if (wid == 0) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    __syncthreads();
+    return v;
+}
+
+// a = F 2^-32 (1/m) (as k_fix_to_acc), v += a dt/2 (as k_kick), and with
+// THERMO the kinetic-energy partials of the new v with k_kinetic's block
+// mapping and operation order, so lambda is bit-identical to the unfused tick.
+template <bool THERMO>
+__global__ void __launch_bounds__(kRedThreads) k_nl_finish(StateBuf b, const long long* __restrict__ F,
+                                                           size_t fstride, uint32_t n, double half_dt,
+                                                           double* __restrict__ kpart) {
+    __shared__ double sh[kRedThreads / 32];
+    double ks = 0.0;
+    for (uint32_t i = blockIdx.x * kRedThreads + threadIdx.x; i < n; i += gridDim.x * kRedThreads) {
+        double im = b.inv_mass[i];
+        double ax = xmul(xmul(__ll2double_rn(F[i]), kFixInv), im);
+        double ay = xmul(xmul(__ll2double_rn(F[fstride + i]), kFixInv), im);
+        double az = xmul(xmul(__ll2double_rn(F[2 * fstride + i]), kFixInv), im);
+        b.ax[i] = ax;
+        b.ay[i] = ay;
+        b.az[i] = az;
+        double vx = xadd(b.vx[i], xmul(ax, half_dt));
+        double vy = xadd(b.vy[i], xmul(ay, half_dt));
+        double vz = xadd(b.vz[i], xmul(az, half_dt));
+        b.vx[i] = vx;
+        b.vy[i] = vy;
+        b.vz[i] = vz;
+        if (THERMO) {
+            double l2 = xadd(xadd(xmul(vx, vx), xmul(vy, vy)), xmul(vz, vz));
+            ks = xadd(ks, xmul(xmul(0.5, b.mass[i]), l2));
+        }
+    }
+    if (THERMO) {
+        ks = block_sum_d<kRedThreads>(ks, sh);
+        if (threadIdx.x == 0) kpart[blockIdx.x] = ks;
+    }
+}
+
+NlState* nl_of(gx_handle* h) {
+    if (!h->nl) h->nl = new NlState();
+    return static_cast<NlState*>(h->nl);
+}
+
+double skin_of(const gx_handle* h, const NlState* s) { return s->skin >= 0.0 ? s->skin : 0.1 * h->fs.rc; }
+
+}  // namespace
+
+void nl_free(gx_handle* h) {
+    if (!h || !h->nl) return;
+    NlState* s = static_cast<NlState*>(h->nl);
+    cudaFree(s->list);
+    cudaFree(s->cnt);
+    cudaFree(s->ref);
+    cudaFree(s->flag);
+    cudaFree(s->cl.count);
+    cudaFree(s->cl.start);
+    cudaFree(s->cl.fill);
+    for (auto q : s->cl.scan_levels) cudaFree(q);
+    delete s;
+    h->nl = nullptr;
+}
+
+// The list path applies to the mixed pass without gravity or bond springs,
+// with at least 3 list-grid cells per axis and atom indices below 2^27.
+bool nl_eligible(gx_handle* h) {
+    if (h->precision != GX_MIXED || h->p.enable_gravity) return false;
+    if (h->p.enable_bond_interaction && h->nbonds > 0) return false;
+    if (h->n == 0 || h->n >= (1u << 27)) return false;
+    NlState* s = nl_of(h);
+    double rl = h->fs.rc + skin_of(h, s);
+    int ok = 0;
+    GridGeom g = make_grid(h->p.box, rl, &ok);
+    return ok && g.n[0] >= 3 && g.n[1] >= 3 && g.n[2] >= 3;
+}
+
+// Allocates the list state (outside any capture) and requests a rebuild
+// when the handle's order no longer matches the list.
+int nl_prepare(gx_handle* h, bool* stale) {
+    NlState* s = nl_of(h);
+    *stale = false;
+    const double skin = skin_of(h, s);
+    int ok = 0;
+    GridGeom g = make_grid(h->p.box, h->fs.rc + skin, &ok);
+    if (!ok) return set_err(h, GX_ERR_ARG, "neighbour-list grid is empty or too large");
+    const double vol = h->p.box[0] * h->p.box[1] * h->p.box[2];
+    const double rl = h->fs.rc + skin;
+    const double expect = (double)h->n / vol * (4.0 / 3.0) * 3.14159265358979 * rl * rl * rl;
+    int cap_nb = (int)std::ceil(2.0 * expect) + 32;
+    cap_nb = (cap_nb + 7) & ~7;
+    if (cap_nb > 1024) cap_nb = 1024;
+    if (!s->flag) {
+        GX_CUDA(h, cudaMalloc(&s->flag, 4 * sizeof(uint32_t)));
+        GX_CUDA(h, cudaMemsetAsync(s->flag, 0, 4 * sizeof(uint32_t), h->stream));
+    }
+    if (s->cap < h->cap || s->cap_nb < cap_nb) {
+        cudaFree(s->list);
+        cudaFree(s->cnt);
+        cudaFree(s->ref);
+        s->list = nullptr;
+        s->cnt = nullptr;
+        s->ref = nullptr;
+        s->cap = 0;
+        GX_CUDA(h, cudaMalloc(&s->list, (size_t)cap_nb * h->cap * sizeof(uint32_t)));
+        GX_CUDA(h, cudaMalloc(&s->cnt, h->cap * sizeof(uint32_t)));
+        GX_CUDA(h, cudaMalloc(&s->ref, h->cap * sizeof(float4)));
+        GX_CUDA(h, cudaMemsetAsync(s->ref, 0, h->cap * sizeof(float4), h->stream));
+        s->cap = h->cap;
+        s->cap_nb = cap_nb;
+        h->nl_valid = false;
+        *stale = true;
+    }
+    if (std::memcmp(&g, &s->lg, sizeof g) != 0 || s->skin_used != skin) {
+        s->lg = g;
+        s->skin_used = skin;
+        h->nl_valid = false;
+        *stale = true;
+    }
+    const size_t cl_cap = s->cl.cap_cells;
+    int rc = ensure_cells(h, s->cl, g.ncell);
+    if (rc) return rc;
+    if (s->cl.cap_cells != cl_cap) *stale = true;
+    if (!h->nl_valid) {
+        const uint32_t one = 1u;
+        GX_CUDA(h, cudaMemcpyAsync(s->flag, &one, sizeof one, cudaMemcpyHostToDevice, h->stream));
+        h->nl_valid = true;
+    }
+    return GX_OK;
+}
+
+// One tick of the list path up to and including the second kick; with
+// `kpart` also the kinetic-energy partials (nb blocks) for the thermostat.
+int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nb_out) {
+    NlState* s = nl_of(h);
+    const uint32_t n = (uint32_t)h->n;
+    const GridGeom& g = s->lg;
+    StateBuf& b = h->buf[h->cur];
+    StateBuf& o = h->buf[h->cur ^ 1];
+    const double half_dt = 0.5 * h->p.dt;
+    const float lim = (float)(0.5 * s->skin_used * (1.0 - 1e-4));
+    prof_begin(h, "nl_advance");
+    GX_LAUNCH(h, k_nl_advance, nblk(n, 256), 256, b, n, lambda, half_dt, h->p.dt, 0.5 * h->p.box[0],
+              0.5 * h->p.box[1], 0.5 * h->p.box[2], h->p.enable_boundaries ? 1 : 0, g, h->key_sorted, h->pos4, s->ref,
+              lim * lim, s->flag, h->derr);
+    prof_end(h, "nl_advance");
+    prof_begin(h, "nl_rebuild");
+    launch_cell_keys(h, g, b, n, h->key, s->flag);
+    int rc = counting_sort(h, s->cl, g.ncell, h->key, n, h->perm, s->flag);
+    if (rc) return rc;
+    launch_gather(h, b, o, h->perm, h->key, h->key_sorted, n, h->pos_of_slot, s->flag);
+    GX_LAUNCH(h, k_nl_copy, nblk(n, 256), 256, o, b, n, s->flag);
+    GX_LAUNCH(h, k_nl_stage, nblk(n, 256), 256, g, b, h->key_sorted, n, h->pos4, s->ref, s->flag);
+    const float rl = (float)((h->fs.rc + s->skin_used) * (1.0 + 1e-6));
+    GX_LAUNCH(h, k_nl_build, nblk(n, kNlThreads), kNlThreads, g, h->pos4, h->key_sorted, s->cl.start, n, rl * rl,
+              s->list, s->cap, s->cap_nb, s->cnt, s->flag);
+    GX_LAUNCH(h, k_nl_end, 1, 1, s->flag, h->p.enable_boundaries ? 1 : 0);
+    prof_end(h, "nl_rebuild");
+    GX_CUDA(h, cudaMemsetAsync(h->dcount, 0, 4 * sizeof(unsigned long long), h->stream));
+    LawF32 L = make_law32(h);
+    prof_begin(h, "force_nl");
+    GX_LAUNCH(h, k_nl_force, nblk(n, kNlThreads), kNlThreads, g, h->pos4, h->key_sorted, s->cl.start, n, L,
+              h->d_pairf, s->list, s->cap, s->cap_nb, s->cnt, h->F, h->cap, h->dcount + 1, h->dcount + 0, h->derr);
+    prof_end(h, "force_nl");
+    GX_LAUNCH(h, k_nl_fix_to_double, 1, 1, h->dcount + 1, h->dscal + 2, h->dscal + 3);
+    int nb = (int)nblk(n, kRedThreads);
+    if (nb > 1184) nb = 1184;  // the block count of launch_kinetic
+    if (nb < 1) nb = 1;
+    prof_begin(h, "nl_finish");
+    if (kpart)
+        GX_LAUNCH(h, k_nl_finish<true>, nb, kRedThreads, b, h->F, h->cap, n, half_dt, kpart);
+    else
+        GX_LAUNCH(h, k_nl_finish<false>, nb, kRedThreads, b, h->F, h->cap, n, half_dt, nullptr);
+    prof_end(h, "nl_finish");
+    if (nb_out) *nb_out = nb;
+    return GX_OK;
+}
+
+// Rebuilds performed so far (reads the device counter; synchronises).
+int nl_rebuilds(gx_handle* h, uint64_t* out) {
+    *out = 0;
+    if (!h->nl) return GX_OK;
+    NlState* s = static_cast<NlState*>(h->nl);
+    if (!s->flag) return GX_OK;
+    uint32_t f[2] = {0, 0};
+    GX_CUDA(h, cudaMemcpyAsync(f, s->flag, sizeof f, cudaMemcpyDeviceToHost, h->stream));
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    *out = f[1];
+    return GX_OK;
+}
+
+int nl_set_skin(gx_handle* h, double skin) {
+    NlState* s = nl_of(h);
+    s->skin = skin;
+    h->nl_valid = false;
+    return GX_OK;
+}
+
+}  // namespace gx

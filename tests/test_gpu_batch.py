@@ -22,6 +22,7 @@ def _single(wl, steps):
     from genesis_b200._lib import Handle
     cfg = wl.config()
     h = Handle(cfg, "mixed")
+    h.set_kernel_variant(1)  # the batch re-sorts every tick, like variants 1-4
     u = wl.generate()
     h.set_universe(u)
     st = h.step(steps)

@@ -1,0 +1,138 @@
+"""The persistent neighbour-list pass (kernel variant 5) against the oracle
+and against the per-tick re-sort variants.
+
+Variant 5 evaluates the same pair set {d < r_c} as every other variant, in a
+cell-local frame anchored at the last rebuild, so its FP32 forces can differ
+from variants 1-4 in the last bits: the checks are the mixed path's error
+bound against the FP64 oracle (force rel-RMS <= 1e-5), agreement of whole
+trajectories with variant 1, exact pair counts, determinism, and the
+overflow fallback (atoms whose list overflows scan their cells directly).
+"""
+from __future__ import annotations
+
+import dataclasses
+
+import numpy as np
+import pytest
+
+from genesis_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+MIXED_RMS = 1e-5
+
+
+def _handle(cfg, variant=5):
+    from genesis_b200._lib import Handle
+    h = Handle(cfg, "mixed")
+    h.set_kernel_variant(variant)
+    return h
+
+
+def _lattice(n_side=16, temperature=60.0, coul=False, seed=0):
+    wl = W.Workload("nl check", n_side=n_side, temperature=temperature, steps=10, seed=seed,
+                    electrostatics=coul)
+    return wl.config(), wl.generate()
+
+
+def _relnorm(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.mark.parametrize("coul", [False, True])
+def test_first_tick_forces_match_fp64_oracle(gpu, orc, coul):
+    cfg, u = _lattice(18, coul=coul)
+    h = _handle(cfg)
+    h.set_universe(u)
+    st = h.step(1)
+    _, _, acc = h.get_state()
+    _, _, acc_ref, st_ref = orc.ticks(cfg, u.pos, u.vel, None, u.elem, u.charge, u.mass, 1)
+    assert _relnorm(acc, acc_ref) <= MIXED_RMS
+    assert abs(st["potential"][0] - st_ref[0, 1]) <= 1e-5 * abs(st_ref[0, 1])
+    assert abs(int(st["pairs"][0]) - int(st_ref[0, 4])) <= 2
+
+
+@pytest.mark.parametrize("thermo", [False, True])
+def test_trajectory_follows_per_tick_variant(gpu, thermo):
+    cfg, u = _lattice(16, temperature=120.0, coul=True)
+    if thermo:
+        cfg.enable_thermostat = True
+        cfg.thermostat_temperature = 40.0
+    out = []
+    for variant in (1, 5):
+        h = _handle(cfg, variant)
+        h.set_universe(u)
+        st = h.step(40)
+        out.append((h.get_state(), st, h))
+    (p1, v1, a1), s1, _ = out[0]
+    (p5, v5, a5), s5, h5 = out[1]
+    assert np.max(np.abs(p1 - p5)) <= 1e-6
+    assert _relnorm(v5, v1) <= 1e-5
+    assert np.max(np.abs(s5["potential"] - s1["potential"]) / np.abs(s1["potential"])) <= 1e-5
+    assert np.max(np.abs(s5["pairs"].astype(np.int64) - s1["pairs"].astype(np.int64))) <= 2
+    if thermo:
+        assert np.max(np.abs(s5["lambda"] - s1["lambda"])) <= 1e-6
+    assert h5.list_rebuilds() >= 1
+
+
+def test_zero_skin_rebuilds_every_tick(gpu):
+    cfg, u = _lattice(12)
+    h = _handle(cfg)
+    h.set_list_skin(0.0)
+    h.set_universe(u)
+    h.step(7)
+    assert h.list_rebuilds() == 7
+
+
+def test_default_skin_reuses_the_list(gpu):
+    cfg, u = _lattice(14, temperature=20.0)
+    h = _handle(cfg)
+    h.set_universe(u)
+    h.step(30)
+    assert 1 <= h.list_rebuilds() < 30
+
+
+def test_list_path_is_deterministic_and_graph_invariant(gpu):
+    cfg, u = _lattice(14, coul=True)
+    runs = []
+    for graph in (False, True, True):
+        h = _handle(cfg)
+        h.set_universe(u)
+        st = h.step(12, graph=graph)
+        runs.append((h.get_state(), st))
+    for r in runs[1:]:
+        for x, y in zip(runs[0][0], r[0]):
+            assert np.array_equal(x, y)
+        assert np.array_equal(runs[0][1], r[1])
+
+
+def test_overflowing_lists_fall_back_to_cell_scans(gpu, orc):
+    # a dense clump far above the average density overflows the per-atom lists
+    cfg, u = _lattice(12, temperature=10.0)
+    rng = np.random.default_rng(4)
+    pos = u.pos.copy()
+    k = 300
+    d = rng.normal(size=(k, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r = 4.0 * rng.random(k) ** (1.0 / 3.0) + 0.3
+    pos[:k] = d * r[:, None]
+    u2 = dataclasses.replace(u, pos=pos)
+    h = _handle(cfg)
+    h.set_universe(u2)
+    st = h.step(1)
+    _, _, acc = h.get_state()
+    _, _, acc_ref, st_ref = orc.ticks(cfg, u2.pos, u2.vel, None, u2.elem, u2.charge, u2.mass, 1)
+    assert _relnorm(acc, acc_ref) <= MIXED_RMS
+    assert abs(int(st["pairs"][0]) - int(st_ref[0, 4])) <= 2
+
+
+def test_state_round_trip_after_list_ticks(gpu):
+    # set_dynamic after list ticks writes through the list-grid order
+    cfg, u = _lattice(12)
+    h = _handle(cfg)
+    h.set_universe(u)
+    h.step(5)
+    pos, vel, acc = h.get_state()
+    h.set_dynamic(pos, vel, acc)
+    p2, v2, a2 = h.get_state()
+    assert np.array_equal(pos, p2) and np.array_equal(vel, v2) and np.array_equal(acc, a2)

@@ -267,8 +267,8 @@ def test_mixed_kernel_variants_bit_identical(gpu, ionic):
         assert np.array_equal(out[0][3], o[3])
 
 
-@pytest.mark.parametrize("prec", ["fp64", "mixed"])
-def test_graph_replay_matches_eager_ticks(gpu, prec):
+@pytest.mark.parametrize("prec,variant", [("fp64", 0), ("mixed", 1), ("mixed", 5)])
+def test_graph_replay_matches_eager_ticks(gpu, prec, variant):
     wl, cfg, u = _c1(n_side=12)
     cfg.enable_thermostat = True
     cfg.thermostat_temperature = 30.0
@@ -276,6 +276,7 @@ def test_graph_replay_matches_eager_ticks(gpu, prec):
     res = []
     for graph in (False, True):
         h = _handle(cfg, prec)
+        h.set_kernel_variant(variant)
         h.set_universe(u)
         parts = [h.step(3, graph=graph), h.step(6, graph=graph)]
         h.step(1, stats=False, graph=graph)
@@ -294,7 +295,8 @@ def test_autotune_leaves_state_unchanged(gpu):
     a.step(2)
     before = a.get_state()
     best, ms = a.autotune(reps=2)
-    assert best in ms and best in (1, 2, 3, 4)
+    assert best in ms and best in (1, 2, 3, 4, 5)
+    assert 5 in ms and 0 in ms  # the list path was timed against the best single-pass tick
     after = a.get_state()
     for x, y in zip(before, after):
         assert np.array_equal(x, y)
