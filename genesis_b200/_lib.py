@@ -235,16 +235,16 @@ class Handle:
 
     def set_kernel_variant(self, variant: int):
         """Mixed pair pass: 0 automatic, 1 thread per atom, 2 warp-tiled,
-        3 staged rows, 4 per-thread candidate lists, 5 persistent neighbour
-        list."""
+        3 staged rows, 4 per-thread candidate lists, 5 persistent full
+        neighbour list, 6 persistent half list with far-end atomics."""
         self._check(self.lib.gx_set_kernel_variant(self.h, variant))
 
     def autotune(self, reps: int = 5):
         """Times every applicable pair-pass variant and keeps the fastest;
         returns (variant, {variant: ms}) -- ms per pass for 1-4, ms per tick
-        for 5 and for 0 (the tick of the best of 1-4)."""
+        for 5, 6 and 0 (the tick of the best of 1-4)."""
         best = C.c_int()
-        ms = np.full(6, -1.0)
+        ms = np.full(7, -1.0)
         self._check(self.lib.gx_autotune(self.h, reps, C.byref(best), _ptr(ms, C.c_double)))
         return best.value, {v: float(t) for v, t in enumerate(ms) if t >= 0}
 

@@ -668,7 +668,7 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
     // One tick.  With `uniform` the launch sequence does not depend on host
     // state, so it can be captured: the first kick always applies the lambda
     // slot (1.0 unless a Berendsen scale is pending; v * 1.0 == v) and resets it.
-    const bool use_nl = n && (h->kernel_variant == 5 || h->kernel_variant == 0) && nl_eligible(h);
+    const bool use_nl = n && (h->kernel_variant >= 5 || h->kernel_variant == 0) && nl_eligible(h);
     if (use_nl) {
         bool stale = false;
         if ((rc = nl_prepare(h, &stale))) return rc;
@@ -793,7 +793,7 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
 }
 
 int gx_set_kernel_variant(gx_handle* h, int variant) {
-    if (!h || variant < 0 || variant > 5) return GX_ERR_ARG;
+    if (!h || variant < 0 || variant > 6) return GX_ERR_ARG;
     h->kernel_variant = variant;
     invalidate_graphs(h);
     return GX_OK;
@@ -803,7 +803,7 @@ int gx_autotune(gx_handle* h, int reps, int* best, double* ms) {
     int rc = require_state(h);
     if (rc) return rc;
     if (reps < 1) reps = 1;
-    for (int v = 0; v < 6; ++v)
+    for (int v = 0; v < 7; ++v)
         if (ms) ms[v] = -1.0;
     if (h->precision != GX_MIXED || h->n == 0) {
         if (best) *best = h->kernel_variant;
@@ -851,10 +851,10 @@ int gx_autotune(gx_handle* h, int reps, int* best, double* ms) {
             GX_LAUNCH(h, k_soa_to_aos, nblk(n, 256), 256, b0.ax, b0.ay, b0.az, b0.slot, snap + 6 * (size_t)n, n);
             cudaMemcpyAsync(&lam0, h->dscal, sizeof lam0, cudaMemcpyDeviceToHost, h->stream);
             cudaStreamSynchronize(h->stream);
-            const int vs[2] = {pick, 5};
-            double tt[2] = {1e300, 1e300};
-            const int ticks = reps < 4 ? 4 : reps;
-            for (int q = 0; q < 2 && !rc; ++q) {
+            const int vs[3] = {pick, 5, 6};
+            double tt[3] = {1e300, 1e300, 1e300};
+            const int ticks = reps < 20 ? 20 : reps;  // long enough to include list rebuilds
+            for (int q = 0; q < 3 && !rc; ++q) {
                 h->kernel_variant = vs[q];
                 invalidate_graphs(h);
                 double t = 0.0;
@@ -877,8 +877,13 @@ int gx_autotune(gx_handle* h, int reps, int* best, double* ms) {
             if (ms) {
                 ms[0] = tt[0] < 1e300 ? tt[0] : -1.0;
                 ms[5] = tt[1] < 1e300 ? tt[1] : -1.0;
+                ms[6] = tt[2] < 1e300 ? tt[2] : -1.0;
             }
-            if (!rc && tt[1] < tt[0]) pick = 5;
+            if (!rc) {
+                int q = tt[1] < tt[0] ? 1 : 0;
+                if (tt[2] < tt[q]) q = 2;
+                pick = vs[q];
+            }
         }
     }
     h->kernel_variant = rc ? saved : pick;

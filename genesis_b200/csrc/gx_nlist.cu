@@ -1,5 +1,5 @@
 // gx_nlist.cu -- the mixed pair pass over a persistent neighbour list
-// (kernel variant 5).
+// (kernel variants 5 and 6).
 //
 // The reference rebuilds its cell list and pair list every tick
 // (ForceSystem::run, src/systems/forces.rs:228-232).  The pair SET it
@@ -44,6 +44,7 @@ struct NlState {
     GridGeom lg{};            // list grid: cells >= r_c + skin
     double skin = -1.0;       // < 0: default (0.1 r_c)
     double skin_used = 0.0;
+    int half = -1;            // list kind built: 0 full, 1 half (variant 6)
     int cap_nb = 0;           // list entries per atom
     size_t cap = 0;           // atoms the buffers hold
     uint32_t* list = nullptr; // entry e of atom p at list[e * cap + p]
@@ -180,7 +181,10 @@ __global__ void k_nl_stage(GridGeom g, StateBuf b, const uint32_t* __restrict__ 
     ref[i] = p;
 }
 
-// Full list of the pairs within r_l (r_l^2 = rl2) over the 27 home-grid cells.
+// List of the pairs within r_l (r_l^2 = rl2) over the 27 home-grid cells:
+// every neighbour (full list), or with HALF only those at a later sorted
+// position (each pair once).
+template <bool HALF>
 __global__ void __launch_bounds__(kNlThreads) k_nl_build(GridGeom g, const float4* __restrict__ pos4,
                                                           const uint32_t* __restrict__ home,
                                                           const uint32_t* __restrict__ start, uint32_t n, float rl2,
@@ -190,19 +194,23 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_build(GridGeom g, const float
     uint32_t p = blockIdx.x * kNlThreads + threadIdx.x;
     if (p >= n) return;
     float4 pi = pos4[p];
+    const uint32_t c = home[p];
     uint32_t cx, cy, cz;
-    decode(g, home[p], cx, cy, cz);
+    decode(g, c, cx, cy, cz);
     uint32_t m = 0;
     for (uint32_t code = 0; code < 27; ++code) {
         uint32_t B = cell_at(g, cx, cy, cz, code);
+        // atoms are sorted by cell: a lower cell index means every q < p
+        if (HALF && B < c) continue;
         float sx, sy, sz;
         code_shift(g, code, sx, sy, sz);
         uint32_t lo = start[B], hi = start[B + 1];
+        if (HALF && B == c) lo = p + 1;
         for (uint32_t q = lo; q < hi; ++q) {
             if (q == p) continue;
             float4 pj = pos4[q];
             float dx = delta1(pi.x, pj.x, sx), dy = delta1(pi.y, pj.y, sy), dz = delta1(pi.z, pj.z, sz);
-            if (dist2(dx, dy, dz) < rl2) {
+            if (dist2(dx, dy, dz) < rl2 && (!HALF || q > p)) {
                 if (m < (uint32_t)cap_nb) list[(size_t)m * stride + p] = q | (code << 27);
                 ++m;
             }
@@ -244,22 +252,34 @@ struct PairAcc {
     unsigned long long np = 0;
 };
 
+// far != null: also subtract the pair force from the far end q (HALF lists).
 __device__ __forceinline__ void nl_pair(const LawF32& L, const PairF* st, int ki, float4 pi, float4 pj, float sx,
-                                        float sy, float sz, bool once, PairAcc& a, uint32_t* err) {
+                                        float sy, float sz, bool once, PairAcc& a, uint32_t* err,
+                                        long long* far = nullptr, uint32_t q = 0, size_t fstride = 0) {
     float dx = delta1(pi.x, pj.x, sx), dy = delta1(pi.y, pj.y, sy), dz = delta1(pi.z, pj.z, sz);
     float d2 = dist2(dx, dy, dz);
     if (!(d2 < L.rc2) || d2 == 0.f) return;
     float fs, v;
     pair_f32(L, st[ki * L.nkinds + __float_as_int(pj.w)], d2, fs, v);
-    a.fx += quant(fmul(dx, fs), err);
-    a.fy += quant(fmul(dy, fs), err);
-    a.fz += quant(fmul(dz, fs), err);
+    long long qx = quant(fmul(dx, fs), err), qy = quant(fmul(dy, fs), err), qz = quant(fmul(dz, fs), err);
+    a.fx += qx;
+    a.fy += qy;
+    a.fz += qz;
+    if (far) {
+        atomicAdd((unsigned long long*)&far[q], (unsigned long long)(-qx));
+        atomicAdd((unsigned long long*)&far[fstride + q], (unsigned long long)(-qy));
+        atomicAdd((unsigned long long*)&far[2 * fstride + q], (unsigned long long)(-qz));
+    }
     if (once) {
         a.vq += quant(v, err);
         ++a.np;
     }
 }
 
+// Full list: each thread sums its own atom's forces and stores them.  HALF:
+// each pair once, the far end's force through 64-bit integer atomics (F must
+// be zero on entry); both give the same fixed-point sums.
+template <bool HALF>
 __global__ void __launch_bounds__(kNlThreads) k_nl_force(GridGeom g, const float4* __restrict__ pos4,
                                                           const uint32_t* __restrict__ home,
                                                           const uint32_t* __restrict__ start, uint32_t n, LawF32 L,
@@ -271,9 +291,15 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force(GridGeom g, const float
                                                           unsigned long long* __restrict__ npairs,
                                                           uint32_t* __restrict__ err) {
     __shared__ PairF st[kMaxKinds * kMaxKinds];
+    __shared__ float4 s_shift[27];
     __shared__ unsigned long long shu[kNlThreads / 32];
     int nk2 = L.nkinds * L.nkinds;
     for (int t = threadIdx.x; t < nk2; t += kNlThreads) st[t] = tab[t];
+    if (threadIdx.x < 27) {
+        float sx, sy, sz;
+        code_shift(g, threadIdx.x, sx, sy, sz);
+        s_shift[threadIdx.x] = make_float4(sx, sy, sz, 0.f);
+    }
     __syncthreads();
     uint32_t p = blockIdx.x * kNlThreads + threadIdx.x;
     PairAcc a;
@@ -282,27 +308,52 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force(GridGeom g, const float
         int ki = __float_as_int(pi.w);
         uint32_t m = cnt[p];
         if (m <= (uint32_t)cap_nb) {
-            for (uint32_t e = 0; e < m; ++e) {
-                uint32_t w = list[(size_t)e * stride + p];
+            // four entries per round, every load issued before any pair math
+            const uint32_t* lp = list + p;
+            uint32_t e = 0;
+            for (; e + 4 <= m; e += 4) {
+                uint32_t w[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) w[k] = __ldg(lp + (size_t)(e + k) * stride);
+                float4 pj[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) pj[k] = __ldg(pos4 + (w[k] & kIdxMask));
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    float4 sh = s_shift[w[k] >> 27];
+                    uint32_t q = w[k] & kIdxMask;
+                    nl_pair(L, st, ki, pi, pj[k], sh.x, sh.y, sh.z, q > p, a, err, HALF ? F : nullptr, q, fstride);
+                }
+            }
+            for (; e < m; ++e) {
+                uint32_t w = __ldg(lp + (size_t)e * stride);
+                float4 sh = s_shift[w >> 27];
                 uint32_t q = w & kIdxMask;
-                float sx, sy, sz;
-                code_shift(g, w >> 27, sx, sy, sz);
-                nl_pair(L, st, ki, pi, pos4[q], sx, sy, sz, q > p, a, err);
+                nl_pair(L, st, ki, pi, __ldg(pos4 + q), sh.x, sh.y, sh.z, q > p, a, err, HALF ? F : nullptr, q, fstride);
             }
         } else {  // overflowed list: scan the home-grid cells directly
             uint32_t cx, cy, cz;
             decode(g, home[p], cx, cy, cz);
+            const uint32_t c = home[p];
             for (uint32_t code = 0; code < 27; ++code) {
                 uint32_t B = cell_at(g, cx, cy, cz, code);
+                if (HALF && B < c) continue;
                 float sx, sy, sz;
                 code_shift(g, code, sx, sy, sz);
                 for (uint32_t q = start[B], hi = start[B + 1]; q < hi; ++q)
-                    if (q != p) nl_pair(L, st, ki, pi, pos4[q], sx, sy, sz, q > p, a, err);
+                    if (HALF ? q > p : q != p)
+                        nl_pair(L, st, ki, pi, pos4[q], sx, sy, sz, q > p, a, err, HALF ? F : nullptr, q, fstride);
             }
         }
-        F[p] = a.fx;
-        F[fstride + p] = a.fy;
-        F[2 * fstride + p] = a.fz;
+        if (HALF) {
+            atomicAdd((unsigned long long*)&F[p], (unsigned long long)a.fx);
+            atomicAdd((unsigned long long*)&F[fstride + p], (unsigned long long)a.fy);
+            atomicAdd((unsigned long long*)&F[2 * fstride + p], (unsigned long long)a.fz);
+        } else {
+            F[p] = a.fx;
+            F[fstride + p] = a.fy;
+            F[2 * fstride + p] = a.fz;
+        }
     }
     unsigned long long s = block_sum_u<kNlThreads>((unsigned long long)a.vq, shu);
     unsigned long long np = block_sum_u<kNlThreads>(a.np, shu);
@@ -440,6 +491,12 @@ int nl_prepare(gx_handle* h, bool* stale) {
         h->nl_valid = false;
         *stale = true;
     }
+    const int half = h->kernel_variant == 5 ? 0 : 1;  // 6 and automatic: half list
+    if (half != s->half) {
+        s->half = half;
+        h->nl_valid = false;
+        *stale = true;
+    }
     if (std::memcmp(&g, &s->lg, sizeof g) != 0 || s->skin_used != skin) {
         s->lg = g;
         s->skin_used = skin;
@@ -481,14 +538,18 @@ int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nb_out) {
     GX_LAUNCH(h, k_nl_copy, nblk(n, 256), 256, o, b, n, s->flag);
     GX_LAUNCH(h, k_nl_stage, nblk(n, 256), 256, g, b, h->key_sorted, n, h->pos4, s->ref, s->flag);
     const float rl = (float)((h->fs.rc + s->skin_used) * (1.0 + 1e-6));
-    GX_LAUNCH(h, k_nl_build, nblk(n, kNlThreads), kNlThreads, g, h->pos4, h->key_sorted, s->cl.start, n, rl * rl,
+    const bool halfl = s->half == 1;
+    auto build = halfl ? k_nl_build<true> : k_nl_build<false>;
+    GX_LAUNCH(h, build, nblk(n, kNlThreads), kNlThreads, g, h->pos4, h->key_sorted, s->cl.start, n, rl * rl,
               s->list, s->cap, s->cap_nb, s->cnt, s->flag);
     GX_LAUNCH(h, k_nl_end, 1, 1, s->flag, h->p.enable_boundaries ? 1 : 0);
     prof_end(h, "nl_rebuild");
     GX_CUDA(h, cudaMemsetAsync(h->dcount, 0, 4 * sizeof(unsigned long long), h->stream));
     LawF32 L = make_law32(h);
     prof_begin(h, "force_nl");
-    GX_LAUNCH(h, k_nl_force, nblk(n, kNlThreads), kNlThreads, g, h->pos4, h->key_sorted, s->cl.start, n, L,
+    if (halfl) GX_CUDA(h, cudaMemsetAsync(h->F, 0, 3 * h->cap * sizeof(long long), h->stream));
+    auto force = halfl ? k_nl_force<true> : k_nl_force<false>;
+    GX_LAUNCH(h, force, nblk(n, kNlThreads), kNlThreads, g, h->pos4, h->key_sorted, s->cl.start, n, L,
               h->d_pairf, s->list, s->cap, s->cap_nb, s->cnt, h->F, h->cap, h->dcount + 1, h->dcount + 0, h->derr);
     prof_end(h, "force_nl");
     GX_LAUNCH(h, k_nl_fix_to_double, 1, 1, h->dcount + 1, h->dscal + 2, h->dscal + 3);

@@ -102,33 +102,37 @@ void gx_destroy(gx_handle* h);
 const char* gx_last_error(const gx_handle* h);
 const char* gx_status_string(int status);
 int gx_set_precision(gx_handle* h, int precision);
-/* Tuning knob of the mixed pair pass: 0 = automatic (5 where it applies,
+/* Tuning knob of the mixed pair pass: 0 = automatic (6 where it applies,
  * else 4), 1 = one thread per atom over the canonical half shell,
  * 2 = warp-tiled cell pairs with ballot compaction, 3 = thread per atom with
  * staged rows, 4 = thread per atom with per-thread candidate lists (all
  * four re-sort the atoms by the force grid every tick, as the reference
  * rebuilds its grid, src/systems/forces.rs:228-232), 5 = persistent
  * neighbour list: pairs within r_c + skin on a grid of cells >= r_c + skin,
- * rebuilt (re-sort included) only when an atom has moved more than skin/2;
- * needs no gravity, no bond spring and >= 3 list-grid cells per axis, else
- * it falls back to 4.  Variants 2 and 3 need >= 3 force-grid cells per axis
- * and fall back to 1 otherwise.  Variants 1-4 give bit-identical forces
- * (fixed-point sums); 5 evaluates the same pair set in a cell-local frame
- * whose origin is the atom's cell at the last rebuild, so its FP32 forces
- * can differ from 1-4 in the last bits (same error bound). */
+ * rebuilt (re-sort included) only when an atom has moved more than skin/2,
+ * one thread per atom over its full list, no atomics; 6 = the same with a
+ * half list (each pair once, the far end's force through integer atomics).
+ * 5 and 6 need no gravity, no bond spring and >= 3 list-grid cells per
+ * axis, else they fall back to 4.  Variants 2 and 3 need >= 3 force-grid
+ * cells per axis and fall back to 1 otherwise.  Variants 1-4 give
+ * bit-identical forces, and so do 5 and 6 (fixed-point sums); 5 and 6
+ * evaluate the same pair set in a cell-local frame whose origin is the
+ * atom's cell at the last rebuild, so their FP32 forces can differ from 1-4
+ * in the last bits (same error bound). */
 int gx_set_kernel_variant(gx_handle* h, int variant);
 /* Autotuner: times `reps` mixed pair passes of variants 1-4 on the resident
  * state (left bit-identical: they give the same fixed-point sums) and, where
- * variant 5 applies, full ticks of the best of them against full ticks of
- * variant 5, each from a snapshot of (x, v, a) restored afterwards.  Selects
- * the fastest and returns it in *best.  ms[1..4], when given, receive the
- * per-pass milliseconds, ms[0] and ms[5] the per-tick milliseconds of the
- * best pass variant and of variant 5 (-1 = not run); ms has 6 entries. */
+ * variants 5 and 6 apply, full ticks of the best of them against full ticks
+ * of 5 and of 6, each from a snapshot of (x, v, a) restored afterwards.
+ * Selects the fastest and returns it in *best.  ms[1..4], when given,
+ * receive the per-pass milliseconds, ms[0], ms[5], ms[6] the per-tick
+ * milliseconds of the best pass variant, of 5 and of 6 (-1 = not run);
+ * ms has 7 entries. */
 int gx_autotune(gx_handle* h, int reps, int* best, double* ms);
-/* No counterpart in the reference.  Skin of the variant-5 neighbour list
+/* No counterpart in the reference.  Skin of the variant-5/6 neighbour list
  * (default 0.1 r_c); 0 rebuilds every tick. */
 int gx_set_list_skin(gx_handle* h, double skin);
-/* Number of variant-5 list rebuilds so far (synchronises the stream). */
+/* Number of variant-5/6 list rebuilds so far (synchronises the stream). */
 int gx_list_rebuilds(gx_handle* h, uint64_t* rebuilds);
 
 /* ---- state ----------------------------------------------------------- */

@@ -1,7 +1,8 @@
-"""The persistent neighbour-list pass (kernel variant 5) against the oracle
-and against the per-tick re-sort variants.
+"""The persistent neighbour-list passes (kernel variants 5: full list, 6:
+half list with far-end atomics) against the oracle, each other and the
+per-tick re-sort variants.
 
-Variant 5 evaluates the same pair set {d < r_c} as every other variant, in a
+Variants 5 and 6 evaluate the same pair set {d < r_c} as every other variant, in a
 cell-local frame anchored at the last rebuild, so its FP32 forces can differ
 from variants 1-4 in the last bits: the checks are the mixed path's error
 bound against the FP64 oracle (force rel-RMS <= 1e-5), agreement of whole
@@ -39,10 +40,10 @@ def _relnorm(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
-@pytest.mark.parametrize("coul", [False, True])
-def test_first_tick_forces_match_fp64_oracle(gpu, orc, coul):
+@pytest.mark.parametrize("coul,variant", [(False, 5), (True, 5), (False, 6), (True, 6)])
+def test_first_tick_forces_match_fp64_oracle(gpu, orc, coul, variant):
     cfg, u = _lattice(18, coul=coul)
-    h = _handle(cfg)
+    h = _handle(cfg, variant)
     h.set_universe(u)
     st = h.step(1)
     _, _, acc = h.get_state()
@@ -50,6 +51,24 @@ def test_first_tick_forces_match_fp64_oracle(gpu, orc, coul):
     assert _relnorm(acc, acc_ref) <= MIXED_RMS
     assert abs(st["potential"][0] - st_ref[0, 1]) <= 1e-5 * abs(st_ref[0, 1])
     assert abs(int(st["pairs"][0]) - int(st_ref[0, 4])) <= 2
+
+
+@pytest.mark.parametrize("thermo", [False, True])
+def test_full_and_half_lists_are_bit_identical(gpu, thermo):
+    cfg, u = _lattice(14, temperature=150.0, coul=True)
+    if thermo:
+        cfg.enable_thermostat = True
+        cfg.thermostat_temperature = 40.0
+    out = []
+    for variant in (5, 6):
+        h = _handle(cfg, variant)
+        h.set_universe(u)
+        st = h.step(25, graph=True)
+        out.append((h.get_state(), st, h.list_rebuilds()))
+    for x, y in zip(out[0][0], out[1][0]):
+        assert np.array_equal(x, y)
+    assert np.array_equal(out[0][1], out[1][1])
+    assert out[0][2] == out[1][2]
 
 
 @pytest.mark.parametrize("thermo", [False, True])
@@ -106,7 +125,8 @@ def test_list_path_is_deterministic_and_graph_invariant(gpu):
         assert np.array_equal(runs[0][1], r[1])
 
 
-def test_overflowing_lists_fall_back_to_cell_scans(gpu, orc):
+@pytest.mark.parametrize("variant", [5, 6])
+def test_overflowing_lists_fall_back_to_cell_scans(gpu, orc, variant):
     # a dense clump far above the average density overflows the per-atom lists
     cfg, u = _lattice(12, temperature=10.0)
     rng = np.random.default_rng(4)
@@ -117,7 +137,7 @@ def test_overflowing_lists_fall_back_to_cell_scans(gpu, orc):
     r = 4.0 * rng.random(k) ** (1.0 / 3.0) + 0.3
     pos[:k] = d * r[:, None]
     u2 = dataclasses.replace(u, pos=pos)
-    h = _handle(cfg)
+    h = _handle(cfg, variant)
     h.set_universe(u2)
     st = h.step(1)
     _, _, acc = h.get_state()

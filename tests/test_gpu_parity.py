@@ -267,7 +267,7 @@ def test_mixed_kernel_variants_bit_identical(gpu, ionic):
         assert np.array_equal(out[0][3], o[3])
 
 
-@pytest.mark.parametrize("prec,variant", [("fp64", 0), ("mixed", 1), ("mixed", 5)])
+@pytest.mark.parametrize("prec,variant", [("fp64", 0), ("mixed", 1), ("mixed", 5), ("mixed", 6)])
 def test_graph_replay_matches_eager_ticks(gpu, prec, variant):
     wl, cfg, u = _c1(n_side=12)
     cfg.enable_thermostat = True
@@ -295,8 +295,8 @@ def test_autotune_leaves_state_unchanged(gpu):
     a.step(2)
     before = a.get_state()
     best, ms = a.autotune(reps=2)
-    assert best in ms and best in (1, 2, 3, 4, 5)
-    assert 5 in ms and 0 in ms  # the list path was timed against the best single-pass tick
+    assert best in ms and best in (1, 2, 3, 4, 5, 6)
+    assert 5 in ms and 6 in ms and 0 in ms  # the list paths were timed against the best single-pass tick
     after = a.get_state()
     for x, y in zip(before, after):
         assert np.array_equal(x, y)
