@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--workload", default="c3")
     ap.add_argument("--n-side", type=int, default=0, help="override the lattice edge (testing only)")
     ap.add_argument("--no-extras", action="store_true", help="skip fp64/e2e/cpu legs (testing only)")
+    ap.add_argument("--variant", type=int, default=-1,
+                    help="fix the mixed pair-pass variant instead of autotuning (profiling only)")
     return ap.parse_args()
 
 
@@ -312,7 +314,11 @@ def ours_arm(args, dist):
 
     h = Handle(cfg, "mixed", dev)
     h.set_universe(u)
-    variant, tune_ms = h.autotune(reps=3)  # picks the pair-pass work shape; state unchanged
+    if args.variant >= 0:
+        h.set_kernel_variant(args.variant)
+        variant, tune_ms = args.variant, {}
+    else:
+        variant, tune_ms = h.autotune(reps=3)  # picks the pair-pass work shape; state unchanged
     tick = run_ticks(h, wl, cfg, Wm, 0)
     h.synchronize()
     dist.barrier()
