@@ -232,6 +232,39 @@ def cpu_reference(wl, cfg, u, budget_s: float, threads: int) -> dict:
 # ---------------------------------------------------------------- arms
 
 
+def accuracy_leg(dev: int, steps: int = 10000) -> dict:
+    """NVE energy conservation of the mixed path against the plain FP64 path
+    on the C1 workload (4,096 atoms, LJ, 60 K): relative drift of E = K + V
+    over `steps` ticks (slope of a straight-line fit times the run length),
+    RMS of the per-tick change of E, and the L1 distance of the two final
+    g(r) histograms (256 bins to r = 17.25, normalised to unit sum)."""
+    import numpy as np
+
+    from genesis_b200 import workloads as W
+    from genesis_b200._lib import Handle
+
+    wl = W.C1
+    cfg = wl.config()
+    u = wl.generate()
+    out = {"workload": f"{wl.name}: {u.n} atoms, 60 K, NVE, {steps} ticks"}
+    hists = {}
+    for prec in ("fp64", "mixed"):
+        with Handle(cfg, prec, dev) as h:
+            h.set_universe(u)
+            st = h.step(steps, stats=True, graph=True)
+            E = st["kinetic"] + st["potential"]
+            t = np.arange(len(E))
+            slope = np.polyfit(t, E, 1)[0]
+            e0 = abs(E[0])
+            c, _, _, _ = h.radial_distribution(17.25, 256)
+            hists[prec] = c / max(c.sum(), 1)
+            out[prec] = {"drift_rel": float(slope * steps / e0), "step_rms_rel": float(np.std(np.diff(E)) / e0),
+                         "E0": float(E[0]), "E_end": float(E[-1])}
+    out["drift_ratio_mixed_over_fp64"] = abs(out["mixed"]["drift_rel"]) / max(abs(out["fp64"]["drift_rel"]), 1e-300)
+    out["gr_L1_mixed_vs_fp64"] = float(np.abs(hists["mixed"] - hists["fp64"]).sum())
+    return out
+
+
 def adjoint_leg(dev: int) -> dict:
     """Wall-clock cost of one adjoint gradient on the C5 workload (8,000
     atoms, 200 NVE ticks, checkpoint every 20), the cost of the 40 forward
@@ -465,6 +498,10 @@ def ours_arm(args, dist):
 
         # adjoint (C5): gradients of <V> and of the g(r) fitting loss with
         # respect to the 10 sigma + 10 epsilon_k, against 40 central differences
+        try:
+            extras["accuracy"] = accuracy_leg(dev)
+        except Exception as e:  # noqa: BLE001
+            extras["accuracy_error"] = repr(e)
         try:
             extras["adjoint"] = adjoint_leg(dev)
         except Exception as e:  # noqa: BLE001

@@ -57,33 +57,27 @@ __device__ __forceinline__ void pair_f32(const LawF32& L, const PairF& t, float 
         float s12 = fmul(s6, s6);
         float vl = fmul(t.eps4, fsub(s12, s6));
         float ml = fmul(fmul(t.eps24, inv_r), fmaf(2.f, s12, -s6));
-        float u = fmul(fsub(r, L.lj_ron), L.inv_lj_w);
-        if (u <= 0.f) {
-            f = ml;
-            v = vl;
-        } else if (u < 1.f) {
-            float sw, dsdu;
-            switch5(u, sw, dsdu);
-            float dsw = fmul(dsdu, L.inv_lj_w);
-            f = fmaf(ml, sw, -fmul(vl, dsw));
-            v = fmul(vl, sw);
-        }
+        // u clamped to [0, 1] instead of branching: S(0) = 1 and S'(0) = -0
+        // give f = fmaf(ml, 1, +-0) = ml and v = vl exactly, S(1) = 0 gives
+        // zeros, so the result is bit-identical to skipping the switch
+        // outside (r_on, r_c) -- and no lane of a warp diverges on it.
+        float u = fminf(fmaxf(fmul(fsub(r, L.lj_ron), L.inv_lj_w), 0.f), 1.f);
+        float sw, dsdu;
+        switch5(u, sw, dsdu);
+        float dsw = fmul(dsdu, L.inv_lj_w);
+        f = fmaf(ml, sw, -fmul(vl, dsw));
+        v = fmul(vl, sw);
     }
     if (L.coul && d < L.coul_rc) {
         float inv_r = d < 0.5f ? 2.f : inv_d;
         float vc = fmul(t.qq, inv_r);
         float mc = fmul(vc, inv_r);
-        float u = fmul(fsub(d, L.coul_ron), L.inv_coul_w);
-        if (u <= 0.f) {
-            f = fadd(f, mc);
-            v = fadd(v, vc);
-        } else if (u < 1.f) {
-            float sw, dsdu;
-            switch5(u, sw, dsdu);
-            float dsw = fmul(dsdu, L.inv_coul_w);
-            f = fadd(f, fmaf(mc, sw, -fmul(vc, dsw)));
-            v = fadd(v, fmul(vc, sw));
-        }
+        float u = fminf(fmaxf(fmul(fsub(d, L.coul_ron), L.inv_coul_w), 0.f), 1.f);  // as above
+        float sw, dsdu;
+        switch5(u, sw, dsdu);
+        float dsw = fmul(dsdu, L.inv_coul_w);
+        f = fadd(f, fmaf(mc, sw, -fmul(vc, dsw)));
+        v = fadd(v, fmul(vc, sw));
     }
     fs = fmul(f, inv_d);
 }
