@@ -60,7 +60,7 @@ EXPORTS = (
     "gx_radial_distribution_noalloc", "gx_set_kernel_variant", "gx_autotune",
     "gx_batch_create", "gx_batch_destroy", "gx_batch_last_error", "gx_batch_set_state",
     "gx_batch_step", "gx_batch_get_state", "gx_adjoint_forward", "gx_adjoint_backward",
-    "gx_set_list_skin", "gx_list_rebuilds",
+    "gx_set_list_skin", "gx_list_rebuilds", "gx_batch_set_mode", "gx_batch_get_mode", "gx_batch_autotune",
 )
 
 _lib = None
@@ -487,6 +487,23 @@ class Batch:
         self._check(self.lib.gx_batch_step(self.b, nsteps, _ptr(st, C.c_double), C.byref(ms)))
         return st, ms.value
 
+    def set_mode(self, mode: int):
+        """1 = persistent launch (one CTA per replica), 2 = all-replica graph."""
+        self._check(self.lib.gx_batch_set_mode(self.b, mode))
+
+    @property
+    def mode(self) -> int:
+        m = C.c_int()
+        self._check(self.lib.gx_batch_get_mode(self.b, C.byref(m)))
+        return m.value
+
+    def autotune(self, ticks: int = 10):
+        """Times both modes from a snapshot, keeps the faster: (mode, {mode: ms per tick})."""
+        m = C.c_int()
+        ms = np.zeros(2)
+        self._check(self.lib.gx_batch_autotune(self.b, ticks, C.byref(m), _ptr(ms, C.c_double)))
+        return m.value, {1: float(ms[0]), 2: float(ms[1])}
+
     def get_state(self):
         n = int(self.natoms.sum())
         pos, vel, acc = (np.empty((n, 3)) for _ in range(3))
@@ -511,6 +528,9 @@ def _declare_batch(lib):
         "gx_batch_set_state": (C.c_int, [vp, C.POINTER(C.c_uint32), dp, dp, dp, C.POINTER(C.c_uint8), dp, dp]),
         "gx_batch_step": (C.c_int, [vp, C.c_int, dp, dp]),
         "gx_batch_get_state": (C.c_int, [vp, dp, dp, dp]),
+        "gx_batch_set_mode": (C.c_int, [vp, C.c_int]),
+        "gx_batch_get_mode": (C.c_int, [vp, C.POINTER(C.c_int)]),
+        "gx_batch_autotune": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), dp]),
     }
     for name, (res, args) in proto.items():
         f = getattr(lib, name)

@@ -28,40 +28,11 @@
 #include <string>
 #include <vector>
 
-#include "gx_pair_f32.cuh"
-
-namespace gx {
-LawF32 make_law32(const gx_handle* h);
-}
+#include "gx_batch.cuh"
 
 using namespace gx;
 
 namespace {
-
-constexpr int kBThreads = 512;
-constexpr uint32_t kBMaxCells = 4096;  // cells per replica held in shared memory
-
-struct RepDesc {
-    GridGeom g;
-    uint32_t base, n;
-    double half_box[3];
-    double target, tau;
-    int thermo;
-};
-
-struct BatchArrays {
-    double *x, *y, *z, *vx, *vy, *vz, *ax, *ay, *az, *mass, *inv_mass;
-    uint8_t* kind;
-    uint32_t *key, *idx, *skey;
-    float4* pos4;
-    long long* F;  // 3 * total, SoA
-    size_t total;
-};
-
-struct BatchParams {
-    double dt, half_dt, k_thermal;
-    int boundaries, nsteps;
-};
 
 __device__ __forceinline__ unsigned long long warp_sum_u(unsigned long long v) {
 #pragma unroll
@@ -95,7 +66,7 @@ __global__ void __launch_bounds__(kBThreads, 2)
     const GridGeom& g = R.g;
     const uint32_t base = R.base, n = R.n, ncell = g.ncell;
     const int nk = L.nkinds;
-    double K = 0.0, Vlast = 0.0, lam_last = 1.0;
+    double Vlast = 0.0, lam_last = 1.0;
     unsigned long long np_last = 0;
 
     for (int step = 0; step < P.nsteps; ++step) {
@@ -283,7 +254,6 @@ __global__ void __launch_bounds__(kBThreads, 2)
                 }
             }
             s_lambda = l;
-            K = ks;
             Vlast = xmul(__ll2double_rn((long long)vs), kFixInv);
             lam_last = l;
             np_last = ns;
@@ -313,30 +283,12 @@ __global__ void __launch_bounds__(kBThreads, 2)
         out[4 * r + 1] = Vlast;
         out[4 * r + 2] = lam_last;
         out[4 * r + 3] = (double)np_last;
-        (void)K;
     }
 }
 
 }  // namespace
 
-struct gx_batch {
-    gx_params p;
-    LawF32 L;
-    int nrep = 0;
-    std::vector<RepDesc> reps;
-    RepDesc* d_reps = nullptr;
-    int* d_order = nullptr;
-    BatchArrays A{};
-    size_t total = 0;
-    PairF* d_tab = nullptr;
-    double* d_out = nullptr;
-    uint32_t* d_err = nullptr;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev[2] = {};
-    std::string err;
-    double pair_sigma[kNElem * kNElem], pair_eps[kNElem * kNElem];
-    bool has_state = false;
-};
+
 
 namespace {
 
@@ -402,8 +354,6 @@ int gx_batch_create(const gx_params* p, int nrep, const double* box, const doubl
         RepDesc& d = b->reps[r];
         d.g = make_grid(box + 3 * r, rc, &ok);
         if (!ok) return berr(b, GX_ERR_ARG, "invalid replica box");
-        if (d.g.ncell > kBMaxCells)
-            return berr(b, GX_ERR_CAPACITY, "a replica grid exceeds 4096 force cells (use a gx_handle per universe)");
         for (int k = 0; k < 3; ++k) d.half_box[k] = 0.5 * box[3 * r + k];
         double T = target_T ? target_T[r] : p->thermostat_temperature;
         d.thermo = (p->enable_thermostat && T > 0.0) ? 1 : 0;
@@ -429,6 +379,8 @@ int gx_batch_create(const gx_params* p, int nrep, const double* box, const doubl
 void gx_batch_destroy(gx_batch* b) {
     if (!b) return;
     if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_flat_free(b->flat);
+    b->flat = nullptr;
     free_arrays(b);
     cudaFree(b->d_reps);
     cudaFree(b->d_order);
@@ -488,6 +440,9 @@ int gx_batch_set_state(gx_batch* b, const uint32_t* natoms, const double* pos, c
         }
     b->L.nkinds = nk;
     GXB_CUDA(b, cudaSetDevice(b->p.device));
+    GXB_CUDA(b, cudaStreamSynchronize(b->stream));
+    batch_flat_free(b->flat);  // replica ranges, kinds and sizes change
+    b->flat = nullptr;
     GXB_CUDA(b, cudaMemcpy(b->d_tab, tab, sizeof tab, cudaMemcpyHostToDevice));
     free_arrays(b);
     size_t cap = total < 1 ? 1 : total;
@@ -547,11 +502,21 @@ int gx_batch_step(gx_batch* b, int nsteps, double* stats, double* device_ms) {
     P.k_thermal = b->p.thermal_constant;
     P.boundaries = b->p.enable_boundaries ? 1 : 0;
     P.nsteps = nsteps;
+    if (b->mode == 1)
+        for (const RepDesc& d : b->reps)
+            if (d.g.ncell > kBMaxCells)
+                return berr(b, GX_ERR_CAPACITY,
+                            "a replica grid exceeds 4096 force cells (the persistent mode keeps them in shared memory)");
     GXB_CUDA(b, cudaEventRecord(b->ev[0], b->stream));
-    if (nsteps > 0)
-        k_batch<<<b->nrep, kBThreads, 0, b->stream>>>(b->d_reps, b->d_order, b->A, b->L, b->d_tab, P, b->d_out,
-                                                      b->d_err);
-    GXB_CUDA(b, cudaGetLastError());
+    if (b->mode == 1) {
+        if (nsteps > 0)
+            k_batch<<<b->nrep, kBThreads, 0, b->stream>>>(b->d_reps, b->d_order, b->A, b->L, b->d_tab, P, b->d_out,
+                                                          b->d_err);
+        GXB_CUDA(b, cudaGetLastError());
+    } else {
+        int rc = batch_flat_step(b, nsteps, nullptr);
+        if (rc) return rc;
+    }
     GXB_CUDA(b, cudaEventRecord(b->ev[1], b->stream));
     uint32_t e = 0;
     GXB_CUDA(b, cudaMemcpyAsync(&e, b->d_err, sizeof e, cudaMemcpyDeviceToHost, b->stream));
@@ -569,6 +534,46 @@ int gx_batch_step(gx_batch* b, int nsteps, double* stats, double* device_ms) {
         if (e & kErrSaturation) return berr(b, GX_ERR_SATURATION, "fixed-point force saturated");
     }
     return GX_OK;
+}
+
+int gx_batch_set_mode(gx_batch* b, int mode) {
+    if (!b || mode < 0 || mode > 2) return GX_ERR_ARG;
+    b->mode = mode == 0 ? 2 : mode;
+    return GX_OK;
+}
+
+int gx_batch_get_mode(gx_batch* b, int* mode) {
+    if (!b || !mode) return GX_ERR_ARG;
+    *mode = b->mode;
+    return GX_OK;
+}
+
+int gx_batch_autotune(gx_batch* b, int ticks, int* mode, double* ms) {
+    if (!b || ticks < 1) return GX_ERR_ARG;
+    if (!b->has_state) return berr(b, GX_ERR_STATE, "no state uploaded (call gx_batch_set_state first)");
+    const size_t n9 = 9 * b->A.total;
+    double* snap = nullptr;
+    GXB_CUDA(b, cudaMalloc(&snap, n9 * sizeof(double)));
+    // x y z vx vy vz ax ay az are the first nine columns of one allocation
+    GXB_CUDA(b, cudaMemcpyAsync(snap, b->A.x, n9 * sizeof(double), cudaMemcpyDeviceToDevice, b->stream));
+    const int saved = b->mode;
+    double t[2] = {0.0, 0.0};
+    int rc = GX_OK;
+    for (int m = 1; m <= 2 && !rc; ++m) {
+        b->mode = m;
+        double w = 0.0;
+        if (!(rc = gx_batch_step(b, 1, nullptr, &w)) && !(rc = gx_batch_step(b, ticks, nullptr, &w))) t[m - 1] = w;
+        cudaMemcpyAsync(b->A.x, snap, n9 * sizeof(double), cudaMemcpyDeviceToDevice, b->stream);
+    }
+    cudaStreamSynchronize(b->stream);
+    cudaFree(snap);
+    b->mode = rc ? saved : (t[1] <= t[0] ? 2 : 1);
+    if (mode) *mode = b->mode;
+    if (ms) {
+        ms[0] = t[0] / ticks;
+        ms[1] = t[1] / ticks;
+    }
+    return rc;
 }
 
 int gx_batch_get_state(gx_batch* b, double* pos, double* vel, double* acc) {

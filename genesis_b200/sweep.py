@@ -20,12 +20,15 @@ def make_replicas(count: int = 256, seed: int = 0):
     return [W.replica_workload(r) for r in W.sweep_replicas(count, seed)]
 
 
-def run_batched(wls, steps: int, device: int = 0):
-    """Returns (replica-steps/s from the launch's CUDA-event time, stats, ms)."""
+def run_batched(wls, steps: int, device: int = 0, mode: int = 2):
+    """Returns (replica-steps/s from the step call's CUDA-event time, stats,
+    ms).  mode 1: one persistent launch, one CTA per replica; mode 2: every
+    phase as one kernel over all replicas, CUDA-graph replay."""
     base = wls[0].config()
     b = Batch(base, [wl.config().size for wl in wls], [wl.thermostat_temperature for wl in wls], device)
+    b.set_mode(mode)
     b.set_universes([wl.generate() for wl in wls])
-    b.step(2)  # warm-up launch
+    b.step(2)  # warm-up (and, in mode 2, graph capture)
     st, ms = b.step(steps)
     b.close()
     return len(wls) * steps / (ms * 1e-3), st, ms

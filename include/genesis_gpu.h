@@ -255,6 +255,18 @@ int gx_batch_set_state(gx_batch* b, const uint32_t* natoms, const double* pos, c
  * CUDA-event time of the launch. */
 int gx_batch_step(gx_batch* b, int nsteps, double* stats, double* device_ms);
 int gx_batch_get_state(gx_batch* b, double* pos, double* vel, double* acc);
+/* Execution mode: 1 = one persistent launch, one CTA per replica (every
+ * replica grid <= 4096 force cells, else GX_ERR_CAPACITY at the step);
+ * 2 = every phase of the tick as one kernel over the atoms of all
+ * replicas (a global cell index, per-replica geometry), captured once as a
+ * CUDA graph; 0 = the default (2).  Both give each NVE replica the same bits
+ * as a gx_handle on pair-pass variants 1-4. */
+int gx_batch_set_mode(gx_batch* b, int mode);
+int gx_batch_get_mode(gx_batch* b, int* mode);
+/* Times `ticks` ticks in each mode from a snapshot of the state (restored
+ * afterwards), keeps the faster; ms[0], ms[1] (may be NULL) receive the
+ * per-tick device milliseconds of modes 1 and 2. */
+int gx_batch_autotune(gx_batch* b, int ticks, int* mode, double* ms);
 
 /* ---- adjoint: derivatives of short NVE horizons ----------------------- */
 

@@ -31,11 +31,12 @@ def _single(wl, steps):
     return out, st
 
 
-def _batch(wls, steps):
+def _batch(wls, steps, mode=2):
     from genesis_b200._lib import Batch
     base = wls[0].config()
     base.enable_thermostat = wls[0].thermostat
     b = Batch(base, [wl.config().size for wl in wls], [wl.thermostat_temperature for wl in wls])
+    b.set_mode(mode)
     b.set_universes([wl.generate() for wl in wls])
     st, ms = b.step(steps)
     out = b.get_state()
@@ -43,9 +44,10 @@ def _batch(wls, steps):
     return out, st, ms
 
 
-def test_batch_nve_matches_single_universes_bit_for_bit(gpu):
+@pytest.mark.parametrize("mode", [1, 2])
+def test_batch_nve_matches_single_universes_bit_for_bit(gpu, mode):
     wls = _replicas(thermo=False)
-    out, st, ms = _batch(wls, 6)
+    out, st, ms = _batch(wls, 6, mode)
     assert ms > 0
     for k, wl in enumerate(wls):
         ref, rst = _single(wl, 6)
@@ -55,9 +57,10 @@ def test_batch_nve_matches_single_universes_bit_for_bit(gpu):
         assert st[k, 1] == rst["potential"][-1]
 
 
-def test_batch_nvt_matches_single_universes(gpu):
+@pytest.mark.parametrize("mode", [1, 2])
+def test_batch_nvt_matches_single_universes(gpu, mode):
     wls = _replicas(thermo=True)
-    out, st, _ = _batch(wls, 5)
+    out, st, _ = _batch(wls, 5, mode)
     for k, wl in enumerate(wls):
         ref, rst = _single(wl, 5)
         for x, y in zip(out[k], ref):
@@ -66,9 +69,39 @@ def test_batch_nvt_matches_single_universes(gpu):
         assert abs(st[k, 2] - rst["lambda"][-1]) <= 1e-12
 
 
-def test_batch_rejects_oversized_replica_grid(gpu):
+def test_persistent_mode_rejects_oversized_replica_grid(gpu):
     from genesis_b200._lib import Batch, GxError
+    wl = W.Replica(n_side=8, temperature=40.0, seed=3)
+    u = W.replica_workload(wl).generate()
     base = W.C1.config()
+    b = Batch(base, [(500.0, 500.0, 500.0)], [50.0])  # 86^3 force cells > 4096
+    b.set_universes([u])
+    b.set_mode(1)
     with pytest.raises(GxError) as e:
-        Batch(base, [(500.0, 500.0, 500.0)], [50.0])  # 86^3 force cells > 4096
+        b.step(1)
     assert e.value.status == -4
+    b.set_mode(2)  # the all-replica graph has no per-replica cell limit
+    b.step(2)
+    b.close()
+
+
+def test_batch_modes_agree_and_autotune_restores_state(gpu):
+    wls = _replicas(thermo=True)
+    a, sa, _ = _batch(wls, 8, mode=1)
+    c, sc, _ = _batch(wls, 8, mode=2)
+    for x, y in zip(a, c):
+        for p, q in zip(x, y):
+            assert np.linalg.norm(p - q) <= 1e-12 * max(np.linalg.norm(q), 1e-300)
+    from genesis_b200._lib import Batch
+    base = wls[0].config()
+    base.enable_thermostat = True
+    b = Batch(base, [wl.config().size for wl in wls], [wl.thermostat_temperature for wl in wls])
+    b.set_universes([wl.generate() for wl in wls])
+    before = b.get_state()
+    mode, ms = b.autotune(ticks=3)
+    assert mode in (1, 2) and ms[1] > 0 and ms[2] > 0
+    after = b.get_state()
+    for x, y in zip(before, after):
+        for p, q in zip(x, y):
+            assert np.array_equal(p, q)
+    b.close()
