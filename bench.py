@@ -531,6 +531,7 @@ def ours_arm(args, dist):
                            "parallelism": f"{dist.world} independent replicas (one per GPU)",
                            "pair_pass_variant": variant, "autotune_ms": tune_ms,
                            "neighbour_list_rebuilds_in_timed_ticks": rebuilds,
+                           "neighbour_list_skin_and_threads_per_atom": h.list_config(),
                            "cuda_graph": True},
                 "gpu_launches": launches, "clocks": clk, "roofline": roof, "roofline_hbm": roof_hbm,
                 "kernels": kernels, "memory_kernels": mem, "pairs_per_tick": pairs}

@@ -61,6 +61,7 @@ EXPORTS = (
     "gx_batch_create", "gx_batch_destroy", "gx_batch_last_error", "gx_batch_set_state",
     "gx_batch_step", "gx_batch_get_state", "gx_adjoint_forward", "gx_adjoint_backward",
     "gx_set_list_skin", "gx_list_rebuilds", "gx_batch_set_mode", "gx_batch_get_mode", "gx_batch_autotune",
+    "gx_get_list_config", "gx_set_list_threads",
 )
 
 _lib = None
@@ -114,6 +115,8 @@ def load(path: str | Path | None = None) -> C.CDLL:
         "gx_adjoint_forward": (C.c_int, [vp, C.POINTER(GxAdjointSpec), dp, dp]),
         "gx_set_list_skin": (C.c_int, [vp, _D]),
         "gx_list_rebuilds": (C.c_int, [vp, u64p]),
+        "gx_get_list_config": (C.c_int, [vp, dp, C.POINTER(C.c_int)]),
+        "gx_set_list_threads": (C.c_int, [vp, C.c_int]),
         "gx_adjoint_backward": (C.c_int, [vp, dp, dp, dp, dp, dp, dp, dp]),
     }
     for name, (res, args) in proto.items():
@@ -251,6 +254,15 @@ class Handle:
     def set_list_skin(self, skin: float):
         """Skin of the variant-5 neighbour list (default 0.1 r_c)."""
         self._check(self.lib.gx_set_list_skin(self.h, skin))
+
+    def list_config(self):
+        """(skin, threads per atom) of the variant-5/6 list pass."""
+        skin, tpp = C.c_double(), C.c_int()
+        self._check(self.lib.gx_get_list_config(self.h, C.byref(skin), C.byref(tpp)))
+        return skin.value, tpp.value
+
+    def set_list_threads(self, threads_per_atom: int):
+        self._check(self.lib.gx_set_list_threads(self.h, threads_per_atom))
 
     def list_rebuilds(self) -> int:
         out = C.c_uint64()

@@ -884,6 +884,10 @@ int gx_autotune(gx_handle* h, int reps, int* best, double* ms) {
                 if (tt[2] < tt[q]) q = 2;
                 pick = vs[q];
             }
+            if (!rc && pick >= 5) {  // threads per atom of the list pass, on the list just built
+                h->kernel_variant = pick;
+                rc = nl_tune_tpp(h, reps);
+            }
         }
     }
     h->kernel_variant = rc ? saved : pick;
@@ -896,6 +900,17 @@ int gx_set_list_skin(gx_handle* h, double skin) {
     if (!h || !(skin >= 0.0) || !std::isfinite(skin)) return GX_ERR_ARG;
     invalidate_graphs(h);
     return nl_set_skin(h, skin);
+}
+
+int gx_get_list_config(gx_handle* h, double* skin, int* threads_per_atom) {
+    if (!h) return GX_ERR_ARG;
+    return nl_config(h, skin, threads_per_atom);
+}
+
+int gx_set_list_threads(gx_handle* h, int threads_per_atom) {
+    if (!h) return GX_ERR_ARG;
+    invalidate_graphs(h);
+    return nl_set_tpp(h, threads_per_atom);
 }
 
 int gx_list_rebuilds(gx_handle* h, uint64_t* rebuilds) {

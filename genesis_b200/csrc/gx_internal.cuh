@@ -283,6 +283,9 @@ int nl_prepare(gx_handle* h, bool* graphs_stale);
 int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nblocks);
 int nl_rebuilds(gx_handle* h, uint64_t* out);
 int nl_set_skin(gx_handle* h, double skin);
+int nl_tune_tpp(gx_handle* h, int reps);
+int nl_config(gx_handle* h, double* skin, int* tpp);
+int nl_set_tpp(gx_handle* h, int tpp);
 void nl_free(gx_handle* h);
 
 void launch_kick(gx_handle* h, const StateBuf& b, uint32_t n, double half_dt, const double* lambda);

@@ -45,6 +45,7 @@ struct NlState {
     double skin = -1.0;       // < 0: default (0.1 r_c)
     double skin_used = 0.0;
     int half = -1;            // list kind built: 0 full, 1 half (variant 6)
+    int tpp = 1;              // threads per atom in the list pass (1, 2, 4, 8)
     int cap_nb = 0;           // list entries per atom
     size_t cap = 0;           // atoms the buffers hold
     uint32_t* list = nullptr; // entry e of atom p at list[e * cap + p]
@@ -363,6 +364,115 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force(GridGeom g, const float
     }
 }
 
+// TPP lanes per atom: lane k of an atom's group takes list entries k,
+// k + TPP, ... (more independent gathers in flight, less divergence between
+// list lengths); the group's integer partial sums are combined with
+// shuffles, so every TPP gives the same bits.
+template <bool HALF, int TPP>
+__global__ void __launch_bounds__(kNlThreads) k_nl_force_tpp(GridGeom g, const float4* __restrict__ pos4,
+                                                              const uint32_t* __restrict__ home,
+                                                              const uint32_t* __restrict__ start, uint32_t n,
+                                                              LawF32 L, const PairF* __restrict__ tab,
+                                                              const uint32_t* __restrict__ list, size_t stride,
+                                                              int cap_nb, const uint32_t* __restrict__ cnt,
+                                                              long long* __restrict__ F, size_t fstride,
+                                                              unsigned long long* __restrict__ vacc,
+                                                              unsigned long long* __restrict__ npairs,
+                                                              uint32_t* __restrict__ err) {
+    static_assert(kNlThreads % TPP == 0 && 32 % TPP == 0, "TPP must divide the warp");
+    __shared__ PairF st[kMaxKinds * kMaxKinds];
+    __shared__ float4 s_shift[27];
+    __shared__ unsigned long long shu[kNlThreads / 32];
+    int nk2 = L.nkinds * L.nkinds;
+    for (int t = threadIdx.x; t < nk2; t += kNlThreads) st[t] = tab[t];
+    if (threadIdx.x < 27) {
+        float sx, sy, sz;
+        code_shift(g, threadIdx.x, sx, sy, sz);
+        s_shift[threadIdx.x] = make_float4(sx, sy, sz, 0.f);
+    }
+    __syncthreads();
+    const uint32_t gid = blockIdx.x * kNlThreads + threadIdx.x;
+    const uint32_t p = gid / TPP;
+    const uint32_t sub = threadIdx.x % TPP;
+    PairAcc a;
+    if (p < n) {
+        float4 pi = pos4[p];
+        int ki = __float_as_int(pi.w);
+        uint32_t m = cnt[p];
+        if (m <= (uint32_t)cap_nb) {
+            const uint32_t* lp = list + p;
+            uint32_t e = sub;
+            for (; e + TPP < m; e += 2 * TPP) {  // two entries per round, loads first
+                uint32_t w0 = __ldg(lp + (size_t)e * stride), w1 = __ldg(lp + (size_t)(e + TPP) * stride);
+                float4 p0 = __ldg(pos4 + (w0 & kIdxMask)), p1 = __ldg(pos4 + (w1 & kIdxMask));
+                float4 s0 = s_shift[w0 >> 27], s1 = s_shift[w1 >> 27];
+                uint32_t q0 = w0 & kIdxMask, q1 = w1 & kIdxMask;
+                nl_pair(L, st, ki, pi, p0, s0.x, s0.y, s0.z, q0 > p, a, err, HALF ? F : nullptr, q0, fstride);
+                nl_pair(L, st, ki, pi, p1, s1.x, s1.y, s1.z, q1 > p, a, err, HALF ? F : nullptr, q1, fstride);
+            }
+            if (e < m) {
+                uint32_t w = __ldg(lp + (size_t)e * stride);
+                float4 sh = s_shift[w >> 27];
+                uint32_t q = w & kIdxMask;
+                nl_pair(L, st, ki, pi, __ldg(pos4 + q), sh.x, sh.y, sh.z, q > p, a, err, HALF ? F : nullptr, q,
+                        fstride);
+            }
+        } else {  // overflowed list: the group splits the 27 home-grid cells
+            uint32_t cx, cy, cz;
+            decode(g, home[p], cx, cy, cz);
+            const uint32_t c = home[p];
+            for (uint32_t code = sub; code < 27; code += TPP) {
+                uint32_t B = cell_at(g, cx, cy, cz, code);
+                if (HALF && B < c) continue;
+                float sx, sy, sz;
+                code_shift(g, code, sx, sy, sz);
+                for (uint32_t q = start[B], hi = start[B + 1]; q < hi; ++q)
+                    if (HALF ? q > p : q != p)
+                        nl_pair(L, st, ki, pi, pos4[q], sx, sy, sz, q > p, a, err, HALF ? F : nullptr, q, fstride);
+            }
+        }
+    }
+#pragma unroll
+    for (int o = TPP / 2; o > 0; o >>= 1) {
+        a.fx += __shfl_down_sync(0xffffffffu, a.fx, o, TPP);
+        a.fy += __shfl_down_sync(0xffffffffu, a.fy, o, TPP);
+        a.fz += __shfl_down_sync(0xffffffffu, a.fz, o, TPP);
+    }
+    if (p < n && sub == 0) {
+        if (HALF) {
+            atomicAdd((unsigned long long*)&F[p], (unsigned long long)a.fx);
+            atomicAdd((unsigned long long*)&F[fstride + p], (unsigned long long)a.fy);
+            atomicAdd((unsigned long long*)&F[2 * fstride + p], (unsigned long long)a.fz);
+        } else {
+            F[p] = a.fx;
+            F[fstride + p] = a.fy;
+            F[2 * fstride + p] = a.fz;
+        }
+    }
+    unsigned long long s = block_sum_u<kNlThreads>((unsigned long long)a.vq, shu);
+    unsigned long long np = block_sum_u<kNlThreads>(a.np, shu);
+    if (threadIdx.x == 0) {
+        if (s) atomicAdd(vacc, s);
+        if (np) atomicAdd(npairs, np);
+    }
+}
+
+template <bool HALF>
+void launch_nl_force(gx_handle* h, int tpp, const GridGeom& g, const NlState* s, uint32_t n, const LawF32& L) {
+    const float4* pos4 = h->pos4;
+    const uint32_t* home = h->key_sorted;
+    const uint32_t* start = s->cl.start;
+    if (tpp <= 1) {
+        GX_LAUNCH(h, k_nl_force<HALF>, nblk(n, kNlThreads), kNlThreads, g, pos4, home, start, n, L, h->d_pairf,
+                  s->list, s->cap, s->cap_nb, s->cnt, h->F, h->cap, h->dcount + 1, h->dcount + 0, h->derr);
+        return;
+    }
+    const size_t threads = (size_t)n * tpp;
+    auto k = tpp == 2 ? k_nl_force_tpp<HALF, 2> : (tpp == 4 ? k_nl_force_tpp<HALF, 4> : k_nl_force_tpp<HALF, 8>);
+    GX_LAUNCH(h, k, nblk(threads, kNlThreads), kNlThreads, g, pos4, home, start, n, L, h->d_pairf, s->list, s->cap,
+              s->cap_nb, s->cnt, h->F, h->cap, h->dcount + 1, h->dcount + 0, h->derr);
+}
+
 __global__ void k_nl_fix_to_double(const unsigned long long* __restrict__ v, double* out, double* zero) {
     *out = xmul(__ll2double_rn((long long)*v), kFixInv);
     *zero = 0.0;
@@ -548,9 +658,10 @@ int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nb_out) {
     LawF32 L = make_law32(h);
     prof_begin(h, "force_nl");
     if (halfl) GX_CUDA(h, cudaMemsetAsync(h->F, 0, 3 * h->cap * sizeof(long long), h->stream));
-    auto force = halfl ? k_nl_force<true> : k_nl_force<false>;
-    GX_LAUNCH(h, force, nblk(n, kNlThreads), kNlThreads, g, h->pos4, h->key_sorted, s->cl.start, n, L,
-              h->d_pairf, s->list, s->cap, s->cap_nb, s->cnt, h->F, h->cap, h->dcount + 1, h->dcount + 0, h->derr);
+    if (halfl)
+        launch_nl_force<true>(h, s->tpp, g, s, n, L);
+    else
+        launch_nl_force<false>(h, s->tpp, g, s, n, L);
     prof_end(h, "force_nl");
     GX_LAUNCH(h, k_nl_fix_to_double, 1, 1, h->dcount + 1, h->dscal + 2, h->dscal + 3);
     int nb = (int)nblk(n, kRedThreads);
@@ -576,6 +687,50 @@ int nl_rebuilds(gx_handle* h, uint64_t* out) {
     GX_CUDA(h, cudaMemcpyAsync(f, s->flag, sizeof f, cudaMemcpyDeviceToHost, h->stream));
     GX_CUDA(h, cudaStreamSynchronize(h->stream));
     *out = f[1];
+    return GX_OK;
+}
+
+// Times the list pass at 1, 2, 4 and 8 threads per atom on the current list
+// (`reps` launches each) and keeps the fastest.  The state is not touched:
+// the pass only writes the force scratch, which the next tick overwrites.
+int nl_tune_tpp(gx_handle* h, int reps) {
+    NlState* s = nl_of(h);
+    if (!s->list || !s->cap || h->n == 0) return GX_OK;
+    const uint32_t n = (uint32_t)h->n;
+    const LawF32 L = make_law32(h);
+    const int cand[4] = {1, 2, 4, 8};
+    double best = 1e300;
+    int pick = s->tpp;
+    for (int k = 0; k < 4; ++k) {
+        int rc = gx_timer_mark(h, 14);
+        for (int r = 0; r < reps && !rc; ++r) {
+            if (s->half == 1) launch_nl_force<true>(h, cand[k], s->lg, s, n, L);
+            else launch_nl_force<false>(h, cand[k], s->lg, s, n, L);
+        }
+        double t = 0.0;
+        if (!rc) rc = gx_timer_mark(h, 15);
+        if (!rc) rc = gx_timer_elapsed(h, 14, 15, &t);
+        if (rc) return rc;
+        if (t / reps < best) {
+            best = t / reps;
+            pick = cand[k];
+        }
+    }
+    s->tpp = pick;
+    GX_CUDA(h, cudaMemsetAsync(h->derr, 0, sizeof(uint32_t), h->stream));
+    return GX_OK;
+}
+
+int nl_config(gx_handle* h, double* skin, int* tpp) {
+    NlState* s = nl_of(h);
+    if (skin) *skin = skin_of(h, s);
+    if (tpp) *tpp = s->tpp;
+    return GX_OK;
+}
+
+int nl_set_tpp(gx_handle* h, int tpp) {
+    if (tpp != 1 && tpp != 2 && tpp != 4 && tpp != 8) return set_err(h, GX_ERR_ARG, "threads per atom must be 1, 2, 4 or 8");
+    nl_of(h)->tpp = tpp;
     return GX_OK;
 }
 

@@ -132,6 +132,13 @@ int gx_autotune(gx_handle* h, int reps, int* best, double* ms);
 /* No counterpart in the reference.  Skin of the variant-5/6 neighbour list
  * (default 0.1 r_c); 0 rebuilds every tick. */
 int gx_set_list_skin(gx_handle* h, double skin);
+/* Threads per atom of the variant-5/6 list pass: 1, 2, 4 or 8 lanes share
+ * one atom's list (default 1; the autotuner picks the fastest).  Every
+ * choice gives the same bits (integer sums).  No counterpart in the
+ * reference. */
+int gx_set_list_threads(gx_handle* h, int threads_per_atom);
+/* Skin and threads per atom of the variant-5/6 list pass. */
+int gx_get_list_config(gx_handle* h, double* skin, int* threads_per_atom);
 /* Number of variant-5/6 list rebuilds so far (synchronises the stream). */
 int gx_list_rebuilds(gx_handle* h, uint64_t* rebuilds);
 

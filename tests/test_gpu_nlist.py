@@ -94,6 +94,25 @@ def test_trajectory_follows_per_tick_variant(gpu, thermo):
     assert h5.list_rebuilds() >= 1
 
 
+@pytest.mark.parametrize("variant", [5, 6])
+def test_threads_per_atom_are_bit_identical(gpu, variant):
+    cfg, u = _lattice(14, temperature=150.0, coul=True)
+    cfg.enable_thermostat = True
+    cfg.thermostat_temperature = 40.0
+    out = []
+    for tpp in (1, 2, 4, 8):
+        h = _handle(cfg, variant)
+        h.set_list_threads(tpp)
+        h.set_universe(u)
+        st = h.step(12, graph=True)
+        assert h.list_config()[1] == tpp
+        out.append((h.get_state(), st))
+    for o in out[1:]:
+        for x, y in zip(out[0][0], o[0]):
+            assert np.array_equal(x, y)
+        assert np.array_equal(out[0][1], o[1])
+
+
 def test_zero_skin_rebuilds_every_tick(gpu):
     cfg, u = _lattice(12)
     h = _handle(cfg)
