@@ -46,6 +46,13 @@ class GxAdjointSpec(C.Structure):
                 ("gr_every", C.c_int32), ("gr_rmax", _D), ("gr_width", _D), ("gr_support", _D)]
 
 
+class GxBondObservation(C.Structure):
+    _fields_ = [("tick", C.c_uint64), ("bound_pairs", C.c_uint64), ("bonded_pairs", C.c_uint64),
+                ("bonded_entities", C.c_uint64), ("mean_coordination", _D), ("bonds_formed", C.c_uint64),
+                ("lifetime_sum_ticks", _D), ("open_episodes", C.c_uint64), ("completed_episodes", C.c_uint64),
+                ("completed_ticks", C.c_uint64), ("species_matrix", C.c_uint64 * 100)]
+
+
 TICK_DTYPE = np.dtype([("kinetic", "f8"), ("speed_sum", "f8"), ("potential", "f8"),
                        ("bond_energy", "f8"), ("lambda", "f8"), ("pairs", "u8")])
 
@@ -61,7 +68,7 @@ EXPORTS = (
     "gx_batch_create", "gx_batch_destroy", "gx_batch_last_error", "gx_batch_set_state",
     "gx_batch_step", "gx_batch_get_state", "gx_adjoint_forward", "gx_adjoint_backward",
     "gx_set_list_skin", "gx_list_rebuilds", "gx_batch_set_mode", "gx_batch_get_mode", "gx_batch_autotune",
-    "gx_get_list_config", "gx_set_list_threads",
+    "gx_get_list_config", "gx_set_list_threads", "gx_bond_observe", "gx_bond_tracker_reset", "gx_get_bonds",
 )
 
 _lib = None
@@ -117,6 +124,9 @@ def load(path: str | Path | None = None) -> C.CDLL:
         "gx_list_rebuilds": (C.c_int, [vp, u64p]),
         "gx_get_list_config": (C.c_int, [vp, dp, C.POINTER(C.c_int)]),
         "gx_set_list_threads": (C.c_int, [vp, C.c_int]),
+        "gx_bond_observe": (C.c_int, [vp, _D, _D, C.c_int, C.c_uint64, C.c_int, C.POINTER(GxBondObservation)]),
+        "gx_bond_tracker_reset": (C.c_int, [vp]),
+        "gx_get_bonds": (C.c_int, [vp, u32p, sz, C.POINTER(sz)]),
         "gx_adjoint_backward": (C.c_int, [vp, dp, dp, dp, dp, dp, dp, dp]),
     }
     for name, (res, args) in proto.items():
@@ -404,6 +414,32 @@ class Handle:
         if initial_state:
             return gs, ge, tuple(st)
         return gs, ge
+
+    # -- bond observation ---------------------------------------------------
+    def bond_observe(self, k_bind: float, min_periods: float, tick: int, debounce: int = E.DEBOUNCE,
+                     apply_bonds: bool = True) -> dict:
+        """One tick of bond observation on the device (gx_bond_observe)."""
+        o = GxBondObservation()
+        self._check(self.lib.gx_bond_observe(self.h, k_bind, min_periods, debounce, tick, int(apply_bonds),
+                                             C.byref(o)))
+        d = {f: getattr(o, f) for f, _ in GxBondObservation._fields_ if f != "species_matrix"}
+        d["species_matrix"] = np.array(o.species_matrix[:], dtype=np.uint64).reshape(10, 10)
+        return d
+
+    def bond_tracker_reset(self):
+        self._check(self.lib.gx_bond_tracker_reset(self.h))
+
+    def get_bonds(self) -> np.ndarray:
+        """The handle's bond list, (m, 2) slot pairs."""
+        n = C.c_size_t()
+        cap = max(int(self.lib.gx_num_atoms(self.h)) * 8, 64)
+        out = np.empty((cap, 2), dtype=np.uint32)
+        rc = self.lib.gx_get_bonds(self.h, _ptr(out, C.c_uint32), cap, C.byref(n))
+        if rc == -4:
+            out = np.empty((n.value, 2), dtype=np.uint32)
+            rc = self.lib.gx_get_bonds(self.h, _ptr(out, C.c_uint32), n.value, C.byref(n))
+        self._check(rc)
+        return out[: n.value].copy()
 
     # -- profiling ----------------------------------------------------------
     def profile(self, on: bool = True):

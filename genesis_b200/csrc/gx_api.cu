@@ -397,6 +397,7 @@ void gx_destroy(gx_handle* h) {
     invalidate_graphs(h);
     adjoint_free(h);
     nl_free(h);
+    tracker_free(h);
     free_buf(h->buf[0]);
     free_buf(h->buf[1]);
     cudaFree(h->key);
@@ -445,6 +446,7 @@ int gx_set_state(gx_handle* h, size_t n, const double* pos, const double* vel, c
     h->cur = 0;
     h->sorted = false;
     h->nl_valid = false;
+    tracker_free(h);  // new atoms: the open episodes no longer apply
     h->lambda_pending = false;
     invalidate_graphs(h);
     StateBuf& b = h->buf[0];
@@ -901,6 +903,19 @@ int gx_set_list_skin(gx_handle* h, double skin) {
     invalidate_graphs(h);
     return nl_set_skin(h, skin);
 }
+
+}  // extern "C"
+
+namespace gx {
+// The device bond list was rewritten in place (bond observation): captured
+// ticks stay valid unless its length or its buffer changed.
+void bonds_changed(gx_handle* h, size_t nbonds, bool realloc) {
+    if (realloc || nbonds != h->nbonds) invalidate_graphs(h);
+    h->nbonds = nbonds;
+}
+}  // namespace gx
+
+extern "C" {
 
 int gx_get_list_config(gx_handle* h, double* skin, int* threads_per_atom) {
     if (!h) return GX_ERR_ARG;

@@ -232,6 +232,9 @@ struct gx_handle {
     // nl_valid: the list matches buf[cur]'s order and home cells
     void* nl = nullptr;
     bool nl_valid = false;
+
+    // bond observation (gx_bondtrack.cu): open episodes on the device, owned there
+    void* tracker = nullptr;
 };
 
 // Every kernel launch of the library goes through this macro so the
@@ -287,6 +290,7 @@ int nl_tune_tpp(gx_handle* h, int reps);
 int nl_config(gx_handle* h, double* skin, int* tpp);
 int nl_set_tpp(gx_handle* h, int tpp);
 void nl_free(gx_handle* h);
+void tracker_free(gx_handle* h);
 
 void launch_kick(gx_handle* h, const StateBuf& b, uint32_t n, double half_dt, const double* lambda);
 void launch_drift(gx_handle* h, const StateBuf& b, uint32_t n, double dt);

@@ -253,7 +253,8 @@ struct BoundVisit {
         // threshold = k_bind * mix_sigma, analysis/pairs.rs:163
         double threshold = xmul(k_bind, xmul(0.5, xadd(sig[a.elem[i]], sig[a.elem[j]])));
         if (!(d < threshold)) return;
-        uint32_t ea = entity[a.slot[i]], eb = entity[a.slot[j]];
+        // entity ids (EntityId::index), or slot numbers when entity is null
+        uint32_t ea = entity ? entity[a.slot[i]] : a.slot[i], eb = entity ? entity[a.slot[j]] : a.slot[j];
         if (eb < ea) {
             uint32_t t = ea;
             ea = eb;
@@ -519,6 +520,43 @@ int gx_clusters(gx_handle* h, double bond_factor, uint32_t* labels, uint64_t sta
     if (mean_size) *mean_size = (double)n / (double)(c[3] > 0 ? c[3] : 1);
     return GX_OK;
 }
+
+}  // extern "C"
+
+namespace gx {
+
+// bound_pairs_with_grid (src/analysis/pairs.rs:132-174) with the pairs left on
+// the device as slot pairs (a < b): up to cap pairs into out, the number
+// found added to *dcount (device).  Launches only.
+int bound_pairs_device(gx_handle* h, double k_bind, uint32_t* out, size_t cap, unsigned long long* dcount) {
+    uint32_t n = (uint32_t)h->n;
+    AuxPool& P = pool_of(h);
+    int rc = ensure_pool(h, P, n, n);
+    if (rc) return rc;
+    double ms = 0.0;  // bind_cutoff, analysis/pairs.rs:112-114
+    for (int k = 0; k < kNElem; ++k) ms = std::fmax(ms, h->p.sigma[k]);
+    double cutoff = k_bind * ms;
+    int ok = 0;
+    GridGeom g = make_grid(h->p.box, cutoff, &ok);
+    if (!ok) return set_err(h, GX_ERR_ARG, "invalid bond grid");
+    AuxSet a;
+    if ((rc = build_aux(h, P, g, nullptr, n, a))) return rc;
+    BoundVisit v;
+    v.k_bind = k_bind;
+    for (int k = 0; k < kNElem; ++k) v.sig[k] = h->p.sigma[k];
+    v.entity = nullptr;
+    v.out = out;
+    v.cap = cap;
+    v.cnt = dcount;
+    prof_begin(h, "bound_pairs");
+    if (n) GX_LAUNCH(h, k_pairs, nblk(n, 128), 128, g, a, h->p.box[0], h->p.box[1], h->p.box[2], cutoff * cutoff, v);
+    prof_end(h, "bound_pairs");
+    return GX_OK;
+}
+
+}  // namespace gx
+
+extern "C" {
 
 int gx_bound_pairs(gx_handle* h, double k_bind, uint32_t* pairs, size_t cap, size_t* npairs) {
     int rc = require(h);

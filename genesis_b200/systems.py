@@ -133,6 +133,7 @@ class GpuWorld:
                          entity=world.entity)
         self.host_dirty = False
         self.device_dirty = False
+        self.bonds_on_device = False  # the device bond list came from gx_bond_observe
         self.slot_of_entity = {int(e): i for i, e in enumerate(world.entity)}
 
     def to_device(self):
@@ -234,7 +235,7 @@ class GpuForceSystem(_GpuSystem):
 
     def run(self, ctx):
         self._enter()
-        if self.bonds_on:
+        if self.bonds_on and not self.gpu.bonds_on_device:
             self.gpu.set_bonds_from_world()
         V, Vb, _ = self.gpu.h.forces()
         ctx.resources["PotentialEnergy"] = V
@@ -330,16 +331,14 @@ def persistence_ticks(cfg, ea: int, eb: int) -> int:
 
 
 class GpuBondObservation(_GpuSystem):
-    """BondObservationSystem (src/systems/bonds.rs:58-185): bound pairs on the
-    device (gx_bound_pairs), episodes and persistence on the host, the result
-    written to the Bonds column that the next force pass reads."""
+    """BondObservationSystem (src/systems/bonds.rs:58-185) on the device
+    (gx_bond_observe): bound pairs, episodes, persistence and the summary all
+    stay on the GPU; the persistent pairs become the device bond list the next
+    force pass reads, and are mirrored into the host Bonds column."""
 
     def __init__(self, gpu: GpuWorld, cfg):
         super().__init__(gpu)
         self.cfg = cfg
-        self.tracker = PairTracker(E.DEBOUNCE)
-        self.active_since: dict = {}
-        self.elem_of_entity = {int(e): int(t) for e, t in zip(gpu.world.entity, gpu.world.elem)}
 
     def name(self):
         return "bond-observation"
@@ -350,29 +349,20 @@ class GpuBondObservation(_GpuSystem):
 
     def run(self, ctx):
         self._enter()
-        bp = self.gpu.h.bound_pairs(self.cfg.bond_k_bind)
-        self.tracker.track_tick([(int(a), int(b)) for a, b in bp])
-        persistent: dict = {}
-        for (a, b), ticks in self.tracker.open.items():
-            if ticks < persistence_ticks(self.cfg, self.elem_of_entity[a], self.elem_of_entity[b]):
-                continue
-            persistent.setdefault(a, []).append(b)
-            persistent.setdefault(b, []).append(a)
-        ctx.world.bonds = persistent
-        current = {(min(a, b), max(a, b)) for a, lst in persistent.items() for b in lst}
-        bo = ctx.resources.setdefault("BondObservation", {"bonds_formed": 0, "lifetime_sum_ticks": 0.0})
-        now = ctx.time.tick
-        for p in [p for p in self.active_since if p not in current]:
-            bo["bonds_formed"] += 1
-            bo["lifetime_sum_ticks"] += now - self.active_since.pop(p)
-        for p in current:
-            self.active_since.setdefault(p, now)
-        matrix = np.zeros((E.COUNT, E.COUNT), dtype=np.uint64)
-        for a, b in current:
-            ia, ib = self.elem_of_entity[a], self.elem_of_entity[b]
-            matrix[ia, ib] += 1
-            matrix[ib, ia] += 1
-        bo.update(tick=now, bonded_pairs=len(current), bonded_entities=len(persistent), species_matrix=matrix)
+        st = self.gpu.h.bond_observe(self.cfg.bond_k_bind, self.cfg.bond_min_periods, ctx.time.tick,
+                                     debounce=E.DEBOUNCE, apply_bonds=True)
+        self.gpu.bonds_on_device = True
+        ent = self.gpu.world.entity
+        bonds: dict = {}
+        for a, b in self.gpu.h.get_bonds():
+            ea, eb = int(ent[a]), int(ent[b])
+            bonds.setdefault(ea, []).append(eb)
+            bonds.setdefault(eb, []).append(ea)
+        ctx.world.bonds = bonds
+        bo = ctx.resources.setdefault("BondObservation", {})
+        bo.update(tick=st["tick"], bonded_pairs=st["bonded_pairs"], bonded_entities=st["bonded_entities"],
+                  mean_coordination=st["mean_coordination"], bonds_formed=st["bonds_formed"],
+                  lifetime_sum_ticks=st["lifetime_sum_ticks"], species_matrix=st["species_matrix"])
 
 
 class GpuStats(_GpuSystem):

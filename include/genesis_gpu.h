@@ -229,6 +229,40 @@ int gx_clusters(gx_handle* h, double bond_factor, uint32_t* labels, uint64_t sta
  * order. */
 int gx_bound_pairs(gx_handle* h, double k_bind, uint32_t* pairs, size_t cap, size_t* npairs);
 
+/* ---- bond observation ----------------------------------------------- */
+
+/* One tick of BondObservationSystem::run (src/systems/bonds.rs:73-185) with
+ * its PairTracker (src/analysis/pairs.rs:38-94), on the device: the bound
+ * pairs (d < k_bind * sigma_ij, pairs.rs:132-174), episodes closed after
+ * `debounce` consecutive absent ticks (DEBOUNCE = 2, bonds.rs:27), a pair
+ * persistent once its episode lasts ceil(max(min_periods, 0.1) *
+ * vib_period(eps_ij, sigma_ij, mu_ij) / dt) ticks (element masses,
+ * bonds.rs:94-99), lifetimes from the tick a pair became persistent to the
+ * tick its episode closed.  The open episodes stay on the device between
+ * calls (pairs keyed by slot; gx_set_state starts afresh).  With
+ * apply_bonds the persistent pairs replace the handle's bond list (the Bonds
+ * component the next force pass reads, bonds.rs:116-121). */
+typedef struct {
+    uint64_t tick;               /* Time::tick passed in */
+    uint64_t bound_pairs;        /* bound pairs this tick */
+    uint64_t bonded_pairs;       /* BondObservation::bonded_pairs */
+    uint64_t bonded_entities;    /* BondObservation::bonded_entities */
+    double mean_coordination;    /* BondObservation::mean_coordination */
+    uint64_t bonds_formed;       /* cumulative, BondObservation::bonds_formed */
+    double lifetime_sum_ticks;   /* cumulative, BondObservation::lifetime_sum_ticks */
+    uint64_t open_episodes;      /* PairTracker::open_count */
+    uint64_t completed_episodes; /* PairTracker::completed().len() */
+    uint64_t completed_ticks;    /* sum of the completed episodes' ticks */
+    uint64_t species_matrix[GX_NELEM * GX_NELEM]; /* BondObservation::species_matrix */
+} gx_bond_observation;
+
+int gx_bond_observe(gx_handle* h, double k_bind, double min_periods, int debounce, uint64_t tick,
+                    int apply_bonds, gx_bond_observation* out);
+/* Drops the open episodes and the cumulative counts. */
+int gx_bond_tracker_reset(gx_handle* h);
+/* The handle's bond list as slot pairs (a < b for observed bonds). */
+int gx_get_bonds(gx_handle* h, uint32_t* pairs, size_t cap, size_t* nbonds);
+
 /* Per-tick column sync of a drop-in system whose ECS lives on the host:
  * overwrite Position, Velocity and Acceleration (slot order, AoS f64) of the
  * resident atoms without touching the static columns (AtomType, Mass,

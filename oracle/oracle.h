@@ -130,6 +130,24 @@ int orc_adjoint_trajectory(const orc_params* p, size_t n, double* pos, double* v
                            const uint8_t* elem, const double* charge, const double* mass,
                            int nsteps, int nthreads, double* potential);
 
+/* ---- bond observation (oracle_bonds.cpp) ----
+ * A stateful restatement of PairTracker + BondObservationSystem::run
+ * (src/analysis/pairs.rs:38-94, src/systems/bonds.rs:73-185), pairs keyed by
+ * slot.  orc_bond_observe feeds one tick's bound pairs (slot pairs, any
+ * orientation) and returns stats[8] = {bonded_pairs, bonded_entities,
+ * mean_coordination, bonds_formed, lifetime_sum_ticks, open episodes,
+ * completed episodes, completed ticks}, the 10x10 species matrix and the
+ * persistent pairs (a < b, ascending) -- the Bonds adjacency. */
+typedef struct orc_tracker orc_tracker;
+orc_tracker* orc_tracker_new(int debounce);
+void orc_tracker_free(orc_tracker* t);
+void orc_tracker_close_all(orc_tracker* t);
+uint64_t orc_bond_threshold(const orc_params* p, double min_periods, int ea, int eb);
+int orc_bond_observe(orc_tracker* t, const orc_params* p, double min_periods, size_t nbound,
+                     const uint32_t* bound, const uint8_t* elem_of_slot, uint64_t tick,
+                     double* stats, uint64_t* matrix, uint32_t* persistent, size_t cap,
+                     size_t* npersistent);
+
 /* ---- lenses: src/analysis/mod.rs, src/analysis/pairs.rs ---- */
 int orc_radial_distribution(size_t n, const double* pos, const double box[3],
                             double r_max, size_t nbins, uint64_t* counts,

@@ -34,7 +34,8 @@ class OrcParams(C.Structure):
 
 
 def build(force: bool = False) -> Path:
-    src = [HERE / n for n in ("oracle.cpp", "oracle_dual.cpp", "oracle.h", "oracle_grid.h", "Makefile")]
+    src = [HERE / n for n in ("oracle.cpp", "oracle_dual.cpp", "oracle_bonds.cpp", "oracle.h", "oracle_grid.h",
+                               "Makefile")]
     if force or not LIB.exists() or any(p.stat().st_mtime > LIB.stat().st_mtime for p in src):
         subprocess.run(["make", "-s", "-C", str(HERE), "-B" if force else "liboracle.so"], check=True)
     return LIB
@@ -82,6 +83,12 @@ def load() -> C.CDLL:
             "orc_adjoint_forward": (C.c_int, [pp, sz, dp, dp, dp, u8p, dp, dp, C.c_int, C.c_int, C.c_int, _D, _D,
                                               _D, C.c_int, dp, dp, dp, dp]),
             "orc_adjoint_trajectory": (C.c_int, [pp, sz, dp, dp, dp, u8p, dp, dp, C.c_int, C.c_int, dp]),
+            "orc_tracker_new": (C.c_void_p, [C.c_int]),
+            "orc_tracker_free": (None, [C.c_void_p]),
+            "orc_tracker_close_all": (None, [C.c_void_p]),
+            "orc_bond_threshold": (C.c_uint64, [pp, _D, C.c_int, C.c_int]),
+            "orc_bond_observe": (C.c_int, [C.c_void_p, pp, _D, sz, u32p, u8p, C.c_uint64, dp, u64p, u32p, sz,
+                                           C.POINTER(sz)]),
         }
         for name, (res, args) in proto.items():
             f = getattr(lib, name)
@@ -358,3 +365,48 @@ def adjoint_trajectory(cfg, pos, vel, acc, elem, charge, mass, nsteps, nthreads=
     if rc != 0:
         raise ValueError(f"orc_adjoint_trajectory failed ({rc})")
     return pos, vel, acc, V
+
+
+BOND_STATS = ("bonded_pairs", "bonded_entities", "mean_coordination", "bonds_formed", "lifetime_sum_ticks",
+              "open_episodes", "completed_episodes", "completed_ticks")
+
+
+class BondTracker:
+    """PairTracker + BondObservationSystem (oracle_bonds.cpp), pairs by slot."""
+
+    def __init__(self, cfg, debounce: int = 2, min_periods: float | None = None):
+        self.lib = load()
+        self.p = params(cfg)
+        self.min_periods = cfg.bond_min_periods if min_periods is None else min_periods
+        self.t = self.lib.orc_tracker_new(debounce)
+
+    def threshold(self, ea: int, eb: int) -> int:
+        return int(self.lib.orc_bond_threshold(C.byref(self.p), self.min_periods, ea, eb))
+
+    def observe(self, bound, elem_of_slot, tick: int):
+        """bound: (k, 2) slot pairs of this tick.  Returns (stats dict with a
+        10x10 'species_matrix', persistent pairs (m, 2) ascending)."""
+        bound = np.ascontiguousarray(np.asarray(bound, dtype=np.uint32).reshape(-1, 2))
+        elem = np.ascontiguousarray(elem_of_slot, dtype=np.uint8)
+        st = np.zeros(8)
+        mat = np.zeros(100, dtype=np.uint64)
+        cap = max(len(bound), 1)
+        out = np.zeros((cap, 2), dtype=np.uint32)
+        n = C.c_size_t()
+        rc = self.lib.orc_bond_observe(self.t, C.byref(self.p), self.min_periods, len(bound), _p(bound, C.c_uint32),
+                                       _p(elem, C.c_uint8), tick, _p(st, C.c_double), _p(mat, C.c_uint64),
+                                       _p(out, C.c_uint32), cap, C.byref(n))
+        if rc != 0:
+            raise ValueError("orc_bond_observe failed")
+        d = dict(zip(BOND_STATS, st.tolist()))
+        d["species_matrix"] = mat.reshape(10, 10)
+        return d, out[: n.value].copy()
+
+    def close_all(self):
+        self.lib.orc_tracker_close_all(self.t)
+
+    def __del__(self):
+        try:
+            self.lib.orc_tracker_free(self.t)
+        except Exception:
+            pass

@@ -178,7 +178,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_params_layout_matches_header():
-    from genesis_b200._lib import GxAdjointSpec, GxParams, GxTickStats
+    from genesis_b200._lib import GxAdjointSpec, GxBondObservation, GxParams, GxTickStats
     src = """
 #include <stddef.h>
 #include <stdio.h>
@@ -189,6 +189,8 @@ int main(void) {
          offsetof(gx_tick_stats, pairs));
   printf("%zu %zu %zu\\n", sizeof(gx_adjoint_spec), offsetof(gx_adjoint_spec, gr_rmax),
          offsetof(gx_adjoint_spec, gr_support));
+  printf("%zu %zu %zu\\n", sizeof(gx_bond_observation), offsetof(gx_bond_observation, lifetime_sum_ticks),
+         offsetof(gx_bond_observation, species_matrix));
   return 0;
 }
 """
@@ -200,7 +202,9 @@ int main(void) {
         got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     want = [ctypes.sizeof(GxParams), GxParams.enable_electrostatics.offset, GxParams.precision.offset,
             GxParams.device.offset, ctypes.sizeof(GxTickStats), GxTickStats.pairs.offset,
-            ctypes.sizeof(GxAdjointSpec), GxAdjointSpec.gr_rmax.offset, GxAdjointSpec.gr_support.offset]
+            ctypes.sizeof(GxAdjointSpec), GxAdjointSpec.gr_rmax.offset, GxAdjointSpec.gr_support.offset,
+            ctypes.sizeof(GxBondObservation), GxBondObservation.lifetime_sum_ticks.offset,
+            GxBondObservation.species_matrix.offset]
     assert got == want
 
 
