@@ -314,6 +314,98 @@ def adjoint_leg(dev: int) -> dict:
             "timing": "host wall clock around the synchronous C-ABI calls"}
 
 
+def ionic_leg(dev: int, cpu: bool, steps: int | None = None, cpu_budget_s: float = 10.0) -> dict:
+    """The C2 workload run whole: 32,768 Na+/O- atoms (32^3 lattice), LJ +
+    Coulomb, Berendsen at 300 K, bond observation every tick with the
+    persistent pairs driving the spring from the next tick on, 5,000 ticks,
+    through the mixed and the plain FP64 path; the mixed pass's force error
+    against FP64 on the final state with its bonds; with `cpu`, the oracle's
+    threaded tick plus the same observation on the host cores over a
+    bounded sample."""
+    import numpy as np
+
+    from genesis_b200 import elements as E
+    from genesis_b200 import workloads as W
+    from genesis_b200._lib import Handle
+
+    wl = W.C2
+    cfg, u = wl.config(), wl.generate()
+    steps = steps or wl.steps
+    kb, mp = cfg.bond_k_bind, cfg.bond_min_periods
+    out = {"workload": f"{wl.name}: {u.n} atoms, Na+/O- 50/50 shuffled, LJ + Coulomb, Berendsen 300 K, bond "
+                       f"observation every tick (k_bind {kb}, min_periods {mp}) feeding the spring, {steps} ticks",
+           "timing": "host wall clock over the whole run from the generated state: gx_step(1) as a captured "
+                     "tick + gx_bond_observe every tick"}
+    final = {}
+    for prec in ("mixed", "fp64"):
+        with Handle(cfg, prec, dev) as h:
+            h.set_universe(u)
+            variant = None
+            if prec == "mixed":
+                variant, _ = h.autotune(reps=3)  # state unchanged
+            ob = None
+            l0 = h.launches
+            h.synchronize()
+            t0 = time.perf_counter()
+            for t in range(1, steps + 1):
+                h.step(1, stats=False, graph=True)
+                ob = h.bond_observe(kb, mp, t)
+            h.synchronize()
+            el = time.perf_counter() - t0
+            launches = h.launches - l0
+            final[prec] = (h.get_state(), h.get_bonds())
+            # the same ticks without the observation, from the final state
+            # with its final bonds: the cost of the tick alone
+            h.step(3, stats=False, graph=True)
+            h.synchronize()
+            k2 = min(steps, 1000)
+            h.mark(0)
+            h.step(k2, stats=False, graph=True)
+            h.mark(1)
+            tick_ms = h.elapsed_ms(0, 1) / k2
+            out[prec] = {"value": u.n * steps / el, "unit": UNIT, "ms_per_step": el * 1e3 / steps,
+                         "tick_only_ms": tick_ms, "gpu_launches": launches, "kernel_variant": variant,
+                         "end": {"bound_pairs": ob["bound_pairs"], "bonded_pairs": ob["bonded_pairs"],
+                                 "bonds_formed": ob["bonds_formed"], "mean_coordination": ob["mean_coordination"],
+                                 "completed_episodes": ob["completed_episodes"]}}
+    out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    (pos, vel, _), bonds = final["mixed"]
+    res = {}
+    for prec in ("mixed", "fp64"):
+        with Handle(cfg, prec, dev) as h:
+            h.set_state(pos, vel, u.elem, charge=u.charge, mass=u.mass, entity=u.entity)
+            h.set_bonds(bonds)
+            V, Vb, _ = h.forces()
+            res[prec] = (h.get_state()[2], V, Vb)
+    am, Vm, Vbm = res["mixed"]
+    a64, V64, Vb64 = res["fp64"]
+    out["force_rel_rms_vs_fp64"] = float(np.linalg.norm(am - a64) / np.linalg.norm(a64))
+    out["potential_rel_err_vs_fp64"] = abs(Vm - V64) / abs(V64)
+    out["bond_energy_rel_err_vs_fp64"] = abs(Vbm - Vb64) / abs(Vb64) if Vb64 else None
+    out["bonds_in_accuracy_state"] = int(len(bonds))
+    if cpu:
+        from oracle import oracle
+
+        threads = os.cpu_count() or 1
+        tr = oracle.BondTracker(cfg, debounce=E.DEBOUNCE)
+        p, v, a = u.pos, u.vel, None
+        bl = np.zeros((0, 2), dtype=np.uint32)
+        ticks, el = 0, 0.0
+        while el < cpu_budget_s or ticks == 0:
+            t0 = time.perf_counter()
+            p, v, a, _ = oracle.ticks(cfg, p, v, a, u.elem, u.charge, u.mass, 1, bonds=bl, nthreads=threads)
+            bp = oracle.bound_pairs(p, u.elem, u.entity, cfg.size, kb, cfg.sigma)
+            _, bl = tr.observe(bp, u.elem, ticks + 1)
+            el += time.perf_counter() - t0
+            ticks += 1
+        out["cpu_baseline"] = {"value": u.n * ticks / el, "unit": UNIT, "cores": threads, "kind": "port",
+                               "sample": f"the first {ticks} ticks of the workload ({el:.1f} s): C++ restatement of "
+                                         f"the reference tick on {threads} host threads + bound pairs + pair "
+                                         "tracker, observed bonds fed back"}
+        out["mixed_over_cpu"] = out["mixed"]["value"] / out["cpu_baseline"]["value"]
+    return out
+
+
 def reference_arm(args, dist):
     if dist.rank != 0:
         return
@@ -511,6 +603,10 @@ def ours_arm(args, dist):
             extras["adjoint"] = adjoint_leg(dev)
         except Exception as e:  # noqa: BLE001
             extras["adjoint_error"] = repr(e)
+        try:
+            extras["ionic"] = ionic_leg(dev, cpu=dist.rank == 0 and dist.world == 1)
+        except Exception as e:  # noqa: BLE001
+            extras["ionic_error"] = repr(e)
 
         if dist.rank == 0 and dist.world == 1:
             try:

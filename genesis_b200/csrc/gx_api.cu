@@ -376,7 +376,7 @@ int gx_create(const gx_params* p, gx_handle** out) {
     cudaError_t e = cudaSetDevice(p->device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&h->dscal, 16 * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&h->dcount, 8 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&h->dcount, 16 * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMalloc(&h->derr, sizeof(uint32_t));
     if (e != cudaSuccess) {
         int rc = cuda_err(h, e, "gx_create");
@@ -385,7 +385,7 @@ int gx_create(const gx_params* p, gx_handle** out) {
     }
     double init[16] = {1.0, 0, 0, 0, 0, 1.0};
     cudaMemcpy(h->dscal, init, sizeof init, cudaMemcpyHostToDevice);
-    cudaMemset(h->dcount, 0, 8 * sizeof(unsigned long long));
+    cudaMemset(h->dcount, 0, 16 * sizeof(unsigned long long));
     cudaMemset(h->derr, 0, sizeof(uint32_t));
     *out = h;
     return GX_OK;
@@ -398,6 +398,7 @@ void gx_destroy(gx_handle* h) {
     adjoint_free(h);
     nl_free(h);
     tracker_free(h);
+    lens_free(h);
     free_buf(h->buf[0]);
     free_buf(h->buf[1]);
     cudaFree(h->key);
@@ -449,6 +450,8 @@ int gx_set_state(gx_handle* h, size_t n, const double* pos, const double* vel, c
     tracker_free(h);  // new atoms: the open episodes no longer apply
     h->lambda_pending = false;
     invalidate_graphs(h);
+    h->nbonds = 0;  // bonds name slots of the previous atoms
+    GX_CUDA(h, cudaMemsetAsync(dnbonds(h), 0, sizeof(unsigned long long), h->stream));
     StateBuf& b = h->buf[0];
     uint32_t un = (uint32_t)n;
     std::vector<double> tmp(n);
@@ -529,15 +532,21 @@ int gx_set_bonds(gx_handle* h, size_t nbonds, const uint32_t* pairs) {
     if (nbonds && !pairs) return GX_ERR_ARG;
     for (size_t k = 0; k < 2 * nbonds; ++k)
         if (pairs[k] >= h->n) return set_err(h, GX_ERR_ARG, "bond slot out of range");
-    if (nbonds > 2 * h->cap + (size_t)kRedCap * 64) return set_err(h, GX_ERR_CAPACITY, "too many bonds");
+    // earlier ticks on the stream may still read the list
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
     if (nbonds > h->bonds_cap) {
         cudaFree(h->bonds);
         h->bonds = nullptr;
         GX_CUDA(h, cudaMalloc(&h->bonds, 2 * nbonds * sizeof(uint32_t)));
         h->bonds_cap = nbonds;
+        invalidate_graphs(h);  // captured ticks hold the old buffer
     }
-    if (nbonds) GX_CUDA(h, cudaMemcpy(h->bonds, pairs, 2 * nbonds * sizeof(uint32_t), cudaMemcpyHostToDevice));
-    if (nbonds != h->nbonds) invalidate_graphs(h);
+    unsigned long long cnt = nbonds;
+    if (nbonds)
+        GX_CUDA(h, cudaMemcpyAsync(h->bonds, pairs, 2 * nbonds * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                   h->stream));
+    GX_CUDA(h, cudaMemcpyAsync(dnbonds(h), &cnt, sizeof cnt, cudaMemcpyHostToDevice, h->stream));
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
     h->nbonds = nbonds;
     return GX_OK;
 }
@@ -731,7 +740,7 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
     if (drec) GX_CUDA(h, cudaMemsetAsync(h->dcount + 5, 0, sizeof(unsigned long long), h->stream));
     const bool graph = use_graph && n && !h->prof_on;
     const uint64_t key = ((uint64_t)n << 20) ^ ((uint64_t)h->precision << 1) ^ ((uint64_t)h->kernel_variant << 3) ^
-                         ((uint64_t)(h->nbonds > 0) << 6) ^ ((uint64_t)thermo << 7) ^ ((uint64_t)h->cap << 8) ^
+                         ((uint64_t)bonds_on(h) << 6) ^ ((uint64_t)thermo << 7) ^ ((uint64_t)h->cap << 8) ^
                          ((uint64_t)use_nl << 62) ^ 1u;
     for (int s = 0; s < nsteps; ++s) {
         if (!graph) {
@@ -907,10 +916,10 @@ int gx_set_list_skin(gx_handle* h, double skin) {
 }  // extern "C"
 
 namespace gx {
-// The device bond list was rewritten in place (bond observation): captured
-// ticks stay valid unless its length or its buffer changed.
+// The device bond list and its device count were rewritten in place (bond
+// observation): captured ticks stay valid unless the buffer changed.
 void bonds_changed(gx_handle* h, size_t nbonds, bool realloc) {
-    if (realloc || nbonds != h->nbonds) invalidate_graphs(h);
+    if (realloc) invalidate_graphs(h);
     h->nbonds = nbonds;
 }
 }  // namespace gx

@@ -1,24 +1,30 @@
 // gx_bondtrack.cu -- bond observation on the device: BondObservationSystem::run
 // (src/systems/bonds.rs:73-185) with its PairTracker (src/analysis/pairs.rs:38-94).
 //
-// The reference keeps the open episodes in hash maps on the host.  Here they
-// live on the device as arrays sorted by pair key ((slot a << 32) | slot b,
-// a < b; the slot-entity map is fixed for a handle).  One observation:
+// The reference keeps the open episodes in hash maps on the host.  Here a
+// pair (slot a < slot b; the slot-entity map is fixed for a handle) belongs
+// to its lower slot, and the open episodes of slot a sit in column a of
+// slabs laid out [k * stride + a], k < count[a], sorted by b, so that one
+// thread per slot reads them coalesced.  One observation:
 //
-//   1. the tick's bound pairs (bound_pairs_with_grid, pairs.rs:132-174),
-//      found on the device as slot pairs;
-//   2. the open keys and the tick's keys sorted together (CUB radix sort;
-//      the open entry of a key precedes its current entries);
-//   3. one thread per key: the episode's new tick count, missing count and
+//   1. the tick's bound pairs (bound_pairs_with_grid, pairs.rs:132-174) are
+//      appended to their owner's bucket, in the same column layout;
+//   2. one thread per slot sorts its bucket and merges it with its open
+//      episodes: each episode's new tick count, missing count and
 //      persistence (track_tick, pairs.rs:61-85; threshold bonds.rs:94-99),
 //      closing it after `debounce` absent ticks -- a closed persistent pair
 //      is a formed bond with lifetime now - since (bonds.rs:155-167);
-//   4. scans compact the open set and emit the persistent pairs, which
-//      become the handle's bond list (the Bonds component the next force
-//      pass reads, bonds.rs:116-121), with the species matrix and the number
-//      of bonded atoms.
-// Every count is an integer, so the result does not depend on scheduling.
-#include <cub/device/device_radix_sort.cuh>
+//   3. a scan of the per-slot persistent counts places the persistent pairs,
+//      in (a, b) order, in the handle's bond list (the Bonds component the
+//      next force pass reads, bonds.rs:116-121), with the species matrix and
+//      the number of bonded atoms, and commits the new episodes.
+// Every launch is sized by the atom count alone, so after a first eager
+// observation the launches are captured as a CUDA graph (one per cell-buffer
+// parity; the tick number is read from device memory), and the host
+// synchronises once, for the summary.  A bucket, slab or bond list too shallow for the
+// tick leaves the open episodes as they were: the host deepens it and
+// observes the tick again.  Every count is an integer, so the result does
+// not depend on scheduling.
 #include <cub/device/device_scan.cuh>
 
 #include <cmath>
@@ -28,201 +34,381 @@
 
 namespace gx {
 
-int bound_pairs_device(gx_handle* h, double k_bind, uint32_t* out, size_t cap, unsigned long long* dcount);
+int bound_buckets_device(gx_handle* h, void** pool, double k_bind, uint32_t* bucket, uint32_t* bcnt, uint32_t depth,
+                         size_t stride);
+void aux_pool_free(void* pool);
 void bonds_changed(gx_handle* h, size_t nbonds, bool realloc);
 
 namespace {
 
 constexpr uint64_t kNever = ~0ull;
-constexpr uint32_t kCurrent = 0x80000000u;
+// A new episode's missing-count word: the count in bits 0-15, and for a
+// persistent pair the flag kPers with its rank among the column's
+// persistent pairs in bits 16-30.
+constexpr uint32_t kPers = 0x80000000u;
+constexpr uint32_t kMissMask = 0xFFFFu;
+constexpr uint32_t kMaxDebounce = 0xFFFFu, kMaxSlab = 0x7FFFu;
+constexpr int kThreads = 64;  // 512 blocks at 32,768 atoms: every SM busy
 // device counters: [0] bound pairs this tick, [1] completed episodes,
 // [2] their ticks, [3] bonds formed, [4] lifetime sum, [5] bonded atoms,
-// [6..105] species matrix, [106] open episodes after, [107] persistent pairs
-constexpr int kNCount = 108;
+// [6..105] species matrix, [106] open episodes after, [107] persistent pairs,
+// [108] deepest bucket when deeper than allotted, [109] deepest slab column
+// likewise, [110] nonzero when the tick was not committed
+constexpr int kNCount = 112;
+constexpr int kOpenAfter = 106, kPersistent = 107, kNeedBucket = 108, kNeedSlab = 109, kRedo = 110;
 // AtomType::mass, src/components/atom_type.rs:80-93
 const double kElemMass[kNElem] = {1.008, 4.0026, 12.011, 14.007, 15.999, 22.99, 28.085, 30.974, 32.06, 55.845};
 
 inline unsigned nblk(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
-__global__ void k_bt_keys(const uint64_t* __restrict__ key, size_t M, const uint32_t* __restrict__ bound, size_t C,
-                          uint64_t* __restrict__ ck, uint32_t* __restrict__ cv) {
-    size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < M) {
-        ck[s] = key[s];
-        cv[s] = (uint32_t)s;
-    } else if (s < M + C) {
-        size_t j = s - M;
-        uint32_t a = bound[2 * j], b = bound[2 * j + 1];
-        if (b < a) {
-            uint32_t t = a;
-            a = b;
-            b = t;
-        }
-        ck[s] = ((uint64_t)a << 32) | b;
-        cv[s] = kCurrent | (uint32_t)j;
-    }
-}
+}  // namespace
 
-__global__ void k_bt_merge(const uint64_t* __restrict__ ck, const uint32_t* __restrict__ cv, size_t total,
-                           const uint32_t* __restrict__ ticks, const uint32_t* __restrict__ miss,
-                           const uint64_t* __restrict__ since, uint64_t* __restrict__ nkey,
-                           uint32_t* __restrict__ nticks, uint32_t* __restrict__ nmiss, uint64_t* __restrict__ nsince,
-                           uint32_t* __restrict__ keep, uint32_t* __restrict__ pers, const uint32_t* __restrict__ thr,
-                           const uint8_t* __restrict__ elem, const uint32_t* __restrict__ pos_of_slot,
-                           uint32_t debounce, uint64_t now, unsigned long long* __restrict__ dc) {
-    size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= total) return;
-    keep[s] = 0u;
-    pers[s] = 0u;
-    const uint64_t k = ck[s];
-    if (s > 0 && ck[s - 1] == k) return;  // not the first entry of its key
-    long long o = -1;
-    bool cur = false;
-    for (size_t t = s; t < total && ck[t] == k; ++t) {
-        const uint32_t v = cv[t];
-        if (v & kCurrent) cur = true;
-        else o = v;
+// Open episodes of every slot, column layout.
+struct Slab {
+    uint32_t* b = nullptr;      // partner slot
+    uint32_t* ticks = nullptr;  // ticks bound (pairs.rs:64-67)
+    uint32_t* miss = nullptr;   // consecutive absent ticks
+    uint64_t* since = nullptr;  // tick the pair became persistent, or never
+    uint32_t* cnt = nullptr;    // episodes per slot
+};
+
+namespace {
+
+// A slot's column: this tick's partners and its open episodes, read from the
+// bucket and slab (Global) or from per-thread copies when short (Local).
+struct GlobalCol {
+    uint32_t* bucket;
+    const Slab* o;
+    size_t S;
+    uint32_t a;
+    __device__ uint32_t cur(uint32_t i) const { return bucket[(size_t)i * S + a]; }
+    __device__ void set_cur(uint32_t i, uint32_t v) const { bucket[(size_t)i * S + a] = v; }
+    __device__ uint32_t b(uint32_t j) const { return o->b[(size_t)j * S + a]; }
+    __device__ uint32_t ticks(uint32_t j) const { return o->ticks[(size_t)j * S + a]; }
+    __device__ uint32_t miss(uint32_t j) const { return o->miss[(size_t)j * S + a]; }
+    __device__ uint64_t since(uint32_t j) const { return o->since[(size_t)j * S + a]; }
+};
+
+constexpr uint32_t kLocal = 16;
+
+struct LocalCol {
+    uint32_t c_[kLocal], b_[kLocal], t_[kLocal], m_[kLocal];
+    uint64_t s_[kLocal];
+    __device__ uint32_t cur(uint32_t i) const { return c_[i]; }
+    __device__ void set_cur(uint32_t i, uint32_t v) { c_[i] = v; }
+    __device__ uint32_t b(uint32_t j) const { return b_[j]; }
+    __device__ uint32_t ticks(uint32_t j) const { return t_[j]; }
+    __device__ uint32_t miss(uint32_t j) const { return m_[j]; }
+    __device__ uint64_t since(uint32_t j) const { return s_[j]; }
+};
+
+struct MergeOut {
+    uint32_t nw, np;
+    unsigned long long done, done_ticks, formed, life;
+};
+
+// Sorts the column's c partners and merges them with its oc open episodes:
+// track_tick (pairs.rs:61-85) and the persistence and bond bookkeeping of
+// BondObservationSystem::run (bonds.rs:130-171) for one slot.
+template <class Col>
+__device__ MergeOut merge_column(Col& col, uint32_t c, uint32_t oc, uint32_t a, int ea, size_t S, uint32_t slab,
+                                 const Slab& w, const uint32_t* sthr, const uint8_t* __restrict__ eslot,
+                                 uint32_t* __restrict__ mark, unsigned int* sm, uint32_t debounce, uint64_t now) {
+    for (uint32_t i = 1; i < c; ++i) {  // ascending (a column holds a few)
+        const uint32_t v = col.cur(i);
+        uint32_t j = i;
+        for (; j > 0; --j) {
+            const uint32_t u = col.cur(j - 1);
+            if (u <= v) break;
+            col.set_cur(j, u);
+        }
+        col.set_cur(j, v);
     }
-    uint32_t tk, ms;
-    uint64_t sn;
-    if (cur) {  // pairs.rs:64-67: bound this tick
-        tk = (o >= 0 ? ticks[o] : 0u) + 1u;
-        ms = 0u;
-        sn = o >= 0 ? since[o] : kNever;
-    } else {  // pairs.rs:69-84: open but absent
-        tk = ticks[o];
-        ms = miss[o] + 1u;
-        sn = since[o];
-        if (ms >= debounce) {
-            atomicAdd(&dc[1], 1ull);
-            atomicAdd(&dc[2], (unsigned long long)tk);
-            if (sn != kNever) {
-                atomicAdd(&dc[3], 1ull);
-                atomicAdd(&dc[4], (unsigned long long)(now - sn));
+    MergeOut r = {0u, 0u, 0ull, 0ull, 0ull, 0ull};
+    uint32_t i = 0, j = 0, last = 0xFFFFFFFFu;
+    while (i < c || j < oc) {
+        const uint32_t bc = i < c ? col.cur(i) : 0xFFFFFFFFu;
+        if (i < c && bc == last) {  // the same pair twice (an axis of 2 cells)
+            ++i;
+            continue;
+        }
+        const uint32_t bo = j < oc ? col.b(j) : 0xFFFFFFFFu;
+        uint32_t b, tk, ms;
+        uint64_t sn;
+        if (bc <= bo) {  // pairs.rs:64-67: bound this tick
+            b = bc;
+            last = bc;
+            ++i;
+            if (bc == bo) {
+                tk = col.ticks(j) + 1u;
+                sn = col.since(j);
+                ++j;
+            } else {
+                tk = 1u;
+                sn = kNever;
             }
-            return;
+            ms = 0u;
+        } else {  // pairs.rs:69-84: open but absent
+            b = bo;
+            tk = col.ticks(j);
+            ms = col.miss(j) + 1u;
+            sn = col.since(j);
+            ++j;
+            if (ms >= debounce) {
+                ++r.done;
+                r.done_ticks += tk;
+                if (sn != kNever) {
+                    ++r.formed;
+                    r.life += now - sn;
+                }
+                continue;
+            }
+        }
+        const int eb = eslot[b];
+        const bool p = tk >= sthr[ea * kNElem + eb];
+        if (p && sn == kNever) sn = now;  // active_since.entry(p).or_insert(now), bonds.rs:169-171
+        if (r.nw < slab) {
+            const size_t q = (size_t)r.nw * S + a;
+            w.b[q] = b;
+            w.ticks[q] = tk;
+            w.miss[q] = ms | (p ? kPers | (r.np << 16) : 0u);
+            w.since[q] = sn;
+        }
+        ++r.nw;
+        if (p) {
+            ++r.np;
+            mark[a] = 1u;
+            mark[b] = 1u;
+            atomicAdd(&sm[ea * kNElem + eb], 1u);  // bonds.rs:143-147
+            atomicAdd(&sm[eb * kNElem + ea], 1u);
         }
     }
-    const uint32_t a = (uint32_t)(k >> 32), b = (uint32_t)k;
-    const int ea = elem[pos_of_slot[a]], eb = elem[pos_of_slot[b]];
-    const bool p = tk >= thr[ea * kNElem + eb];
-    if (p && sn == kNever) sn = now;  // active_since.entry(p).or_insert(now), bonds.rs:169-171
-    keep[s] = 1u;
-    pers[s] = p ? 1u : 0u;
-    nkey[s] = k;
-    nticks[s] = tk;
-    nmiss[s] = ms;
-    nsince[s] = sn;
+    return r;
 }
 
-__global__ void k_bt_compact(size_t total, const uint32_t* __restrict__ keep, const uint32_t* __restrict__ keep_pos,
-                             const uint32_t* __restrict__ pers, const uint32_t* __restrict__ pers_pos,
-                             const uint64_t* __restrict__ nkey, const uint32_t* __restrict__ nticks,
-                             const uint32_t* __restrict__ nmiss, const uint64_t* __restrict__ nsince,
-                             uint64_t* __restrict__ key, uint32_t* __restrict__ ticks, uint32_t* __restrict__ miss,
-                             uint64_t* __restrict__ since, uint32_t* __restrict__ bonds, uint32_t* __restrict__ mark,
-                             const uint8_t* __restrict__ elem, const uint32_t* __restrict__ pos_of_slot,
-                             unsigned long long* __restrict__ dc) {
-    size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= total) return;
-    if (s == total - 1) {
-        dc[106] = keep_pos[s] + keep[s];
-        dc[107] = pers_pos[s] + pers[s];
+__global__ void __launch_bounds__(kThreads)
+    k_bt_merge(uint32_t n, size_t S, uint32_t depth, uint32_t slab, uint32_t* __restrict__ bucket,
+               const uint32_t* __restrict__ bcnt, Slab o, Slab w, uint32_t* __restrict__ pcnt,
+               uint32_t* __restrict__ mark, const uint32_t* __restrict__ thr, const uint8_t* __restrict__ eslot,
+               uint32_t debounce, const uint64_t* __restrict__ now_p, unsigned long long* __restrict__ dc) {
+    __shared__ unsigned long long sc[6];  // completed, their ticks, formed, lifetime, open after, bound pairs
+    __shared__ unsigned int sm[kNElem * kNElem];
+    __shared__ uint32_t sthr[kNElem * kNElem];
+    for (int k = threadIdx.x; k < kNElem * kNElem; k += kThreads) {
+        sm[k] = 0u;
+        sthr[k] = thr[k];
     }
-    if (!keep[s]) return;
-    const uint32_t q = keep_pos[s];
-    key[q] = nkey[s];
-    ticks[q] = nticks[s];
-    miss[q] = nmiss[s];
-    since[q] = nsince[s];
-    if (!pers[s]) return;
-    const uint32_t a = (uint32_t)(nkey[s] >> 32), b = (uint32_t)nkey[s];
-    const uint32_t w = pers_pos[s];
-    if (bonds) {
-        bonds[2 * w] = a;
-        bonds[2 * w + 1] = b;
+    if (threadIdx.x < 6) sc[threadIdx.x] = 0ull;
+    __syncthreads();
+    const uint32_t a = blockIdx.x * kThreads + threadIdx.x;
+    if (a < n) {
+        uint32_t c = bcnt[a];
+        if (c) atomicAdd(&sc[5], (unsigned long long)c);  // every pair found, repeats included
+        if (c > depth) {
+            atomicMax(&dc[kNeedBucket], (unsigned long long)c);
+            c = depth;
+        }
+        const uint32_t oc = o.cnt[a];
+        const uint64_t now = *now_p;
+        const int ea = eslot[a];
+        MergeOut r;
+        if (c <= kLocal && oc <= kLocal) {
+            LocalCol col;  // independent loads, issued together
+            for (uint32_t i = 0; i < c; ++i) col.c_[i] = bucket[(size_t)i * S + a];
+            for (uint32_t j = 0; j < oc; ++j) {
+                const size_t e = (size_t)j * S + a;
+                col.b_[j] = o.b[e];
+                col.t_[j] = o.ticks[e];
+                col.m_[j] = o.miss[e];
+                col.s_[j] = o.since[e];
+            }
+            r = merge_column(col, c, oc, a, ea, S, slab, w, sthr, eslot, mark, sm, debounce, now);
+        } else {
+            GlobalCol col{bucket, &o, S, a};
+            r = merge_column(col, c, oc, a, ea, S, slab, w, sthr, eslot, mark, sm, debounce, now);
+        }
+        if (r.nw > slab) atomicMax(&dc[kNeedSlab], (unsigned long long)r.nw);
+        w.cnt[a] = r.nw < slab ? r.nw : slab;
+        pcnt[a] = r.np;
+        if (r.done) {
+            atomicAdd(&sc[0], r.done);
+            atomicAdd(&sc[1], r.done_ticks);
+        }
+        if (r.formed) {
+            atomicAdd(&sc[2], r.formed);
+            atomicAdd(&sc[3], r.life);
+        }
+        if (r.nw) atomicAdd(&sc[4], (unsigned long long)r.nw);
     }
-    const int ea = elem[pos_of_slot[a]], eb = elem[pos_of_slot[b]];
-    atomicAdd(&dc[6 + ea * kNElem + eb], 1ull);  // bonds.rs:143-147
-    atomicAdd(&dc[6 + eb * kNElem + ea], 1ull);
-    if (atomicExch(&mark[a], 1u) == 0u) atomicAdd(&dc[5], 1ull);
-    if (atomicExch(&mark[b], 1u) == 0u) atomicAdd(&dc[5], 1ull);
+    __syncthreads();
+    for (int k = threadIdx.x; k < kNElem * kNElem; k += kThreads)
+        if (sm[k]) atomicAdd(&dc[6 + k], (unsigned long long)sm[k]);
+    if (threadIdx.x < 4 && sc[threadIdx.x]) atomicAdd(&dc[1 + threadIdx.x], sc[threadIdx.x]);
+    if (threadIdx.x == 4 && sc[4]) atomicAdd(&dc[kOpenAfter], sc[4]);
+    if (threadIdx.x == 5 && sc[5]) atomicAdd(&dc[0], sc[5]);
+}
+
+// The element of every slot (fixed while the tracker lives).
+__global__ void k_bt_eslot(uint32_t n, const uint8_t* __restrict__ elem, const uint32_t* __restrict__ pos_of_slot,
+                           uint8_t* __restrict__ eslot) {
+    const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a < n) eslot[a] = elem[pos_of_slot[a]];
+}
+
+// One thread per slab entry (blockIdx.y = row): commits this tick's
+// episodes and writes the persistent pairs at their column's offset plus
+// their rank, so that no thread walks a column.
+__global__ void __launch_bounds__(kThreads)
+    k_bt_emit(uint32_t n, size_t S, uint32_t depth, uint32_t slab, size_t bonds_cap, Slab w, Slab o,
+              const uint32_t* __restrict__ pcnt, const uint32_t* __restrict__ poff, const uint32_t* __restrict__ mark,
+              uint32_t* __restrict__ bonds, unsigned long long* __restrict__ nbonds_dev,
+              unsigned long long* __restrict__ dc) {
+    __shared__ unsigned int smark;
+    if (threadIdx.x == 0) smark = 0u;
+    __syncthreads();
+    // the same decision in every thread: the scan and the overflow maxima
+    // are complete before this launch
+    const unsigned long long total = n ? (unsigned long long)poff[n - 1] + pcnt[n - 1] : 0ull;
+    const bool redo = dc[kNeedBucket] > depth || dc[kNeedSlab] > slab || (bonds && total > bonds_cap);
+    const uint32_t a = blockIdx.x * kThreads + threadIdx.x;
+    const uint32_t k = blockIdx.y;
+    if (k == 0) {
+        if (a < n && mark[a]) atomicAdd(&smark, 1u);
+        if (a == 0) {
+            dc[kPersistent] = total;
+            if (redo) dc[kRedo] = 1ull;
+            else if (bonds) *nbonds_dev = total;
+        }
+    }
+    if (a < n && !redo) {
+        const uint32_t c = w.cnt[a];
+        if (k == 0) o.cnt[a] = c;
+        if (k < c) {
+            const size_t e = (size_t)k * S + a;
+            const uint32_t b = w.b[e], m = w.miss[e];
+            o.b[e] = b;
+            o.ticks[e] = w.ticks[e];
+            o.miss[e] = m & kMissMask;
+            o.since[e] = w.since[e];
+            if ((m & kPers) && bonds) {
+                const size_t q = (size_t)poff[a] + ((m >> 16) & kMaxSlab);
+                bonds[2 * q] = a;
+                bonds[2 * q + 1] = b;
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && smark) atomicAdd(&dc[5], (unsigned long long)smark);
 }
 
 }  // namespace
 
+// What a captured observation depends on.
+struct ObsKey {
+    uint64_t n, depth, slab, apply, debounce, bonds_cap;
+    double k_bind;
+    const void *bonds, *pos_of_slot, *elem, *x, *bucket, *open, *next;
+};
+
 struct BondTracker {
-    size_t cap = 0;   // open episodes + bound pairs a merge can hold
-    size_t bcap = 0;  // bound pairs of one tick
-    size_t ncap = 0;  // atoms (marks)
-    size_t M = 0;     // open episodes
-    uint64_t *key = nullptr, *since = nullptr, *ck = nullptr, *ck2 = nullptr, *nkey = nullptr, *nsince = nullptr;
-    uint32_t *ticks = nullptr, *miss = nullptr, *cv = nullptr, *cv2 = nullptr, *nticks = nullptr, *nmiss = nullptr;
-    uint32_t *keep = nullptr, *keep_pos = nullptr, *pers = nullptr, *pers_pos = nullptr;
-    uint32_t *bound = nullptr, *mark = nullptr, *thr = nullptr;
+    size_t S = 0;        // column stride: the handle's atom capacity
+    uint32_t depth = 0;  // bucket rows
+    uint32_t slab = 0;   // open-episode rows
+    Slab open, next;     // committed episodes, this tick's
+    uint32_t *bucket = nullptr, *bcnt = nullptr, *pcnt = nullptr, *poff = nullptr, *mark = nullptr;
+    uint32_t* thr = nullptr;
+    uint8_t* eslot = nullptr;  // element of each slot
     unsigned long long* dc = nullptr;
     void* temp = nullptr;
     size_t temp_bytes = 0;
     double thr_min_periods = -1.0;
     uint64_t completed = 0, completed_ticks = 0, formed = 0, lifetime = 0;
+    void* aux = nullptr;                   // bond-grid staging (gx_lens.cu)
+    uint64_t* dnow = nullptr;              // the tick observed (device)
+    uint64_t* hnow = nullptr;              // its pinned host copy
+    unsigned long long* hcounts = nullptr;  // pinned summary
+    bool warm = false;                     // an eager observation has allocated everything
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    ObsKey gkey[2];
+    uint64_t gkernels[2] = {0, 0};
 };
+
+static void slab_free(Slab& s) {
+    void* ps[] = {s.b, s.ticks, s.miss, s.since, s.cnt};
+    for (void* p : ps) cudaFree(p);
+    s = Slab();
+}
 
 void tracker_free(gx_handle* h) {
     if (!h || !h->tracker) return;
     BondTracker* t = static_cast<BondTracker*>(h->tracker);
-    void* ps[] = {t->key, t->since, t->ck, t->ck2, t->nkey, t->nsince, t->ticks, t->miss, t->cv, t->cv2,
-                  t->nticks, t->nmiss, t->keep, t->keep_pos, t->pers, t->pers_pos, t->bound, t->mark,
-                  t->thr, t->dc, t->temp};
+    slab_free(t->open);
+    slab_free(t->next);
+    void* ps[] = {t->bucket, t->bcnt, t->pcnt, t->poff, t->mark, t->thr, t->dc, t->temp, t->dnow, t->eslot};
     for (void* p : ps) cudaFree(p);
+    cudaFreeHost(t->hnow);
+    cudaFreeHost(t->hcounts);
+    for (auto& g : t->gexec)
+        if (g) cudaGraphExecDestroy(g);
+    aux_pool_free(t->aux);
     delete t;
     h->tracker = nullptr;
 }
 
 namespace {
 
-// Grows the merge arrays to hold `need` entries, keeping the open episodes.
-int ensure_merge(gx_handle* h, BondTracker* t, size_t need) {
-    if (need <= t->cap) return GX_OK;
-    size_t cap = need + need / 2 + 1024;
-    auto grow = [&](void** p, size_t elem, bool keep_old) -> int {
-        void* q = nullptr;
-        GX_CUDA(h, cudaMalloc(&q, cap * elem));
-        if (keep_old && *p && t->M) GX_CUDA(h, cudaMemcpyAsync(q, *p, t->M * elem, cudaMemcpyDeviceToDevice, h->stream));
-        GX_CUDA(h, cudaStreamSynchronize(h->stream));
-        cudaFree(*p);
-        *p = q;
-        return GX_OK;
-    };
-    int rc = 0;
-    rc |= grow((void**)&t->key, 8, true);
-    rc |= grow((void**)&t->since, 8, true);
-    rc |= grow((void**)&t->ticks, 4, true);
-    rc |= grow((void**)&t->miss, 4, true);
-    rc |= grow((void**)&t->ck, 8, false);
-    rc |= grow((void**)&t->ck2, 8, false);
-    rc |= grow((void**)&t->nkey, 8, false);
-    rc |= grow((void**)&t->nsince, 8, false);
-    rc |= grow((void**)&t->cv, 4, false);
-    rc |= grow((void**)&t->cv2, 4, false);
-    rc |= grow((void**)&t->nticks, 4, false);
-    rc |= grow((void**)&t->nmiss, 4, false);
-    rc |= grow((void**)&t->keep, 4, false);
-    rc |= grow((void**)&t->keep_pos, 4, false);
-    rc |= grow((void**)&t->pers, 4, false);
-    rc |= grow((void**)&t->pers_pos, 4, false);
-    if (rc) return GX_ERR_OOM;
-    t->cap = cap;
-    // temporary storage for the sort and the two scans at this capacity
-    size_t b1 = 0, b2 = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, b1, t->ck, t->ck2, t->cv, t->cv2, (int)cap, 0, 64, h->stream);
-    cub::DeviceScan::ExclusiveSum(nullptr, b2, t->keep, t->keep_pos, (int)cap, h->stream);
-    size_t b = b1 > b2 ? b1 : b2;
-    if (b > t->temp_bytes) {
-        cudaFree(t->temp);
-        t->temp = nullptr;
-        GX_CUDA(h, cudaMalloc(&t->temp, b));
-        t->temp_bytes = b;
+// A slab of `rows` rows into `s`; with `old`, its first `keep_rows` rows and
+// its counts are carried over (same stride; `old` may be `s`).
+int slab_alloc(gx_handle* h, Slab& s, size_t S, uint32_t rows, const Slab* old, uint32_t keep_rows) {
+    Slab t;
+    const size_t m = (size_t)rows * S;
+    GX_CUDA(h, cudaMalloc(&t.b, m * sizeof(uint32_t)));
+    GX_CUDA(h, cudaMalloc(&t.ticks, m * sizeof(uint32_t)));
+    GX_CUDA(h, cudaMalloc(&t.miss, m * sizeof(uint32_t)));
+    GX_CUDA(h, cudaMalloc(&t.since, m * sizeof(uint64_t)));
+    GX_CUDA(h, cudaMalloc(&t.cnt, S * sizeof(uint32_t)));
+    if (old && old->b) {
+        const size_t k = (size_t)keep_rows * S;
+        GX_CUDA(h, cudaMemcpyAsync(t.b, old->b, k * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream));
+        GX_CUDA(h, cudaMemcpyAsync(t.ticks, old->ticks, k * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream));
+        GX_CUDA(h, cudaMemcpyAsync(t.miss, old->miss, k * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream));
+        GX_CUDA(h, cudaMemcpyAsync(t.since, old->since, k * sizeof(uint64_t), cudaMemcpyDeviceToDevice, h->stream));
+        GX_CUDA(h, cudaMemcpyAsync(t.cnt, old->cnt, S * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream));
+    } else {
+        GX_CUDA(h, cudaMemsetAsync(t.cnt, 0, S * sizeof(uint32_t), h->stream));
     }
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    slab_free(s);
+    s = t;
+    return GX_OK;
+}
+
+// First use: per-slot arrays at the handle's capacity, shallow bucket and slabs.
+int tracker_init(gx_handle* h, BondTracker* t) {
+    if (t->dc) return GX_OK;
+    const size_t S = h->cap;
+    t->S = S;
+    t->depth = 8;
+    t->slab = 8;
+    GX_CUDA(h, cudaMalloc(&t->dc, kNCount * sizeof(unsigned long long)));
+    GX_CUDA(h, cudaMalloc(&t->dnow, sizeof(uint64_t)));
+    GX_CUDA(h, cudaMallocHost(&t->hnow, sizeof(uint64_t)));
+    GX_CUDA(h, cudaMallocHost(&t->hcounts, kNCount * sizeof(unsigned long long)));
+    GX_CUDA(h, cudaMalloc(&t->bucket, (size_t)t->depth * S * sizeof(uint32_t)));
+    GX_CUDA(h, cudaMalloc(&t->bcnt, S * sizeof(uint32_t)));
+    GX_CUDA(h, cudaMalloc(&t->pcnt, S * sizeof(uint32_t)));
+    GX_CUDA(h, cudaMalloc(&t->poff, S * sizeof(uint32_t)));
+    GX_CUDA(h, cudaMalloc(&t->mark, S * sizeof(uint32_t)));
+    GX_CUDA(h, cudaMalloc(&t->eslot, S));
+    if (h->n)
+        GX_LAUNCH(h, k_bt_eslot, nblk(h->n, 256), 256, (uint32_t)h->n, h->buf[h->cur].elem, h->pos_of_slot, t->eslot);
+    int rc = slab_alloc(h, t->open, S, t->slab, nullptr, 0);
+    if (!rc) rc = slab_alloc(h, t->next, S, t->slab, nullptr, 0);
+    if (rc) return rc;
+    size_t tb = 0;
+    GX_CUDA(h, cub::DeviceScan::ExclusiveSum(nullptr, tb, t->pcnt, t->poff, (int)S, h->stream));
+    GX_CUDA(h, cudaMalloc(&t->temp, tb ? tb : 1));
+    t->temp_bytes = tb;
     return GX_OK;
 }
 
@@ -246,6 +432,90 @@ int upload_thresholds(gx_handle* h, BondTracker* t, double min_periods) {
     return GX_OK;
 }
 
+// The launches of one observation, from the tick number in t->dnow to the
+// summary in t->hcounts.
+int observe_launches(gx_handle* h, BondTracker* t, double k_bind, uint32_t debounce, bool apply) {
+    const uint32_t n = (uint32_t)h->n;
+    const size_t S = t->S;
+    GX_CUDA(h, cudaMemsetAsync(t->dc, 0, kNCount * sizeof(unsigned long long), h->stream));
+    if (n) {
+        GX_CUDA(h, cudaMemsetAsync(t->bcnt, 0, n * sizeof(uint32_t), h->stream));
+        GX_CUDA(h, cudaMemsetAsync(t->mark, 0, n * sizeof(uint32_t), h->stream));
+        int rc = bound_buckets_device(h, &t->aux, k_bind, t->bucket, t->bcnt, t->depth, S);
+        if (rc) return rc;
+        prof_begin(h, "bond_merge");
+        GX_LAUNCH(h, k_bt_merge, nblk(n, kThreads), kThreads, n, S, t->depth, t->slab, t->bucket, t->bcnt, t->open,
+                  t->next, t->pcnt, t->mark, t->thr, t->eslot, debounce, t->dnow, t->dc);
+        size_t tb = t->temp_bytes;
+        GX_CUDA(h, cub::DeviceScan::ExclusiveSum(t->temp, tb, t->pcnt, t->poff, (int)n, h->stream));
+        GX_LAUNCH(h, k_bt_emit, dim3(nblk(n, kThreads), t->slab), kThreads, n, S, t->depth, t->slab,
+                  apply ? h->bonds_cap : 0,
+                  t->next, t->open, t->pcnt, t->poff, t->mark, apply ? h->bonds : nullptr, dnbonds(h), t->dc);
+        prof_end(h, "bond_merge");
+    } else if (apply) {
+        GX_CUDA(h, cudaMemsetAsync(dnbonds(h), 0, sizeof(unsigned long long), h->stream));
+    }
+    GX_CUDA(h, cudaMemcpyAsync(t->hcounts, t->dc, kNCount * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                               h->stream));
+    return GX_OK;
+}
+
+// One attempt at the tick, captured once its launches are known to need no
+// allocation; the summary lands in t->hcounts.
+int observe_once(gx_handle* h, BondTracker* t, double k_bind, uint32_t debounce, uint64_t tick, bool apply,
+                 bool graph) {
+    *t->hnow = tick;  // the previous observation synchronised: its copy has run
+    GX_CUDA(h, cudaMemcpyAsync(t->dnow, t->hnow, sizeof(uint64_t), cudaMemcpyHostToDevice, h->stream));
+    if (!graph || !t->warm || h->prof_on) {
+        int rc = observe_launches(h, t, k_bind, debounce, apply);
+        if (rc) return rc;
+    } else {
+        ObsKey k;
+        std::memset(&k, 0, sizeof k);
+        k.n = h->n;
+        k.depth = t->depth;
+        k.slab = t->slab;
+        k.apply = apply;
+        k.debounce = debounce;
+        k.bonds_cap = h->bonds_cap;
+        k.k_bind = k_bind;
+        k.bonds = h->bonds;
+        k.pos_of_slot = h->pos_of_slot;
+        k.elem = h->buf[h->cur].elem;
+        k.x = h->buf[h->cur].x;
+        k.bucket = t->bucket;
+        k.open = t->open.b;
+        k.next = t->next.b;
+        const int par = h->cur & 1;
+        if (!t->gexec[par] || std::memcmp(&k, &t->gkey[par], sizeof k) != 0) {
+            if (t->gexec[par]) cudaGraphExecDestroy(t->gexec[par]);
+            t->gexec[par] = nullptr;
+            const uint64_t l0 = h->launches;
+            GX_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+            int rc = observe_launches(h, t, k_bind, debounce, apply);
+            cudaGraph_t gr = nullptr;
+            cudaError_t ce = cudaStreamEndCapture(h->stream, &gr);
+            if (rc || ce != cudaSuccess) {
+                if (gr) cudaGraphDestroy(gr);
+                return rc ? rc : cuda_err(h, ce, "cudaStreamEndCapture");
+            }
+            cudaGraphExec_t ex = nullptr;
+            ce = cudaGraphInstantiate(&ex, gr, 0);
+            cudaGraphDestroy(gr);
+            if (ce != cudaSuccess) return cuda_err(h, ce, "cudaGraphInstantiate");
+            t->gexec[par] = ex;
+            t->gkey[par] = k;
+            t->gkernels[par] = h->launches - l0;
+            h->launches = l0;
+        }
+        GX_CUDA(h, cudaGraphLaunch(t->gexec[par], h->stream));
+        h->launches += t->gkernels[par];
+    }
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    GX_CUDA(h, cudaGetLastError());
+    return GX_OK;
+}
+
 }  // namespace
 }  // namespace gx
 
@@ -256,95 +526,67 @@ extern "C" {
 int gx_bond_observe(gx_handle* h, double k_bind, double min_periods, int debounce, uint64_t tick, int apply_bonds,
                     gx_bond_observation* out) {
     if (!h || !out || debounce < 1 || !(k_bind > 0.0)) return GX_ERR_ARG;
+    if ((uint32_t)debounce > kMaxDebounce) return set_err(h, GX_ERR_ARG, "debounce above 65535 ticks");
     if (!h->cap) return set_err(h, GX_ERR_STATE, "no state uploaded (call gx_set_state first)");
     if (!h->tracker) h->tracker = new BondTracker();
     BondTracker* t = static_cast<BondTracker*>(h->tracker);
-    const size_t n = h->n;
-    int rc = upload_thresholds(h, t, min_periods);
+    int rc = tracker_init(h, t);
+    if (!rc) rc = upload_thresholds(h, t, min_periods);
     if (rc) return rc;
-    if (!t->dc) GX_CUDA(h, cudaMalloc(&t->dc, kNCount * sizeof(unsigned long long)));
-    if (t->ncap < n || !t->mark) {
-        cudaFree(t->mark);
-        t->mark = nullptr;
-        GX_CUDA(h, cudaMalloc(&t->mark, (n ? n : 1) * sizeof(uint32_t)));
-        t->ncap = n;
-    }
-    if (t->bcap < 8 * n + 1024 || !t->bound) {
-        cudaFree(t->bound);
-        t->bound = nullptr;
-        t->bcap = 8 * n + 1024;
-        GX_CUDA(h, cudaMalloc(&t->bound, 2 * t->bcap * sizeof(uint32_t)));
-    }
-    // 1. bound pairs; grow and repeat once if this tick has more than fit
-    unsigned long long C = 0;
-    for (int attempt = 0; attempt < 2; ++attempt) {
-        GX_CUDA(h, cudaMemsetAsync(t->dc, 0, kNCount * sizeof(unsigned long long), h->stream));
-        if ((rc = bound_pairs_device(h, k_bind, t->bound, t->bcap, t->dc))) return rc;
-        GX_CUDA(h, cudaMemcpyAsync(&C, t->dc, sizeof C, cudaMemcpyDeviceToHost, h->stream));
-        GX_CUDA(h, cudaStreamSynchronize(h->stream));
-        if (C <= t->bcap) break;
-        cudaFree(t->bound);
-        t->bound = nullptr;
-        t->bcap = (size_t)C + C / 2;
-        GX_CUDA(h, cudaMalloc(&t->bound, 2 * t->bcap * sizeof(uint32_t)));
-    }
-    if (C > t->bcap) return set_err(h, GX_ERR_CAPACITY, "bound-pair buffer");
-    const size_t M = t->M, total = M + (size_t)C;
-    if ((rc = ensure_merge(h, t, total))) return rc;
-    // the bond list must hold every persistent pair (at most all of them)
-    const bool grow_bonds = apply_bonds && total > h->bonds_cap;
-    if (grow_bonds) {
-        cudaFree(h->bonds);
-        h->bonds = nullptr;
-        size_t bc = total + total / 2 + 1024;
-        GX_CUDA(h, cudaMalloc(&h->bonds, 2 * bc * sizeof(uint32_t)));
-        h->bonds_cap = bc;
+    bool grew_bonds = false;
+    if (apply_bonds && !h->bonds) {  // a first bond list: the spring is on from now
+        GX_CUDA(h, cudaMalloc(&h->bonds, 2 * 1024 * sizeof(uint32_t)));
+        h->bonds_cap = 1024;
         h->nbonds = 0;
+        grew_bonds = true;
     }
-    StateBuf& b = h->buf[h->cur];
-    uint64_t persistent = 0, open_after = 0, counts[kNCount];
-    std::memset(counts, 0, sizeof counts);
-    if (total) {
-        // 2. sort the open keys and this tick's keys together
-        GX_LAUNCH(h, k_bt_keys, nblk(total, 256), 256, t->key, M, t->bound, (size_t)C, t->ck, t->cv);
-        int bits = 1;
-        while (bits < 32 && (1ull << bits) < (unsigned long long)n) ++bits;
-        size_t tb = t->temp_bytes;
-        GX_CUDA(h, cub::DeviceRadixSort::SortPairs(t->temp, tb, t->ck, t->ck2, t->cv, t->cv2, (int)total, 0, 32 + bits,
-                                                    h->stream));
-        // 3. advance every episode
-        GX_LAUNCH(h, k_bt_merge, nblk(total, 256), 256, t->ck2, t->cv2, total, t->ticks, t->miss, t->since, t->nkey,
-                  t->nticks, t->nmiss, t->nsince, t->keep, t->pers, t->thr, b.elem, h->pos_of_slot,
-                  (uint32_t)debounce, tick, t->dc);
-        // 4. compact the open set, emit the persistent pairs
-        tb = t->temp_bytes;
-        GX_CUDA(h, cub::DeviceScan::ExclusiveSum(t->temp, tb, t->keep, t->keep_pos, (int)total, h->stream));
-        tb = t->temp_bytes;
-        GX_CUDA(h, cub::DeviceScan::ExclusiveSum(t->temp, tb, t->pers, t->pers_pos, (int)total, h->stream));
-        GX_CUDA(h, cudaMemsetAsync(t->mark, 0, (n ? n : 1) * sizeof(uint32_t), h->stream));
-        GX_LAUNCH(h, k_bt_compact, nblk(total, 256), 256, total, t->keep, t->keep_pos, t->pers, t->pers_pos,
-                  t->nkey, t->nticks, t->nmiss, t->nsince, t->key, t->ticks, t->miss, t->since,
-                  apply_bonds ? h->bonds : nullptr, t->mark, b.elem, h->pos_of_slot, t->dc);
-        GX_CUDA(h, cudaMemcpyAsync(counts, t->dc, sizeof counts, cudaMemcpyDeviceToHost, h->stream));
-        GX_CUDA(h, cudaStreamSynchronize(h->stream));
-        GX_CUDA(h, cudaGetLastError());
-        open_after = counts[106];
-        persistent = counts[107];
+    const unsigned long long* counts = t->hcounts;
+    for (int attempt = 0;; ++attempt) {
+        if ((rc = observe_once(h, t, k_bind, (uint32_t)debounce, tick, apply_bonds != 0, attempt == 0))) return rc;
+        if (!counts[kRedo]) break;
+        if (attempt >= 3) return set_err(h, GX_ERR_CAPACITY, "bond observation did not fit after deepening");
+        // nothing was committed: deepen what overflowed and observe again
+        if (counts[kNeedBucket] > t->depth) {
+            const uint32_t d = (uint32_t)(counts[kNeedBucket] + counts[kNeedBucket] / 2 + 2);
+            cudaFree(t->bucket);
+            t->bucket = nullptr;
+            GX_CUDA(h, cudaMalloc(&t->bucket, (size_t)d * t->S * sizeof(uint32_t)));
+            t->depth = d;
+        }
+        if (counts[kNeedSlab] > t->slab) {
+            if (counts[kNeedSlab] > kMaxSlab)
+                return set_err(h, GX_ERR_CAPACITY, "more than 32767 open bond episodes on one atom");
+            uint32_t d = (uint32_t)(counts[kNeedSlab] + counts[kNeedSlab] / 2 + 2);
+            if (d > kMaxSlab) d = kMaxSlab;
+            if ((rc = slab_alloc(h, t->open, t->S, d, &t->open, t->slab))) return rc;
+            if ((rc = slab_alloc(h, t->next, t->S, d, nullptr, 0))) return rc;
+            t->slab = d;
+        }
+        if (apply_bonds && counts[kPersistent] > h->bonds_cap) {
+            cudaFree(h->bonds);
+            h->bonds = nullptr;
+            h->nbonds = 0;
+            const size_t bc = counts[kPersistent] + counts[kPersistent] / 2 + 1024;
+            GX_CUDA(h, cudaMalloc(&h->bonds, 2 * bc * sizeof(uint32_t)));
+            h->bonds_cap = bc;
+            grew_bonds = true;
+        }
     }
-    t->M = (size_t)open_after;
+    t->warm = true;
+    const uint64_t persistent = counts[kPersistent];
     t->completed += counts[1];
     t->completed_ticks += counts[2];
     t->formed += counts[3];
     t->lifetime += counts[4];
-    if (apply_bonds) bonds_changed(h, (size_t)persistent, grow_bonds);
+    if (apply_bonds) bonds_changed(h, (size_t)persistent, grew_bonds);
     out->tick = tick;
-    out->bound_pairs = C;
+    out->bound_pairs = counts[0];
     out->bonded_pairs = persistent;
     out->bonded_entities = counts[5];
     out->mean_coordination = counts[5] ? 2.0 * (double)persistent / (double)counts[5] : 0.0;  // bonds.rs:173-177
     out->bonds_formed = t->formed;
     out->lifetime_sum_ticks = (double)t->lifetime;
-    out->open_episodes = open_after;
+    out->open_episodes = counts[kOpenAfter];
     out->completed_episodes = t->completed;
     out->completed_ticks = t->completed_ticks;
     for (int k = 0; k < kNElem * kNElem; ++k) out->species_matrix[k] = counts[6 + k];

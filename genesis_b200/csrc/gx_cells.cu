@@ -319,6 +319,13 @@ static void scan_rec(gx_handle* h, CellList& cl, const uint32_t* in, uint32_t* o
     GX_LAUNCH(h, k_scan_add, nblk(n, 256), 256, out, n, sums, gate);
 }
 
+// Exclusive scan of cl.count (ncell + 1 entries) into cl.start.
+void cell_scan(gx_handle* h, CellList& cl, uint32_t ncell) {
+    prof_begin(h, "cell_scan");
+    scan_rec(h, cl, cl.count, cl.start, ncell + 1, 0, nullptr);
+    prof_end(h, "cell_scan");
+}
+
 int counting_sort(gx_handle* h, CellList& cl, uint32_t ncell, const uint32_t* key, uint32_t n, uint32_t* perm,
                   const uint32_t* gate) {
     int rc = ensure_cells(h, cl, ncell);

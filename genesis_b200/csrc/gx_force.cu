@@ -213,17 +213,21 @@ __global__ void k_fix_to_acc(StateBuf b, const long long* __restrict__ F, size_t
 
 // Observed-bond spring (src/systems/forces.rs:305-317, bond_harmonic_raw
 // forces.rs:290-293) for each bond in the list, applied as many times as the
-// reference's pair list holds the pair.  FP64 in both precisions; the mixed
-// path quantises the result into the fixed-point accumulators.
+// reference's pair list holds the pair (once when `key` is null).  FP64 in
+// both precisions; the mixed path quantises the result into the fixed-point
+// accumulators.  The bond count is read on the device (at most `cap`), and
+// the fixed grid strides over it, so the launch does not change with it.
 __global__ void k_bonds(GridGeom g, StateBuf b, const uint32_t* __restrict__ key,
-                        const uint32_t* __restrict__ pos_of_slot, const uint32_t* __restrict__ bonds, size_t nbonds,
-                        LawF64 L, const double* __restrict__ psig, const double* __restrict__ peps, double k_bind,
+                        const uint32_t* __restrict__ pos_of_slot, const uint32_t* __restrict__ bonds,
+                        const unsigned long long* __restrict__ nbonds_dev, size_t cap, LawF64 L,
+                        const double* __restrict__ psig, const double* __restrict__ peps, double k_bind,
                         double r_eq_factor, double curv_factor, int mixed, long long* __restrict__ F, size_t fstride,
                         double* __restrict__ vbpart, unsigned long long* __restrict__ vbfix, uint32_t* __restrict__ err) {
     __shared__ double shd[kForceThreads / 32];
-    size_t t = (size_t)blockIdx.x * kForceThreads + threadIdx.x;
+    const size_t nbonds = min((size_t)*nbonds_dev, cap);
     double vb = 0.0;
-    if (t < nbonds) {
+    for (size_t t = (size_t)blockIdx.x * kForceThreads + threadIdx.x; t < nbonds;
+         t += (size_t)gridDim.x * kForceThreads) {
         uint32_t ia = pos_of_slot[bonds[2 * t]], ib = pos_of_slot[bonds[2 * t + 1]];
         double dx = min_image1(xsub(b.x[ia], b.x[ib]), L.box[0]);
         double dy = min_image1(xsub(b.y[ia], b.y[ib]), L.box[1]);
@@ -244,7 +248,7 @@ __global__ void k_bonds(GridGeom g, StateBuf b, const uint32_t* __restrict__ key
                 smooth_f64(d, r_eq, rc_bond, sw, dsw);
                 double fm = xsub(xmul(m, sw), xmul(v, dsw));
                 double vv = xmul(v, sw);
-                int mult = pair_multiplicity(g, key[ia], key[ib]);
+                int mult = key ? pair_multiplicity(g, key[ia], key[ib]) : 1;
                 double inv = xdiv(1.0, d);
                 double nx = xmul(dx, inv), ny = xmul(dy, inv), nz = xmul(dz, inv);
                 for (int r = 0; r < mult; ++r) {
@@ -301,13 +305,36 @@ inline unsigned nblk(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 // Device copies of the FP64 pair table (the mixed table is built in gx_api.cu).
 static double* d_psig(gx_handle* h) { return h->red + 6 * (size_t)h->cap / 64 + 6 * kRedCap; }
 
+int bond_spring(gx_handle* h, bool unit_mult) {
+    if (!bonds_on(h)) {
+        GX_CUDA(h, cudaMemsetAsync(h->dscal + 3, 0, sizeof(double), h->stream));
+        return GX_OK;
+    }
+    const bool mixed = h->precision == GX_MIXED;
+    const size_t rows = (size_t)h->cap / 64 + kRedCap;
+    double* vbpart = h->red + 1 * rows;
+    double* psig = d_psig(h);
+    unsigned grid = nblk(h->bonds_cap, kForceThreads);
+    if (grid > 4 * 148u) grid = 4 * 148u;  // four blocks per SM; the FP64 partials need grid <= rows
+    prof_begin(h, "bonds");
+    GX_LAUNCH(h, k_bonds, grid, kForceThreads, h->fgrid, h->buf[h->cur], unit_mult ? nullptr : h->key_sorted,
+              h->pos_of_slot, h->bonds, dnbonds(h), h->bonds_cap, make_law64(h), psig, psig + kNElem * kNElem,
+              h->fs.bond_k_bind, h->fs.r_eq_factor, h->fs.curv_factor, mixed ? 1 : 0, h->F, h->cap, vbpart,
+              h->dcount + 2, h->derr);
+    prof_end(h, "bonds");
+    if (mixed)
+        GX_LAUNCH(h, k_fix_to_double, 1, 1, h->dcount + 2, h->dscal + 3);
+    else
+        GX_LAUNCH(h, k_sum_rows, 1, 256, vbpart, (int)grid, h->dscal + 3);
+    return GX_OK;
+}
+
 int force_pass(gx_handle* h, bool finalize_acc, double* V, double* Vb, uint64_t* npairs_out, bool sync_out) {
     uint32_t n = (uint32_t)h->n;
     const GridGeom& g = h->fgrid;
     StateBuf& b = h->buf[h->cur];
     size_t rows = (size_t)h->cap / 64 + kRedCap;
     double* vpart = h->red + 0 * rows;
-    double* vbpart = h->red + 1 * rows;
     double* psig = d_psig(h);
     double* peps = psig + kNElem * kNElem;
     GX_CUDA(h, cudaMemsetAsync(h->dcount, 0, 4 * sizeof(unsigned long long), h->stream));
@@ -340,23 +367,13 @@ int force_pass(gx_handle* h, bool finalize_acc, double* V, double* Vb, uint64_t*
                       h->F, h->cap, h->dcount + 1, h->dcount + 0, h->derr);
         prof_end(h, "force_mixed");
     }
-    bool bonds_on = h->p.enable_bond_interaction && h->nbonds > 0;
-    if (bonds_on) {
-        prof_begin(h, "bonds");
-        GX_LAUNCH(h, k_bonds, nblk(h->nbonds, kForceThreads), kForceThreads, 
-            g, b, h->key_sorted, h->pos_of_slot, h->bonds, h->nbonds, L64, psig, peps, h->fs.bond_k_bind,
-            h->fs.r_eq_factor, h->fs.curv_factor, mixed ? 1 : 0, h->F, h->cap, vbpart, h->dcount + 2, h->derr);
-        prof_end(h, "bonds");
-    }
+    int rc = bond_spring(h, false);
+    if (rc) return rc;
     if (mixed) {
         if (finalize_acc && n) GX_LAUNCH(h, k_fix_to_acc, nblk(n, 256), 256, b, h->F, h->cap, n);
         GX_LAUNCH(h, k_fix_to_double, 1, 1, h->dcount + 1, h->dscal + 2);
-        if (bonds_on) GX_LAUNCH(h, k_fix_to_double, 1, 1, h->dcount + 2, h->dscal + 3);
-        else GX_CUDA(h, cudaMemsetAsync(h->dscal + 3, 0, sizeof(double), h->stream));
     } else {
         GX_LAUNCH(h, k_sum_rows, 1, 256, vpart, (int)fb, h->dscal + 2);
-        if (bonds_on) GX_LAUNCH(h, k_sum_rows, 1, 256, vbpart, (int)nblk(h->nbonds, kForceThreads), h->dscal + 3);
-        else GX_CUDA(h, cudaMemsetAsync(h->dscal + 3, 0, sizeof(double), h->stream));
     }
     if (sync_out) {
         double vv[2];

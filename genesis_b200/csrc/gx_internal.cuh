@@ -194,7 +194,7 @@ struct gx_handle {
     // reductions and scalars on device
     double* red = nullptr;         // block partials (several rows of kRedCap)
     double* dscal = nullptr;       // [0]=lambda pending, [1]=K, [2]=V, [3]=Vb, [4]=speed, [5]=one
-    unsigned long long* dcount = nullptr;  // [0]=pairs, [1..3]=fixed V, Vb, ...
+    unsigned long long* dcount = nullptr;  // [0]=pairs, [1..3]=fixed V, Vb, ..., [8]=bond count
     uint32_t* derr = nullptr;      // device error word
     bool lambda_pending = false;
 
@@ -204,7 +204,9 @@ struct gx_handle {
     uint8_t kind_elem[gx::kMaxKinds];
     gx::PairF* d_pairf = nullptr;  // kMaxKinds^2
 
-    // bonds (slot pairs)
+    // bonds (slot pairs).  The spring kernel reads the count from dcount[8],
+    // so a captured tick stays valid while the list changes length in place;
+    // only a new buffer (bonds_cap) changes the launch.
     uint32_t* bonds = nullptr;
     size_t nbonds = 0, bonds_cap = 0;
 
@@ -235,6 +237,7 @@ struct gx_handle {
 
     // bond observation (gx_bondtrack.cu): open episodes on the device, owned there
     void* tracker = nullptr;
+    void* lens = nullptr;     // analysis staging pool (gx_lens.cu)
 };
 
 // Every kernel launch of the library goes through this macro so the
@@ -264,6 +267,7 @@ void prof_end(gx_handle* h, const char* name);
 
 // Launchers implemented in the .cu files.
 int ensure_cells(gx_handle* h, CellList& cl, uint32_t ncell);
+void cell_scan(gx_handle* h, CellList& cl, uint32_t ncell);
 // Counting sort of atoms [0,n) by key into perm (sorted pos -> source index),
 // deterministic (ties keep ascending source index).  cl.start gets cell starts.
 // `gate` (may be null): a device word; the launches do nothing while it is 0.
@@ -278,6 +282,13 @@ void launch_build_pos4(gx_handle* h, const GridGeom& g, const StateBuf& b, const
                        uint32_t n, float4* pos4);
 
 int force_pass(gx_handle* h, bool finalize_acc, double* V, double* Vb, uint64_t* npairs, bool sync_out);
+// The observed-bond spring over the device bond list (count in dcount[8])
+// into F (mixed) or the accelerations (FP64), and its energy into dscal[3].
+// `unit_mult`: every pair within the cutoff occurs once in the reference's
+// pair list (a cell grid of at least 3 cells per axis).
+int bond_spring(gx_handle* h, bool unit_mult);
+inline bool bonds_on(const gx_handle* h) { return h->p.enable_bond_interaction && h->bonds_cap > 0; }
+inline unsigned long long* dnbonds(gx_handle* h) { return h->dcount + 8; }
 void adjoint_free(gx_handle* h);
 
 // Neighbour-list path of the mixed pass (gx_nlist.cu).
@@ -291,6 +302,7 @@ int nl_config(gx_handle* h, double* skin, int* tpp);
 int nl_set_tpp(gx_handle* h, int tpp);
 void nl_free(gx_handle* h);
 void tracker_free(gx_handle* h);
+void lens_free(gx_handle* h);
 
 void launch_kick(gx_handle* h, const StateBuf& b, uint32_t n, double half_dt, const double* lambda);
 void launch_drift(gx_handle* h, const StateBuf& b, uint32_t n, double dt);

@@ -47,18 +47,18 @@ struct AuxPool {
     size_t ncap = 0;
 };
 
-// One pool per handle, keyed by address (handles are few).
-struct PoolEntry {
-    const gx_handle* h;
-    AuxPool pool;
-};
-std::vector<PoolEntry> g_pools;
+void pool_release(AuxPool* P) {
+    if (!P) return;
+    void* ps[] = {P->xyz, P->elem, P->u32, P->parent, P->cnt, P->counts, P->cl.count, P->cl.start, P->cl.fill};
+    for (void* q : ps) cudaFree(q);
+    for (auto q : P->cl.scan_levels) cudaFree(q);
+    delete P;
+}
 
-AuxPool& pool_of(const gx_handle* h) {
-    for (auto& e : g_pools)
-        if (e.h == h) return e.pool;
-    g_pools.push_back(PoolEntry{h, AuxPool{}});
-    return g_pools.back().pool;
+// The handle's pool for the analysis calls, made on first use.
+AuxPool& pool_of(gx_handle* h) {
+    if (!h->lens) h->lens = new AuxPool();
+    return *static_cast<AuxPool*>(h->lens);
 }
 
 inline unsigned nblk(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
@@ -118,6 +118,35 @@ __global__ void k_aux_gather(const uint32_t* __restrict__ perm, uint32_t m, cons
     a.elem[p] = te[q];
     a.slot[p] = tslot[q];
     a.key[p] = key[q];
+}
+
+// The bond grid for the observation: every atom's cell, counted as it is
+// found (count holds ncell + 1 entries), then placed straight into the
+// sorted copy.  The order inside a cell is the order of the placing
+// atomics, which the half-shell enumeration does not depend on: each pair
+// of a cell is visited once (j > i) whatever the order, and pairs across
+// cells by their cells alone.
+__global__ void k_select_count(GridGeom g, StateBuf b, uint32_t m, uint32_t* __restrict__ key,
+                               uint32_t* __restrict__ count) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= m) return;
+    const uint32_t c = cell_of(g, b.x[q], b.y[q], b.z[q]);
+    key[q] = c;
+    atomicAdd(&count[c], 1u);
+}
+
+__global__ void k_place(StateBuf b, uint32_t m, const uint32_t* __restrict__ key, const uint32_t* __restrict__ start,
+                        uint32_t* __restrict__ fill, AuxSet a) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= m) return;
+    const uint32_t c = key[q];
+    const uint32_t p = start[c] + atomicAdd(&fill[c], 1u);
+    a.x[p] = b.x[q];
+    a.y[p] = b.y[q];
+    a.z[p] = b.z[q];
+    a.elem[p] = b.elem[q];
+    a.slot[p] = b.slot[q];
+    a.key[p] = c;
 }
 
 // Canonical half-shell enumeration with the exact check_pair test
@@ -267,6 +296,98 @@ struct BoundVisit {
         }
     }
 };
+
+// Bound pairs routed to their owner: the pair (slot a < slot b) is appended
+// to a's bucket [k * stride + a] (k < depth; the count runs on past the
+// depth, so an overflow shows, and the counts sum to the number of pairs
+// found, duplicates of a 2-cell axis included).  The enumeration is
+// k_pairs' (the same cells, candidates and exact test), with 16 lanes per
+// atom: lane 0 scans the atom's own cell, lane k + 1 the half-shell
+// neighbour k, so that the chains of dependent loads run side by side.
+constexpr int kBucketLanes = 16;
+
+// min_image1 for a difference whose square is all that is used: within
+// 0.49 L the rounded quotient is below one half, round() gives zero and the
+// reference's d - L * 0 is d itself (up to the sign of a zero).
+__device__ __forceinline__ double near_image1(double d, double L) {
+    return fabs(d) <= xmul(0.49, L) ? d : min_image1(d, L);
+}
+static_assert(kBucketLanes >= 14, "one lane per half-shell cell and the own cell");
+
+struct BucketArgs {
+    double k_bind;
+    double sig[kNElem];
+    uint32_t* bucket;
+    uint32_t* bcnt;
+    uint32_t depth;
+    size_t stride;
+};
+
+__global__ void __launch_bounds__(256) k_bound_buckets(GridGeom g, AuxSet a, double box0, double box1, double box2,
+                                                       double cd2, BucketArgs v) {
+    // the offsets and sigmas, indexed per lane and per atom, from shared
+    // memory (constant-index copies: no per-thread copy of the parameters)
+    __shared__ int8_t half[13][3];
+    __shared__ double sig[kNElem];
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < 13; ++q) {
+            half[q][0] = g.half[q][0];
+            half[q][1] = g.half[q][1];
+            half[q][2] = g.half[q][2];
+        }
+#pragma unroll
+        for (int q = 0; q < kNElem; ++q) sig[q] = v.sig[q];
+    }
+    __syncthreads();
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i = t / kBucketLanes;
+    const int k = (int)(t % kBucketLanes) - 1;
+    if (i < a.m && k < g.nhalf) {
+        const uint32_t c = a.key[i];
+        uint32_t B, lo;
+        if (k < 0) {
+            B = c;
+            lo = i + 1;
+        } else {
+            uint32_t cx, cy, cz;
+            decode(g, c, cx, cy, cz);
+            B = encode(g, wrap_add(cx, half[k][0], g.n[0]), wrap_add(cy, half[k][1], g.n[1]),
+                       wrap_add(cz, half[k][2], g.n[2]));
+            lo = a.start[B];
+        }
+        const uint32_t hi = a.start[B + 1];
+        const double xi = a.x[i], yi = a.y[i], zi = a.z[i];
+        const double si = sig[a.elem[i]];
+        const uint32_t slot_i = a.slot[i];
+        for (uint32_t j = lo; j < hi; ++j) {
+            double dx = near_image1(xsub(xi, a.x[j]), box0);
+            double dy = near_image1(xsub(yi, a.y[j]), box1);
+            double dz = near_image1(xsub(zi, a.z[j]), box2);
+            double d2 = xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
+            if (d2 >= cd2) continue;
+            double threshold = xmul(v.k_bind, xmul(0.5, xadd(si, sig[a.elem[j]])));  // pairs.rs:163
+            // d = sqrt(d2) (correctly rounded) against the threshold, decided
+            // on d2 away from the boundary: beyond 1e-12 relative either way
+            // the rounded root cannot fall on the other side
+            const double t2 = xmul(threshold, threshold);
+            if (d2 >= xmul(t2, 1.0 + 1e-12)) continue;
+            if (d2 > xmul(t2, 1.0 - 1e-12) || d2 <= 1e-30) {
+                double d = xsqrt(d2);
+                if (d <= kEpsF64) continue;  // check_pair, grid.rs:201-225
+                if (!(d < threshold)) continue;
+            }
+            uint32_t sa = slot_i, sb = a.slot[j];
+            if (sb < sa) {
+                uint32_t q = sa;
+                sa = sb;
+                sb = q;
+            }
+            uint32_t r = atomicAdd(&v.bcnt[sa], 1u);
+            if (r < v.depth) v.bucket[(size_t)r * v.stride + sa] = sb;
+        }
+    }
+}
 
 __global__ void k_iota(uint32_t* p, uint32_t n) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -525,12 +646,23 @@ int gx_clusters(gx_handle* h, double bond_factor, uint32_t* labels, uint64_t sta
 
 namespace gx {
 
+void lens_free(gx_handle* h) {
+    pool_release(static_cast<AuxPool*>(h->lens));
+    h->lens = nullptr;
+}
+
+void aux_pool_free(void* pool) { pool_release(static_cast<AuxPool*>(pool)); }
+
 // bound_pairs_with_grid (src/analysis/pairs.rs:132-174) with the pairs left on
-// the device as slot pairs (a < b): up to cap pairs into out, the number
-// found added to *dcount (device).  Launches only.
-int bound_pairs_device(gx_handle* h, double k_bind, uint32_t* out, size_t cap, unsigned long long* dcount) {
+// the device in their owners' buckets (k_bound_buckets).  The staging lives
+// in the caller's pool (*pool, made on first use), so that its addresses
+// stay fixed for a captured observation.  Launches only; the caller zeroes
+// bcnt.
+int bound_buckets_device(gx_handle* h, void** pool, double k_bind, uint32_t* bucket, uint32_t* bcnt, uint32_t depth,
+                         size_t stride) {
     uint32_t n = (uint32_t)h->n;
-    AuxPool& P = pool_of(h);
+    if (!*pool) *pool = new AuxPool();
+    AuxPool& P = *static_cast<AuxPool*>(*pool);
     int rc = ensure_pool(h, P, n, n);
     if (rc) return rc;
     double ms = 0.0;  // bind_cutoff, analysis/pairs.rs:112-114
@@ -539,17 +671,36 @@ int bound_pairs_device(gx_handle* h, double k_bind, uint32_t* out, size_t cap, u
     int ok = 0;
     GridGeom g = make_grid(h->p.box, cutoff, &ok);
     if (!ok) return set_err(h, GX_ERR_ARG, "invalid bond grid");
+    if ((rc = ensure_cells(h, P.cl, g.ncell))) return rc;
     AuxSet a;
-    if ((rc = build_aux(h, P, g, nullptr, n, a))) return rc;
-    BoundVisit v;
+    a.x = P.xyz + 3 * P.cap;
+    a.y = a.x + P.cap;
+    a.z = a.y + P.cap;
+    a.elem = P.elem + P.cap;
+    a.slot = P.u32 + P.cap;
+    a.key = P.u32 + 3 * P.cap;
+    a.start = P.cl.start;
+    a.m = n;
+    uint32_t* key = P.u32 + 2 * P.cap;
+    const StateBuf& b = h->buf[h->cur];
+    prof_begin(h, "bond_grid");
+    GX_CUDA(h, cudaMemsetAsync(P.cl.count, 0, ((size_t)g.ncell + 1) * sizeof(uint32_t), h->stream));
+    GX_CUDA(h, cudaMemsetAsync(P.cl.fill, 0, (size_t)g.ncell * sizeof(uint32_t), h->stream));
+    if (n) GX_LAUNCH(h, k_select_count, nblk(n, 256), 256, g, b, n, key, P.cl.count);
+    cell_scan(h, P.cl, g.ncell);
+    if (n) GX_LAUNCH(h, k_place, nblk(n, 256), 256, b, n, key, P.cl.start, P.cl.fill, a);
+    prof_end(h, "bond_grid");
+    BucketArgs v;
     v.k_bind = k_bind;
     for (int k = 0; k < kNElem; ++k) v.sig[k] = h->p.sigma[k];
-    v.entity = nullptr;
-    v.out = out;
-    v.cap = cap;
-    v.cnt = dcount;
+    v.bucket = bucket;
+    v.bcnt = bcnt;
+    v.depth = depth;
+    v.stride = stride;
     prof_begin(h, "bound_pairs");
-    if (n) GX_LAUNCH(h, k_pairs, nblk(n, 128), 128, g, a, h->p.box[0], h->p.box[1], h->p.box[2], cutoff * cutoff, v);
+    if (n)
+        GX_LAUNCH(h, k_bound_buckets, nblk((size_t)n * kBucketLanes, 256), 256, g, a, h->p.box[0], h->p.box[1],
+                  h->p.box[2], cutoff * cutoff, v);
     prof_end(h, "bound_pairs");
     return GX_OK;
 }

@@ -552,11 +552,12 @@ void nl_free(gx_handle* h) {
     h->nl = nullptr;
 }
 
-// The list path applies to the mixed pass without gravity or bond springs,
-// with at least 3 list-grid cells per axis and atom indices below 2^27.
+// The list path applies to the mixed pass without gravity, with at least 3
+// list-grid cells per axis (so the force grid has at least 3 too, and every
+// pair within the cutoff occurs once in the reference's pair list) and atom
+// indices below 2^27.
 bool nl_eligible(gx_handle* h) {
     if (h->precision != GX_MIXED || h->p.enable_gravity) return false;
-    if (h->p.enable_bond_interaction && h->nbonds > 0) return false;
     if (h->n == 0 || h->n >= (1u << 27)) return false;
     NlState* s = nl_of(h);
     double rl = h->fs.rc + skin_of(h, s);
@@ -664,6 +665,7 @@ int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nb_out) {
         launch_nl_force<false>(h, s->tpp, g, s, n, L);
     prof_end(h, "force_nl");
     GX_LAUNCH(h, k_nl_fix_to_double, 1, 1, h->dcount + 1, h->dscal + 2, h->dscal + 3);
+    if (bonds_on(h) && (rc = bond_spring(h, true))) return rc;  // into F before it becomes a
     int nb = (int)nblk(n, kRedThreads);
     if (nb > 1184) nb = 1184;  // the block count of launch_kinetic
     if (nb < 1) nb = 1;

@@ -113,3 +113,87 @@ def test_reset_and_new_state_start_afresh(gpu):
     h.set_universe(u)
     st = h.bond_observe(cfg.bond_k_bind, 0.2, 1)
     assert st["completed_episodes"] == 0 and st["open_episodes"] == st["bound_pairs"]
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _initial_bonds(orc, cfg, u):
+    bonds = orc.bound_pairs(u.pos, u.elem, u.entity, cfg.size, cfg.bond_k_bind, cfg.sigma)
+    return np.ascontiguousarray(bonds, dtype=np.uint32).reshape(-1, 2)
+
+
+@pytest.mark.parametrize("variant", [5, 6])
+def test_list_path_spring_matches_oracle(gpu, orc, variant):
+    # the persistent-list passes apply the spring too (one occurrence per
+    # pair: the list grid, and so the force grid, has at least 3 cells per axis)
+    from genesis_b200._lib import Handle
+    cfg, u = _ionic()
+    bonds = _initial_bonds(orc, cfg, u)
+    assert len(bonds) > 0
+    h = Handle(cfg, "mixed")
+    h.set_kernel_variant(variant)
+    h.set_universe(u)
+    h.set_bonds(bonds)
+    st = h.step(1)
+    assert h.list_rebuilds() >= 1  # the list path ran
+    _, _, acc = h.get_state()
+    _, _, acc_ref, st_ref = orc.ticks(cfg, u.pos, u.vel, None, u.elem, u.charge, u.mass, 1, bonds=bonds)
+    assert _rel(acc, acc_ref) <= 1e-5
+    vb, vb_ref = st["bond_energy"][0], st_ref[0, 2]
+    assert vb_ref != 0.0 and abs(vb - vb_ref) <= 1e-6 * abs(vb_ref) + 1e-7
+
+
+@pytest.mark.parametrize("precision,variant", [("fp64", 0), ("mixed", 1), ("mixed", 5), ("mixed", 6)])
+def test_bond_count_changes_inside_captured_ticks(gpu, orc, precision, variant):
+    # the spring reads the bond count on the device: captured ticks follow a
+    # list that shrinks, empties and refills in place exactly as eager ticks do
+    from genesis_b200._lib import Handle
+    cfg, u = _ionic()
+    bonds = _initial_bonds(orc, cfg, u)
+    runs = []
+    for graph in (False, True):
+        h = Handle(cfg, precision)
+        h.set_kernel_variant(variant)
+        h.set_universe(u)
+        sts = []
+        for sel in (bonds, bonds[: len(bonds) // 2], bonds[:0], bonds[::3]):
+            h.set_bonds(np.ascontiguousarray(sel))
+            sts.append(h.step(4, graph=graph))
+        runs.append((h.get_state(), sts))
+    (s0, t0), (s1, t1) = runs
+    assert np.all(t0[2]["bond_energy"] == 0.0) and np.all(t0[0]["bond_energy"] != 0.0)
+    if precision == "mixed":  # order-independent fixed-point sums: bit-identical
+        for x, y in zip(s0, s1):
+            assert np.array_equal(x, y)
+        for a, b in zip(t0, t1):
+            assert np.array_equal(a, b)
+    else:  # FP64 spring forces meet at an atom through atomics
+        for x, y in zip(s0, s1):
+            assert _rel(x, y) <= 1e-13
+        for a, b in zip(t0, t1):
+            assert np.allclose(a["bond_energy"], b["bond_energy"], rtol=1e-13, atol=0.0)
+
+
+def test_observed_bonds_drive_the_list_path(gpu):
+    # bond observation feeding the spring on the default mixed path (the
+    # persistent list): captured and eager ticks agree bit for bit
+    from genesis_b200._lib import Handle
+    cfg, u = _ionic(n_side=8)
+    out = []
+    for graph in (False, True):
+        h = Handle(cfg, "mixed")
+        h.set_universe(u)
+        most, obs = 0, []
+        for tick in range(1, 81):
+            h.step(1, stats=False, graph=graph)
+            ob = h.bond_observe(cfg.bond_k_bind, 0.1, tick)
+            most = max(most, ob["bonded_pairs"])
+            obs.append(tuple(ob[k] for k in KEYS))
+        assert h.list_rebuilds() >= 1 and most > 0
+        out.append((h.get_state(), obs, h.get_bonds()))
+    for x, y in zip(out[0][0], out[1][0]):
+        assert np.array_equal(x, y)
+    assert out[0][1] == out[1][1]
+    assert np.array_equal(out[0][2], out[1][2])
