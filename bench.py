@@ -50,7 +50,7 @@ BYTES_PER_ATOM = {
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c3")
@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip fp64/e2e/cpu legs (testing only)")
     ap.add_argument("--variant", type=int, default=-1,
                     help="fix the mixed pair-pass variant instead of autotuning (profiling only)")
+    ap.add_argument("--leg", default="", choices=["", "ionic", "accuracy", "adjoint"],
+                    help="run one extra leg alone and print its JSON (profiling only)")
+    ap.add_argument("--leg-steps", type=int, default=0, help="ticks of the --leg run (0: the workload's own)")
     return ap.parse_args()
 
 
@@ -126,6 +129,11 @@ class Clocks:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                  "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            # nvidia-smi takes a moment to start: the timed region begins
+            # once the first sample is in, so every sample falls inside it
+            t0 = time.perf_counter()
+            while time.perf_counter() - t0 < 3.0 and not Path(self.path).read_text().strip():
+                time.sleep(0.02)
         except Exception:
             self.proc = None
 
@@ -615,6 +623,7 @@ def ours_arm(args, dist):
             except Exception as e:  # noqa: BLE001
                 extras["cpu_baseline_error"] = repr(e)
 
+    list_cfg = h.list_config()
     h.close()
     if dist.rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": K, "warmup": Wm,
@@ -627,7 +636,7 @@ def ours_arm(args, dist):
                            "parallelism": f"{dist.world} independent replicas (one per GPU)",
                            "pair_pass_variant": variant, "autotune_ms": tune_ms,
                            "neighbour_list_rebuilds_in_timed_ticks": rebuilds,
-                           "neighbour_list_skin_and_threads_per_atom": h.list_config(),
+                           "neighbour_list_skin_and_threads_per_atom": list_cfg,
                            "cuda_graph": True},
                 "gpu_launches": launches, "clocks": clk, "roofline": roof, "roofline_hbm": roof_hbm,
                 "kernels": kernels, "memory_kernels": mem, "pairs_per_tick": pairs}
@@ -643,6 +652,16 @@ def main():
     try:
         if args.impl == "reference":
             reference_arm(args, dist)
+        elif args.leg:
+            dev = dist.local
+            if args.leg == "ionic":
+                out = ionic_leg(dev, cpu=False, steps=args.leg_steps or None)
+            elif args.leg == "accuracy":
+                out = accuracy_leg(dev, args.leg_steps or 10000)
+            else:
+                out = adjoint_leg(dev)
+            if dist.rank == 0:
+                print(json.dumps({"leg": args.leg, **out}), flush=True)
         else:
             ours_arm(args, dist)
     finally:

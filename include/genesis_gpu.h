@@ -274,8 +274,9 @@ int gx_set_dynamic(gx_handle* h, const double* pos, const double* vel, const dou
 /* The reference sweeps temperatures with one fresh Universe per T, run one
  * after another (examples/temperature_sweep.rs:70-113).  A gx_batch holds
  * nrep independent universes of uneven sizes that share the laws in `base`
- * (mixed precision) and advances all of them in one persistent launch, one
- * CTA per replica.  box: 3 doubles per replica; target_T: Berendsen target
+ * (mixed precision) and advances all of them together: as one captured
+ * graph of all-replica kernels, or in one persistent launch with one CTA per
+ * replica (gx_batch_set_mode).  box: 3 doubles per replica; target_T: Berendsen target
  * per replica (<= 0 or base->enable_thermostat == 0: NVE); NULL uses
  * base->thermostat_temperature.  Each replica's force grid must have >= 1
  * and <= 4096 cells. */
