@@ -51,8 +51,15 @@ struct NlState {
     uint32_t* list = nullptr; // entry e of atom p at list[e * cap + p]
     uint32_t* cnt = nullptr;  // entries per atom (> cap_nb: overflowed)
     float4* ref = nullptr;    // home-frame positions at the last rebuild
-    uint32_t* flag = nullptr; // [0] rebuild requested, [1] rebuilds done, [2] half-box translations since (mod 2)
+    uint32_t* flag = nullptr; // [0] rebuild requested, [1] rebuilds done, [2] half-box translations since (mod 2),
+                              // [3] runs of a captured rebuild body
     CellList cl;
+    // A captured tick puts the rebuild in the body of a conditional (IF)
+    // graph node, set from flag[0], so that a tick without a rebuild does
+    // not launch it at all.  The body is captured from a second stream.
+    cudaStream_t side = nullptr;
+    uint64_t body_kernels = 0;  // kernels in the body (counted when it runs)
+    uint32_t body_runs_seen = 0;
 };
 
 namespace {
@@ -222,6 +229,13 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_build(GridGeom g, const float
 
 // End of the list work of a tick: a rebuild starts a fresh frame; otherwise
 // this tick's wrap added one half-box translation.
+// The rebuild body's condition: the flag k_nl_advance raised.
+__global__ void k_nl_set_cond(cudaGraphConditionalHandle hc, const uint32_t* __restrict__ flag) {
+    cudaGraphSetConditional(hc, flag[0] != 0u ? 1u : 0u);
+}
+
+__global__ void k_nl_body_done(uint32_t* flag) { flag[3] += 1u; }
+
 __global__ void k_nl_end(uint32_t* flag, int wrap) {
     if (flag[0]) {
         flag[1] += 1u;
@@ -548,6 +562,7 @@ void nl_free(gx_handle* h) {
     cudaFree(s->cl.start);
     cudaFree(s->cl.fill);
     for (auto q : s->cl.scan_levels) cudaFree(q);
+    if (s->side) cudaStreamDestroy(s->side);
     delete s;
     h->nl = nullptr;
 }
@@ -584,7 +599,9 @@ int nl_prepare(gx_handle* h, bool* stale) {
     if (!s->flag) {
         GX_CUDA(h, cudaMalloc(&s->flag, 4 * sizeof(uint32_t)));
         GX_CUDA(h, cudaMemsetAsync(s->flag, 0, 4 * sizeof(uint32_t), h->stream));
+        s->body_runs_seen = 0;
     }
+    if (!s->side) GX_CUDA(h, cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking));
     if (s->cap < h->cap || s->cap_nb < cap_nb) {
         cudaFree(s->list);
         cudaFree(s->cnt);
@@ -641,20 +658,63 @@ int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nb_out) {
               0.5 * h->p.box[1], 0.5 * h->p.box[2], h->p.enable_boundaries ? 1 : 0, g, h->key_sorted, h->pos4, s->ref,
               lim * lim, s->flag, h->derr);
     prof_end(h, "nl_advance");
+    // inside a capture: the rebuild goes into the body of an IF node
+    cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
+    GX_CUDA(h, cudaStreamIsCapturing(h->stream, &cst));
+    const bool cond = cst == cudaStreamCaptureStatusActive;
+    cudaStream_t main_stream = h->stream;
+    uint64_t body_l0 = 0;
+    if (cond) {
+        cudaStreamCaptureStatus st;
+        unsigned long long id = 0;
+        cudaGraph_t gr = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        GX_CUDA(h, cudaStreamGetCaptureInfo(h->stream, &st, &id, &gr, &deps, &nd));
+        cudaGraphConditionalHandle hc;
+        GX_CUDA(h, cudaGraphConditionalHandleCreate(&hc, gr, 0, cudaGraphCondAssignDefault));
+        GX_LAUNCH(h, k_nl_set_cond, 1, 1, hc, s->flag);
+        GX_CUDA(h, cudaStreamGetCaptureInfo(h->stream, &st, &id, &gr, &deps, &nd));
+        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+        cp.conditional.handle = hc;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node = nullptr;
+        GX_CUDA(h, cudaGraphAddNode(&node, gr, deps, nd, &cp));
+        GX_CUDA(h, cudaStreamUpdateCaptureDependencies(h->stream, &node, 1, cudaStreamSetCaptureDependencies));
+        GX_CUDA(h, cudaStreamBeginCaptureToGraph(s->side, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                 cudaStreamCaptureModeRelaxed));
+        h->stream = s->side;
+        body_l0 = h->launches;
+    }
     prof_begin(h, "nl_rebuild");
-    launch_cell_keys(h, g, b, n, h->key, s->flag);
-    int rc = counting_sort(h, s->cl, g.ncell, h->key, n, h->perm, s->flag);
+    auto rebuild = [&]() -> int {
+        launch_cell_keys(h, g, b, n, h->key, s->flag);
+        int r = counting_sort(h, s->cl, g.ncell, h->key, n, h->perm, s->flag);
+        if (r) return r;
+        launch_gather(h, b, o, h->perm, h->key, h->key_sorted, n, h->pos_of_slot, s->flag);
+        GX_LAUNCH(h, k_nl_copy, nblk(n, 256), 256, o, b, n, s->flag);
+        GX_LAUNCH(h, k_nl_stage, nblk(n, 256), 256, g, b, h->key_sorted, n, h->pos4, s->ref, s->flag);
+        const float rl = (float)((h->fs.rc + s->skin_used) * (1.0 + 1e-6));
+        auto build = s->half == 1 ? k_nl_build<true> : k_nl_build<false>;
+        GX_LAUNCH(h, build, nblk(n, kNlThreads), kNlThreads, g, h->pos4, h->key_sorted, s->cl.start, n, rl * rl,
+                  s->list, s->cap, s->cap_nb, s->cnt, s->flag);
+        return GX_OK;
+    };
+    int rc = rebuild();
+    if (cond) {
+        if (!rc) GX_LAUNCH(h, k_nl_body_done, 1, 1, s->flag);
+        s->body_kernels = h->launches - body_l0;
+        h->launches = body_l0;  // counted when the body runs (nl_rebuilds)
+        cudaGraph_t body = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(s->side, &body);
+        h->stream = main_stream;
+        if (!rc && ce != cudaSuccess) rc = cuda_err(h, ce, "cudaStreamEndCapture (rebuild body)");
+    }
     if (rc) return rc;
-    launch_gather(h, b, o, h->perm, h->key, h->key_sorted, n, h->pos_of_slot, s->flag);
-    GX_LAUNCH(h, k_nl_copy, nblk(n, 256), 256, o, b, n, s->flag);
-    GX_LAUNCH(h, k_nl_stage, nblk(n, 256), 256, g, b, h->key_sorted, n, h->pos4, s->ref, s->flag);
-    const float rl = (float)((h->fs.rc + s->skin_used) * (1.0 + 1e-6));
-    const bool halfl = s->half == 1;
-    auto build = halfl ? k_nl_build<true> : k_nl_build<false>;
-    GX_LAUNCH(h, build, nblk(n, kNlThreads), kNlThreads, g, h->pos4, h->key_sorted, s->cl.start, n, rl * rl,
-              s->list, s->cap, s->cap_nb, s->cnt, s->flag);
     GX_LAUNCH(h, k_nl_end, 1, 1, s->flag, h->p.enable_boundaries ? 1 : 0);
     prof_end(h, "nl_rebuild");
+    const bool halfl = s->half == 1;
     GX_CUDA(h, cudaMemsetAsync(h->dcount, 0, 4 * sizeof(unsigned long long), h->stream));
     LawF32 L = make_law32(h);
     prof_begin(h, "force_nl");
@@ -685,10 +745,13 @@ int nl_rebuilds(gx_handle* h, uint64_t* out) {
     if (!h->nl) return GX_OK;
     NlState* s = static_cast<NlState*>(h->nl);
     if (!s->flag) return GX_OK;
-    uint32_t f[2] = {0, 0};
+    uint32_t f[4] = {0, 0, 0, 0};
     GX_CUDA(h, cudaMemcpyAsync(f, s->flag, sizeof f, cudaMemcpyDeviceToHost, h->stream));
     GX_CUDA(h, cudaStreamSynchronize(h->stream));
     *out = f[1];
+    // the kernels of the captured rebuild bodies that ran since the last read
+    h->launches += (uint64_t)(f[3] - s->body_runs_seen) * s->body_kernels;
+    s->body_runs_seen = f[3];
     return GX_OK;
 }
 

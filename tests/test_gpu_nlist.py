@@ -175,3 +175,34 @@ def test_state_round_trip_after_list_ticks(gpu):
     h.set_dynamic(pos, vel, acc)
     p2, v2, a2 = h.get_state()
     assert np.array_equal(pos, p2) and np.array_equal(vel, v2) and np.array_equal(acc, a2)
+
+
+@pytest.mark.parametrize("variant", [5, 6])
+def test_captured_rebuilds_run_only_when_flagged(gpu, variant):
+    # a captured tick holds the rebuild in a conditional graph node set from
+    # the displacement flag: the same ticks and rebuilds as eager execution,
+    # with the rebuild kernels launched only on the ticks that rebuild
+    cfg, u = _lattice(14, temperature=300.0, coul=True)
+    out = []
+    for graph in (False, True):
+        h = _handle(cfg, variant)  # the default skin, 0.1 r_c: a rebuild every few ticks at 300 K
+        h.set_universe(u)
+        l0 = h.launches
+        st = h.step(40, graph=graph)
+        rb = h.list_rebuilds()
+        out.append((h.get_state(), st, rb, h.launches - l0))
+    (s0, t0, r0, n0), (s1, t1, r1, n1) = out
+    for x, y in zip(s0, s1):
+        assert np.array_equal(x, y)
+    assert np.array_equal(t0, t1)
+    assert r0 == r1 and 3 <= r0 < 40
+    assert n1 < n0  # eager launches every gated rebuild kernel on every tick
+
+
+def test_zero_skin_captured_rebuild_every_tick(gpu):
+    cfg, u = _lattice(12)
+    h = _handle(cfg)
+    h.set_list_skin(0.0)
+    h.set_universe(u)
+    h.step(7, graph=True)
+    assert h.list_rebuilds() == 7
