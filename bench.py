@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip fp64/e2e/cpu legs (testing only)")
     ap.add_argument("--variant", type=int, default=-1,
                     help="fix the mixed pair-pass variant instead of autotuning (profiling only)")
+    ap.add_argument("--skin", type=float, default=-1.0,
+                    help="neighbour-list skin in length units instead of 0.1 r_c (profiling only; 0 = rebuild every tick)")
     ap.add_argument("--leg", default="", choices=["", "ionic", "accuracy", "adjoint"],
                     help="run one extra leg alone and print its JSON (profiling only)")
     ap.add_argument("--leg-steps", type=int, default=0, help="ticks of the --leg run (0: the workload's own)")
@@ -450,6 +452,8 @@ def ours_arm(args, dist):
     extras = {}
 
     h = Handle(cfg, "mixed", dev)
+    if args.skin >= 0:
+        h.set_list_skin(args.skin)
     h.set_universe(u)
     if args.variant >= 0:
         h.set_kernel_variant(args.variant)
