@@ -104,6 +104,14 @@ class Dist:
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
+    def all_gather_object(self, obj) -> list:
+        """Every rank's `obj`, in rank order (one collective)."""
+        if not self.pg:
+            return [obj]
+        out = [None] * self.world
+        self.pg.all_gather_object(out, obj)
+        return out
+
     def close(self):
         if self.pg:
             self.pg.destroy_process_group()
@@ -589,21 +597,34 @@ def ours_arm(args, dist):
         try:
             from genesis_b200 import sweep
 
-            wls = sweep.make_replicas(256, seed=dist.rank)
+            # one sweep of 256 replicas shared over the ranks (size-balanced,
+            # no collective until the per-replica results are gathered)
+            wls = sweep.make_replicas(256, seed=0)
+            sizes = [wl.n_atoms for wl in wls]
+            parts = sweep.partition(sizes, dist.world)
+            mine = [wls[i] for i in parts[dist.rank]]
             sweep_steps = 2000
-            vb, _, msb = sweep.run_batched(wls, sweep_steps, dev, mode=2)
-            vp, _, msp = sweep.run_batched(wls, sweep_steps, dev, mode=1)
+            _, stb, msb = sweep.run_batched(mine, sweep_steps, dev, mode=2)
+            _, _, msp = sweep.run_batched(mine, sweep_steps, dev, mode=1)
             seq_steps = 50
-            vs, mss = sweep.run_sequential(wls, seq_steps, dev)
+            _, mss = sweep.run_sequential(mine, seq_steps, dev)
+            msb, msp, mss = dist.max(msb), dist.max(msp), dist.max(mss)
+            vb = len(wls) * sweep_steps / (msb * 1e-3)
+            vp = len(wls) * sweep_steps / (msp * 1e-3)
+            vs = len(wls) * seq_steps / (mss * 1e-3)
+            stats = sweep.assemble(parts, dist.all_gather_object(np.asarray(stb).tolist()))
             best = max(vb, vp)
             extras["replica_sweep"] = {
                 "metric": "replica-steps/s", "replicas": len(wls), "atoms": sweep.atoms(wls),
-                "batched": {"value": dist.world * best, "steps": sweep_steps,
+                "scaling": "strong: one sweep shared over the ranks",
+                "atoms_per_rank": [int(sum(sizes[i] for i in p)) for p in parts],
+                "batched": {"value": best, "steps": sweep_steps,
                             "mode": "all-replica graph" if vb >= vp else "persistent launch",
-                            "all_replica_graph": {"value": dist.world * vb, "ms": msb},
-                            "persistent_launch": {"value": dist.world * vp, "ms": msp}},
-                "sequential": {"value": dist.world * vs, "steps_per_replica": seq_steps, "ms": mss},
+                            "all_replica_graph": {"value": vb, "ms": msb},
+                            "persistent_launch": {"value": vp, "ms": msp}},
+                "sequential": {"value": vs, "steps_per_replica": seq_steps, "ms": mss},
                 "batched_over_sequential": best / vs,
+                "final_kinetic_sum": float(stats[:, 0].sum()), "final_pairs_sum": float(stats[:, 3].sum()),
                 "workload": "256 replicas, n^3 atoms with n = round(N^(1/3)) in [8, 25], N log-uniform in "
                             "[512, 16384], 10-element LJ mixture, Berendsen T uniform in [20, 120] K"}
         except Exception as e:  # noqa: BLE001

@@ -52,3 +52,41 @@ def run_sequential(wls, steps: int, device: int = 0):
 
 def atoms(wls) -> int:
     return int(sum(wl.n_atoms for wl in wls))
+
+
+def partition(sizes, world: int) -> list[list[int]]:
+    """Shards a sweep over `world` GPUs: replicas are independent, so each
+    rank advances its own share in one gx_batch with no collective on the
+    data path.  Size-balanced greedy packing: the largest replica first,
+    each to the rank with the fewest atoms so far (ties to the lower rank).
+    Returns each rank's replica indices in increasing order."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    loads = [0] * world
+    parts: list[list[int]] = [[] for _ in range(world)]
+    for i in sorted(range(len(sizes)), key=lambda i: (-int(sizes[i]), i)):
+        r = min(range(world), key=lambda r: (loads[r], r))
+        parts[r].append(i)
+        loads[r] += int(sizes[i])
+    return [sorted(p) for p in parts]
+
+
+def assemble(parts: list[list[int]], per_rank_stats: list) -> np.ndarray:
+    """Puts the per-replica rows each rank returned (in its partition's
+    order) back into the sweep's replica order."""
+    n = sum(len(p) for p in parts)
+    rows = [np.asarray(s) for s in per_rank_stats]
+    width = next((r.shape[1] for r in rows if r.size), 0)
+    out = np.zeros((n, width))
+    seen = np.zeros(n, dtype=bool)
+    for idx, r in zip(parts, rows):
+        if len(idx) != len(r):
+            raise ValueError("a rank returned a different number of replicas than it was given")
+        for k, i in enumerate(idx):
+            if seen[i]:
+                raise ValueError(f"replica {i} returned twice")
+            seen[i] = True
+            out[i] = r[k]
+    if not seen.all():
+        raise ValueError("replicas missing from the gathered results")
+    return out
