@@ -69,6 +69,7 @@ EXPORTS = (
     "gx_batch_step", "gx_batch_get_state", "gx_adjoint_forward", "gx_adjoint_backward",
     "gx_set_list_skin", "gx_list_rebuilds", "gx_batch_set_mode", "gx_batch_get_mode", "gx_batch_autotune",
     "gx_get_list_config", "gx_set_list_threads", "gx_bond_observe", "gx_bond_tracker_reset", "gx_get_bonds",
+    "gx_bond_components",
 )
 
 _lib = None
@@ -127,6 +128,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
         "gx_bond_observe": (C.c_int, [vp, _D, _D, C.c_int, C.c_uint64, C.c_int, C.POINTER(GxBondObservation)]),
         "gx_bond_tracker_reset": (C.c_int, [vp]),
         "gx_get_bonds": (C.c_int, [vp, u32p, sz, C.POINTER(sz)]),
+        "gx_bond_components": (C.c_int, [vp, u32p, dp, sz, C.POINTER(sz)]),
         "gx_adjoint_backward": (C.c_int, [vp, dp, dp, dp, dp, dp, dp, dp]),
     }
     for name, (res, args) in proto.items():
@@ -425,6 +427,19 @@ class Handle:
         d = {f: getattr(o, f) for f, _ in GxBondObservation._fields_ if f != "species_matrix"}
         d["species_matrix"] = np.array(o.species_matrix[:], dtype=np.uint64).reshape(10, 10)
         return d
+
+    def bond_components(self):
+        """(labels per slot: the smallest slot of the atom's bond component,
+        0xFFFFFFFF for an atom in no bond; the raw pair energy of each bond in
+        get_bonds() order)."""
+        n = int(self.lib.gx_num_atoms(self.h))
+        nb = C.c_size_t()
+        self._check(self.lib.gx_bond_components(self.h, None, None, 0, C.byref(nb)))
+        labels = np.empty(n, dtype=np.uint32)
+        energy = np.empty(max(nb.value, 1))
+        self._check(self.lib.gx_bond_components(self.h, _ptr(labels, C.c_uint32), _ptr(energy, C.c_double),
+                                                len(energy), C.byref(nb)))
+        return labels, energy[: nb.value].copy()
 
     def bond_tracker_reset(self):
         self._check(self.lib.gx_bond_tracker_reset(self.h))

@@ -4,6 +4,8 @@
 //   g(r), partial g(r)        radial_distribution(_between) src/analysis/mod.rs:87-201
 //   friends-of-friends        clusters                  src/analysis/mod.rs:221-307
 //   bound pairs               bound_pairs_with_grid     src/analysis/pairs.rs:132-174
+//   bond-graph components     bond_components           src/analysis/mod.rs:331-411
+//                             + pair_potential_raw      src/physics/forces.rs:355-384
 //
 // Each lens builds its own grid (cell = the lens cutoff) over the selected
 // atoms with the same counting sort as the force pass, then enumerates the
@@ -296,6 +298,63 @@ struct BoundVisit {
         }
     }
 };
+
+// Components of the bond list (bond_components, src/analysis/mod.rs:331-411):
+// union-find over the bonds, the label of a bonded slot is its root (the
+// smallest slot of the component), an atom in no bond gets 0xFFFFFFFF.
+__global__ void k_bond_unite(const uint32_t* __restrict__ bonds, size_t nb, uint32_t n, uint32_t* par,
+                             uint32_t* __restrict__ mark) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nb) return;
+    const uint32_t a = bonds[2 * k], b = bonds[2 * k + 1];
+    if (a >= n || b >= n) return;
+    mark[a] = 1u;
+    mark[b] = 1u;
+    if (a != b) uf_unite(par, a, b);
+}
+
+__global__ void k_bond_labels(uint32_t* par, const uint32_t* __restrict__ mark, uint32_t n,
+                              uint32_t* __restrict__ label) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) label[i] = mark[i] ? uf_root(par, i) : 0xFFFFFFFFu;
+}
+
+// pair_potential_raw (src/physics/forces.rs:360-384) of each bond at the
+// current positions, in the reference's operation order: r = max(|min
+// image of pa - pb|, 1e-9) (bond_structure.rs:113), unswitched LJ without
+// the core clamp (lj_raw, forces.rs:346-353), + k_e q_a q_b / r, + the
+// harmonic term 0.5 k (r - r_eq)^2 with k = well_curvature, r_eq =
+// equilibrium_distance (forces.rs:193-195, 281-283).
+struct RawLaw {
+    double sig[kNElem * kNElem], eps[kNElem * kNElem], qq[kNElem * kNElem];
+    double curv_factor, r_eq_factor;
+    double box[3];
+    int coulomb, bond;
+};
+
+__global__ void k_bond_energy(const uint32_t* __restrict__ bonds, size_t nb, StateBuf b,
+                              const uint32_t* __restrict__ pos_of_slot, RawLaw L, double* __restrict__ energy) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nb) return;
+    const uint32_t ia = pos_of_slot[bonds[2 * k]], ib = pos_of_slot[bonds[2 * k + 1]];
+    const double dx = min_image1(xsub(b.x[ia], b.x[ib]), L.box[0]);
+    const double dy = min_image1(xsub(b.y[ia], b.y[ib]), L.box[1]);
+    const double dz = min_image1(xsub(b.z[ia], b.z[ib]), L.box[2]);
+    const double r = fmax(xsqrt(xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz))), 1e-9);
+    const int t = b.elem[ia] * kNElem + b.elem[ib];
+    const double sg = L.sig[t], ep = L.eps[t];
+    const double s = xdiv(sg, r);
+    const double s6 = xmul(xmul(xmul(xmul(xmul(s, s), s), s), s), s);
+    const double s12 = xmul(s6, s6);
+    double v = xmul(xmul(4.0, ep), xsub(s12, s6));
+    if (L.coulomb) v = xadd(v, xdiv(L.qq[t], r));
+    if (L.bond) {
+        const double kk = xdiv(xmul(L.curv_factor, ep), xmul(sg, sg));
+        const double dr = xsub(r, xmul(sg, L.r_eq_factor));
+        v = xadd(v, xmul(xmul(xmul(0.5, kk), dr), dr));
+    }
+    energy[k] = v;
+}
 
 // Bound pairs routed to their owner: the pair (slot a < slot b) is appended
 // to a's bucket [k * stride + a] (k < depth; the count runs on past the
@@ -591,6 +650,54 @@ int gx_radial_distribution_between(gx_handle* h, uint8_t ta, uint8_t tb, double 
                                    double* dr_out) {
     if (ta >= kNElem || tb >= kNElem) return GX_ERR_ARG;
     return gr_common(h, ta, tb, r_max, nbins, sample_cap, counts, bins, r_max_out, dr_out);
+}
+
+int gx_bond_components(gx_handle* h, uint32_t* labels, double* edge_energy, size_t energy_cap, size_t* nbonds) {
+    int rc = require(h);
+    if (rc) return rc;
+    const uint32_t n = (uint32_t)h->n;
+    const size_t nb = h->bonds ? h->nbonds : 0;
+    if (nbonds) *nbonds = nb;
+    if (edge_energy && energy_cap < nb) return set_err(h, GX_ERR_CAPACITY, "edge_energy holds fewer than nbonds");
+    if (n == 0) return GX_OK;
+    AuxPool& P = pool_of(h);
+    if ((rc = ensure_pool(h, P, n, n))) return rc;
+    const StateBuf& b = h->buf[h->cur];
+    if (labels) {
+        GX_LAUNCH(h, k_iota, nblk(n, 256), 256, P.parent, n);
+        GX_CUDA(h, cudaMemsetAsync(P.size, 0, n * sizeof(uint32_t), h->stream));
+        if (nb) GX_LAUNCH(h, k_bond_unite, nblk(nb, 256), 256, h->bonds, nb, n, P.parent, P.size);
+        GX_LAUNCH(h, k_bond_labels, nblk(n, 256), 256, P.parent, P.size, n, P.entity);
+        GX_CUDA(h, cudaMemcpyAsync(labels, P.entity, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    }
+    double* tmp = nullptr;
+    if (edge_energy && nb) {
+        RawLaw L;
+        for (int a = 0; a < kNElem; ++a)
+            for (int c = 0; c < kNElem; ++c) {  // mix_sigma, mix_epsilon (forces.rs:127-134)
+                L.sig[a * kNElem + c] = 0.5 * (h->p.sigma[a] + h->p.sigma[c]);
+                L.eps[a * kNElem + c] = h->p.thermal_constant * std::sqrt(h->p.epsilon_k[a] * h->p.epsilon_k[c]);
+                L.qq[a * kNElem + c] = h->p.coulomb_constant * h->p.charge[a] * h->p.charge[c];
+            }
+        L.curv_factor = 72.0 * std::pow(2.0, -1.0 / 3.0);
+        L.r_eq_factor = std::pow(2.0, 1.0 / 6.0);
+        for (int k = 0; k < 3; ++k) L.box[k] = h->p.box[k];
+        L.coulomb = h->p.enable_electrostatics ? 1 : 0;
+        L.bond = h->p.enable_bond_interaction ? 1 : 0;
+        double* dst = P.xyz;
+        if (nb > 6 * P.cap) {
+            GX_CUDA(h, cudaMalloc(&tmp, nb * sizeof(double)));
+            dst = tmp;
+        }
+        GX_LAUNCH(h, k_bond_energy, nblk(nb, 256), 256, h->bonds, nb, b, h->pos_of_slot, L, dst);
+        cudaError_t e = cudaMemcpyAsync(edge_energy, dst, nb * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        cudaFree(tmp);
+        if (e != cudaSuccess) return cuda_err(h, e, "gx_bond_components");
+    }
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    GX_CUDA(h, cudaGetLastError());
+    return GX_OK;
 }
 
 int gx_clusters(gx_handle* h, double bond_factor, uint32_t* labels, uint64_t stats[4], double* mean_size) {

@@ -23,6 +23,7 @@ import numpy as np
 
 from . import elements as E
 from ._lib import Handle
+from .chemistry import BondStructureLens
 
 
 # ---------------------------------------------------------------- scheduler
@@ -365,6 +366,34 @@ class GpuBondObservation(_GpuSystem):
                   lifetime_sum_ticks=st["lifetime_sum_ticks"], species_matrix=st["species_matrix"])
 
 
+class GpuBondStructure(_GpuSystem):
+    """BondStructureSystem (src/systems/bond_structure.rs:25-246) every
+    interval ticks: the components of the persistent-bond graph and each
+    bond's raw energy from the device (gx_bond_components), the composition
+    histogram and the lifecycle events on the host (genesis_b200.chemistry)."""
+
+    def __init__(self, gpu: GpuWorld, interval: int):
+        super().__init__(gpu)
+        self.interval = max(int(interval), 1)
+        self.lens = BondStructureLens()
+
+    def name(self):
+        return "bond-structure"
+
+    def access(self):
+        return Access(reads=["Bonds", "AtomType", "Position"], resources_read=["Config"],
+                      resources_write=["ChemicalStructure"])
+
+    def run(self, ctx):
+        if ctx.time.tick % self.interval != 0:
+            return
+        self._enter()
+        labels, energy = self.gpu.h.bond_components()
+        cs = self.lens.sample(labels, self.gpu.world.elem, self.gpu.h.get_bonds(), energy, len(ctx.world))
+        cs["tick"] = ctx.time.tick
+        ctx.resources["ChemicalStructure"] = cs
+
+
 class GpuStats(_GpuSystem):
     """StatsSystem (src/systems/aggregate.rs:36-144): K, T, E = K + V + E_bond."""
 
@@ -404,6 +433,7 @@ def build_schedule(cfg, gpu: GpuWorld) -> Scheduler:
         s.add_system(GpuThermostat(gpu))
     if cfg.enable_bond_observation:
         s.add_system(GpuBondObservation(gpu, cfg))
+        s.add_system(GpuBondStructure(gpu, cfg.structure_interval))
     s.add_system(GpuStructure(gpu, cfg.structure_interval))
     s.add_system(GpuStats(gpu, cfg))
     return s

@@ -260,6 +260,16 @@ int gx_bond_observe(gx_handle* h, double k_bind, double min_periods, int debounc
                     int apply_bonds, gx_bond_observation* out);
 /* Drops the open episodes and the cumulative counts. */
 int gx_bond_tracker_reset(gx_handle* h);
+/* The connected components of the handle's bond list, for the bond-graph
+ * chemistry lens (bond_components, src/analysis/mod.rs:331-411, used by
+ * BondStructureSystem, src/systems/bond_structure.rs:66-117).  labels (may
+ * be NULL; n entries, slot order): the smallest slot of the atom's
+ * component, 0xFFFFFFFF for an atom in no bond.  edge_energy (may be NULL;
+ * energy_cap >= *nbonds entries, gx_get_bonds order): the raw unswitched
+ * pair energy of each bond at the current positions (pair_potential_raw,
+ * src/physics/forces.rs:355-384), whose sums over a component's bonds are
+ * its binding energy.  *nbonds (may be NULL) receives the bond count. */
+int gx_bond_components(gx_handle* h, uint32_t* labels, double* edge_energy, size_t energy_cap, size_t* nbonds);
 /* The handle's bond list as slot pairs (a < b for observed bonds). */
 int gx_get_bonds(gx_handle* h, uint32_t* pairs, size_t cap, size_t* nbonds);
 

@@ -26,9 +26,10 @@ def test_schedule_order_matches_build_schedule(gpu):
     from genesis_b200.systems import GpuUniverse
     cfg = W.C2.scaled(6).config()
     gu = GpuUniverse(cfg, W.C2.scaled(6).generate(), "fp64")
-    # build_schedule's order; the bond-graph lens (BondStructureSystem) is not part of this build
+    # build_schedule's order (src/universe/mod.rs:355-392)
     assert gu.scheduler.names() == ["velocity_half_kick", "position_drift", "boundary", "forces",
-                                    "velocity_half_kick", "thermostat", "bond-observation", "structure", "stats"]
+                                    "velocity_half_kick", "thermostat", "bond-observation", "bond-structure",
+                                    "structure", "stats"]
 
 
 def test_plain_schedule_matches_oracle_ticks(gpu, orc):
