@@ -689,7 +689,8 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
     auto tick_nl = [&](bool uniform) -> int {
         const bool pend = uniform || h->lambda_pending;
         int nb = 0;
-        int r = nl_tick(h, pend ? h->dscal + 0 : nullptr, thermo ? kpart : nullptr, &nb);
+        // the potential and pair count only where a record takes them
+        int r = nl_tick(h, pend ? h->dscal + 0 : nullptr, thermo ? kpart : nullptr, &nb, drec != nullptr);
         if (r) return r;
         if (pend) GX_LAUNCH(h, k_fill_d, 1, 32, h->dscal, 1, 1.0);
         h->lambda_pending = false;

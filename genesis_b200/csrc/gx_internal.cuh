@@ -294,7 +294,7 @@ void adjoint_free(gx_handle* h);
 // Neighbour-list path of the mixed pass (gx_nlist.cu).
 bool nl_eligible(gx_handle* h);
 int nl_prepare(gx_handle* h, bool* graphs_stale);
-int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nblocks);
+int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nblocks, bool energy);
 int nl_rebuilds(gx_handle* h, uint64_t* out);
 int nl_set_skin(gx_handle* h, double skin);
 int nl_tune_tpp(gx_handle* h, int reps);

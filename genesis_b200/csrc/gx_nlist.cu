@@ -293,8 +293,10 @@ __device__ __forceinline__ void nl_pair(const LawF32& L, const PairF* st, int ki
 
 // Full list: each thread sums its own atom's forces and stores them.  HALF:
 // each pair once, the far end's force through 64-bit integer atomics (F must
-// be zero on entry); both give the same fixed-point sums.
-template <bool HALF>
+// be zero on entry); both give the same fixed-point sums.  Without ENERGY
+// (ticks that record nothing) the potential and the pair count are left
+// out: the forces are the same bits.
+template <bool HALF, bool ENERGY>
 __global__ void __launch_bounds__(kNlThreads) k_nl_force(GridGeom g, const float4* __restrict__ pos4,
                                                           const uint32_t* __restrict__ home,
                                                           const uint32_t* __restrict__ start, uint32_t n, LawF32 L,
@@ -337,14 +339,15 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force(GridGeom g, const float
                 for (int k = 0; k < 4; ++k) {
                     float4 sh = s_shift[w[k] >> 27];
                     uint32_t q = w[k] & kIdxMask;
-                    nl_pair(L, st, ki, pi, pj[k], sh.x, sh.y, sh.z, q > p, a, err, HALF ? F : nullptr, q, fstride);
+                    nl_pair(L, st, ki, pi, pj[k], sh.x, sh.y, sh.z, ENERGY && q > p, a, err, HALF ? F : nullptr, q, fstride);
                 }
             }
             for (; e < m; ++e) {
                 uint32_t w = __ldg(lp + (size_t)e * stride);
                 float4 sh = s_shift[w >> 27];
                 uint32_t q = w & kIdxMask;
-                nl_pair(L, st, ki, pi, __ldg(pos4 + q), sh.x, sh.y, sh.z, q > p, a, err, HALF ? F : nullptr, q, fstride);
+                nl_pair(L, st, ki, pi, __ldg(pos4 + q), sh.x, sh.y, sh.z, ENERGY && q > p, a, err, HALF ? F : nullptr, q,
+                        fstride);
             }
         } else {  // overflowed list: scan the home-grid cells directly
             uint32_t cx, cy, cz;
@@ -357,7 +360,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force(GridGeom g, const float
                 code_shift(g, code, sx, sy, sz);
                 for (uint32_t q = start[B], hi = start[B + 1]; q < hi; ++q)
                     if (HALF ? q > p : q != p)
-                        nl_pair(L, st, ki, pi, pos4[q], sx, sy, sz, q > p, a, err, HALF ? F : nullptr, q, fstride);
+                        nl_pair(L, st, ki, pi, pos4[q], sx, sy, sz, ENERGY && q > p, a, err, HALF ? F : nullptr, q, fstride);
             }
         }
         if (HALF) {
@@ -370,11 +373,13 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force(GridGeom g, const float
             F[2 * fstride + p] = a.fz;
         }
     }
-    unsigned long long s = block_sum_u<kNlThreads>((unsigned long long)a.vq, shu);
-    unsigned long long np = block_sum_u<kNlThreads>(a.np, shu);
-    if (threadIdx.x == 0) {
-        if (s) atomicAdd(vacc, s);
-        if (np) atomicAdd(npairs, np);
+    if (ENERGY) {
+        unsigned long long s = block_sum_u<kNlThreads>((unsigned long long)a.vq, shu);
+        unsigned long long np = block_sum_u<kNlThreads>(a.np, shu);
+        if (threadIdx.x == 0) {
+            if (s) atomicAdd(vacc, s);
+            if (np) atomicAdd(npairs, np);
+        }
     }
 }
 
@@ -382,7 +387,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force(GridGeom g, const float
 // k + TPP, ... (more independent gathers in flight, less divergence between
 // list lengths); the group's integer partial sums are combined with
 // shuffles, so every TPP gives the same bits.
-template <bool HALF, int TPP>
+template <bool HALF, int TPP, bool ENERGY>
 __global__ void __launch_bounds__(kNlThreads) k_nl_force_tpp(GridGeom g, const float4* __restrict__ pos4,
                                                               const uint32_t* __restrict__ home,
                                                               const uint32_t* __restrict__ start, uint32_t n,
@@ -421,15 +426,15 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force_tpp(GridGeom g, const f
                 float4 p0 = __ldg(pos4 + (w0 & kIdxMask)), p1 = __ldg(pos4 + (w1 & kIdxMask));
                 float4 s0 = s_shift[w0 >> 27], s1 = s_shift[w1 >> 27];
                 uint32_t q0 = w0 & kIdxMask, q1 = w1 & kIdxMask;
-                nl_pair(L, st, ki, pi, p0, s0.x, s0.y, s0.z, q0 > p, a, err, HALF ? F : nullptr, q0, fstride);
-                nl_pair(L, st, ki, pi, p1, s1.x, s1.y, s1.z, q1 > p, a, err, HALF ? F : nullptr, q1, fstride);
+                nl_pair(L, st, ki, pi, p0, s0.x, s0.y, s0.z, ENERGY && q0 > p, a, err, HALF ? F : nullptr, q0, fstride);
+                nl_pair(L, st, ki, pi, p1, s1.x, s1.y, s1.z, ENERGY && q1 > p, a, err, HALF ? F : nullptr, q1, fstride);
             }
             if (e < m) {
                 uint32_t w = __ldg(lp + (size_t)e * stride);
                 float4 sh = s_shift[w >> 27];
                 uint32_t q = w & kIdxMask;
-                nl_pair(L, st, ki, pi, __ldg(pos4 + q), sh.x, sh.y, sh.z, q > p, a, err, HALF ? F : nullptr, q,
-                        fstride);
+                nl_pair(L, st, ki, pi, __ldg(pos4 + q), sh.x, sh.y, sh.z, ENERGY && q > p, a, err, HALF ? F : nullptr,
+                        q, fstride);
             }
         } else {  // overflowed list: the group splits the 27 home-grid cells
             uint32_t cx, cy, cz;
@@ -442,7 +447,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force_tpp(GridGeom g, const f
                 code_shift(g, code, sx, sy, sz);
                 for (uint32_t q = start[B], hi = start[B + 1]; q < hi; ++q)
                     if (HALF ? q > p : q != p)
-                        nl_pair(L, st, ki, pi, pos4[q], sx, sy, sz, q > p, a, err, HALF ? F : nullptr, q, fstride);
+                        nl_pair(L, st, ki, pi, pos4[q], sx, sy, sz, ENERGY && q > p, a, err, HALF ? F : nullptr, q, fstride);
             }
         }
     }
@@ -463,26 +468,33 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force_tpp(GridGeom g, const f
             F[2 * fstride + p] = a.fz;
         }
     }
-    unsigned long long s = block_sum_u<kNlThreads>((unsigned long long)a.vq, shu);
-    unsigned long long np = block_sum_u<kNlThreads>(a.np, shu);
-    if (threadIdx.x == 0) {
-        if (s) atomicAdd(vacc, s);
-        if (np) atomicAdd(npairs, np);
+    if (ENERGY) {
+        unsigned long long s = block_sum_u<kNlThreads>((unsigned long long)a.vq, shu);
+        unsigned long long np = block_sum_u<kNlThreads>(a.np, shu);
+        if (threadIdx.x == 0) {
+            if (s) atomicAdd(vacc, s);
+            if (np) atomicAdd(npairs, np);
+        }
     }
 }
 
 template <bool HALF>
-void launch_nl_force(gx_handle* h, int tpp, const GridGeom& g, const NlState* s, uint32_t n, const LawF32& L) {
+void launch_nl_force(gx_handle* h, int tpp, const GridGeom& g, const NlState* s, uint32_t n, const LawF32& L,
+                     bool energy) {
     const float4* pos4 = h->pos4;
     const uint32_t* home = h->key_sorted;
     const uint32_t* start = s->cl.start;
     if (tpp <= 1) {
-        GX_LAUNCH(h, k_nl_force<HALF>, nblk(n, kNlThreads), kNlThreads, g, pos4, home, start, n, L, h->d_pairf,
-                  s->list, s->cap, s->cap_nb, s->cnt, h->F, h->cap, h->dcount + 1, h->dcount + 0, h->derr);
+        auto k1 = energy ? k_nl_force<HALF, true> : k_nl_force<HALF, false>;
+        GX_LAUNCH(h, k1, nblk(n, kNlThreads), kNlThreads, g, pos4, home, start, n, L, h->d_pairf, s->list, s->cap,
+                  s->cap_nb, s->cnt, h->F, h->cap, h->dcount + 1, h->dcount + 0, h->derr);
         return;
     }
     const size_t threads = (size_t)n * tpp;
-    auto k = tpp == 2 ? k_nl_force_tpp<HALF, 2> : (tpp == 4 ? k_nl_force_tpp<HALF, 4> : k_nl_force_tpp<HALF, 8>);
+    auto k = energy ? (tpp == 2 ? k_nl_force_tpp<HALF, 2, true>
+                                : (tpp == 4 ? k_nl_force_tpp<HALF, 4, true> : k_nl_force_tpp<HALF, 8, true>))
+                    : (tpp == 2 ? k_nl_force_tpp<HALF, 2, false>
+                                : (tpp == 4 ? k_nl_force_tpp<HALF, 4, false> : k_nl_force_tpp<HALF, 8, false>));
     GX_LAUNCH(h, k, nblk(threads, kNlThreads), kNlThreads, g, pos4, home, start, n, L, h->d_pairf, s->list, s->cap,
               s->cap_nb, s->cnt, h->F, h->cap, h->dcount + 1, h->dcount + 0, h->derr);
 }
@@ -645,7 +657,7 @@ int nl_prepare(gx_handle* h, bool* stale) {
 
 // One tick of the list path up to and including the second kick; with
 // `kpart` also the kinetic-energy partials (nb blocks) for the thermostat.
-int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nb_out) {
+int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nb_out, bool energy) {
     NlState* s = nl_of(h);
     const uint32_t n = (uint32_t)h->n;
     const GridGeom& g = s->lg;
@@ -720,9 +732,9 @@ int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nb_out) {
     prof_begin(h, "force_nl");
     if (halfl) GX_CUDA(h, cudaMemsetAsync(h->F, 0, 3 * h->cap * sizeof(long long), h->stream));
     if (halfl)
-        launch_nl_force<true>(h, s->tpp, g, s, n, L);
+        launch_nl_force<true>(h, s->tpp, g, s, n, L, energy);
     else
-        launch_nl_force<false>(h, s->tpp, g, s, n, L);
+        launch_nl_force<false>(h, s->tpp, g, s, n, L, energy);
     prof_end(h, "force_nl");
     GX_LAUNCH(h, k_nl_fix_to_double, 1, 1, h->dcount + 1, h->dscal + 2, h->dscal + 3);
     if (bonds_on(h) && (rc = bond_spring(h, true))) return rc;  // into F before it becomes a
@@ -769,8 +781,8 @@ int nl_tune_tpp(gx_handle* h, int reps) {
     for (int k = 0; k < 4; ++k) {
         int rc = gx_timer_mark(h, 14);
         for (int r = 0; r < reps && !rc; ++r) {
-            if (s->half == 1) launch_nl_force<true>(h, cand[k], s->lg, s, n, L);
-            else launch_nl_force<false>(h, cand[k], s->lg, s, n, L);
+            if (s->half == 1) launch_nl_force<true>(h, cand[k], s->lg, s, n, L, false);
+            else launch_nl_force<false>(h, cand[k], s->lg, s, n, L, false);
         }
         double t = 0.0;
         if (!rc) rc = gx_timer_mark(h, 15);

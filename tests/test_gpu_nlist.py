@@ -206,3 +206,20 @@ def test_zero_skin_captured_rebuild_every_tick(gpu):
     h.set_universe(u)
     h.step(7, graph=True)
     assert h.list_rebuilds() == 7
+
+
+@pytest.mark.parametrize("variant", [5, 6])
+def test_ticks_without_records_give_the_same_state(gpu, variant):
+    # a tick that records nothing skips the potential and the pair count in
+    # the list pass; the forces, and so the trajectory, are the same bits
+    cfg, u = _lattice(14, temperature=200.0, coul=True)
+    cfg.enable_thermostat = True
+    cfg.thermostat_temperature = 60.0
+    out = []
+    for stats in (True, False):
+        h = _handle(cfg, variant)
+        h.set_universe(u)
+        h.step(30, stats=stats, graph=True)
+        out.append(h.get_state())
+    for x, y in zip(out[0], out[1]):
+        assert np.array_equal(x, y)
