@@ -32,7 +32,7 @@ class GxParams(C.Structure):
         ("enable_electrostatics", C.c_int32), ("enable_gravity", C.c_int32),
         ("enable_bond_interaction", C.c_int32), ("enable_thermostat", C.c_int32),
         ("enable_boundaries", C.c_int32), ("precision", C.c_int32), ("device", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("enable_collisions", C.c_int32), ("reserved", C.c_int32 * 2), ("particle_radius", _D),
     ]
 
 
@@ -69,7 +69,7 @@ EXPORTS = (
     "gx_batch_step", "gx_batch_get_state", "gx_adjoint_forward", "gx_adjoint_backward",
     "gx_set_list_skin", "gx_list_rebuilds", "gx_batch_set_mode", "gx_batch_get_mode", "gx_batch_autotune",
     "gx_get_list_config", "gx_set_list_threads", "gx_bond_observe", "gx_bond_tracker_reset", "gx_get_bonds",
-    "gx_bond_components",
+    "gx_bond_components", "gx_collisions", "gx_collision_count",
 )
 
 _lib = None
@@ -129,6 +129,8 @@ def load(path: str | Path | None = None) -> C.CDLL:
         "gx_bond_tracker_reset": (C.c_int, [vp]),
         "gx_get_bonds": (C.c_int, [vp, u32p, sz, C.POINTER(sz)]),
         "gx_bond_components": (C.c_int, [vp, u32p, dp, sz, C.POINTER(sz)]),
+        "gx_collisions": (C.c_int, [vp, u64p]),
+        "gx_collision_count": (C.c_int, [vp, u64p]),
         "gx_adjoint_backward": (C.c_int, [vp, dp, dp, dp, dp, dp, dp, dp]),
     }
     for name, (res, args) in proto.items():
@@ -173,6 +175,8 @@ def params(cfg, precision: str | int = "fp64", device: int = 0) -> GxParams:
     p.enable_bond_interaction = int(cfg.enable_bond_interaction)
     p.enable_thermostat = int(cfg.enable_thermostat)
     p.enable_boundaries = int(cfg.enable_boundaries)
+    p.enable_collisions = int(cfg.enable_collisions)
+    p.particle_radius = float(cfg.particle_radius)
     p.precision = _PRECISION[precision] if isinstance(precision, str) else int(precision)
     p.device = device
     return p
@@ -440,6 +444,18 @@ class Handle:
         self._check(self.lib.gx_bond_components(self.h, _ptr(labels, C.c_uint32), _ptr(energy, C.c_double),
                                                 len(energy), C.byref(nb)))
         return labels, energy[: nb.value].copy()
+
+    def collisions(self) -> int:
+        """One CollisionSystem pass on the resident state; the pairs that collided."""
+        c = C.c_uint64()
+        self._check(self.lib.gx_collisions(self.h, C.byref(c)))
+        return c.value
+
+    def collision_count(self) -> int:
+        """Collisions counted by every pass so far."""
+        c = C.c_uint64()
+        self._check(self.lib.gx_collision_count(self.h, C.byref(c)))
+        return c.value
 
     def bond_tracker_reset(self):
         self._check(self.lib.gx_bond_tracker_reset(self.h))

@@ -42,6 +42,7 @@ class Config:
     enable_movement: bool = True
     enable_boundaries: bool = True
     enable_collisions: bool = False
+    particle_radius: float = 0.4  # physics.particle_radius (config/mod.rs:98-100)
     enable_forces: bool = True
     enable_electrostatics: bool = False
     enable_gravity: bool = False
@@ -111,7 +112,7 @@ def from_toml(text: str) -> Config:
     c.speed_limit = _num(p["speed_limit"], "speed_limit")
     c.gravity_constant = _num(p["gravity_constant"], "gravity_constant")
     for k in ("thermal_constant", "coulomb_constant", "coulomb_cutoff", "gravity_cutoff",
-              "thermostat_temperature", "thermostat_tau"):
+              "thermostat_temperature", "thermostat_tau", "particle_radius"):
         if k in p:
             setattr(c, k, _num(p[k], k))
     # Affinity table overrides (ElementTable::apply_overrides, physics/forces.rs:90-109;

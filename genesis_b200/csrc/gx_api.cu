@@ -399,6 +399,7 @@ void gx_destroy(gx_handle* h) {
     nl_free(h);
     tracker_free(h);
     lens_free(h);
+    collide_free(h);
     free_buf(h->buf[0]);
     free_buf(h->buf[1]);
     cudaFree(h->key);
@@ -680,6 +681,7 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
     // state, so it can be captured: the first kick always applies the lambda
     // slot (1.0 unless a Berendsen scale is pending; v * 1.0 == v) and resets it.
     const bool use_nl = n && (h->kernel_variant >= 5 || h->kernel_variant == 0) && nl_eligible(h);
+    if (n && h->p.enable_collisions && (rc = collide_prepare(h))) return rc;  // CollisionSystem: allocate first
     if (use_nl) {
         bool stale = false;
         if ((rc = nl_prepare(h, &stale))) return rc;
@@ -719,6 +721,7 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
         if (n) {                                                        // ForceSystem
             int r = rebuild_cells(h);
             if (!r) r = force_pass(h, true, nullptr, nullptr, nullptr, false);
+            if (!r && h->p.enable_collisions) r = collide_pass(h);     // CollisionSystem
             if (r) return r;
         }
         launch_kick(h, h->buf[h->cur], n, 0.5 * h->p.dt, nullptr);  // VelocityHalfKick
@@ -801,6 +804,18 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
         if (e & kErrSaturation) return set_err(h, GX_ERR_SATURATION, "fixed-point force saturated");
         if (e & kErrTimeout) return set_err(h, GX_ERR_TIMEOUT, "shared-memory staging wait timed out");
     }
+    return GX_OK;
+}
+
+int gx_collisions(gx_handle* h, uint64_t* collisions) {
+    int rc = require_state(h);
+    if (rc) return rc;
+    if (collisions) *collisions = 0;
+    if ((rc = collide_prepare(h)) || (rc = commit_lambda(h)) || (rc = collide_pass(h))) return rc;
+    unsigned long long pass = 0, total = 0;
+    if ((rc = collide_read(h, &pass, &total))) return rc;
+    GX_CUDA(h, cudaGetLastError());
+    if (collisions) *collisions = pass;
     return GX_OK;
 }
 

@@ -238,6 +238,7 @@ struct gx_handle {
     // bond observation (gx_bondtrack.cu): open episodes on the device, owned there
     void* tracker = nullptr;
     void* lens = nullptr;     // analysis staging pool (gx_lens.cu)
+    void* coll = nullptr;     // collision pass state (gx_lens.cu)
 };
 
 // Every kernel launch of the library goes through this macro so the
@@ -303,6 +304,12 @@ int nl_set_tpp(gx_handle* h, int tpp);
 void nl_free(gx_handle* h);
 void tracker_free(gx_handle* h);
 void lens_free(gx_handle* h);
+// CollisionSystem on the device (gx_lens.cu): allocations outside any
+// capture, one pass (launches), its counters (synchronises), release.
+int collide_prepare(gx_handle* h);
+int collide_pass(gx_handle* h);
+int collide_read(gx_handle* h, unsigned long long* pass, unsigned long long* total);
+void collide_free(gx_handle* h);
 
 void launch_kick(gx_handle* h, const StateBuf& b, uint32_t n, double half_dt, const double* lambda);
 void launch_drift(gx_handle* h, const StateBuf& b, uint32_t n, double dt);

@@ -4,6 +4,7 @@
 //   g(r), partial g(r)        radial_distribution(_between) src/analysis/mod.rs:87-201
 //   friends-of-friends        clusters                  src/analysis/mod.rs:221-307
 //   bound pairs               bound_pairs_with_grid     src/analysis/pairs.rs:132-174
+//   elastic collisions        CollisionSystem::run      src/systems/collisions.rs:40-88
 //   bond-graph components     bond_components           src/analysis/mod.rs:331-411
 //                             + pair_potential_raw      src/physics/forces.rs:355-384
 //
@@ -298,6 +299,86 @@ struct BoundVisit {
         }
     }
 };
+
+// CollisionSystem (src/systems/collisions.rs:40-88) on the collision grid
+// (cell >= 2r): one thread per atom visits its own cell and every offset,
+// as the FP64 force pass does, so a pair is seen as often as the reference's
+// pair list holds it.  The impulse of elastic_pair
+// (src/physics/collision.rs:16-32) is computed from the velocities before
+// the pass; the atom's own half of it is exactly the negation of what its
+// partner computes (the displacement, the relative velocity and the normal
+// all flip sign exactly), so each thread sums its own velocity change with
+// no atomics.  A collision is counted once per pair-list entry (through the
+// canonical half shell, or j > i in the own cell).
+__global__ void __launch_bounds__(128) k_collide(GridGeom g, AuxSet a, StateBuf b,
+                                                 const uint32_t* __restrict__ pos_of_slot, double box0, double box1,
+                                                 double box2, double cd2, double* __restrict__ dv, size_t stride,
+                                                 unsigned long long* __restrict__ count) {
+    __shared__ unsigned int sc;
+    if (threadIdx.x == 0) sc = 0u;
+    __syncthreads();
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < a.m) {
+        const uint32_t c = a.key[i];
+        uint32_t cx, cy, cz;
+        decode(g, c, cx, cy, cz);
+        const double xi = a.x[i], yi = a.y[i], zi = a.z[i];
+        const uint32_t si = a.slot[i], pi = pos_of_slot[si];
+        const double vxi = b.vx[pi], vyi = b.vy[pi], vzi = b.vz[pi], mi = b.mass[pi];
+        double dvx = 0.0, dvy = 0.0, dvz = 0.0;
+        unsigned int cnt = 0u;
+        for (int k = -1; k < g.nfull; ++k) {
+            const uint32_t B = k < 0 ? c
+                                     : encode(g, wrap_add(cx, g.full[k][0], g.n[0]), wrap_add(cy, g.full[k][1], g.n[1]),
+                                              wrap_add(cz, g.full[k][2], g.n[2]));
+            for (uint32_t j = a.start[B], hi = a.start[B + 1]; j < hi; ++j) {
+                if (j == i) continue;
+                const double dx = min_image1(xsub(xi, a.x[j]), box0);
+                const double dy = min_image1(xsub(yi, a.y[j]), box1);
+                const double dz = min_image1(xsub(zi, a.z[j]), box2);
+                const double d2 = xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
+                if (d2 >= cd2) continue;
+                const double d = xsqrt(d2);
+                if (d <= kEpsF64) continue;  // check_pair, grid.rs:201-225
+                const uint32_t pj = pos_of_slot[a.slot[j]];
+                const double mj = b.mass[pj];
+                if (mi <= 0.0 || mj <= 0.0) continue;
+                const double inv = xdiv(1.0, d);
+                const double nx = xmul(dx, inv), ny = xmul(dy, inv), nz = xmul(dz, inv);
+                const double rx = xsub(vxi, b.vx[pj]), ry = xsub(vyi, b.vy[pj]), rz = xsub(vzi, b.vz[pj]);
+                const double vn = xadd(xadd(xmul(rx, nx), xmul(ry, ny)), xmul(rz, nz));
+                if (vn >= 0.0) continue;  // separating: no impulse
+                const double jj = xdiv(xmul(-2.0, vn), xadd(xdiv(1.0, mi), xdiv(1.0, mj)));
+                const double im = xdiv(1.0, mi);
+                const double ax = xmul(xmul(nx, jj), im), ay = xmul(xmul(ny, jj), im), az = xmul(xmul(nz, jj), im);
+                if (ax == 0.0 && ay == 0.0 && az == 0.0) continue;
+                dvx = xadd(dvx, ax);
+                dvy = xadd(dvy, ay);
+                dvz = xadd(dvz, az);
+                if (k < 0 ? j > i : k < g.nhalf) ++cnt;
+            }
+        }
+        dv[si] = dvx;
+        dv[stride + si] = dvy;
+        dv[2 * stride + si] = dvz;
+        if (cnt) atomicAdd(&sc, cnt);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && sc) atomicAdd(count, (unsigned long long)sc);
+}
+
+// vel += dv for every atom once any pair collided (collisions.rs:80-84).
+__global__ void k_apply_dv(StateBuf b, const uint32_t* __restrict__ pos_of_slot, const double* __restrict__ dv,
+                           size_t stride, uint32_t n, const unsigned long long* __restrict__ count) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n || *count == 0ull) return;
+    const uint32_t p = pos_of_slot[s];
+    b.vx[p] = xadd(b.vx[p], dv[s]);
+    b.vy[p] = xadd(b.vy[p], dv[stride + s]);
+    b.vz[p] = xadd(b.vz[p], dv[2 * stride + s]);
+}
+
+__global__ void k_add_total(unsigned long long* c) { c[1] += c[0]; }
 
 // Components of the bond list (bond_components, src/analysis/mod.rs:331-411):
 // union-find over the bonds, the label of a bonded slot is its root (the
@@ -652,6 +733,14 @@ int gx_radial_distribution_between(gx_handle* h, uint8_t ta, uint8_t tb, double 
     return gr_common(h, ta, tb, r_max, nbins, sample_cap, counts, bins, r_max_out, dr_out);
 }
 
+int gx_collision_count(gx_handle* h, uint64_t* total) {
+    if (!h || !total) return GX_ERR_ARG;
+    unsigned long long pass = 0, all = 0;
+    int rc = collide_read(h, &pass, &all);
+    *total = all;
+    return rc;
+}
+
 int gx_bond_components(gx_handle* h, uint32_t* labels, double* edge_energy, size_t energy_cap, size_t* nbonds) {
     int rc = require(h);
     if (rc) return rc;
@@ -756,6 +845,89 @@ namespace gx {
 void lens_free(gx_handle* h) {
     pool_release(static_cast<AuxPool*>(h->lens));
     h->lens = nullptr;
+}
+
+// The collision pass's own staging, so that a captured tick holds fixed
+// addresses: the binned copy of the atoms, the velocity changes (3 x cap by
+// slot) and the counters ([0] this pass, [1] cumulative).
+struct CollideState {
+    AuxPool* pool = nullptr;
+    double* dv = nullptr;
+    size_t cap = 0;
+    unsigned long long* cnt = nullptr;
+};
+
+void collide_free(gx_handle* h) {
+    CollideState* c = static_cast<CollideState*>(h->coll);
+    if (!c) return;
+    pool_release(c->pool);
+    cudaFree(c->dv);
+    cudaFree(c->cnt);
+    delete c;
+    h->coll = nullptr;
+}
+
+static GridGeom collide_grid(gx_handle* h, int* ok) {
+    return make_grid(h->p.box, 2.0 * h->p.particle_radius, ok);  // CollisionSystem::new, collisions.rs:16-21
+}
+
+// Allocations of the pass, outside any capture.
+int collide_prepare(gx_handle* h) {
+    if (!(h->p.particle_radius > 0.0)) return set_err(h, GX_ERR_ARG, "particle_radius must be positive");
+    int ok = 0;
+    GridGeom g = collide_grid(h, &ok);
+    if (!ok) return set_err(h, GX_ERR_ARG, "collision grid is empty or too large");
+    if (!h->coll) h->coll = new CollideState();
+    CollideState* c = static_cast<CollideState*>(h->coll);
+    if (!c->pool) c->pool = new AuxPool();
+    int rc = ensure_pool(h, *c->pool, h->n, h->n);
+    if (!rc) rc = ensure_cells(h, c->pool->cl, g.ncell);
+    if (rc) return rc;
+    if (c->cap < h->cap) {
+        cudaFree(c->dv);
+        c->dv = nullptr;
+        GX_CUDA(h, cudaMalloc(&c->dv, 3 * h->cap * sizeof(double)));
+        c->cap = h->cap;
+    }
+    if (!c->cnt) {
+        GX_CUDA(h, cudaMalloc(&c->cnt, 2 * sizeof(unsigned long long)));
+        GX_CUDA(h, cudaMemsetAsync(c->cnt, 0, 2 * sizeof(unsigned long long), h->stream));
+    }
+    return GX_OK;
+}
+
+// The counters of the last pass and of all passes (synchronises).
+int collide_read(gx_handle* h, unsigned long long* pass, unsigned long long* total) {
+    *pass = *total = 0;
+    CollideState* c = static_cast<CollideState*>(h->coll);
+    if (!c || !c->cnt) return GX_OK;
+    unsigned long long v[2] = {0, 0};
+    GX_CUDA(h, cudaMemcpyAsync(v, c->cnt, sizeof v, cudaMemcpyDeviceToHost, h->stream));
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    *pass = v[0];
+    *total = v[1];
+    return GX_OK;
+}
+
+// One pass on the handle's stream (launches only; collide_prepare first).
+int collide_pass(gx_handle* h) {
+    const uint32_t n = (uint32_t)h->n;
+    if (!n) return GX_OK;
+    CollideState* c = static_cast<CollideState*>(h->coll);
+    int ok = 0;
+    GridGeom g = collide_grid(h, &ok);
+    AuxSet a;
+    int rc = build_aux(h, *c->pool, g, nullptr, n, a);
+    if (rc) return rc;
+    const double contact = 2.0 * h->p.particle_radius;
+    prof_begin(h, "collisions");
+    GX_CUDA(h, cudaMemsetAsync(c->cnt, 0, sizeof(unsigned long long), h->stream));
+    GX_LAUNCH(h, k_collide, nblk(n, 128), 128, g, a, h->buf[h->cur], h->pos_of_slot, h->p.box[0], h->p.box[1],
+              h->p.box[2], contact * contact, c->dv, c->cap, c->cnt);
+    GX_LAUNCH(h, k_apply_dv, nblk(n, 256), 256, h->buf[h->cur], h->pos_of_slot, c->dv, c->cap, n, c->cnt);
+    GX_LAUNCH(h, k_add_total, 1, 1, c->cnt);
+    prof_end(h, "collisions");
+    return GX_OK;
 }
 
 void aux_pool_free(void* pool) { pool_release(static_cast<AuxPool*>(pool)); }

@@ -738,6 +738,7 @@ int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nb_out, bool
     prof_end(h, "force_nl");
     GX_LAUNCH(h, k_nl_fix_to_double, 1, 1, h->dcount + 1, h->dscal + 2, h->dscal + 3);
     if (bonds_on(h) && (rc = bond_spring(h, true))) return rc;  // into F before it becomes a
+    if (h->p.enable_collisions && (rc = collide_pass(h))) return rc;  // CollisionSystem, before the second kick
     int nb = (int)nblk(n, kRedThreads);
     if (nb > 1184) nb = 1184;  // the block count of launch_kinetic
     if (nb < 1) nb = 1;

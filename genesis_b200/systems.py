@@ -366,6 +366,24 @@ class GpuBondObservation(_GpuSystem):
                   lifetime_sum_ticks=st["lifetime_sum_ticks"], species_matrix=st["species_matrix"])
 
 
+class GpuCollisions(_GpuSystem):
+    """CollisionSystem (src/systems/collisions.rs:23-88): elastic impulses
+    between the pairs within 2 * particle_radius (gx_collisions)."""
+
+    def name(self):
+        return "collisions"
+
+    def access(self):
+        return Access(reads=["Position", "Velocity", "Mass"], writes=["Velocity"], resources_read=["Config"],
+                      resources_write=["CollisionCounter"])
+
+    def run(self, ctx):
+        self._enter()
+        c = self.gpu.h.collisions()
+        self._leave()
+        ctx.resources["CollisionCounter"] = ctx.resources.get("CollisionCounter", 0) + c
+
+
 class GpuBondStructure(_GpuSystem):
     """BondStructureSystem (src/systems/bond_structure.rs:25-246) every
     interval ticks: the components of the persistent-bond graph and each
@@ -428,6 +446,8 @@ def build_schedule(cfg, gpu: GpuWorld) -> Scheduler:
     if cfg.enable_boundaries:
         s.add_system(GpuBoundary(gpu))
     s.add_system(GpuForceSystem(gpu, cfg.enable_bond_interaction))
+    if cfg.enable_collisions:
+        s.add_system(GpuCollisions(gpu))
     s.add_system(GpuVelocityHalfKick(gpu))
     if cfg.enable_thermostat:
         s.add_system(GpuThermostat(gpu))

@@ -75,7 +75,9 @@ typedef struct {
     int32_t enable_boundaries;     /* systems.enable_boundaries */
     int32_t precision;             /* gx_precision */
     int32_t device;                /* CUDA device ordinal */
-    int32_t reserved[3];           /* must be zero */
+    int32_t enable_collisions;     /* systems.enable_collisions */
+    int32_t reserved[2];           /* must be zero */
+    double particle_radius;        /* physics.particle_radius (collision contact at 2 r) */
 } gx_params;
 
 /* Per-tick observables, what StatsSystem reads after the force schedule
@@ -272,6 +274,18 @@ int gx_bond_tracker_reset(gx_handle* h);
 int gx_bond_components(gx_handle* h, uint32_t* labels, double* edge_energy, size_t energy_cap, size_t* nbonds);
 /* The handle's bond list as slot pairs (a < b for observed bonds). */
 int gx_get_bonds(gx_handle* h, uint32_t* pairs, size_t cap, size_t* nbonds);
+
+/* CollisionSystem::run (src/systems/collisions.rs:40-88) once on the
+ * resident state: the pairs within 2 * particle_radius on a grid of that
+ * cell (reference multiplicity on axes of 2 cells), the elastic impulse of
+ * each approaching pair (elastic_pair, src/physics/collision.rs:16-32) from
+ * the velocities before the pass, applied to every velocity once any pair
+ * collided.  *collisions (may be NULL) receives the pairs that collided.
+ * With gx_params.enable_collisions, gx_step runs the same pass after the
+ * force pass of every tick (src/universe/mod.rs:362-365). */
+int gx_collisions(gx_handle* h, uint64_t* collisions);
+/* Collisions counted by every pass so far (CollisionCounter). */
+int gx_collision_count(gx_handle* h, uint64_t* total);
 
 /* Per-tick column sync of a drop-in system whose ECS lives on the host:
  * overwrite Position, Velocity and Acceleration (slot order, AoS f64) of the

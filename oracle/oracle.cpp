@@ -470,6 +470,56 @@ void orc_stats(size_t n, const double* vel, const double* mass, double* kinetic,
     *speed_sum = sp;
 }
 
+// elastic_pair, src/physics/collision.rs:16-32: the velocity changes of both
+// particles (n points from 2 towards 1; Vec3 `/ x` scales by 1/x,
+// src/math/mod.rs); false when they separate or a mass is not positive.
+static bool elastic_pair(double m1, V3 v1, double m2, V3 v2, V3 n, V3* dv1, V3* dv2) {
+    *dv1 = V3{0.0, 0.0, 0.0};
+    *dv2 = V3{0.0, 0.0, 0.0};
+    if (m1 <= 0.0 || m2 <= 0.0) return false;
+    V3 vrel = sub(v1, v2);
+    double vn = vrel.x * n.x + vrel.y * n.y + vrel.z * n.z;
+    if (vn >= 0.0) return false;
+    double j = -2.0 * vn / (1.0 / m1 + 1.0 / m2);
+    V3 jv = scale(n, j);
+    *dv1 = scale(jv, 1.0 / m1);
+    *dv2 = scale(scale(jv, 1.0 / m2), -1.0);
+    return true;
+}
+
+// CollisionSystem::run, src/systems/collisions.rs:40-88: the pairs within 2r
+// on a grid of cell 2r, impulses from the velocities before the pass, summed
+// per particle in pair order and applied when any pair collided.  Returns
+// the collisions counted.
+static size_t collisions_impl(const orc_params* p, size_t n, const double* pos, double* vel, const double* mass) {
+    if (n == 0) return 0;
+    const double contact = 2.0 * p->particle_radius;
+    Grid g(p->box, contact);
+    g.build(pos, n);
+    std::vector<V3> dv(n, V3{0.0, 0.0, 0.0});
+    size_t count = 0;
+    g.neighbors(pos, contact, [&](uint32_t a, uint32_t b, V3 delta, double d) {
+        V3 da, db;
+        elastic_pair(mass[a], at(vel, a), mass[b], at(vel, b), scale(delta, 1.0 / d), &da, &db);
+        if (da.x != 0.0 || da.y != 0.0 || da.z != 0.0) {
+            dv[a] = add(dv[a], da);
+            dv[b] = add(dv[b], db);
+            ++count;
+        }
+    });
+    if (count)
+        for (size_t i = 0; i < n; ++i) {
+            vel[3 * i] += dv[i].x;
+            vel[3 * i + 1] += dv[i].y;
+            vel[3 * i + 2] += dv[i].z;
+        }
+    return count;
+}
+
+size_t orc_collisions(const orc_params* p, size_t n, const double* pos, double* vel, const double* mass) {
+    return collisions_impl(p, n, pos, vel, mass);
+}
+
 int orc_ticks(const orc_params* p, size_t n, double* pos, double* vel, double* acc, const uint8_t* elem,
               const double* charge, const double* mass, size_t nbonds, const uint32_t* bonds, int nticks,
               int nthreads, double* out_stats) {
@@ -481,6 +531,7 @@ int orc_ticks(const orc_params* p, size_t n, double* pos, double* vel, double* a
             par_chunks(n, nt, [&](size_t lo, size_t hi) { wrap_range(pos, p->box, lo, hi); });
         double V = 0.0, Vb = 0.0;
         size_t np = forces_impl(p, n, pos, elem, charge, mass, nbonds, bonds, acc, &V, &Vb, nt);
+        if (p->enable_collisions) collisions_impl(p, n, pos, vel, mass);  // universe/mod.rs:363-365
         par_chunks(n, nt, [&](size_t lo, size_t hi) { half_kick_range(vel, acc, p->dt, lo, hi); });
         double K = 0.0, lam = 1.0;
         if (p->enable_thermostat)

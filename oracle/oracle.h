@@ -53,8 +53,14 @@ typedef struct {
     int32_t enable_bond_interaction;
     int32_t enable_thermostat;
     int32_t enable_boundaries;
-    int32_t reserved;
+    int32_t enable_collisions;
+    int32_t reserved[2];
+    double particle_radius;
 } orc_params;
+
+/* One CollisionSystem pass (src/systems/collisions.rs:40-88) on vel; returns
+ * the collisions counted. */
+size_t orc_collisions(const orc_params* p, size_t n, const double* pos, double* vel, const double* mass);
 
 /* ---- pair laws: src/physics/forces.rs ---- */
 void orc_lj_table(const orc_params* p, double* pair_sigma /*100*/,

@@ -29,7 +29,8 @@ class OrcParams(C.Structure):
         ("thermostat_temperature", _D), ("thermostat_tau", _D),
         ("enable_electrostatics", C.c_int32), ("enable_gravity", C.c_int32),
         ("enable_bond_interaction", C.c_int32), ("enable_thermostat", C.c_int32),
-        ("enable_boundaries", C.c_int32), ("reserved", C.c_int32),
+        ("enable_boundaries", C.c_int32), ("enable_collisions", C.c_int32), ("reserved", C.c_int32 * 2),
+        ("particle_radius", C.c_double),
     ]
 
 
@@ -75,6 +76,7 @@ def load() -> C.CDLL:
             "orc_thermostat": (C.c_int, [sz, dp, dp, _D, _D, _D, dp, dp]),
             "orc_stats": (None, [sz, dp, dp, dp, dp]),
             "orc_ticks": (C.c_int, [pp, sz, dp, dp, dp, u8p, dp, dp, sz, u32p, C.c_int, C.c_int, dp]),
+            "orc_collisions": (sz, [pp, sz, dp, dp, dp]),
             "orc_radial_distribution": (C.c_int, [sz, dp, dp, _D, sz, u64p, dp, dp, dp]),
             "orc_radial_distribution_between": (C.c_int, [sz, dp, u8p, C.c_uint8, C.c_uint8, dp, _D, sz, u64p, dp,
                                                           dp, dp]),
@@ -127,6 +129,8 @@ def params(cfg) -> OrcParams:
     p.enable_bond_interaction = int(cfg.enable_bond_interaction)
     p.enable_thermostat = int(cfg.enable_thermostat)
     p.enable_boundaries = int(cfg.enable_boundaries)
+    p.enable_collisions = int(cfg.enable_collisions)
+    p.particle_radius = float(cfg.particle_radius)
     return p
 
 
@@ -266,6 +270,16 @@ def stats(vel, mass):
 
 
 TICK_FIELDS = ("kinetic", "potential", "bond_energy", "lambda", "pairs")
+
+
+def collisions(cfg, pos, vel, mass):
+    """One CollisionSystem pass: (velocities after, collisions counted)."""
+    lib = load()
+    pos = _f64(pos)
+    vel = _f64(vel).copy()
+    c = lib.orc_collisions(C.byref(params(cfg)), len(pos), _p(pos, C.c_double), _p(vel, C.c_double),
+                           _p(_f64(mass), C.c_double))
+    return vel, int(c)
 
 
 def ticks(cfg, pos, vel, acc, elem, charge, mass, nticks, bonds=None, nthreads=1):
