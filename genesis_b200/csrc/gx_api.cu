@@ -285,7 +285,9 @@ int rebuild_cells(gx_handle* h) {
 
 int check_kinds(gx_handle* h) {
     if (h->precision == GX_MIXED && h->nkinds > kMaxKinds)
-        return set_err(h, GX_ERR_UNSUPPORTED, "mixed precision supports at most 16 distinct (element, charge) kinds");
+        return set_err(h, GX_ERR_UNSUPPORTED,
+                       "mixed precision supports at most 16 distinct (element, charge) kinds, (element, charge, mass) "
+                       "with gravity");
     return GX_OK;
 }
 
@@ -307,6 +309,7 @@ int upload_pairf(gx_handle* h) {
             // symmetric by construction: (i, j) and (j, i) must round identically
             int lo = a < b ? a : b, hi = a < b ? b : a;
             t.qq = (float)(h->p.coulomb_constant * h->kind_charge[lo] * h->kind_charge[hi]);
+            t.gm = (float)(h->p.gravity_constant * h->kind_mass[lo] * h->kind_mass[hi]);
         }
     GX_CUDA(h, cudaMemcpy(h->d_pairf, tab, sizeof tab, cudaMemcpyHostToDevice));
     return GX_OK;
@@ -425,8 +428,6 @@ void gx_destroy(gx_handle* h) {
 
 int gx_set_precision(gx_handle* h, int precision) {
     if (!h || (precision != GX_FP64 && precision != GX_MIXED)) return GX_ERR_ARG;
-    if (precision == GX_MIXED && h->p.enable_gravity)
-        return set_err(h, GX_ERR_UNSUPPORTED, "gravity is only implemented in the FP64 path");
     h->precision = precision;
     h->sorted = false;
     invalidate_graphs(h);
@@ -456,18 +457,22 @@ int gx_set_state(gx_handle* h, size_t n, const double* pos, const double* vel, c
     StateBuf& b = h->buf[0];
     uint32_t un = (uint32_t)n;
     std::vector<double> tmp(n);
-    // kinds: distinct (element, charge) pairs, first-seen order
+    // kinds: distinct (element, charge) pairs -- with gravity (element,
+    // charge, mass) -- in first-seen order
     h->nkinds = 0;
     std::vector<uint8_t> kind(n);
+    const bool by_mass = h->p.enable_gravity != 0;
     for (size_t i = 0; i < n; ++i) {
         double q = charge ? charge[i] : h->p.charge[elem[i]];
+        double m = by_mass ? (mass ? mass[i] : kElementMass[elem[i]]) : 0.0;
         int found = -1;
         for (int k = 0; k < h->nkinds && k < kMaxKinds; ++k)
-            if (h->kind_elem[k] == elem[i] && h->kind_charge[k] == q) found = k;
+            if (h->kind_elem[k] == elem[i] && h->kind_charge[k] == q && h->kind_mass[k] == m) found = k;
         if (found < 0) {
             if (h->nkinds < kMaxKinds) {
                 h->kind_elem[h->nkinds] = elem[i];
                 h->kind_charge[h->nkinds] = q;
+                h->kind_mass[h->nkinds] = m;
             }
             found = h->nkinds++;
         }

@@ -334,7 +334,7 @@ int gx_batch_create(const gx_params* p, int nrep, const double* box, const doubl
             max_pair = std::fmax(max_pair, s);
         }
     }
-    if (p->enable_gravity) return berr(b, GX_ERR_UNSUPPORTED, "gravity is only implemented in the FP64 path");
+    if (p->enable_gravity) return berr(b, GX_ERR_UNSUPPORTED, "batched replicas do not support gravity");
     double lj_rc = std::fmax(p->lj_cutoff_factor, 1.0) * max_pair;
     double coul_rc = p->enable_electrostatics ? std::fmax(p->coulomb_cutoff, 1.0) * max_sigma : 0.0;
     double rc = std::fmax(lj_rc, coul_rc);

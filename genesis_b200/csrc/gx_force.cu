@@ -348,7 +348,6 @@ int force_pass(gx_handle* h, bool finalize_acc, double* V, double* Vb, uint64_t*
         prof_end(h, "force_f64");
     } else {
         LawF32 L = make_law32(h);
-        if (h->p.enable_gravity) return set_err(h, GX_ERR_UNSUPPORTED, "gravity is only implemented in the FP64 path");
         GX_CUDA(h, cudaMemsetAsync(h->F, 0, 3 * h->cap * sizeof(long long), h->stream));
         // staged kernels pack atom indices in 27 bits and need >= 3 cells per axis
         const int var = h->kernel_variant;
@@ -406,6 +405,10 @@ LawF32 make_law32(const gx_handle* h) {
     L.coul_rc = (float)h->fs.coul_rc;
     L.coul_ron = (float)h->fs.coul_ron;
     L.inv_coul_w = L.coul ? (float)(1.0 / (h->fs.coul_rc - h->fs.coul_ron)) : 0.f;
+    L.grav = h->p.enable_gravity ? 1 : 0;
+    L.grav_rc = (float)h->fs.grav_rc;
+    L.grav_ron = (float)h->fs.grav_ron;
+    L.inv_grav_w = L.grav ? (float)(1.0 / (h->fs.grav_rc - h->fs.grav_ron)) : 0.f;
     L.nkinds = h->nkinds;
     return L;
 }

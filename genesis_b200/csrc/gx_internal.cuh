@@ -134,7 +134,7 @@ struct ForceSetup {
 // Mixed-path pair table entry, one per (kind_i, kind_j).
 struct PairF {
     float sigma, half_sigma, inv_half_sigma, eps4;
-    float eps24, qq, pad0, pad1;
+    float eps24, qq, gm, pad1;  // qq = k_e q_i q_j, gm = G m_i m_j
 };
 
 // Device buffers of one atom set in cell-sorted order.
@@ -201,6 +201,7 @@ struct gx_handle {
     // mixed kinds
     int nkinds = 0;
     double kind_charge[gx::kMaxKinds];
+    double kind_mass[gx::kMaxKinds];  // part of the kind only with gravity
     uint8_t kind_elem[gx::kMaxKinds];
     gx::PairF* d_pairf = nullptr;  // kMaxKinds^2
 

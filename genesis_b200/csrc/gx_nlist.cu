@@ -579,12 +579,12 @@ void nl_free(gx_handle* h) {
     h->nl = nullptr;
 }
 
-// The list path applies to the mixed pass without gravity, with at least 3
-// list-grid cells per axis (so the force grid has at least 3 too, and every
-// pair within the cutoff occurs once in the reference's pair list) and atom
-// indices below 2^27.
+// The list path applies to the mixed pass with at least 3 list-grid cells
+// per axis (so the force grid has at least 3 too, and every pair within the
+// cutoff occurs once in the reference's pair list) and atom indices below
+// 2^27.
 bool nl_eligible(gx_handle* h) {
-    if (h->precision != GX_MIXED || h->p.enable_gravity) return false;
+    if (h->precision != GX_MIXED) return false;
     if (h->n == 0 || h->n >= (1u << 27)) return false;
     NlState* s = nl_of(h);
     double rl = h->fs.rc + skin_of(h, s);

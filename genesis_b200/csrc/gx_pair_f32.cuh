@@ -4,7 +4,9 @@
 // and the quintic switch on [r_on, r_c] (force_switched_scalar, lj_raw,
 // smooth_cutoff, switched: src/physics/forces.rs:270-353), plus Coulomb with
 // the absolute core max(d, 0.5) and its own switch on d
-// (src/systems/forces.rs:282-289).  Returns the force magnitude divided by d
+// (src/systems/forces.rs:282-289), plus gravity -G m_i m_j / r^2 with the
+// same core and its own switch (forces.rs:291-299, gravity_raw
+// src/physics/forces.rs:338-341).  Returns the force magnitude divided by d
 // (so F_vec = delta * fs) and the switched potential.
 //
 // Every operation is an explicit round-to-nearest intrinsic or fmaf, so the
@@ -20,6 +22,8 @@ namespace gx {
 struct LawF32 {
     float rc2, lj_rc, lj_ron, inv_lj_w, coul_rc, coul_ron, inv_coul_w;
     int coul, nkinds;
+    int grav = 0;
+    float grav_rc = 0.f, grav_ron = 0.f, inv_grav_w = 0.f;
 };
 
 __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
@@ -78,6 +82,17 @@ __device__ __forceinline__ void pair_f32(const LawF32& L, const PairF& t, float 
         float dsw = fmul(dsdu, L.inv_coul_w);
         f = fadd(f, fmaf(mc, sw, -fmul(vc, dsw)));
         v = fadd(v, fmul(vc, sw));
+    }
+    if (L.grav && d < L.grav_rc) {
+        float inv_r = d < 0.5f ? 2.f : inv_d;
+        float vg = -fmul(t.gm, inv_r);  // attractive
+        float mg = fmul(vg, inv_r);
+        float u = fminf(fmaxf(fmul(fsub(d, L.grav_ron), L.inv_grav_w), 0.f), 1.f);  // as above
+        float sw, dsdu;
+        switch5(u, sw, dsdu);
+        float dsw = fmul(dsdu, L.inv_grav_w);
+        f = fadd(f, fmaf(mg, sw, -fmul(vg, dsw)));
+        v = fadd(v, fmul(vg, sw));
     }
     fs = fmul(f, inv_d);
 }

@@ -114,8 +114,7 @@ int gx_set_precision(gx_handle* h, int precision);
  * rebuilt (re-sort included) only when an atom has moved more than skin/2,
  * one thread per atom over its full list, no atomics; 6 = the same with a
  * half list (each pair once, the far end's force through integer atomics).
- * 5 and 6 need no gravity, no bond spring and >= 3 list-grid cells per
- * axis, else they fall back to 4.  Variants 2 and 3 need >= 3 force-grid
+ * 5 and 6 need >= 3 list-grid cells per axis, else they fall back to 4.  Variants 2 and 3 need >= 3 force-grid
  * cells per axis and fall back to 1 otherwise.  Variants 1-4 give
  * bit-identical forces, and so do 5 and 6 (fixed-point sums); 5 and 6
  * evaluate the same pair set in a cell-local frame whose origin is the

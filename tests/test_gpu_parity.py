@@ -377,3 +377,36 @@ def test_nonfinite_position_is_reported(gpu):
         with pytest.raises(GxError) as e:
             h.forces()
         assert e.value.status == -6
+
+
+@pytest.mark.parametrize("precision,variant", [("fp64", 0), ("mixed", 1), ("mixed", 6)])
+def test_gravity_matches_fp64_oracle(gpu, orc, precision, variant):
+    # gravity in the FP32 pair law (-G m_i m_j / r^2 with its own switch);
+    # with per-atom masses off the element table the kinds carry the mass
+    import dataclasses
+    wl = W.Workload("gravity check", n_side=12, temperature=60.0, steps=10, seed=3, electrostatics=True)
+    cfg, u = wl.config(), wl.generate()
+    cfg.enable_gravity = True
+    cfg.gravity_constant = 5.0
+    if precision == "mixed":  # 10 elements x 2 masses: more kinds than the FP32 table holds
+        rng = np.random.default_rng(1)
+        u2 = dataclasses.replace(u, mass=u.mass * np.where(rng.random(u.n) < 0.5, 1.0, 1.5))
+        with pytest.raises(Exception, match="kinds"):
+            _handle(cfg, "mixed").set_universe(u2)
+    u = dataclasses.replace(u, mass=u.mass * 1.3)  # masses off the element table, one per element
+    h = _handle(cfg, precision)
+    if variant:
+        h.set_kernel_variant(variant)
+    h.set_universe(u)
+    st = h.step(1)
+    _, _, acc = h.get_state()
+    _, _, acc_ref, st_ref = orc.ticks(cfg, u.pos, u.vel, None, u.elem, u.charge, u.mass, 1)
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    assert np.linalg.norm(acc - acc_ref) / np.linalg.norm(acc_ref) <= tol
+    assert abs(st["potential"][0] - st_ref[0, 1]) <= tol * abs(st_ref[0, 1])
+    # the gravity term is really in play
+    cfg0 = dataclasses.replace(cfg, enable_gravity=False)
+    _, _, acc0, _ = orc.ticks(cfg0, u.pos, u.vel, None, u.elem, u.charge, u.mass, 1)
+    assert np.linalg.norm(acc0 - acc_ref) / np.linalg.norm(acc_ref) > 1e-3
+    if variant == 6:
+        assert h.list_rebuilds() >= 1  # the neighbour-list path ran
