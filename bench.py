@@ -518,6 +518,9 @@ def ours_arm(args, dist):
             "flop_per_launch": pairs * flop_pp, "pairs_per_launch": pairs, "launch_ms": force_ms,
             "share_of_step": f_ms / tot_ms if tot_ms else None}
     hbm = measured_peaks().get("hbm_gbs")
+    hbm_src = "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    if not hbm:  # the file is written by the driver of each run; else an earlier measurement on this pool
+        hbm, hbm_src = 6650.0, "fallback 6650 GB/s (of fallback: an earlier copy-bandwidth measurement)"
     mem = {}
     for k, (nl, kms) in prof.items():
         if k in BYTES_PER_ATOM and nl and BYTES_PER_ATOM[k]:
@@ -528,8 +531,8 @@ def ours_arm(args, dist):
     roof_hbm = None
     if top_mem:
         roof_hbm = {"kernel": top_mem[0], "bound": "hbm", "achieved": top_mem[1]["GB/s"], "peak": hbm,
-                    "unit": "GB/s", "frac": top_mem[1]["frac"], "peak_source": "MEASURED_PEAKS.json hbm_gbs"
-                    if hbm else "fallback 6650 GB/s", "traffic": ncu_traffic(top_mem[0])}
+                    "unit": "GB/s", "frac": top_mem[1]["frac"], "peak_source": hbm_src,
+                    "traffic": ncu_traffic(top_mem[0])}
     kernels = {k: {"launches": v[0], "ms": v[1], "share": v[1] / tot_ms if tot_ms else None}
                for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}
 
