@@ -191,7 +191,11 @@ __global__ void k_nl_stage(GridGeom g, StateBuf b, const uint32_t* __restrict__ 
 
 // List of the pairs within r_l (r_l^2 = rl2) over the 27 home-grid cells:
 // every neighbour (full list), or with HALF only those at a later sorted
-// position (each pair once).
+// position (each pair once).  A neighbour cell whose nearest point is out of
+// reach of the atom is skipped whole, and the cell's periodic shift is added
+// to the atom once per cell; the resulting rounding differences (an ulp of
+// a cell length) lie well inside the 1e-6 relative margin of r_l, so the
+// list still holds every pair within r_c + skin.
 template <bool HALF>
 __global__ void __launch_bounds__(kNlThreads) k_nl_build(GridGeom g, const float4* __restrict__ pos4,
                                                           const uint32_t* __restrict__ home,
@@ -201,24 +205,33 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_build(GridGeom g, const float
     if (gated_off(gate)) return;
     uint32_t p = blockIdx.x * kNlThreads + threadIdx.x;
     if (p >= n) return;
-    float4 pi = pos4[p];
+    const float4 pi = pos4[p];
     const uint32_t c = home[p];
     uint32_t cx, cy, cz;
     decode(g, c, cx, cy, cz);
+    // atoms of a cell sit within [0, cell) of its frame up to staging rounding
+    const float slack = 1e-3f;
     uint32_t m = 0;
     for (uint32_t code = 0; code < 27; ++code) {
-        uint32_t B = cell_at(g, cx, cy, cz, code);
+        const int ox = (int)(code % 3u) - 1, oy = (int)((code / 3u) % 3u) - 1, oz = (int)(code / 9u) - 1;
+        const uint32_t B = cell_at(g, cx, cy, cz, code);
         // atoms are sorted by cell: a lower cell index means every q < p
         if (HALF && B < c) continue;
+        const float mx = fmaxf((ox > 0 ? g.cellf[0] - pi.x : (ox < 0 ? pi.x : 0.f)) - slack, 0.f);
+        const float my = fmaxf((oy > 0 ? g.cellf[1] - pi.y : (oy < 0 ? pi.y : 0.f)) - slack, 0.f);
+        const float mz = fmaxf((oz > 0 ? g.cellf[2] - pi.z : (oz < 0 ? pi.z : 0.f)) - slack, 0.f);
+        if (dist2(mx, my, mz) >= rl2) continue;  // the whole cell is out of reach
         float sx, sy, sz;
         code_shift(g, code, sx, sy, sz);
-        uint32_t lo = start[B], hi = start[B + 1];
-        if (HALF && B == c) lo = p + 1;
+        const float qx = fadd(pi.x, sx), qy = fadd(pi.y, sy), qz = fadd(pi.z, sz);
+        uint32_t lo = start[B];
+        const uint32_t hi = start[B + 1];
+        if (HALF && B == c) lo = p + 1;  // HALF: every candidate lies after p
+#pragma unroll 4
         for (uint32_t q = lo; q < hi; ++q) {
-            if (q == p) continue;
-            float4 pj = pos4[q];
-            float dx = delta1(pi.x, pj.x, sx), dy = delta1(pi.y, pj.y, sy), dz = delta1(pi.z, pj.z, sz);
-            if (dist2(dx, dy, dz) < rl2 && (!HALF || q > p)) {
+            if (!HALF && q == p) continue;
+            const float4 pj = pos4[q];
+            if (dist2(fsub(qx, pj.x), fsub(qy, pj.y), fsub(qz, pj.z)) < rl2) {
                 if (m < (uint32_t)cap_nb) list[(size_t)m * stride + p] = q | (code << 27);
                 ++m;
             }
@@ -227,8 +240,6 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_build(GridGeom g, const float
     cnt[p] = m;
 }
 
-// End of the list work of a tick: a rebuild starts a fresh frame; otherwise
-// this tick's wrap added one half-box translation.
 // The rebuild body's condition: the flag k_nl_advance raised.
 __global__ void k_nl_set_cond(cudaGraphConditionalHandle hc, const uint32_t* __restrict__ flag) {
     cudaGraphSetConditional(hc, flag[0] != 0u ? 1u : 0u);
