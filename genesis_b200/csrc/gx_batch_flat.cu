@@ -15,11 +15,14 @@
 //   k_fb_stage    FP32 cell-local positions in sorted order, zero forces
 //   k_fb_force    one thread per atom over its replica's canonical half
 //                 shell, pair_f32, int64 fixed-point sums (k_force_mixed's
-//                 arithmetic), potential and pair count per replica
+//                 arithmetic), potential and pair count per replica on
+//                 the tick that reports them
 //   k_fb_finish   a = F 2^-32 / m, second kick
 //   k_fb_thermo   one block per replica: kinetic energy in a fixed order,
 //                 the replica's Berendsen lambda (thermostat.rs:52-71)
-// One tick is captured once as a CUDA graph and replayed.  At the end of a
+// One tick is captured once as a CUDA graph in two forms, with and without
+// the potential and pair count; a step call replays the quiet form and ends
+// with the reporting one (the forces are the same bits).  At the end of a
 // step call the pending scales are applied (k_fb_commit), as the persistent
 // mode does.  Every operation on a replica's atoms is the single-universe
 // mixed path's, so an NVE replica reproduces gx_step (pair-pass variants
@@ -58,13 +61,14 @@ struct BatchFlat {
     double* lam = nullptr;              // pending Berendsen scale per replica
     unsigned long long* acc = nullptr;  // [2 nrep]: fixed-point V, pair count
     gx_handle* ctx = nullptr;           // launch context of the shared counting sort
-    cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t graph[2] = {};      // tick without / with the potential and pair count
     uint64_t graph_kernels = 0;
 };
 
 void batch_flat_free(BatchFlat* f) {
     if (!f) return;
-    if (f->graph) cudaGraphExecDestroy(f->graph);
+    for (cudaGraphExec_t g : f->graph)
+        if (g) cudaGraphExecDestroy(g);
     cudaFree(f->geo);
     cudaFree(f->th);
     cudaFree(f->rep_of);
@@ -150,6 +154,7 @@ __global__ void k_fb_stage(const RepGeo* __restrict__ geo, const uint32_t* __res
 
 // k_force_mixed on the atom's own replica grid (canonical half shell, the
 // same shifts, minimum image on axes with fewer than 3 cells).
+template <bool ENERGY>
 __global__ void __launch_bounds__(kFbThreads) k_fb_force(const RepGeo* __restrict__ geo, const float4* __restrict__ pos4,
                                                           const uint32_t* __restrict__ skey,
                                                           const uint32_t* __restrict__ srep,
@@ -200,7 +205,6 @@ __global__ void __launch_bounds__(kFbThreads) k_fb_force(const RepGeo* __restric
                 }
                 float d2 = dist2(dx, dy, dz);
                 if (!(d2 < L.rc2) || d2 == 0.f) continue;
-                ++np;
                 float fs, v;
                 pair_f32(L, st[ki * L.nkinds + __float_as_int(pj.w)], d2, fs, v);
                 long long qx = quant(fmul(dx, fs), err), qy = quant(fmul(dy, fs), err), qz = quant(fmul(dz, fs), err);
@@ -210,13 +214,17 @@ __global__ void __launch_bounds__(kFbThreads) k_fb_force(const RepGeo* __restric
                 atomicAdd((unsigned long long*)&F[j], (unsigned long long)(-qx));
                 atomicAdd((unsigned long long*)&F[fstride + j], (unsigned long long)(-qy));
                 atomicAdd((unsigned long long*)&F[2 * fstride + j], (unsigned long long)(-qz));
-                vq += quant(v, err);
+                if (ENERGY) {
+                    vq += quant(v, err);
+                    ++np;
+                }
             }
         }
         atomicAdd((unsigned long long*)&F[s], (unsigned long long)fx);
         atomicAdd((unsigned long long*)&F[fstride + s], (unsigned long long)fy);
         atomicAdd((unsigned long long*)&F[2 * fstride + s], (unsigned long long)fz);
     }
+    if (!ENERGY) return;
     // per-replica potential and pair count: one atomic per warp when the
     // warp lies in one replica (the usual case), else one per lane
     const uint32_t r0 = __shfl_sync(0xffffffffu, r, 0);
@@ -390,8 +398,10 @@ int flat_prepare(gx_batch* b) {
     return GX_OK;
 }
 
-// One tick, all replicas (launches only: capturable).
-int flat_tick(gx_batch* b, BatchParams P) {
+// One tick, all replicas (launches only: capturable).  Without energy the
+// force pass leaves the replicas' potential and pair count at zero: the
+// forces are the same bits, and only the last tick of a step call reports.
+int flat_tick(gx_batch* b, BatchParams P, bool energy) {
     BatchFlat* f = b->flat;
     gx_handle* h = f->ctx;
     const uint32_t n = (uint32_t)b->total;
@@ -402,8 +412,12 @@ int flat_tick(gx_batch* b, BatchParams P) {
     int rc = counting_sort(h, h->cl, f->ncell, A.key, n, A.idx);
     if (rc) return ferr(b, rc, h->err);
     GX_LAUNCH(h, k_fb_stage, nblk(n, 256), 256, f->geo, f->rep_of, A, A.idx, A.key, n, f->srep, fs);
-    GX_LAUNCH(h, k_fb_force, nblk(n, kFbThreads), kFbThreads, f->geo, A.pos4, A.skey, f->srep, h->cl.start, n, b->L,
-              b->d_tab, A.F, fs, f->acc, b->d_err);
+    if (energy)
+        GX_LAUNCH(h, k_fb_force<true>, nblk(n, kFbThreads), kFbThreads, f->geo, A.pos4, A.skey, f->srep, h->cl.start,
+                  n, b->L, b->d_tab, A.F, fs, f->acc, b->d_err);
+    else
+        GX_LAUNCH(h, k_fb_force<false>, nblk(n, kFbThreads), kFbThreads, f->geo, A.pos4, A.skey, f->srep,
+                  h->cl.start, n, b->L, b->d_tab, A.F, fs, f->acc, b->d_err);
     GX_LAUNCH(h, k_fb_finish, nblk(n, 256), 256, A, A.idx, n, P.half_dt, fs);
     GX_LAUNCH(h, k_fb_thermo, b->nrep, kFbRed, f->th, A, f->lam, f->acc, P.k_thermal, b->d_out);
     return GX_OK;
@@ -426,24 +440,25 @@ int batch_flat_step(gx_batch* b, int nsteps, uint64_t* launches) {
     gx_handle* h = f->ctx;
     const uint64_t l0 = h->launches;
     if (!b->total) return GX_OK;
-    if (!f->graph) {
+    for (int e = 0; e < 2; ++e) {
+        if (f->graph[e]) continue;
         cudaGraph_t g = nullptr;
         GXF_CUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         const uint64_t c0 = h->launches;
-        int trc = flat_tick(b, P);
+        int trc = flat_tick(b, P, e == 1);
         cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
         if (trc || ce != cudaSuccess) {
             if (g) cudaGraphDestroy(g);
             return trc ? trc : ferr(b, GX_ERR_CUDA, cudaGetErrorString(ce));
         }
-        ce = cudaGraphInstantiate(&f->graph, g, 0);
+        ce = cudaGraphInstantiate(&f->graph[e], g, 0);
         cudaGraphDestroy(g);
         if (ce != cudaSuccess) return ferr(b, GX_ERR_CUDA, cudaGetErrorString(ce));
         f->graph_kernels = h->launches - c0;
         h->launches = c0;
     }
     for (int s = 0; s < nsteps; ++s) {
-        GXF_CUDA(b, cudaGraphLaunch(f->graph, b->stream));
+        GXF_CUDA(b, cudaGraphLaunch(f->graph[s == nsteps - 1], b->stream));
         h->launches += f->graph_kernels;
     }
     GX_LAUNCH(h, k_fb_commit, b->nrep, kFbRed, f->th, b->A, f->lam, b->d_out);
