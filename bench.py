@@ -64,7 +64,7 @@ def parse():
                     help="fix the mixed pair-pass variant instead of autotuning (profiling only)")
     ap.add_argument("--skin", type=float, default=-1.0,
                     help="neighbour-list skin in length units instead of 0.1 r_c (profiling only; 0 = rebuild every tick)")
-    ap.add_argument("--leg", default="", choices=["", "ionic", "accuracy", "adjoint"],
+    ap.add_argument("--leg", default="", choices=["", "ionic", "accuracy", "adjoint", "xyz"],
                     help="run one extra leg alone and print its JSON (profiling only)")
     ap.add_argument("--leg-steps", type=int, default=0, help="ticks of the --leg run (0: the workload's own)")
     return ap.parse_args()
@@ -211,6 +211,77 @@ def ncu_traffic(kernel: str) -> float | None:
                 except Exception:
                     return None
     return None
+
+
+def hbm_peak() -> tuple[float, str]:
+    hbm = measured_peaks().get("hbm_gbs")
+    if hbm:
+        return hbm, "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    # the file is written by the driver of each run; else an earlier measurement on this pool
+    return 6650.0, "fallback 6650 GB/s (of fallback: an earlier copy-bandwidth measurement)"
+
+
+XYZ_READ_BYTES_PER_ATOM = 29  # x, y, z f64 + element u8 + the slot's sorted position u32
+
+
+def xyz_leg(h, elem, tick: int, cpu: bool, reps: int = 5) -> dict:
+    """XYZ frame export (export::write_frame) of the resident state: the
+    device formatter's kernels (profiled), end to end into a pinned host
+    buffer, the bytes against the oracle's printf text, and that text's
+    single-thread CPU time (the reference formats its frame in one loop)."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    n = C.c_size_t()
+    rc = h.lib.gx_xyz_frame(h.h, tick, None, 0, C.byref(n))
+    if rc not in (0, -4):
+        h._check(rc)
+    size = n.value
+    buf = torch.empty(size, dtype=torch.uint8, pin_memory=True)
+    ptr = C.cast(C.c_void_p(buf.data_ptr()), C.c_char_p)
+    for _ in range(2):
+        h._check(h.lib.gx_xyz_frame(h.h, tick, ptr, size, C.byref(n)))
+    h.profile(True)
+    walls = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        h._check(h.lib.gx_xyz_frame(h.h, tick, ptr, size, C.byref(n)))
+        walls.append(time.perf_counter() - t0)
+    prof = h.profile_read(reset=True)
+    h.profile(False)
+    atoms = len(elem)
+    text = bytes(buf.numpy()[:size])
+    wall = float(np.median(walls))
+    out = {"workload": f"one XYZ frame of the resident state: {atoms} atoms, {size} bytes of text",
+           "bytes": size, "e2e": {"ms": wall * 1e3, "atoms_per_s": atoms / wall, "GB_per_s": size / wall / 1e9,
+                                   "timing": "host wall clock, median of 5 gx_xyz_frame calls into pinned memory "
+                                             "(both kernels, the scan, the size read-back and the D2H copy)"}}
+    hbm, src = hbm_peak()
+    kern = {}
+    for k, (nl, kms) in prof.items():
+        if k.startswith("xyz_") and nl:
+            per = kms / nl
+            alg = XYZ_READ_BYTES_PER_ATOM * atoms + (size if k == "xyz_write" else 0)
+            kern[k] = {"launch_ms": per, "algorithmic_bytes": alg, "GB/s": alg / (per * 1e-3) / 1e9}
+    out["kernels"] = kern
+    if "xyz_write" in kern:
+        a = kern["xyz_write"]["GB/s"]
+        out["roofline"] = {"kernel": "xyz_write", "bound": "hbm", "achieved": a, "peak": hbm, "unit": "GB/s",
+                           "frac": a / hbm, "peak_source": src, "traffic": ncu_traffic("xyz_write")}
+    if cpu:
+        from oracle import oracle
+
+        pos, _, _ = h.get_state()
+        t0 = time.perf_counter()
+        want = oracle.xyz_frame(tick, pos, elem)
+        tc = time.perf_counter() - t0
+        out["matches_oracle"] = want == text
+        out["cpu_baseline"] = {"ms": tc * 1e3, "atoms_per_s": atoms / tc, "cores": 1, "kind": "port",
+                               "sample": "the same frame, C restatement (printf %.6f) on one host thread"}
+        out["e2e_over_cpu"] = tc / wall
+    return out
 
 
 def run_ticks(h, wl, cfg, steps: int, start_tick: int) -> int:
@@ -517,10 +588,7 @@ def ours_arm(args, dist):
             "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
             "flop_per_launch": pairs * flop_pp, "pairs_per_launch": pairs, "launch_ms": force_ms,
             "share_of_step": f_ms / tot_ms if tot_ms else None}
-    hbm = measured_peaks().get("hbm_gbs")
-    hbm_src = "MEASURED_PEAKS.json hbm_gbs (of measured)"
-    if not hbm:  # the file is written by the driver of each run; else an earlier measurement on this pool
-        hbm, hbm_src = 6650.0, "fallback 6650 GB/s (of fallback: an earlier copy-bandwidth measurement)"
+    hbm, hbm_src = hbm_peak()
     mem = {}
     for k, (nl, kms) in prof.items():
         if k in BYTES_PER_ATOM and nl and BYTES_PER_ATOM[k]:
@@ -602,6 +670,12 @@ def ours_arm(args, dist):
             he.close()
         except Exception as e:  # noqa: BLE001
             extras["e2e_error"] = repr(e)
+
+        # XYZ frame export of the resident state (export::write_frame)
+        try:
+            extras["xyz_frame"] = xyz_leg(h, u.elem, tick, cpu=dist.rank == 0 and dist.world == 1)
+        except Exception as e:  # noqa: BLE001
+            extras["xyz_frame_error"] = repr(e)
 
         # batched temperature sweep: replica-steps/s in one persistent launch vs
         # the same replicas one after another through gx_step
@@ -698,6 +772,19 @@ def main():
                 out = ionic_leg(dev, cpu=False, steps=args.leg_steps or None, variant=args.variant)
             elif args.leg == "accuracy":
                 out = accuracy_leg(dev, args.leg_steps or 10000)
+            elif args.leg == "xyz":
+                import dataclasses
+
+                from genesis_b200 import workloads as W
+                from genesis_b200._lib import Handle
+
+                wl = W.C3 if args.n_side <= 0 else dataclasses.replace(W.C3, n_side=args.n_side)
+                cfg, u = wl.config(), wl.generate()
+                h = Handle(cfg, "mixed", dev)
+                h.set_universe(u)
+                h.step(2)
+                out = xyz_leg(h, u.elem, 2, cpu=True)
+                h.close()
             else:
                 out = adjoint_leg(dev)
             if dist.rank == 0:

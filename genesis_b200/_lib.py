@@ -69,7 +69,7 @@ EXPORTS = (
     "gx_batch_step", "gx_batch_get_state", "gx_adjoint_forward", "gx_adjoint_backward",
     "gx_set_list_skin", "gx_list_rebuilds", "gx_batch_set_mode", "gx_batch_get_mode", "gx_batch_autotune",
     "gx_get_list_config", "gx_set_list_threads", "gx_bond_observe", "gx_bond_tracker_reset", "gx_get_bonds",
-    "gx_bond_components", "gx_collisions", "gx_collision_count",
+    "gx_bond_components", "gx_collisions", "gx_collision_count", "gx_xyz_frame",
 )
 
 _lib = None
@@ -131,6 +131,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
         "gx_bond_components": (C.c_int, [vp, u32p, dp, sz, C.POINTER(sz)]),
         "gx_collisions": (C.c_int, [vp, u64p]),
         "gx_collision_count": (C.c_int, [vp, u64p]),
+        "gx_xyz_frame": (C.c_int, [vp, C.c_uint64, C.c_char_p, sz, C.POINTER(sz)]),
         "gx_adjoint_backward": (C.c_int, [vp, dp, dp, dp, dp, dp, dp, dp]),
     }
     for name, (res, args) in proto.items():
@@ -471,6 +472,17 @@ class Handle:
             rc = self.lib.gx_get_bonds(self.h, _ptr(out, C.c_uint32), n.value, C.byref(n))
         self._check(rc)
         return out[: n.value].copy()
+
+    def xyz_frame(self, tick: int) -> bytes:
+        """The XYZ frame of the current state as export::write_frame writes
+        it (src/export/mod.rs:152-172), formatted on the device."""
+        n = C.c_size_t()
+        rc = self.lib.gx_xyz_frame(self.h, int(tick), None, 0, C.byref(n))
+        if rc != -4:
+            self._check(rc)
+        buf = C.create_string_buffer(n.value)
+        self._check(self.lib.gx_xyz_frame(self.h, int(tick), buf, n.value, C.byref(n)))
+        return buf.raw[: n.value]
 
     # -- profiling ----------------------------------------------------------
     def profile(self, on: bool = True):

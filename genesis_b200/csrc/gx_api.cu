@@ -403,6 +403,7 @@ void gx_destroy(gx_handle* h) {
     tracker_free(h);
     lens_free(h);
     collide_free(h);
+    export_free(h);
     free_buf(h->buf[0]);
     free_buf(h->buf[1]);
     cudaFree(h->key);

@@ -240,6 +240,7 @@ struct gx_handle {
     void* tracker = nullptr;
     void* lens = nullptr;     // analysis staging pool (gx_lens.cu)
     void* coll = nullptr;     // collision pass state (gx_lens.cu)
+    void* xport = nullptr;    // XYZ frame buffers (gx_export.cu)
 };
 
 // Every kernel launch of the library goes through this macro so the
@@ -311,6 +312,7 @@ int collide_prepare(gx_handle* h);
 int collide_pass(gx_handle* h);
 int collide_read(gx_handle* h, unsigned long long* pass, unsigned long long* total);
 void collide_free(gx_handle* h);
+void export_free(gx_handle* h);  // gx_export.cu
 
 void launch_kick(gx_handle* h, const StateBuf& b, uint32_t n, double half_dt, const double* lambda);
 void launch_drift(gx_handle* h, const StateBuf& b, uint32_t n, double dt);

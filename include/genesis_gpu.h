@@ -286,6 +286,20 @@ int gx_collisions(gx_handle* h, uint64_t* collisions);
 /* Collisions counted by every pass so far (CollisionCounter). */
 int gx_collision_count(gx_handle* h, uint64_t* total);
 
+/* ---- export ------------------------------------------------------------ */
+
+/* One XYZ position frame of the current state, replaces export::write_frame
+ * (src/export/mod.rs:152-172) minus the file write: "{n}\nframe {tick}\n",
+ * then "{symbol} {x:.6} {y:.6} {z:.6}\n" per atom in slot order (the order
+ * the caller gathered the world in).  Each coordinate is the exact value of
+ * the double rounded to 6 decimals, ties to even, with '-' whenever the sign
+ * bit is set, "NaN", "inf", "-inf": the bytes Rust's `{:.6}` prints.  The
+ * text is formatted on the device and copied into out (cap bytes, no
+ * terminating NUL); *len receives its size.  GX_ERR_CAPACITY when cap is
+ * short (out may be NULL: a size query), GX_ERR_UNSUPPORTED for a
+ * coordinate of magnitude >= 2^100. */
+int gx_xyz_frame(gx_handle* h, uint64_t tick, char* out, size_t cap, size_t* len);
+
 /* Per-tick column sync of a drop-in system whose ECS lives on the host:
  * overwrite Position, Velocity and Acceleration (slot order, AoS f64) of the
  * resident atoms without touching the static columns (AtomType, Mass,

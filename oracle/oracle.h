@@ -62,6 +62,10 @@ typedef struct {
  * the collisions counted. */
 size_t orc_collisions(const orc_params* p, size_t n, const double* pos, double* vel, const double* mass);
 
+/* export::write_frame's text (src/export/mod.rs:152-172) for n atoms (pos
+ * n x 3, elem 0..9); returns its size and copies it to out when cap allows. */
+size_t orc_xyz_frame(size_t n, uint64_t tick, const double* pos, const uint8_t* elem, char* out, size_t cap);
+
 /* ---- pair laws: src/physics/forces.rs ---- */
 void orc_lj_table(const orc_params* p, double* pair_sigma /*100*/,
                   double* pair_eps /*100*/, double* rc, double* r_on);

@@ -35,8 +35,8 @@ class OrcParams(C.Structure):
 
 
 def build(force: bool = False) -> Path:
-    src = [HERE / n for n in ("oracle.cpp", "oracle_dual.cpp", "oracle_bonds.cpp", "oracle.h", "oracle_grid.h",
-                               "Makefile")]
+    src = [HERE / n for n in ("oracle.cpp", "oracle_dual.cpp", "oracle_bonds.cpp", "oracle_export.cpp", "oracle.h",
+                               "oracle_grid.h", "Makefile")]
     if force or not LIB.exists() or any(p.stat().st_mtime > LIB.stat().st_mtime for p in src):
         subprocess.run(["make", "-s", "-C", str(HERE), "-B" if force else "liboracle.so"], check=True)
     return LIB
@@ -77,6 +77,7 @@ def load() -> C.CDLL:
             "orc_stats": (None, [sz, dp, dp, dp, dp]),
             "orc_ticks": (C.c_int, [pp, sz, dp, dp, dp, u8p, dp, dp, sz, u32p, C.c_int, C.c_int, dp]),
             "orc_collisions": (sz, [pp, sz, dp, dp, dp]),
+            "orc_xyz_frame": (sz, [sz, C.c_uint64, dp, C.POINTER(C.c_uint8), C.c_char_p, sz]),
             "orc_radial_distribution": (C.c_int, [sz, dp, dp, _D, sz, u64p, dp, dp, dp]),
             "orc_radial_distribution_between": (C.c_int, [sz, dp, u8p, C.c_uint8, C.c_uint8, dp, _D, sz, u64p, dp,
                                                           dp, dp]),
@@ -280,6 +281,38 @@ def collisions(cfg, pos, vel, mass):
     c = lib.orc_collisions(C.byref(params(cfg)), len(pos), _p(pos, C.c_double), _p(vel, C.c_double),
                            _p(_f64(mass), C.c_double))
     return vel, int(c)
+
+
+def xyz_frame(tick, pos, elem) -> bytes:
+    """export::write_frame's text (src/export/mod.rs:152-172) through the C
+    library's printf (oracle_export.cpp)."""
+    lib = load()
+    pos = _f64(pos)
+    elem = np.ascontiguousarray(elem, dtype=np.uint8)
+    n = len(elem)
+    ep = elem.ctypes.data_as(C.POINTER(C.c_uint8))
+    size = lib.orc_xyz_frame(n, int(tick), _p(pos, C.c_double), ep, None, 0)
+    buf = C.create_string_buffer(size)
+    lib.orc_xyz_frame(n, int(tick), _p(pos, C.c_double), ep, buf, size)
+    return buf.raw[:size]
+
+
+def xyz_frame_py(tick, pos, elem) -> bytes:
+    """The same text from Python's own fixed-point formatting (exact value,
+    ties to even), pure-Python loops for small cases: pins the C path."""
+    symbols = ("H", "He", "C", "N", "O", "Na", "Si", "P", "S", "Fe")
+
+    def f6(x):
+        x = float(x)
+        if x != x:
+            return "NaN"
+        if x in (float("inf"), float("-inf")):
+            return "inf" if x > 0 else "-inf"
+        return f"{x:.6f}"
+
+    lines = [f"{len(elem)}", f"frame {int(tick)}"]
+    lines += [f"{symbols[int(e)]} {f6(p[0])} {f6(p[1])} {f6(p[2])}" for p, e in zip(pos, elem)]
+    return ("\n".join(lines) + "\n").encode()
 
 
 def ticks(cfg, pos, vel, acc, elem, charge, mass, nticks, bonds=None, nthreads=1):
