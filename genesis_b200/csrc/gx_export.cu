@@ -20,11 +20,13 @@
 // caller's host buffer.  Integer and byte work only: HBM-bound, 25 bytes
 // read per atom per pass plus the text written once.
 //
-// Exact decimal conversion: x = m 2^e with m < 2^53; n = round(|x| 10^6) is
-// computed in 128-bit integers (m 10^6 < 2^73, shifted left by at most 47
-// or right with the remainder compared against one half).  Magnitudes up to
-// 2^100 are formatted; larger ones make the call fail with
-// GX_ERR_UNSUPPORTED.
+// Exact decimal conversion: x = m 2^e with m < 2^53.  For e >= 0, x is an
+// integer (< 2^100 here); otherwise n = round(m 10^6 2^e) comes from 128-bit
+// shifts (m 10^6 < 2^73) with the remainder compared against one half, and
+// the integer part is m >> -e plus a possible carry of the rounding: no
+// division.  Digits come from 32-bit divisions by 10 whenever the integer
+// part is below 2^32.  Magnitudes up to 2^100 are formatted; larger ones
+// make the call fail with GX_ERR_UNSUPPORTED.
 #include <cub/cub.cuh>
 
 #include <cstdio>
@@ -44,15 +46,50 @@ constexpr unsigned long long kE19 = 10000000000000000000ull;
 __constant__ char kSymbol[kNElem][2] = {{'H', 0},   {'H', 'e'}, {'C', 0},   {'N', 0},   {'O', 0},
                                         {'N', 'a'}, {'S', 'i'}, {'P', 0},   {'S', 0},   {'F', 'e'}};
 
+__constant__ unsigned long long kPow10[20] = {1ull,
+                                              10ull,
+                                              100ull,
+                                              1000ull,
+                                              10000ull,
+                                              100000ull,
+                                              1000000ull,
+                                              10000000ull,
+                                              100000000ull,
+                                              1000000000ull,
+                                              10000000000ull,
+                                              100000000000ull,
+                                              1000000000000ull,
+                                              10000000000000ull,
+                                              100000000000000ull,
+                                              1000000000000000ull,
+                                              10000000000000000ull,
+                                              100000000000000000ull,
+                                              1000000000000000000ull,
+                                              10000000000000000000ull};
+
+// Decimal digits of v (1 for 0): log10 from the bit length, corrected by
+// one comparison with a power of ten.
+__device__ __forceinline__ int ndig64(unsigned long long v) {
+    const int t = ((64 - __clzll(v | 1ull)) * 1233) >> 12;  // <= 19
+    const int d = t + 1 - (v < kPow10[t] ? 1 : 0);
+    return d > 1 ? d : 1;
+}
+
+// |x| rounded to 6 decimals, ties to even: integer part ip and the six
+// decimals frac, nd = the digits of ip.
 struct Fixed6 {
-    unsigned __int128 n;  // round(|x| 10^6), ties to even
-    int neg;              // sign bit
-    int kind;             // 0 finite, 1 NaN, 2 infinite, 3 out of range
+    unsigned __int128 ip;
+    unsigned frac;
+    int nd;
+    int neg;   // sign bit
+    int kind;  // 0 finite, 1 NaN, 2 infinite, 3 out of range
 };
 
 __device__ __forceinline__ Fixed6 to_fixed6(double x) {
     Fixed6 r;
-    r.n = 0;
+    r.ip = 0;
+    r.frac = 0;
+    r.nd = 1;
     r.kind = 0;
     const unsigned long long bits = (unsigned long long)__double_as_longlong(x);
     r.neg = (int)(bits >> 63);
@@ -67,63 +104,43 @@ __device__ __forceinline__ Fixed6 to_fixed6(double x) {
         return r;
     }
     const unsigned long long m = ex ? (fr | (1ull << 52)) : fr;
-    const int e = (ex ? ex : 1) - 1075;
-    const unsigned __int128 p = (unsigned __int128)m * 1000000u;  // < 2^73
-    if (e >= 0) {
-        r.n = p << e;  // e <= 47
+    const int e = (ex ? ex : 1) - 1075;  // |x| = m 2^e
+    if (e >= 0) {  // an integer: m 2^e < 2^100
+        r.ip = (unsigned __int128)m << e;
+        if ((r.ip >> 64) == 0) {
+            r.nd = ndig64((unsigned long long)r.ip);
+        } else {
+            const unsigned long long hi = (unsigned long long)(r.ip / kE19);
+            r.nd = ndig64(hi) + 19;
+        }
         return r;
     }
     const int s = -e;
-    if (s > 74) return r;  // p < 2^73 <= half an ulp of the result: rounds to 0
+    if (s > 74) return r;  // m 10^6 < 2^73 <= half an ulp of 2^-s: rounds to 0
+    // n = round(m 10^6 / 2^s); the integer part before rounding is m >> s
+    // and n - (m >> s) 10^6 lies in [0, 10^6], 10^6 being a carry
+    const unsigned __int128 p = (unsigned __int128)m * 1000000u;
     const unsigned __int128 q = p >> s;
     const unsigned __int128 rem = p - (q << s);
     const unsigned __int128 half = (unsigned __int128)1 << (s - 1);
-    r.n = q + ((rem > half || (rem == half && (q & 1))) ? 1 : 0);
+    const unsigned __int128 n = q + ((rem > half || (rem == half && (q & 1))) ? 1 : 0);
+    unsigned long long ip = s < 64 ? (m >> s) : 0ull;  // < 2^52
+    unsigned f = (unsigned)(n - (unsigned __int128)ip * 1000000u);
+    if (f >= 1000000u) {
+        ++ip;
+        f -= 1000000u;
+    }
+    r.ip = ip;
+    r.frac = f;
+    r.nd = ndig64(ip);
     return r;
-}
-
-__device__ __forceinline__ int digits64(unsigned long long v) {
-    int d = 1;
-    while (v >= 10) {
-        v /= 10;
-        ++d;
-    }
-    return d;
-}
-
-// Integer part split for printing: hi 10^19 + lo, hi = 0 when it fits in lo.
-// n < 2^64 (|x| below about 1.8e13, every coordinate of a simulation box)
-// takes 64-bit divisions by constants; only larger values pay for the
-// 128-bit ones.
-__device__ __forceinline__ void split_int(const Fixed6& f, unsigned long long& hi, unsigned long long& lo,
-                                          unsigned& frac) {
-    if ((f.n >> 64) == 0) {
-        const unsigned long long n = (unsigned long long)f.n;
-        const unsigned long long ip = n / 1000000ull;
-        frac = (unsigned)(n - ip * 1000000ull);
-        hi = 0;
-        lo = ip;  // < 2^64 / 10^6 < 10^19
-        return;
-    }
-    const unsigned __int128 ip = f.n / 1000000u;
-    frac = (unsigned)(f.n - ip * 1000000u);
-    if ((ip >> 64) == 0 && (unsigned long long)ip < kE19) {
-        hi = 0;
-        lo = (unsigned long long)ip;
-    } else {
-        hi = (unsigned long long)(ip / kE19);
-        lo = (unsigned long long)(ip - (unsigned __int128)hi * kE19);
-    }
 }
 
 __device__ __forceinline__ int fixed6_len(const Fixed6& f) {
     if (f.kind == 1) return 3;
     if (f.kind == 2) return 3 + f.neg;
     if (f.kind == 3) return 0;
-    unsigned long long hi, lo;
-    unsigned frac;
-    split_int(f, hi, lo, frac);
-    return f.neg + (hi ? digits64(hi) + 19 : digits64(lo)) + 7;
+    return f.neg + f.nd + 7;
 }
 
 // Writes the text of f at out (fixed6_len(f) bytes).
@@ -141,25 +158,41 @@ __device__ __forceinline__ char* fixed6_put(const Fixed6& f, char* out) {
         out[2] = 'f';
         return out + 3;
     }
-    unsigned long long hi, lo;
-    unsigned frac;
-    split_int(f, hi, lo, frac);
-    const int nlo = hi ? 19 : digits64(lo);
-    const int nhi = hi ? digits64(hi) : 0;
-    char* p = out + nhi + nlo;
-    for (int k = 0; k < nlo; ++k) {
-        *--p = (char)('0' + lo % 10);
-        lo /= 10;
+    char* p = out + f.nd;
+    if ((f.ip >> 32) == 0) {  // every coordinate of a simulation box
+        unsigned v = (unsigned)f.ip;
+        do {
+            const unsigned q = v / 10u;
+            *--p = (char)('0' + (v - q * 10u));
+            v = q;
+        } while (v);
+    } else {
+        unsigned long long lo, hi = 0;
+        if ((f.ip >> 64) == 0) {
+            lo = (unsigned long long)f.ip;
+        } else {
+            hi = (unsigned long long)(f.ip / kE19);
+            lo = (unsigned long long)(f.ip - (unsigned __int128)hi * kE19);
+        }
+        const int nlo = hi ? 19 : f.nd;
+        for (int k = 0; k < nlo; ++k) {
+            const unsigned long long q = lo / 10u;
+            *--p = (char)('0' + (unsigned)(lo - q * 10u));
+            lo = q;
+        }
+        while (hi) {
+            const unsigned long long q = hi / 10u;
+            *--p = (char)('0' + (unsigned)(hi - q * 10u));
+            hi = q;
+        }
     }
-    for (int k = 0; k < nhi; ++k) {
-        *--p = (char)('0' + hi % 10);
-        hi /= 10;
-    }
-    out += nhi + nlo;
+    out += f.nd;
     *out++ = '.';
+    unsigned fr = f.frac;
     for (int k = 5; k >= 0; --k) {
-        out[k] = (char)('0' + frac % 10);
-        frac /= 10;
+        const unsigned q = fr / 10u;
+        out[k] = (char)('0' + (fr - q * 10u));
+        fr = q;
     }
     return out + 6;
 }

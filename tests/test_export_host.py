@@ -92,6 +92,11 @@ def _rand_values(n=40000, seed=3):
     return list(np.where(rng.random(n) < 0.5, -mags, mags)) + list(rng.uniform(-200, 200, n))
 
 
+def _ndig64(v: int) -> int:
+    t = (max(v, 1).bit_length() * 1233) >> 12
+    return max(t + 1 - (1 if v < 10 ** t else 0), 1)
+
+
 def _fixed6_int(x: float) -> str:
     """The device formatter's algorithm (gx_export.cu to_fixed6 and
     fixed6_put) in Python integers."""
@@ -100,21 +105,36 @@ def _fixed6_int(x: float) -> str:
     assert ex != 0x7FF and ex < 1023 + 100
     m = (fr | (1 << 52)) if ex else fr
     e = (ex if ex else 1) - 1075
-    p = m * 10 ** 6
-    assert p < 2 ** 73
     if e >= 0:
-        n = p << e
-        assert n < 2 ** 128
+        ip, frac = m << e, 0
+        assert ip < 2 ** 100
+    elif -e > 74:
+        ip, frac = 0, 0
     else:
         s = -e
-        if s > 74:
-            n = 0
-        else:
-            q, rem, half = p >> s, p & ((1 << s) - 1), 1 << (s - 1)
-            n = q + (1 if rem > half or (rem == half and q & 1) else 0)
-    ip, frac = divmod(n, 10 ** 6)
-    assert len(str(ip)) <= 31
+        p = m * 10 ** 6
+        assert p < 2 ** 73
+        q, rem, half = p >> s, p & ((1 << s) - 1), 1 << (s - 1)
+        n = q + (1 if rem > half or (rem == half and q & 1) else 0)
+        ip = m >> s
+        frac = n - ip * 10 ** 6
+        assert 0 <= frac <= 10 ** 6
+        if frac == 10 ** 6:
+            ip, frac = ip + 1, 0
+    nd = _ndig64(ip) if ip < 2 ** 64 else _ndig64(ip // 10 ** 19) + 19
+    assert nd == len(str(ip)) <= 31
     return ("-" if neg else "") + f"{ip}.{frac:06d}"
+
+
+def test_digit_count_formula():
+    for d in range(1, 21):
+        for v in (10 ** (d - 1), 10 ** (d - 1) + 1, 2 * 10 ** (d - 1), 10 ** d - 1):
+            if v < 2 ** 64:
+                assert _ndig64(v) == d, v
+    for b in range(64):
+        for v in (2 ** b - 1, 2 ** b, 2 ** b + 1):
+            if v < 2 ** 64:
+                assert _ndig64(v) == len(str(v)), v
 
 
 def test_device_algorithm_matches_correct_rounding():
