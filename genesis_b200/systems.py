@@ -17,6 +17,7 @@ src/systems/bonds.rs:73-185).
 from __future__ import annotations
 
 import math
+import time
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -80,12 +81,32 @@ class World:
         return len(self.elem)
 
 
+class StatsCollector:
+    """StatsCollector (src/stats/mod.rs:151-212): the latest snapshot, a
+    bounded history, and the scheduler's execution count and the main loop's
+    FPS that StatsSystem copies into each snapshot."""
+
+    def __init__(self, history_cap: int = 1024):
+        self.snapshot: dict = {}
+        self.systems_run = 0
+        self.fps = 0.0
+        self.history: list[dict] = []
+        self.history_cap = max(int(history_cap), 1)
+
+    def record(self, snap: dict) -> None:
+        if len(self.history) == self.history_cap:
+            self.history.pop(0)
+        self.snapshot = snap
+        self.history.append(snap)
+
+
 @dataclass
 class SystemContext:
     world: World
     resources: dict
     time: Time
     dt: float
+    stats: StatsCollector = field(default_factory=StatsCollector)
 
 
 class System:
@@ -104,6 +125,7 @@ class Scheduler:
 
     def __init__(self):
         self.systems: list[System] = []
+        self.executions = 0
 
     def add_system(self, s: System):
         self.systems.append(s)
@@ -111,6 +133,8 @@ class Scheduler:
     def run(self, ctx: SystemContext):
         for s in self.systems:
             s.run(ctx)
+            self.executions += 1
+        ctx.stats.systems_run = self.executions  # mod.rs:88: after the whole schedule
 
     def names(self) -> list[str]:
         return [s.name() for s in self.systems]
@@ -413,7 +437,11 @@ class GpuBondStructure(_GpuSystem):
 
 
 class GpuStats(_GpuSystem):
-    """StatsSystem (src/systems/aggregate.rs:36-144): K, T, E = K + V + E_bond."""
+    """StatsSystem (src/systems/aggregate.rs:36-144): K and the speed sum
+    from the device, the resources the other systems wrote, one
+    StatsSnapshot (src/stats/mod.rs:27-91) recorded per tick.  memory_bytes
+    counts the host column mirror's arrays (the reference counts its ECS
+    storage, World::memory_bytes)."""
 
     def __init__(self, gpu: GpuWorld, cfg):
         super().__init__(gpu)
@@ -423,19 +451,39 @@ class GpuStats(_GpuSystem):
         return "stats"
 
     def access(self):
-        return Access(reads=["Velocity", "Mass"], resources_read=["Config", "PotentialEnergy", "BondEnergy"])
+        return Access(reads=["Velocity", "Mass"],
+                      resources_read=["Config", "CollisionCounter", "PotentialEnergy", "StructureStats",
+                                      "BondObservation", "BondEnergy", "ChemicalStructure"])
 
     def run(self, ctx):
         self._enter()
         K, speed = self.gpu.h.stats()
         n = len(ctx.world)
-        V = ctx.resources.get("PotentialEnergy", 0.0)
-        Vb = ctx.resources.get("BondEnergy", 0.0)
+        r = ctx.resources
+        V = r.get("PotentialEnergy", 0.0)
+        Vb = r.get("BondEnergy", 0.0)
+        st = r.get("StructureStats")
+        st = st if st and st.get("tick", 0) > 0 else None
+        bo = r.get("BondObservation") or {}
+        formed = int(bo.get("bonds_formed", 0))
+        ch = r.get("ChemicalStructure")
+        ch = ch if ch and ch.get("tick", 0) > 0 else None
         e_avg = K / n if n else 0.0
-        T = (2.0 / 3.0) * e_avg / self.cfg.thermal_constant if self.cfg.thermal_constant > 0 else 0.0
-        ctx.resources["StatsSnapshot"] = {"tick": ctx.time.tick, "energy_total": K + V + Vb, "kinetic": K,
-                                          "energy_potential": V, "bond_energy": Vb, "temperature_avg": T,
-                                          "mean_speed": speed / n if n else 0.0}
+        k = self.cfg.thermal_constant
+        vol = float(np.prod(self.cfg.size))
+        w = ctx.world
+        mem = sum(a.nbytes for a in (w.pos, w.vel, w.acc, w.elem, w.mass, w.charge, w.entity))
+        snap = {"tick": ctx.time.tick, "time": ctx.time.t, "entities": n, "energy_total": K + V + Vb,
+                "energy_avg": e_avg, "energy_potential": V, "temperature_avg": (2.0 / 3.0) * e_avg / k if k > 0 else 0.0,
+                "mean_speed": speed / n if n else 0.0, "density": n / vol if vol > 0 else 0.0,
+                "collisions": int(r.get("CollisionCounter", 0)), "systems_run": ctx.stats.systems_run,
+                "fps": ctx.stats.fps, "memory_bytes": mem,
+                "structure": st, "bonded_pairs": int(bo.get("bonded_pairs", 0)), "bonds_formed": formed,
+                "bond_lifetime_ticks": bo.get("lifetime_sum_ticks", 0.0) / formed if formed > 0 else 0.0,
+                "bond_energy": Vb, "bond_matrix": [float(c) for c in np.ravel(bo.get("species_matrix", []))],
+                "chemical": ch, "kinetic": K}
+        ctx.resources["StatsSnapshot"] = snap
+        ctx.stats.record(snap)
 
 
 def build_schedule(cfg, gpu: GpuWorld) -> Scheduler:
@@ -469,11 +517,27 @@ class GpuUniverse:
         self.time = Time(cfg.dt)
         self.resources: dict = {"Config": cfg}
         self.scheduler = build_schedule(cfg, self.gpu)
+        self.stats = StatsCollector()
 
     def tick(self):
         self.time.advance()
-        ctx = SystemContext(self.world, self.resources, self.time, self.time.dt)
+        t0 = time.perf_counter()
+        ctx = SystemContext(self.world, self.resources, self.time, self.time.dt, self.stats)
         self.scheduler.run(ctx)
+        elapsed = time.perf_counter() - t0
+        self.stats.fps = 1.0 / elapsed if elapsed > 0 else 0.0  # universe/mod.rs:156-157
+
+    def append_csv(self, path) -> None:
+        """One metrics row of the latest snapshot (export::append_csv)."""
+        from . import export
+        export.append_csv(path, self.stats.snapshot)
+
+    def write_frame(self, prefix) -> str:
+        """The current positions as an XYZ frame (export::write_frame),
+        formatted on the device."""
+        from . import export
+        self.gpu.to_device()
+        return export.write_frame(prefix, self.time.tick, self.gpu.h)
 
     def run_ticks(self, n: int):
         for _ in range(n):

@@ -75,3 +75,39 @@ def test_ionic_schedule_with_bond_observation_matches_oracle(gpu, orc):
     assert most > 0  # the spring acted on observed bonds during the run
     n_host = sum(len(v) for v in w.bonds.values())
     assert n_host == 2 * obs["bonded_pairs"]
+
+
+def test_stats_snapshot_csv_rows_and_frames(gpu, orc, tmp_path):
+    """StatsSystem's full snapshot from the GPU schedule, written as the
+    metrics CSV (export::append_csv) every tick and as an XYZ frame."""
+    from genesis_b200 import export as X
+    from genesis_b200.systems import GpuUniverse
+    wl = W.Workload("ionic csv", n_side=8, temperature=300.0, steps=10, seed=5, electrostatics=True,
+                    thermostat=True, thermostat_temperature=300.0, bond_observation=True, bond_interaction=True,
+                    species=(E.by_name("Na"), E.by_name("O")),
+                    fixed_fractions={E.by_name("Na"): 0.5, E.by_name("O"): 0.5})
+    cfg, u = wl.config(), wl.generate()
+    cfg.bond_min_periods = 0.1
+    cfg.structure_interval = 10
+    gu = GpuUniverse(cfg, u, "fp64")
+    nsys = len(gu.scheduler.systems)
+    path = tmp_path / "metrics.csv"
+    for t in range(1, 41):
+        gu.tick()
+        gu.append_csv(path)
+        s = gu.stats.snapshot
+        assert s["tick"] == t and s["entities"] == len(u.elem) and s["systems_run"] == (t - 1) * nsys
+        assert abs(s["time"] - t * cfg.dt) <= 1e-12 * t
+        assert s["energy_total"] == s["kinetic"] + s["energy_potential"] + s["bond_energy"]
+        assert (s["structure"] is not None) == (t >= 10) and (s["chemical"] is not None) == (t >= 10)
+    lines = path.read_text().splitlines()
+    assert lines[0] == X.CSV_HEADER and len(lines) == 41
+    assert all(len(r.split(",")) == 30 for r in lines[1:])
+    assert lines[-1] == X.csv_row(gu.stats.snapshot)
+    last = lines[-1].split(",")
+    assert last[0] == "40" and last[2] == str(len(u.elem)) and int(last[18]) == gu.stats.snapshot["bonded_pairs"]
+    assert len(gu.stats.history) == 40
+    frame = gu.write_frame(tmp_path / "frame")
+    assert frame.endswith("frame_00000040.xyz")
+    w = gu.sync()
+    assert open(frame, "rb").read() == orc.xyz_frame(40, w.pos, w.elem)
