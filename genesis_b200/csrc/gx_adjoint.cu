@@ -607,6 +607,7 @@ int gx_adjoint_forward(gx_handle* h, const gx_adjoint_spec* spec, double* potent
     int rc = GX_OK;
     if (!h->cap) return set_err(h, GX_ERR_STATE, "no state uploaded (call gx_set_state first)");
     if (h->n == 0) return set_err(h, GX_ERR_ARG, "the adjoint needs at least one atom");
+    h->nl_fresh = false;  // conservative: the passes below may reorder or move the resident state
     if (spec->nsteps < 1 || spec->checkpoint_every < 1) return set_err(h, GX_ERR_ARG, "nsteps and checkpoint_every must be >= 1");
     if (spec->gr_bins < 0 || spec->gr_bins > kAdjMaxBins) return set_err(h, GX_ERR_ARG, "gr_bins must be in [0, 512]");
     if (spec->gr_bins > 0) {

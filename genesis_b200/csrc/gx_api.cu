@@ -450,6 +450,7 @@ int gx_set_state(gx_handle* h, size_t n, const double* pos, const double* vel, c
     h->cur = 0;
     h->sorted = false;
     h->nl_valid = false;
+    h->nl_fresh = false;
     tracker_free(h);  // new atoms: the open episodes no longer apply
     h->lambda_pending = false;
     invalidate_graphs(h);
@@ -579,6 +580,7 @@ int gx_drift(gx_handle* h) {
     commit_lambda(h);
     launch_drift(h, h->buf[h->cur], (uint32_t)h->n, h->p.dt);
     h->sorted = false;
+    h->nl_fresh = false;
     GX_CUDA(h, cudaStreamSynchronize(h->stream));
     GX_CUDA(h, cudaGetLastError());
     return GX_OK;
@@ -589,6 +591,7 @@ int gx_wrap(gx_handle* h) {
     if (rc) return rc;
     launch_wrap(h, h->buf[h->cur], (uint32_t)h->n);
     h->sorted = false;
+    h->nl_fresh = false;
     GX_CUDA(h, cudaStreamSynchronize(h->stream));
     GX_CUDA(h, cudaGetLastError());
     return GX_OK;
@@ -661,6 +664,8 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
     if (nsteps < 0) return GX_ERR_ARG;
     if ((rc = check_kinds(h))) return rc;
     (void)use_graph;
+    const bool fresh0 = h->nl_fresh;
+    h->nl_fresh = false;  // set again below once the ticks ran on the list path
     uint32_t n = (uint32_t)h->n;
     bool thermo = h->p.enable_thermostat && h->p.thermostat_temperature > 0.0;
     double tau = std::fmax(h->p.thermostat_tau, 1.0);
@@ -796,6 +801,7 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
         GX_CUDA(h, cudaGraphLaunch(ex, h->stream));  // the captured tick has not run yet: run it now
     }
     if (use_nl) h->sorted = false;  // buf[cur] is ordered by the list grid, not the force grid
+    h->nl_fresh = nsteps > 0 ? (use_nl && h->nl_valid) : fresh0;
     if (drec) {
         GX_CUDA(h, cudaMemcpyAsync(stats, drec, (size_t)nsteps * sizeof(gx_tick_stats), cudaMemcpyDeviceToHost,
                                    h->stream));
@@ -905,6 +911,7 @@ int gx_autotune(gx_handle* h, int reps, int* best, double* ms) {
                 cudaStreamSynchronize(h->stream);
                 h->lambda_pending = pend0;
                 h->sorted = false;
+                h->nl_fresh = false;  // positions restored behind the list's back
             }
             cudaFree(snap);
             if (ms) {
@@ -981,7 +988,10 @@ int gx_set_dynamic(gx_handle* h, const double* pos, const double* vel, const dou
         GX_CUDA(h, cudaMemcpyAsync(stage, ins[k], 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
         GX_LAUNCH(h, k_aos_to_sorted, nblk(n, 256), 256, stage, h->pos_of_slot, dsts[k][0], dsts[k][1], dsts[k][2], n);
     }
-    if (pos) h->sorted = false;
+    if (pos) {
+        h->sorted = false;
+        h->nl_fresh = false;
+    }
     GX_CUDA(h, cudaStreamSynchronize(h->stream));
     GX_CUDA(h, cudaGetLastError());
     return GX_OK;

@@ -37,6 +37,7 @@ namespace gx {
 int bound_buckets_device(gx_handle* h, void** pool, double k_bind, uint32_t* bucket, uint32_t* bcnt, uint32_t depth,
                          size_t stride);
 void aux_pool_free(void* pool);
+void bound_list_key(const gx_handle* h, double k_bind, const void** list, const void** start);
 void bonds_changed(gx_handle* h, size_t nbonds, bool realloc);
 
 namespace {
@@ -307,7 +308,7 @@ __global__ void __launch_bounds__(kThreads)
 struct ObsKey {
     uint64_t n, depth, slab, apply, debounce, bonds_cap;
     double k_bind;
-    const void *bonds, *pos_of_slot, *elem, *x, *bucket, *open, *next;
+    const void *bonds, *pos_of_slot, *elem, *x, *bucket, *open, *next, *list, *list_start;
 };
 
 struct BondTracker {
@@ -486,6 +487,7 @@ int observe_once(gx_handle* h, BondTracker* t, double k_bind, uint32_t debounce,
         k.bucket = t->bucket;
         k.open = t->open.b;
         k.next = t->next.b;
+        bound_list_key(h, k_bind, &k.list, &k.list_start);
         const int par = h->cur & 1;
         if (!t->gexec[par] || std::memcmp(&k, &t->gkey[par], sizeof k) != 0) {
             if (t->gexec[par]) cudaGraphExecDestroy(t->gexec[par]);

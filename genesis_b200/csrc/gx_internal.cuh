@@ -235,6 +235,9 @@ struct gx_handle {
     // nl_valid: the list matches buf[cur]'s order and home cells
     void* nl = nullptr;
     bool nl_valid = false;
+    // nl_fresh: no position changed since a list-path tick, so the list holds
+    // every pair within r_c of the current positions
+    bool nl_fresh = false;
 
     // bond observation (gx_bondtrack.cu): open episodes on the device, owned there
     void* tracker = nullptr;
@@ -313,6 +316,24 @@ int collide_pass(gx_handle* h);
 int collide_read(gx_handle* h, unsigned long long* pass, unsigned long long* total);
 void collide_free(gx_handle* h);
 void export_free(gx_handle* h);  // gx_export.cu
+
+// Read-only view of the persistent neighbour list (gx_nlist.cu) for the
+// passes that can take their candidates from it.  Entry e of atom p (sorted
+// position) is list[e * stride + p] & idx_mask; atoms whose count exceeds
+// cap_nb overflowed and scan the 27 list-grid cells around home[p] instead.
+struct NlView {
+    const uint32_t* list;
+    size_t stride;
+    int cap_nb;
+    const uint32_t* cnt;
+    GridGeom lg;
+    const uint32_t* start;
+    const uint32_t* home;
+    uint32_t idx_mask;
+};
+// True (and the view) when h->nl_fresh: the list covers every pair within
+// r_c of buf[cur], each unordered pair at least once with q > p.
+bool nl_view(const gx_handle* h, NlView* v);
 
 void launch_kick(gx_handle* h, const StateBuf& b, uint32_t n, double half_dt, const double* lambda);
 void launch_drift(gx_handle* h, const StateBuf& b, uint32_t n, double dt);

@@ -463,6 +463,37 @@ struct BucketArgs {
     size_t stride;
 };
 
+// One candidate of bound_pairs_with_grid (pairs.rs:150-170): the exact
+// test, then (lower slot, higher slot) appended to the lower slot's bucket.
+__device__ __forceinline__ void bound_candidate(double xi, double yi, double zi, double si, uint32_t slot_i, double xj,
+                                                double yj, double zj, double sj, uint32_t slot_j, double box0,
+                                                double box1, double box2, double cd2, const BucketArgs& v) {
+    double dx = near_image1(xsub(xi, xj), box0);
+    double dy = near_image1(xsub(yi, yj), box1);
+    double dz = near_image1(xsub(zi, zj), box2);
+    double d2 = xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
+    if (d2 >= cd2) return;
+    double threshold = xmul(v.k_bind, xmul(0.5, xadd(si, sj)));  // pairs.rs:163
+    // d = sqrt(d2) (correctly rounded) against the threshold, decided
+    // on d2 away from the boundary: beyond 1e-12 relative either way
+    // the rounded root cannot fall on the other side
+    const double t2 = xmul(threshold, threshold);
+    if (d2 >= xmul(t2, 1.0 + 1e-12)) return;
+    if (d2 > xmul(t2, 1.0 - 1e-12) || d2 <= 1e-30) {
+        double d = xsqrt(d2);
+        if (d <= kEpsF64) return;  // check_pair, grid.rs:201-225
+        if (!(d < threshold)) return;
+    }
+    uint32_t sa = slot_i, sb = slot_j;
+    if (sb < sa) {
+        uint32_t q = sa;
+        sa = sb;
+        sb = q;
+    }
+    uint32_t r = atomicAdd(&v.bcnt[sa], 1u);
+    if (r < v.depth) v.bucket[(size_t)r * v.stride + sa] = sb;
+}
+
 __global__ void __launch_bounds__(256) k_bound_buckets(GridGeom g, AuxSet a, double box0, double box1, double box2,
                                                        double cd2, BucketArgs v) {
     // the offsets and sigmas, indexed per lane and per atom, from shared
@@ -500,31 +531,50 @@ __global__ void __launch_bounds__(256) k_bound_buckets(GridGeom g, AuxSet a, dou
         const double xi = a.x[i], yi = a.y[i], zi = a.z[i];
         const double si = sig[a.elem[i]];
         const uint32_t slot_i = a.slot[i];
-        for (uint32_t j = lo; j < hi; ++j) {
-            double dx = near_image1(xsub(xi, a.x[j]), box0);
-            double dy = near_image1(xsub(yi, a.y[j]), box1);
-            double dz = near_image1(xsub(zi, a.z[j]), box2);
-            double d2 = xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
-            if (d2 >= cd2) continue;
-            double threshold = xmul(v.k_bind, xmul(0.5, xadd(si, sig[a.elem[j]])));  // pairs.rs:163
-            // d = sqrt(d2) (correctly rounded) against the threshold, decided
-            // on d2 away from the boundary: beyond 1e-12 relative either way
-            // the rounded root cannot fall on the other side
-            const double t2 = xmul(threshold, threshold);
-            if (d2 >= xmul(t2, 1.0 + 1e-12)) continue;
-            if (d2 > xmul(t2, 1.0 - 1e-12) || d2 <= 1e-30) {
-                double d = xsqrt(d2);
-                if (d <= kEpsF64) continue;  // check_pair, grid.rs:201-225
-                if (!(d < threshold)) continue;
-            }
-            uint32_t sa = slot_i, sb = a.slot[j];
-            if (sb < sa) {
-                uint32_t q = sa;
-                sa = sb;
-                sb = q;
-            }
-            uint32_t r = atomicAdd(&v.bcnt[sa], 1u);
-            if (r < v.depth) v.bucket[(size_t)r * v.stride + sa] = sb;
+        for (uint32_t j = lo; j < hi; ++j)
+            bound_candidate(xi, yi, zi, si, slot_i, a.x[j], a.y[j], a.z[j], sig[a.elem[j]], a.slot[j], box0, box1,
+                            box2, cd2, v);
+    }
+}
+
+// The same decisions with the candidates taken from the persistent neighbour
+// list, which holds every pair within r_c (> the bond cutoff) of the current
+// positions: each unordered pair once, from its lower sorted position.  No
+// bond grid is binned.  kBucketLanes lanes per atom take its entries in turn
+// (short chains of dependent gathers side by side).
+__global__ void __launch_bounds__(256) k_bound_from_list(StateBuf b, uint32_t n, NlView nv, double box0, double box1,
+                                                         double box2, double cd2, BucketArgs v) {
+    __shared__ double sig[kNElem];
+    if (threadIdx.x < kNElem) sig[threadIdx.x] = v.sig[threadIdx.x];
+    __syncthreads();
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t p = (uint32_t)(t / kBucketLanes);
+    const uint32_t lane = (uint32_t)(t % kBucketLanes);
+    if (p >= n) return;
+    const double xi = b.x[p], yi = b.y[p], zi = b.z[p];
+    const double si = sig[b.elem[p]];
+    const uint32_t slot_i = b.slot[p];
+    const uint32_t m = nv.cnt[p];
+    if (m <= (uint32_t)nv.cap_nb) {
+        for (uint32_t e = lane; e < m; e += kBucketLanes) {
+            const uint32_t q = __ldg(nv.list + (size_t)e * nv.stride + p) & nv.idx_mask;
+            if (q > p)
+                bound_candidate(xi, yi, zi, si, slot_i, b.x[q], b.y[q], b.z[q], sig[b.elem[q]], b.slot[q], box0, box1,
+                                box2, cd2, v);
+        }
+    } else {  // overflowed list: the list-grid cells from the home cell on (sorted by cell: q > p)
+        const uint32_t c = nv.home[p];
+        uint32_t cx, cy, cz;
+        decode(nv.lg, c, cx, cy, cz);
+        for (uint32_t code = lane; code < 27; code += kBucketLanes) {
+            const int ox = (int)(code % 3u) - 1, oy = (int)((code / 3u) % 3u) - 1, oz = (int)(code / 9u) - 1;
+            const uint32_t B = encode(nv.lg, wrap_add(cx, ox, nv.lg.n[0]), wrap_add(cy, oy, nv.lg.n[1]),
+                                      wrap_add(cz, oz, nv.lg.n[2]));
+            if (B < c) continue;
+            for (uint32_t q = nv.start[B], hi = nv.start[B + 1]; q < hi; ++q)
+                if (q > p)
+                    bound_candidate(xi, yi, zi, si, slot_i, b.x[q], b.y[q], b.z[q], sig[b.elem[q]], b.slot[q], box0,
+                                    box1, box2, cd2, v);
         }
     }
 }
@@ -932,6 +982,32 @@ int collide_pass(gx_handle* h) {
 
 void aux_pool_free(void* pool) { pool_release(static_cast<AuxPool*>(pool)); }
 
+// The neighbour list can stand in for the bond grid when it holds every pair
+// within the bond cutoff (positions unchanged since a list tick, cutoff
+// below r_c) and the bond grid has at least 3 cells per axis, where the
+// reference's grid reports each pair exactly once.
+bool bound_from_list(const gx_handle* h, double cutoff, const GridGeom& bond_grid, NlView* nv) {
+    if (!(cutoff < 0.99 * h->fs.rc)) return false;
+    for (int k = 0; k < 3; ++k)
+        if (bond_grid.n[k] < 3) return false;
+    return nl_view(h, nv);
+}
+
+// What a captured observation depends on when it takes the list path: the
+// list and its cell starts (null on the bond-grid path).
+void bound_list_key(const gx_handle* h, double k_bind, const void** list, const void** start) {
+    *list = *start = nullptr;
+    double ms = 0.0;
+    for (int k = 0; k < kNElem; ++k) ms = std::fmax(ms, h->p.sigma[k]);
+    int ok = 0;
+    GridGeom g = make_grid(h->p.box, k_bind * ms, &ok);
+    NlView nv;
+    if (ok && bound_from_list(h, k_bind * ms, g, &nv)) {
+        *list = nv.list;
+        *start = nv.start;
+    }
+}
+
 // bound_pairs_with_grid (src/analysis/pairs.rs:132-174) with the pairs left on
 // the device in their owners' buckets (k_bound_buckets).  The staging lives
 // in the caller's pool (*pool, made on first use), so that its addresses
@@ -950,6 +1026,22 @@ int bound_buckets_device(gx_handle* h, void** pool, double k_bind, uint32_t* buc
     int ok = 0;
     GridGeom g = make_grid(h->p.box, cutoff, &ok);
     if (!ok) return set_err(h, GX_ERR_ARG, "invalid bond grid");
+    BucketArgs v;
+    v.k_bind = k_bind;
+    for (int k = 0; k < kNElem; ++k) v.sig[k] = h->p.sigma[k];
+    v.bucket = bucket;
+    v.bcnt = bcnt;
+    v.depth = depth;
+    v.stride = stride;
+    NlView nv;
+    if (bound_from_list(h, cutoff, g, &nv)) {
+        prof_begin(h, "bound_pairs");
+        if (n)
+            GX_LAUNCH(h, k_bound_from_list, nblk((size_t)n * kBucketLanes, 256), 256, h->buf[h->cur], n, nv,
+                      h->p.box[0], h->p.box[1], h->p.box[2], cutoff * cutoff, v);
+        prof_end(h, "bound_pairs");
+        return GX_OK;
+    }
     if ((rc = ensure_cells(h, P.cl, g.ncell))) return rc;
     AuxSet a;
     a.x = P.xyz + 3 * P.cap;
@@ -969,13 +1061,6 @@ int bound_buckets_device(gx_handle* h, void** pool, double k_bind, uint32_t* buc
     cell_scan(h, P.cl, g.ncell);
     if (n) GX_LAUNCH(h, k_place, nblk(n, 256), 256, b, n, key, P.cl.start, P.cl.fill, a);
     prof_end(h, "bond_grid");
-    BucketArgs v;
-    v.k_bind = k_bind;
-    for (int k = 0; k < kNElem; ++k) v.sig[k] = h->p.sigma[k];
-    v.bucket = bucket;
-    v.bcnt = bcnt;
-    v.depth = depth;
-    v.stride = stride;
     prof_begin(h, "bound_pairs");
     if (n)
         GX_LAUNCH(h, k_bound_buckets, nblk((size_t)n * kBucketLanes, 256), 256, g, a, h->p.box[0], h->p.box[1],

@@ -830,4 +830,18 @@ int nl_set_skin(gx_handle* h, double skin) {
     return GX_OK;
 }
 
+bool nl_view(const gx_handle* h, NlView* v) {
+    const NlState* s = static_cast<const NlState*>(h->nl);
+    if (!s || !h->nl_valid || !h->nl_fresh || !s->list || !s->cnt || s->cap < h->n) return false;
+    v->list = s->list;
+    v->stride = s->cap;
+    v->cap_nb = s->cap_nb;
+    v->cnt = s->cnt;
+    v->lg = s->lg;
+    v->start = s->cl.start;
+    v->home = h->key_sorted;
+    v->idx_mask = kIdxMask;
+    return true;
+}
+
 }  // namespace gx

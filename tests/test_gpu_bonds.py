@@ -197,3 +197,42 @@ def test_observed_bonds_drive_the_list_path(gpu):
         assert np.array_equal(x, y)
     assert out[0][1] == out[1][1]
     assert np.array_equal(out[0][2], out[1][2])
+
+
+def test_list_candidates_match_the_bond_grid(gpu):
+    """On the mixed neighbour-list path the observation takes its candidates
+    from the list; rewriting the same positions from the host (which leaves
+    the list unproven for them) sends it through the bond grid instead.  Two
+    handles on one NVE trajectory, one each way: the same summaries and
+    bonds every tick."""
+    from genesis_b200._lib import Handle
+    cfg, u = _ionic()
+    cfg.enable_thermostat = False  # a host rewrite voids a pending Berendsen scale
+    ha, hb = Handle(cfg, "mixed"), Handle(cfg, "mixed")
+    ha.set_universe(u)
+    hb.set_universe(u)
+    seen = 0
+    for tick in range(1, 81):
+        ha.step(1)
+        hb.step(1)
+        hb.set_dynamic(hb.get_state()[0])
+        prof = tick == 30
+        if prof:
+            ha.profile(True)
+            hb.profile(True)
+        oa = ha.bond_observe(cfg.bond_k_bind, 0.2, tick)
+        ob = hb.bond_observe(cfg.bond_k_bind, 0.2, tick)
+        if prof:
+            pa, pb = ha.profile_read(), hb.profile_read()
+            ha.profile(False)
+            hb.profile(False)
+            assert "bound_pairs" in pa and "bond_grid" not in pa  # the list path
+            assert "bond_grid" in pb
+        for k in ("bound_pairs",) + KEYS:
+            assert oa[k] == ob[k], (tick, k, oa[k], ob[k])
+        assert np.array_equal(oa["species_matrix"], ob["species_matrix"])
+        assert np.array_equal(ha.get_bonds(), hb.get_bonds()) or np.array_equal(
+            np.sort(ha.get_bonds().view(np.uint64).ravel()), np.sort(hb.get_bonds().view(np.uint64).ravel()))
+        assert np.array_equal(ha.get_state()[0], hb.get_state()[0])
+        seen = max(seen, oa["bound_pairs"])
+    assert seen > 0
