@@ -23,10 +23,11 @@
 // One tick (all launches captured in one CUDA graph; the rebuild launches
 // read a device flag and do nothing when it is clear):
 //   k_nl_advance   kick (with the pending Berendsen scale), drift, wrap,
-//                  home-frame FP32 staging, displacement check -> flag
+//                  home-frame FP32 staging, displacement check -> flag;
+//                  zeroes the force sums of the half-list pass
 //   [rebuild]      cell keys, counting sort, gather, copy back, staging,
 //                  list build
-//   k_nl_end       rebuild count, frame parity
+//   k_nl_end       rebuild count, frame parity, zeroed energy counters
 //   k_nl_force     one thread per atom over its full list: FP32 pair law,
 //                  fixed-point sums in registers, plain stores (no atomics);
 //                  the potential and pair count take each pair once (q > p)
@@ -114,9 +115,15 @@ __global__ void __launch_bounds__(256) k_nl_advance(StateBuf b, uint32_t n, cons
                                                      int wrap, GridGeom g, const uint32_t* __restrict__ home,
                                                      float4* __restrict__ pos4, const float4* __restrict__ ref,
                                                      float lim2, uint32_t* __restrict__ flag,
-                                                     uint32_t* __restrict__ err) {
+                                                     uint32_t* __restrict__ err, long long* __restrict__ F,
+                                                     size_t fstride) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     bool over = false;
+    if (F && i < n) {  // the half-list pass accumulates into F: zero it here, not in a separate memset
+        F[i] = 0;
+        F[fstride + i] = 0;
+        F[2 * fstride + i] = 0;
+    }
     // translations since the rebuild, this tick's wrap included
     const bool half = ((flag[2] + (wrap ? 1u : 0u)) & 1u) != 0u;
     if (i < n) {
@@ -247,7 +254,9 @@ __global__ void k_nl_set_cond(cudaGraphConditionalHandle hc, const uint32_t* __r
 
 __global__ void k_nl_body_done(uint32_t* flag) { flag[3] += 1u; }
 
-__global__ void k_nl_end(uint32_t* flag, int wrap) {
+__global__ void k_nl_end(uint32_t* flag, int wrap, unsigned long long* __restrict__ counts) {
+    // the force pass's potential, pair and bond-energy counters start at zero
+    counts[0] = counts[1] = counts[2] = counts[3] = 0ull;
     if (flag[0]) {
         flag[1] += 1u;
         flag[0] = 0u;
@@ -679,7 +688,7 @@ int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nb_out, bool
     prof_begin(h, "nl_advance");
     GX_LAUNCH(h, k_nl_advance, nblk(n, 256), 256, b, n, lambda, half_dt, h->p.dt, 0.5 * h->p.box[0],
               0.5 * h->p.box[1], 0.5 * h->p.box[2], h->p.enable_boundaries ? 1 : 0, g, h->key_sorted, h->pos4, s->ref,
-              lim * lim, s->flag, h->derr);
+              lim * lim, s->flag, h->derr, s->half == 1 ? h->F : nullptr, h->cap);
     prof_end(h, "nl_advance");
     // inside a capture: the rebuild goes into the body of an IF node
     cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
@@ -735,13 +744,11 @@ int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nb_out, bool
         if (!rc && ce != cudaSuccess) rc = cuda_err(h, ce, "cudaStreamEndCapture (rebuild body)");
     }
     if (rc) return rc;
-    GX_LAUNCH(h, k_nl_end, 1, 1, s->flag, h->p.enable_boundaries ? 1 : 0);
+    GX_LAUNCH(h, k_nl_end, 1, 1, s->flag, h->p.enable_boundaries ? 1 : 0, h->dcount);
     prof_end(h, "nl_rebuild");
     const bool halfl = s->half == 1;
-    GX_CUDA(h, cudaMemsetAsync(h->dcount, 0, 4 * sizeof(unsigned long long), h->stream));
     LawF32 L = make_law32(h);
     prof_begin(h, "force_nl");
-    if (halfl) GX_CUDA(h, cudaMemsetAsync(h->F, 0, 3 * h->cap * sizeof(long long), h->stream));
     if (halfl)
         launch_nl_force<true>(h, s->tpp, g, s, n, L, energy);
     else
