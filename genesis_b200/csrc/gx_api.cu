@@ -705,7 +705,9 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
         // the potential and pair count only where a record takes them
         int r = nl_tick(h, pend ? h->dscal + 0 : nullptr, thermo ? kpart : nullptr, &nb, drec != nullptr);
         if (r) return r;
-        if (pend) GX_LAUNCH(h, k_fill_d, 1, 32, h->dscal, 1, 1.0);
+        // the scale slot back to 1 once applied; with the thermostat on, its
+        // kernel below overwrites the slot anyway
+        if (pend && !thermo) GX_LAUNCH(h, k_fill_d, 1, 32, h->dscal, 1, 1.0);
         h->lambda_pending = false;
         if (thermo) {
             launch_thermostat_lambda(h, kpart, nb, h->p.thermal_constant, h->p.thermostat_temperature, tau, n,

@@ -543,11 +543,19 @@ __device__ __forceinline__ double block_sum_d(double v, double* sh) {
 // a = F 2^-32 (1/m) (as k_fix_to_acc), v += a dt/2 (as k_kick), and with
 // THERMO the kinetic-energy partials of the new v with k_kinetic's block
 // mapping and operation order, so lambda is bit-identical to the unfused tick.
+// With vsum: also k_nl_fix_to_double's conversion of the potential (ticks
+// without a bond spring, which would write the bond-energy slot after it).
 template <bool THERMO>
 __global__ void __launch_bounds__(kRedThreads) k_nl_finish(StateBuf b, const long long* __restrict__ F,
                                                            size_t fstride, uint32_t n, double half_dt,
-                                                           double* __restrict__ kpart) {
+                                                           double* __restrict__ kpart,
+                                                           const unsigned long long* __restrict__ vsum,
+                                                           double* __restrict__ vout, double* __restrict__ bzero) {
     __shared__ double sh[kRedThreads / 32];
+    if (vsum && blockIdx.x == 0 && threadIdx.x == 0) {
+        *vout = xmul(__ll2double_rn((long long)*vsum), kFixInv);
+        *bzero = 0.0;
+    }
     double ks = 0.0;
     for (uint32_t i = blockIdx.x * kRedThreads + threadIdx.x; i < n; i += gridDim.x * kRedThreads) {
         double im = b.inv_mass[i];
@@ -754,17 +762,21 @@ int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nb_out, bool
     else
         launch_nl_force<false>(h, s->tpp, g, s, n, L, energy);
     prof_end(h, "force_nl");
-    GX_LAUNCH(h, k_nl_fix_to_double, 1, 1, h->dcount + 1, h->dscal + 2, h->dscal + 3);
-    if (bonds_on(h) && (rc = bond_spring(h, true))) return rc;  // into F before it becomes a
+    const bool spring = bonds_on(h);
+    if (spring) GX_LAUNCH(h, k_nl_fix_to_double, 1, 1, h->dcount + 1, h->dscal + 2, h->dscal + 3);
+    if (spring && (rc = bond_spring(h, true))) return rc;  // into F before it becomes a
     if (h->p.enable_collisions && (rc = collide_pass(h))) return rc;  // CollisionSystem, before the second kick
     int nb = (int)nblk(n, kRedThreads);
     if (nb > 1184) nb = 1184;  // the block count of launch_kinetic
     if (nb < 1) nb = 1;
     prof_begin(h, "nl_finish");
+    const unsigned long long* vsum = spring ? nullptr : h->dcount + 1;
     if (kpart)
-        GX_LAUNCH(h, k_nl_finish<true>, nb, kRedThreads, b, h->F, h->cap, n, half_dt, kpart);
+        GX_LAUNCH(h, k_nl_finish<true>, nb, kRedThreads, b, h->F, h->cap, n, half_dt, kpart, vsum, h->dscal + 2,
+                  h->dscal + 3);
     else
-        GX_LAUNCH(h, k_nl_finish<false>, nb, kRedThreads, b, h->F, h->cap, n, half_dt, nullptr);
+        GX_LAUNCH(h, k_nl_finish<false>, nb, kRedThreads, b, h->F, h->cap, n, half_dt, nullptr, vsum, h->dscal + 2,
+                  h->dscal + 3);
     prof_end(h, "nl_finish");
     if (nb_out) *nb_out = nb;
     return GX_OK;
