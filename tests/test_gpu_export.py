@@ -64,10 +64,11 @@ def test_out_of_range_and_size_query(gpu):
     assert h.xyz_frame(3) == b"1\nframe 3\nFe 1.000000 2.000000 3.000000\n"
 
 
-def test_slot_order_after_steps(gpu, orc, tmp_path):
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_slot_order_after_steps(gpu, orc, tmp_path, precision):
     wl = W.C2
     cfg, u = wl.config(), wl.generate()
-    h = _handle(cfg)
+    h = _handle(cfg, precision)
     h.set_universe(u)
     h.step(20)
     pos, _, _ = h.get_state()
