@@ -64,7 +64,7 @@ def parse():
                     help="fix the mixed pair-pass variant instead of autotuning (profiling only)")
     ap.add_argument("--skin", type=float, default=-1.0,
                     help="neighbour-list skin in length units instead of 0.1 r_c (profiling only; 0 = rebuild every tick)")
-    ap.add_argument("--leg", default="", choices=["", "ionic", "accuracy", "adjoint", "xyz"],
+    ap.add_argument("--leg", default="", choices=["", "ionic", "accuracy", "adjoint", "xyz", "sweep"],
                     help="run one extra leg alone and print its JSON (profiling only)")
     ap.add_argument("--leg-steps", type=int, default=0, help="ticks of the --leg run (0: the workload's own)")
     return ap.parse_args()
@@ -772,6 +772,14 @@ def main():
                 out = ionic_leg(dev, cpu=False, steps=args.leg_steps or None, variant=args.variant)
             elif args.leg == "accuracy":
                 out = accuracy_leg(dev, args.leg_steps or 10000)
+            elif args.leg == "sweep":
+                from genesis_b200 import sweep
+
+                wls = sweep.make_replicas(256, seed=0)
+                steps = args.leg_steps or 2000
+                _, _, ms = sweep.run_batched(wls, steps, dev, mode=2)
+                out = {"workload": "256 replicas, all-replica graph", "steps": steps, "ms": ms,
+                       "replica_steps_per_s": len(wls) * steps / (ms * 1e-3), "atoms": sweep.atoms(wls)}
             elif args.leg == "xyz":
                 import dataclasses
 
