@@ -70,6 +70,7 @@ EXPORTS = (
     "gx_set_list_skin", "gx_list_rebuilds", "gx_batch_set_mode", "gx_batch_get_mode", "gx_batch_autotune",
     "gx_get_list_config", "gx_set_list_threads", "gx_bond_observe", "gx_bond_tracker_reset", "gx_get_bonds",
     "gx_bond_components", "gx_collisions", "gx_collision_count", "gx_xyz_frame",
+    "gx_set_step_async",
 )
 
 _lib = None
@@ -132,6 +133,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
         "gx_collisions": (C.c_int, [vp, u64p]),
         "gx_collision_count": (C.c_int, [vp, u64p]),
         "gx_xyz_frame": (C.c_int, [vp, C.c_uint64, C.c_char_p, sz, C.POINTER(sz)]),
+        "gx_set_step_async": (C.c_int, [vp, C.c_int]),
         "gx_adjoint_backward": (C.c_int, [vp, dp, dp, dp, dp, dp, dp, dp]),
     }
     for name, (res, args) in proto.items():
@@ -472,6 +474,11 @@ class Handle:
             rc = self.lib.gx_get_bonds(self.h, _ptr(out, C.c_uint32), n.value, C.byref(n))
         self._check(rc)
         return out[: n.value].copy()
+
+    def set_step_async(self, on: bool = True):
+        """gx_step without records returns without waiting; its errors come
+        back from the next call that waits (gx_set_step_async)."""
+        self._check(self.lib.gx_set_step_async(self.h, int(on)))
 
     def xyz_frame(self, tick: int) -> bytes:
         """The XYZ frame of the current state as export::write_frame writes

@@ -262,6 +262,28 @@ int commit_lambda(gx_handle* h) {
     return GX_OK;
 }
 
+// The device error word of the pair pass as a status (and cleared).
+int step_error(gx_handle* h, uint32_t e) {
+    if (!e) return GX_OK;
+    cudaMemset(h->derr, 0, sizeof(uint32_t));
+    if (e & kErrNonFinite) return set_err(h, GX_ERR_NONFINITE, "non-finite force in the pair pass");
+    if (e & kErrSaturation) return set_err(h, GX_ERR_SATURATION, "fixed-point force saturated");
+    if (e & kErrTimeout) return set_err(h, GX_ERR_TIMEOUT, "shared-memory staging wait timed out");
+    return set_err(h, GX_ERR_CUDA, "unknown device error");
+}
+
+}  // namespace
+
+namespace gx {
+int take_step_errors(gx_handle* h) {
+    if (!h->step_errs_pending) return GX_OK;
+    h->step_errs_pending = false;
+    return step_error(h, *h->herr);
+}
+}  // namespace gx
+
+namespace {
+
 int require_state(gx_handle* h) {
     if (!h) return GX_ERR_ARG;
     if (!h->cap) return set_err(h, GX_ERR_STATE, "no state uploaded (call gx_set_state first)");
@@ -404,6 +426,7 @@ void gx_destroy(gx_handle* h) {
     lens_free(h);
     collide_free(h);
     export_free(h);
+    if (h->herr) cudaFreeHost(h->herr);
     free_buf(h->buf[0]);
     free_buf(h->buf[1]);
     cudaFree(h->key);
@@ -531,7 +554,8 @@ int gx_get_state(gx_handle* h, double* pos, double* vel, double* acc) {
         GX_CUDA(h, cudaStreamSynchronize(h->stream));
     }
     GX_CUDA(h, cudaGetLastError());
-    return GX_OK;
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    return take_step_errors(h);
 }
 
 int gx_set_bonds(gx_handle* h, size_t nbonds, const uint32_t* pairs) {
@@ -808,17 +832,19 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
         GX_CUDA(h, cudaMemcpyAsync(stats, drec, (size_t)nsteps * sizeof(gx_tick_stats), cudaMemcpyDeviceToHost,
                                    h->stream));
     }
-    uint32_t e = 0;
-    GX_CUDA(h, cudaMemcpyAsync(&e, h->derr, sizeof e, cudaMemcpyDeviceToHost, h->stream));
+    if (h->step_async && !drec && h->herr) {
+        // no wait: the error word follows in stream order, read by the next waiting call
+        GX_CUDA(h, cudaMemcpyAsync(h->herr, h->derr, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+        GX_CUDA(h, cudaGetLastError());
+        h->step_errs_pending = true;
+        return GX_OK;
+    }
     GX_CUDA(h, cudaStreamSynchronize(h->stream));
     GX_CUDA(h, cudaGetLastError());
-    if (e) {
-        cudaMemset(h->derr, 0, sizeof(uint32_t));
-        if (e & kErrNonFinite) return set_err(h, GX_ERR_NONFINITE, "non-finite force in the pair pass");
-        if (e & kErrSaturation) return set_err(h, GX_ERR_SATURATION, "fixed-point force saturated");
-        if (e & kErrTimeout) return set_err(h, GX_ERR_TIMEOUT, "shared-memory staging wait timed out");
-    }
-    return GX_OK;
+    h->step_errs_pending = false;
+    uint32_t e = 0;
+    GX_CUDA(h, cudaMemcpy(&e, h->derr, sizeof e, cudaMemcpyDeviceToHost));
+    return step_error(h, e);
 }
 
 int gx_collisions(gx_handle* h, uint64_t* collisions) {
@@ -1002,6 +1028,19 @@ int gx_set_dynamic(gx_handle* h, const double* pos, const double* vel, const dou
 int gx_synchronize(gx_handle* h) {
     if (!h) return GX_ERR_ARG;
     GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    return take_step_errors(h);
+}
+
+int gx_set_step_async(gx_handle* h, int on) {
+    if (!h) return GX_ERR_ARG;
+    if (on && !h->herr) GX_CUDA(h, cudaMallocHost(&h->herr, sizeof(uint32_t)));
+    if (!on) {  // report what an earlier step left before going back to waiting steps
+        GX_CUDA(h, cudaStreamSynchronize(h->stream));
+        int rc = take_step_errors(h);
+        h->step_async = false;
+        return rc;
+    }
+    h->step_async = true;
     return GX_OK;
 }
 

@@ -515,7 +515,7 @@ int observe_once(gx_handle* h, BondTracker* t, double k_bind, uint32_t debounce,
     }
     GX_CUDA(h, cudaStreamSynchronize(h->stream));
     GX_CUDA(h, cudaGetLastError());
-    return GX_OK;
+    return take_step_errors(h);  // an asynchronous step before this observation
 }
 
 }  // namespace

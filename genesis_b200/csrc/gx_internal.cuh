@@ -196,6 +196,11 @@ struct gx_handle {
     double* dscal = nullptr;       // [0]=lambda pending, [1]=K, [2]=V, [3]=Vb, [4]=speed, [5]=one
     unsigned long long* dcount = nullptr;  // [0]=pairs, [1..3]=fixed V, Vb, ..., [8]=bond count
     uint32_t* derr = nullptr;      // device error word
+    // gx_set_step_async: gx_step returns without waiting; its error word is
+    // copied to pinned host memory and reported by the next call that waits
+    bool step_async = false;
+    bool step_errs_pending = false;
+    uint32_t* herr = nullptr;      // pinned copy of derr
     bool lambda_pending = false;
 
     // mixed kinds
@@ -316,6 +321,8 @@ int collide_pass(gx_handle* h);
 int collide_read(gx_handle* h, unsigned long long* pass, unsigned long long* total);
 void collide_free(gx_handle* h);
 void export_free(gx_handle* h);  // gx_export.cu
+// After a wait on the stream: the error word an asynchronous gx_step left.
+int take_step_errors(gx_handle* h);
 
 // Read-only view of the persistent neighbour list (gx_nlist.cu) for the
 // passes that can take their candidates from it.  Entry e of atom p (sorted

@@ -393,8 +393,16 @@ int gx_adjoint_backward(gx_handle* h, const double* dl_dpotential, const double*
 
 /* ---- timing ---------------------------------------------------------- */
 
-/* Waits for the handle's stream. */
+/* Waits for the handle's stream; reports an error an asynchronous gx_step
+ * left (see gx_set_step_async). */
 int gx_synchronize(gx_handle* h);
+/* on = 1: gx_step without per-tick records returns once its work is queued,
+ * without waiting for the GPU; an error its pair pass raised (saturation,
+ * non-finite force, timeout) is returned by the next call that waits:
+ * gx_synchronize, gx_get_state, gx_bond_observe, or gx_set_step_async(h, 0).
+ * Lets a host scheduler queue the force systems and the observation of one
+ * tick behind a single wait.  Default 0: gx_step waits and reports. */
+int gx_set_step_async(gx_handle* h, int on);
 /* Records CUDA event `slot` (0..15) on the handle's stream. */
 int gx_timer_mark(gx_handle* h, int slot);
 /* Milliseconds between two recorded events (waits for the second). */

@@ -410,3 +410,33 @@ def test_gravity_matches_fp64_oracle(gpu, orc, precision, variant):
     assert np.linalg.norm(acc0 - acc_ref) / np.linalg.norm(acc_ref) > 1e-3
     if variant == 6:
         assert h.list_rebuilds() >= 1  # the neighbour-list path ran
+
+
+def test_async_steps_report_errors_at_the_next_wait(gpu):
+    from genesis_b200._lib import GxError
+    wl, cfg, u = _c1(n_side=8)
+    u.pos[5, 1] = np.nan
+    for prec in ("fp64", "mixed"):
+        h = _handle(cfg, prec)
+        h.set_universe(u)
+        h.set_step_async(True)
+        h.step(1, stats=False)  # queued: returns without waiting
+        with pytest.raises(GxError) as e:
+            h.synchronize()
+        assert e.value.status == -6
+        h.synchronize()  # reported once
+
+
+def test_async_steps_give_the_same_ticks(gpu):
+    wl, cfg, u = _c1(n_side=10)
+    out = []
+    for asyn in (False, True):
+        h = _handle(cfg, "mixed")
+        h.set_universe(u)
+        h.set_step_async(asyn)
+        for _ in range(15):
+            h.step(2, stats=False, graph=True)
+        h.synchronize()
+        out.append(h.get_state())
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
