@@ -74,6 +74,7 @@ EXPORTS = (
 )
 
 _lib = None
+_OBS_SCALARS = tuple(f for f, _ in GxBondObservation._fields_ if f != "species_matrix")
 
 
 def load(path: str | Path | None = None) -> C.CDLL:
@@ -431,8 +432,8 @@ class Handle:
         o = GxBondObservation()
         self._check(self.lib.gx_bond_observe(self.h, k_bind, min_periods, debounce, tick, int(apply_bonds),
                                              C.byref(o)))
-        d = {f: getattr(o, f) for f, _ in GxBondObservation._fields_ if f != "species_matrix"}
-        d["species_matrix"] = np.array(o.species_matrix[:], dtype=np.uint64).reshape(10, 10)
+        d = {f: getattr(o, f) for f in _OBS_SCALARS}
+        d["species_matrix"] = np.ctypeslib.as_array(o.species_matrix).astype(np.uint64).reshape(10, 10)
         return d
 
     def bond_components(self):
