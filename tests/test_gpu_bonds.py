@@ -236,3 +236,23 @@ def test_list_candidates_match_the_bond_grid(gpu):
         assert np.array_equal(ha.get_state()[0], hb.get_state()[0])
         seen = max(seen, oa["bound_pairs"])
     assert seen > 0
+
+
+def test_positions_moved_outside_a_tick_leave_the_list_out(gpu):
+    """After gx_drift or gx_set_dynamic the list is not proven for the new
+    positions: the observation bins the bond grid again."""
+    from genesis_b200._lib import Handle
+    cfg, u = _ionic()
+    h = Handle(cfg, "mixed")
+    h.set_universe(u)
+    h.step(2)
+    for tick, move in ((3, None), (4, "drift"), (5, "set_dynamic")):
+        if move == "drift":
+            h.drift()
+        elif move == "set_dynamic":
+            h.set_dynamic(h.get_state()[0])
+        h.profile(True)
+        h.bond_observe(cfg.bond_k_bind, 0.2, tick, apply_bonds=False)
+        prof = h.profile_read()
+        h.profile(False)
+        assert ("bond_grid" in prof) == (move is not None), (move, sorted(prof))
