@@ -42,6 +42,7 @@ namespace gx {
 namespace {
 
 constexpr int kAdjThreads = 128;
+constexpr int kAdjLanes = 8;  // lanes per atom in the pair kernels: each takes every 8th neighbour cell
 constexpr int kAdjMaxBins = 512;
 constexpr double kRonFrac = 0.9;  // r_on = 0.9 rc for every switched term (forces.rs:237, systems/forces.rs:118-124)
 constexpr double kHistScale = 4294967296.0;
@@ -170,6 +171,21 @@ __device__ __forceinline__ uint32_t visit_cell(const GridGeom& g, uint32_t c, ui
                   wrap_add(cz, g.full[k][2], g.n[2]));
 }
 
+// min_image1 for |d| <= 0.49 L without the division: the rounded quotient
+// is zero there and d - L * 0 is d itself, sign of a zero included.
+__device__ __forceinline__ double near_image(double d, double L) {
+    return fabs(d) <= xmul(0.49, L) ? d : min_image1(d, L);
+}
+
+// Sum over the kAdjLanes lanes of one atom (a butterfly: every lane ends
+// with the same bits, and the association is fixed, so recomputed ticks
+// reproduce the forward pass exactly).
+__device__ __forceinline__ double lane_sum(double v) {
+#pragma unroll
+    for (int o = kAdjLanes / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, kAdjLanes);
+    return v;
+}
+
 // ---------------------------------------------------------------------------
 // Kernels (slot order unless noted).
 
@@ -243,10 +259,12 @@ __global__ void k_adj_stage(uint32_t n, const uint32_t* __restrict__ perm, const
     }
 }
 
-// Forward force pass + second kick.  Thread p owns atom perm[p] and gathers
-// its full neighbourhood in the reference's per-pair FP64 arithmetic; the
-// potential and the smoothed histogram take each pair-list entry once
-// (canonical half-shell visits, or j > p within a cell).
+// Forward force pass + second kick.  kAdjLanes lanes own atom perm[p]: lane
+// l visits the neighbour cells l - 1, l - 1 + kAdjLanes, ... (the atom's own
+// cell first) in the reference's per-pair FP64 arithmetic, and lane_sum
+// combines their accelerations; the potential and the smoothed histogram
+// take each pair-list entry once (canonical half-shell visits, or j > p
+// within a cell).  One histogram per warp in shared memory, integer counts.
 template <bool OBS, bool GR>
 __global__ void __launch_bounds__(kAdjThreads)
     k_adj_force(GridGeom g, uint32_t n, LawF64 L, const double* __restrict__ psig, const double* __restrict__ peps,
@@ -254,31 +272,34 @@ __global__ void __launch_bounds__(kAdjThreads)
                 const uint8_t* __restrict__ es, const double* __restrict__ qs, const double* __restrict__ ms,
                 const uint32_t* __restrict__ perm, const double* __restrict__ inv_mass, Vec3Field v, Vec3Field a,
                 double half_dt, double* __restrict__ vpart, GrSpec gs, double* __restrict__ hpart) {
-    __shared__ double shd[kAdjThreads / 32];
-    __shared__ unsigned long long hist[GR ? kAdjMaxBins : 1];
+    constexpr int kWarps = kAdjThreads / 32;
+    __shared__ double shd[kWarps];
+    __shared__ unsigned long long hist[GR ? kWarps : 1][GR ? kAdjMaxBins : 1];
     if (GR)
-        for (int k = threadIdx.x; k < gs.bins; k += kAdjThreads) hist[k] = 0ull;
+        for (int k = threadIdx.x; k < kWarps * gs.bins; k += kAdjThreads) hist[k / gs.bins][k % gs.bins] = 0ull;
     if (GR) __syncthreads();
-    uint32_t p = blockIdx.x * kAdjThreads + threadIdx.x;
+    unsigned long long* wh = hist[GR ? threadIdx.x / 32 : 0];
+    const uint32_t t = blockIdx.x * kAdjThreads + threadIdx.x;
+    const uint32_t p = t / kAdjLanes;
+    const int lane = (int)(t % kAdjLanes);
     double V = 0.0;
+    double ax = 0.0, ay = 0.0, az = 0.0;
     if (p < n) {
         uint32_t c = ks[p], cx, cy, cz;
         decode(g, c, cx, cy, cz);
         double xi = xs.c(0, p), yi = xs.c(1, p), zi = xs.c(2, p);
         int ti = es[p];
         double qi = qs[p], mi = ms[p];
-        uint32_t i = perm[p];
-        double inv_mi = inv_mass[i];
-        double ax = 0.0, ay = 0.0, az = 0.0;
-        for (int k = -1; k < g.nfull; ++k) {
+        double inv_mi = inv_mass[perm[p]];
+        for (int k = lane - 1; k < g.nfull; k += kAdjLanes) {
             uint32_t B = visit_cell(g, c, cx, cy, cz, k);
             bool half = k < g.nhalf;
             uint32_t lo = start[B], hi = start[B + 1];
             for (uint32_t q = lo; q < hi; ++q) {
                 if (q == p) continue;
-                double dx = min_image1(xsub(xi, xs.c(0, q)), L.box[0]);
-                double dy = min_image1(xsub(yi, xs.c(1, q)), L.box[1]);
-                double dz = min_image1(xsub(zi, xs.c(2, q)), L.box[2]);
+                double dx = near_image(xsub(xi, xs.c(0, q)), L.box[0]);
+                double dy = near_image(xsub(yi, xs.c(1, q)), L.box[1]);
+                double dz = near_image(xsub(zi, xs.c(2, q)), L.box[2]);
                 double d2 = xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
                 if (d2 >= L.rc2) continue;
                 double d = xsqrt(d2);
@@ -292,11 +313,11 @@ __global__ void __launch_bounds__(kAdjThreads)
                     int k0 = (int)ceil((d - gs.reach) / gs.dr - 0.5), k1 = (int)floor((d + gs.reach) / gs.dr - 0.5);
                     k0 = k0 < 0 ? 0 : k0;
                     k1 = k1 > gs.bins - 1 ? gs.bins - 1 : k1;
-                    for (int b = k0; b <= k1; ++b) {
-                        double z = d - (b + 0.5) * gs.dr;
+                    for (int bb = k0; bb <= k1; ++bb) {
+                        double z = d - (bb + 0.5) * gs.dr;
                         if (fabs(z) >= gs.reach) continue;
                         double G = exp(z * z * gs.c2);
-                        atomicAdd(&hist[b], (unsigned long long)llrint(G * kHistScale));
+                        atomicAdd(&wh[bb], (unsigned long long)llrint(G * kHistScale));
                     }
                 }
                 if (fmag != 0.0) {
@@ -307,6 +328,13 @@ __global__ void __launch_bounds__(kAdjThreads)
                 }
             }
         }
+    }
+    // every lane of an atom is in the same warp and takes part
+    ax = lane_sum(ax);
+    ay = lane_sum(ay);
+    az = lane_sum(az);
+    if (p < n && lane == 0) {
+        uint32_t i = perm[p];
         a.c(0, i) = ax;
         a.c(1, i) = ay;
         a.c(2, i) = az;
@@ -320,8 +348,12 @@ __global__ void __launch_bounds__(kAdjThreads)
     }
     if (GR) {
         __syncthreads();
-        for (int k = threadIdx.x; k < gs.bins; k += kAdjThreads)
-            hpart[(size_t)blockIdx.x * gs.bins + k] = (double)hist[k] * kHistInv;
+        for (int k = threadIdx.x; k < gs.bins; k += kAdjThreads) {
+            unsigned long long s = 0ull;
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) s += hist[w][k];
+            hpart[(size_t)blockIdx.x * gs.bins + k] = (double)s * kHistInv;
+        }
     }
 }
 
@@ -344,8 +376,12 @@ __global__ void __launch_bounds__(kAdjThreads)
                const double* __restrict__ ms, const uint32_t* __restrict__ perm, Vec3Field Lx, Vec3Field Lv,
                Vec3Field La, double* __restrict__ P, size_t cap, const double* __restrict__ alpha_t, double dt,
                double half_dt, GrSpec gs, const double* __restrict__ bw) {
-    uint32_t p = blockIdx.x * kAdjThreads + threadIdx.x;
-    if (p >= n) return;
+    const uint32_t t = blockIdx.x * kAdjThreads + threadIdx.x;
+    const uint32_t p = t / kAdjLanes;
+    const int lane = (int)(t % kAdjLanes);
+    double gx = 0.0, gy = 0.0, gz = 0.0;
+    double Ps = 0.0, Pe = 0.0, Pr0 = 0.0, Pr1 = 0.0, Pr2 = 0.0;
+    if (p < n) {
     const double alpha = *alpha_t;
     uint32_t c = ks[p], cx, cy, cz;
     decode(g, c, cx, cy, cz);
@@ -354,16 +390,14 @@ __global__ void __launch_bounds__(kAdjThreads)
     int ti = es[p];
     double qi = qs[p], mi = ms[p];
     double ehalf_base = 0.5 / epsk[ti];
-    double gx = 0.0, gy = 0.0, gz = 0.0;
-    double Ps = 0.0, Pe = 0.0, Pr0 = 0.0, Pr1 = 0.0, Pr2 = 0.0;
-    for (int k = -1; k < g.nfull; ++k) {
+    for (int k = lane - 1; k < g.nfull; k += kAdjLanes) {
         uint32_t B = visit_cell(g, c, cx, cy, cz, k);
         uint32_t lo = start[B], hi = start[B + 1];
         for (uint32_t q = lo; q < hi; ++q) {
             if (q == p) continue;
-            double dx = min_image1(xi - xs.c(0, q), L.box[0]);
-            double dy = min_image1(yi - xs.c(1, q), L.box[1]);
-            double dz = min_image1(zi - xs.c(2, q), L.box[2]);
+            double dx = near_image(xi - xs.c(0, q), L.box[0]);
+            double dy = near_image(yi - xs.c(1, q), L.box[1]);
+            double dz = near_image(zi - xs.c(2, q), L.box[2]);
             double d2 = dx * dx + dy * dy + dz * dz;
             if (d2 >= L.rc2) continue;
             double d = sqrt(d2);
@@ -398,6 +432,17 @@ __global__ void __launch_bounds__(kAdjThreads)
             Pr2 += 0.5 * (rho * G.frc[2] + alpha * G.Urc[2]);
         }
     }
+    }
+    // every lane of an atom is in the same warp and takes part
+    gx = lane_sum(gx);
+    gy = lane_sum(gy);
+    gz = lane_sum(gz);
+    Ps = lane_sum(Ps);
+    Pe = lane_sum(Pe);
+    Pr0 = lane_sum(Pr0);
+    Pr1 = lane_sum(Pr1);
+    Pr2 = lane_sum(Pr2);
+    if (p >= n || lane != 0) return;
     uint32_t i = perm[p];
     double g3[3] = {gx, gy, gz};
     for (int k = 0; k < 3; ++k) {
@@ -482,7 +527,7 @@ int adj_alloc(gx_handle* h, AdjBuffers* A, size_t n, int T, int K, int bins) {
     A->owned.clear();
     size_t cap = n < 1 ? 1 : n;
     cap = (cap + 31) & ~(size_t)31;
-    size_t nb = nblk(cap, kAdjThreads);
+    size_t nb = nblk(cap * kAdjLanes, kAdjThreads);
     int binc = bins < 1 ? 1 : bins;
     auto get = [&](void** p, size_t bytes) -> int {
         cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
@@ -563,7 +608,7 @@ int adj_tick(gx_handle* h, AdjBuffers* A, int t, bool obs, double* xsave, bool w
     const double* psig = A->tab;
     const double* peps = A->tab + kNElem * kNElem;
     GrSpec gs = gr_spec(A);
-    unsigned nb = nblk(n, kAdjThreads);
+    unsigned nb = nblk((size_t)n * kAdjLanes, kAdjThreads);
     bool gr = obs && A->bins > 0 && (t % A->every) == 0;
     auto kern = !obs ? k_adj_force<false, false> : (gr ? k_adj_force<true, true> : k_adj_force<true, false>);
     GX_LAUNCH(h, kern, nb, kAdjThreads, g, n, L, psig, peps, A->cl.start, A->ks, xs, A->es, A->qs, A->ms, A->perm,
@@ -699,7 +744,7 @@ int gx_adjoint_backward(gx_handle* h, const double* dl_dpotential, const double*
     const double* epsk = A->tab + 2 * kNElem * kNElem;
     double* out = A->tab + 2 * kNElem * kNElem + kNElem;
     GrSpec gs = gr_spec(A);
-    unsigned nb = nblk(n, kAdjThreads);
+    unsigned nb = nblk((size_t)n * kAdjLanes, kAdjThreads);
     bool has_gr = dl_dgr && A->bins > 0;
     for (int s = A->nck - 1; s >= 0; --s) {
         int t0 = s * K, t1 = t0 + K < T ? t0 + K : T;
