@@ -201,16 +201,21 @@ def measured_peaks() -> dict:
     return {}
 
 
-def ncu_traffic(kernel: str) -> float | None:
-    """DRAM bytes per launch from the committed ncu summary, if present."""
+def ncu_figure(key: str, kernel: str) -> float | None:
+    """A `key[kernel]: value` figure from the committed ncu summaries."""
     for f in (ROOT / "profiles").glob("*.txt"):
         for line in f.read_text().splitlines():
-            if line.startswith(f"traffic_bytes_per_launch[{kernel}]"):
+            if line.startswith(f"{key}[{kernel}]"):
                 try:
                     return float(line.split(":", 1)[1].split()[0])
                 except Exception:
                     return None
     return None
+
+
+def ncu_traffic(kernel: str) -> float | None:
+    """DRAM bytes per launch from the committed ncu summary, if present."""
+    return ncu_figure("traffic_bytes_per_launch", kernel)
 
 
 def hbm_peak() -> tuple[float, str]:
@@ -586,8 +591,13 @@ def ours_arm(args, dist):
     except Exception as e:  # noqa: BLE001
         peak, peak_src = 74.4, f"nominal 148 SM x 128 lanes x 2 x 1.965 GHz ({e})"
     traffic = ncu_traffic(force_k)
+    l1 = ncu_figure("l1tex_throughput_frac", force_k)
     roof = {"kernel": force_k, "bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
+            "limiter": None if l1 is None else {
+                "unit": "L1/TEX throughput, fraction of peak (ncu)", "frac": l1,
+                "note": "the pass is bound by its neighbour gathers and far-end integer reductions in L1/TEX, "
+                        "not by the FP32 pipe (profiles/k_nl_force__c3_262144_atoms.txt)"},
             "flop_per_launch": pairs * flop_pp, "pairs_per_launch": pairs, "launch_ms": force_ms,
             "share_of_step": f_ms / tot_ms if tot_ms else None}
     hbm, hbm_src = hbm_peak()
