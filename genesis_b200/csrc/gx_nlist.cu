@@ -66,6 +66,8 @@ struct NlState {
 namespace {
 
 constexpr int kNlThreads = 128;
+constexpr int kNlBuildThreads = 128;
+constexpr int kNlBuildUnroll = 4;
 constexpr int kRedThreads = 256;
 constexpr uint32_t kIdxMask = (1u << 27) - 1u;
 
@@ -204,13 +206,13 @@ __global__ void k_nl_stage(GridGeom g, StateBuf b, const uint32_t* __restrict__ 
 // a cell length) lie well inside the 1e-6 relative margin of r_l, so the
 // list still holds every pair within r_c + skin.
 template <bool HALF>
-__global__ void __launch_bounds__(kNlThreads) k_nl_build(GridGeom g, const float4* __restrict__ pos4,
+__global__ void __launch_bounds__(kNlBuildThreads) k_nl_build(GridGeom g, const float4* __restrict__ pos4,
                                                           const uint32_t* __restrict__ home,
                                                           const uint32_t* __restrict__ start, uint32_t n, float rl2,
                                                           uint32_t* __restrict__ list, size_t stride, int cap_nb,
                                                           uint32_t* __restrict__ cnt, const uint32_t* __restrict__ gate) {
     if (gated_off(gate)) return;
-    uint32_t p = blockIdx.x * kNlThreads + threadIdx.x;
+    uint32_t p = blockIdx.x * kNlBuildThreads + threadIdx.x;
     if (p >= n) return;
     const float4 pi = pos4[p];
     const uint32_t c = home[p];
@@ -234,7 +236,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_build(GridGeom g, const float
         uint32_t lo = start[B];
         const uint32_t hi = start[B + 1];
         if (HALF && B == c) lo = p + 1;  // HALF: every candidate lies after p
-#pragma unroll 4
+#pragma unroll(kNlBuildUnroll)
         for (uint32_t q = lo; q < hi; ++q) {
             if (!HALF && q == p) continue;
             const float4 pj = pos4[q];
@@ -737,7 +739,8 @@ int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nb_out, bool
         GX_LAUNCH(h, k_nl_stage, nblk(n, 256), 256, g, b, h->key_sorted, n, h->pos4, s->ref, s->flag);
         const float rl = (float)((h->fs.rc + s->skin_used) * (1.0 + 1e-6));
         auto build = s->half == 1 ? k_nl_build<true> : k_nl_build<false>;
-        GX_LAUNCH(h, build, nblk(n, kNlThreads), kNlThreads, g, h->pos4, h->key_sorted, s->cl.start, n, rl * rl,
+        GX_LAUNCH(h, build, nblk(n, kNlBuildThreads), kNlBuildThreads, g, h->pos4, h->key_sorted, s->cl.start, n,
+                  rl * rl,
                   s->list, s->cap, s->cap_nb, s->cnt, s->flag);
         return GX_OK;
     };
