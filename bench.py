@@ -289,6 +289,30 @@ def xyz_leg(h, elem, tick: int, cpu: bool, reps: int = 5) -> dict:
     return out
 
 
+def gr_leg(h, n_atoms: int, reps: int = 3) -> dict:
+    """g(r) of the resident state (radial_distribution, src/analysis/mod.rs:87-133):
+    the reference's call (a subsample of at most 8192 atoms, 256 bins to
+    r_max = 3 r_c = 17.25) and the whole state without the subsample, which
+    gives the pair throughput.  Host wall clock around the synchronous call."""
+    import numpy as np
+
+    walls = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        h.radial_distribution(17.25, 256)
+        walls.append(time.perf_counter() - t0)
+    h.radial_distribution(17.25, 256, sample_cap=n_atoms)  # warm-up: staging sized for every atom
+    t0 = time.perf_counter()
+    counts, _, _, _ = h.radial_distribution(17.25, 256, sample_cap=n_atoms)
+    full = time.perf_counter() - t0
+    pairs = int(counts.sum())
+    return {"workload": f"g(r) of the resident state, 256 bins to r_max 17.25, {n_atoms} atoms",
+            "subsample": {"atoms": min(n_atoms, 8192), "ms": float(np.median(walls)) * 1e3},
+            "full": {"atoms": n_atoms, "ms": full * 1e3, "pairs_within_rmax": pairs,
+                     "pairs_per_s": pairs / full, "position_GB_per_s": 16.0 * n_atoms / full / 1e9},
+            "timing": "host wall clock around each synchronous gx_radial_distribution call"}
+
+
 def run_ticks(h, wl, cfg, steps: int, start_tick: int) -> int:
     """steps ticks through gx_step, with the workload's g(r) every gr_every ticks."""
     from genesis_b200 import elements as E
@@ -682,6 +706,12 @@ def ours_arm(args, dist):
             he.close()
         except Exception as e:  # noqa: BLE001
             extras["e2e_error"] = repr(e)
+
+        # g(r) of the resident state: the reference's subsampled call and the whole state
+        try:
+            extras["gr"] = gr_leg(h, u.n)
+        except Exception as e:  # noqa: BLE001
+            extras["gr_error"] = repr(e)
 
         # XYZ frame export of the resident state (export::write_frame)
         try:

@@ -154,6 +154,13 @@ __global__ void k_place(StateBuf b, uint32_t m, const uint32_t* __restrict__ key
 
 // Canonical half-shell enumeration with the exact check_pair test
 // (src/physics/grid.rs:201-225).  V::operator()(i, j, d) sees aux indices.
+// min_image1 for a difference of which only the length is used: within
+// 0.49 L the rounded quotient is below one half, round() gives zero and the
+// reference's d - L * 0 is d itself (up to the sign of a zero).
+__device__ __forceinline__ double near_image1(double d, double L) {
+    return fabs(d) <= xmul(0.49, L) ? d : min_image1(d, L);
+}
+
 template <class V>
 __global__ void k_pairs(GridGeom g, AuxSet a, double box0, double box1, double box2, double cd2, V visit) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -175,9 +182,9 @@ __global__ void k_pairs(GridGeom g, AuxSet a, double box0, double box1, double b
             }
             uint32_t hi = a.start[B + 1];
             for (uint32_t j = lo; j < hi; ++j) {
-                double dx = min_image1(xsub(xi, a.x[j]), box0);
-                double dy = min_image1(xsub(yi, a.y[j]), box1);
-                double dz = min_image1(xsub(zi, a.z[j]), box2);
+                double dx = near_image1(xsub(xi, a.x[j]), box0);
+                double dy = near_image1(xsub(yi, a.y[j]), box1);
+                double dz = near_image1(xsub(zi, a.z[j]), box2);
                 double d2 = xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
                 if (d2 >= cd2) continue;
                 double d = xsqrt(d2);
@@ -204,14 +211,33 @@ struct NeighborsVisit {
     }
 };
 
+// Up to this many bins, each block counts in shared memory and adds its
+// nonzero bins to the global counts once (integer sums: the same result).
+constexpr uint32_t kGrLocalBins = 1024;
+
 struct GrVisit {
     double r_max, dr;
     unsigned long long* counts;
     uint32_t nbins;
     int ta, tb;
     uint32_t* err;
-    __device__ void begin() const {}
-    __device__ void end() const {}
+    __device__ unsigned* local() const {
+        __shared__ unsigned hist[kGrLocalBins];
+        return hist;
+    }
+    __device__ void begin() const {
+        if (nbins > kGrLocalBins) return;
+        unsigned* h = local();
+        for (uint32_t k = threadIdx.x; k < nbins; k += blockDim.x) h[k] = 0u;
+        __syncthreads();
+    }
+    __device__ void end() const {
+        if (nbins > kGrLocalBins) return;
+        __syncthreads();
+        const unsigned* h = local();
+        for (uint32_t k = threadIdx.x; k < nbins; k += blockDim.x)
+            if (h[k]) atomicAdd(&counts[k], (unsigned long long)h[k]);
+    }
     __device__ void operator()(const AuxSet& a, uint32_t i, uint32_t j, double d) const {
         if (ta >= 0) {
             int x = a.elem[i], y = a.elem[j];
@@ -224,7 +250,10 @@ struct GrVisit {
             atomicOr(err, kErrBinRange);
             return;
         }
-        atomicAdd(&counts[bi], 1ull);
+        if (nbins <= kGrLocalBins)
+            atomicAdd(&local()[bi], 1u);
+        else
+            atomicAdd(&counts[bi], 1ull);
     }
 };
 
@@ -446,12 +475,6 @@ __global__ void k_bond_energy(const uint32_t* __restrict__ bonds, size_t nb, Sta
 // neighbour k, so that the chains of dependent loads run side by side.
 constexpr int kBucketLanes = 16;
 
-// min_image1 for a difference whose square is all that is used: within
-// 0.49 L the rounded quotient is below one half, round() gives zero and the
-// reference's d - L * 0 is d itself (up to the sign of a zero).
-__device__ __forceinline__ double near_image1(double d, double L) {
-    return fabs(d) <= xmul(0.49, L) ? d : min_image1(d, L);
-}
 static_assert(kBucketLanes >= 14, "one lane per half-shell cell and the own cell");
 
 struct BucketArgs {
