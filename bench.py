@@ -313,6 +313,26 @@ def gr_leg(h, n_atoms: int, reps: int = 3) -> dict:
             "timing": "host wall clock around each synchronous gx_radial_distribution call"}
 
 
+def lens_leg(h, k_bind: float) -> dict:
+    """The structure lenses on the resident state: friends-of-friends
+    (clusters, src/analysis/mod.rs:221-307) and the bound pairs
+    (bound_pairs_with_grid, src/analysis/pairs.rs:132-174).  Host wall clock
+    around each synchronous call, the second of two."""
+    out = {}
+    for name, call in (("fof", lambda: h.clusters()), ("bound_pairs", lambda: h.bound_pairs(k_bind))):
+        call()
+        t0 = time.perf_counter()
+        r = call()
+        ms = (time.perf_counter() - t0) * 1e3
+        out[name] = {"ms": ms}
+        if name == "fof":
+            out[name].update({k: r[1][k] for k in ("aggregates", "largest", "bound_pairs")})
+        else:
+            out[name]["pairs"] = int(len(r))
+    out["timing"] = "host wall clock around each synchronous call (labels or pairs copied back)"
+    return out
+
+
 def run_ticks(h, wl, cfg, steps: int, start_tick: int) -> int:
     """steps ticks through gx_step, with the workload's g(r) every gr_every ticks."""
     from genesis_b200 import elements as E
@@ -712,6 +732,12 @@ def ours_arm(args, dist):
             extras["gr"] = gr_leg(h, u.n)
         except Exception as e:  # noqa: BLE001
             extras["gr_error"] = repr(e)
+
+        # the structure lenses (FoF, bound pairs) on the resident state
+        try:
+            extras["lenses"] = lens_leg(h, cfg.bond_k_bind)
+        except Exception as e:  # noqa: BLE001
+            extras["lenses_error"] = repr(e)
 
         # XYZ frame export of the resident state (export::write_frame)
         try:
