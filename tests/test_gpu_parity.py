@@ -3,7 +3,7 @@
 Bit-exact: cell assignment, neighbour pair multisets, bound pairs, FoF labels,
 g(r) bin counts, kick/drift/wrap.  FP64 path: forces, energies, K and lambda
 within 1e-12 relative (norm-wise for vectors).  Mixed path: force relative RMS
-<= 1e-5, deterministic across runs.
+<= 1e-5 (the mixed path's accuracy bound), deterministic across runs.
 """
 from __future__ import annotations
 
