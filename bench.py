@@ -222,7 +222,7 @@ def hbm_peak() -> tuple[float, str]:
     hbm = measured_peaks().get("hbm_gbs")
     if hbm:
         return hbm, "MEASURED_PEAKS.json hbm_gbs (of measured)"
-    # the file is written by the driver of each run; else an earlier measurement on this pool
+    # without the measured file: a copy bandwidth measured earlier on the same B200 model
     return 6650.0, "fallback 6650 GB/s (of fallback: an earlier copy-bandwidth measurement)"
 
 

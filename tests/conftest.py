@@ -14,7 +14,7 @@ def pytest_configure(config):
 
 def _gpu_available() -> bool:
     try:
-        import torch  # noqa: F401  (only to ask the driver; the product does not use torch)
+        import torch  # noqa: F401  (only to ask the CUDA driver for a device; the product does not use torch)
         return torch.cuda.is_available()
     except Exception:
         return False
