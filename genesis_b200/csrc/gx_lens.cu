@@ -873,11 +873,17 @@ int gx_clusters(gx_handle* h, double bond_factor, uint32_t* labels, uint64_t sta
     GX_CUDA(h, cudaStreamSynchronize(h->stream));
     AuxPool& P = pool_of(h);
     if ((rc = ensure_pool(h, P, n, n))) return rc;
-    // max sigma over the particles present (analysis/mod.rs:236-238)
-    std::vector<uint8_t> el(n);
-    GX_CUDA(h, cudaMemcpy(el.data(), h->buf[h->cur].elem, n, cudaMemcpyDeviceToHost));
+    // max sigma over the particles present (analysis/mod.rs:236-238): the
+    // kind table of gx_set_state lists every element present, unless it
+    // overflowed, when the element column is read back
     double max_sigma = 0.0;
-    for (uint8_t t : el) max_sigma = std::fmax(max_sigma, h->p.sigma[t]);
+    if (h->nkinds <= kMaxKinds) {
+        for (int k = 0; k < h->nkinds; ++k) max_sigma = std::fmax(max_sigma, h->p.sigma[h->kind_elem[k]]);
+    } else {
+        std::vector<uint8_t> el(n);
+        GX_CUDA(h, cudaMemcpy(el.data(), h->buf[h->cur].elem, n, cudaMemcpyDeviceToHost));
+        for (uint8_t t : el) max_sigma = std::fmax(max_sigma, h->p.sigma[t]);
+    }
     double cutoff = std::fmax(std::fmax(bond_factor, 0.1) * max_sigma, 1e-9);
     int ok = 0;
     GridGeom g = make_grid(h->p.box, cutoff, &ok);
