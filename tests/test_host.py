@@ -223,3 +223,42 @@ int main(void) { printf("%zu %zu\\n", sizeof(orc_params), offsetof(orc_params, e
         subprocess.run(["gcc", f"-I{ROOT / 'oracle'}", str(c), "-o", str(exe)], check=True)
         got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     assert got == [ctypes.sizeof(OrcParams), OrcParams.enable_boundaries.offset]
+
+
+def test_scheduler_counts_executions_after_the_schedule():
+    """Scheduler::run adds its executions to StatsCollector.systems_run once
+    the whole schedule ran (src/scheduler/mod.rs:83-89), so a system sees the
+    previous ticks' count; the collector keeps a bounded history
+    (src/stats/mod.rs:194-201)."""
+    from genesis_b200.systems import Scheduler, StatsCollector, System, SystemContext, Time, World
+
+    seen = []
+
+    class Probe(System):
+        def name(self):
+            return "probe"
+
+        def run(self, ctx):
+            seen.append(ctx.stats.systems_run)
+            ctx.stats.record({"tick": ctx.time.tick})
+
+    class Noop(System):
+        def name(self):
+            return "noop"
+
+        def run(self, ctx):
+            pass
+
+    s = Scheduler()
+    s.add_system(Noop())
+    s.add_system(Probe())
+    z = np.zeros((0, 3))
+    w = World(pos=z, vel=z, acc=z, elem=np.zeros(0, np.uint8), mass=np.zeros(0), charge=np.zeros(0),
+              entity=np.zeros(0, np.uint32))
+    stats = StatsCollector(history_cap=3)
+    t = Time(0.1)
+    for _ in range(5):
+        t.advance()
+        s.run(SystemContext(w, {}, t, t.dt, stats))
+    assert seen == [0, 2, 4, 6, 8] and stats.systems_run == 10
+    assert [h["tick"] for h in stats.history] == [3, 4, 5] and stats.snapshot["tick"] == 5
