@@ -563,23 +563,24 @@ __global__ void __launch_bounds__(256) k_bound_buckets(GridGeom g, AuxSet a, dou
 // The same decisions with the candidates taken from the persistent neighbour
 // list, which holds every pair within r_c (> the bond cutoff) of the current
 // positions: each unordered pair once, from its lower sorted position.  No
-// bond grid is binned.  kBucketLanes lanes per atom take its entries in turn
-// (short chains of dependent gathers side by side).
+// bond grid is binned.  kListBoundLanes lanes per atom take its entries in
+// turn (short chains of dependent gathers side by side).
+constexpr int kListBoundLanes = 8;
 __global__ void __launch_bounds__(256) k_bound_from_list(StateBuf b, uint32_t n, NlView nv, double box0, double box1,
                                                          double box2, double cd2, BucketArgs v) {
     __shared__ double sig[kNElem];
     if (threadIdx.x < kNElem) sig[threadIdx.x] = v.sig[threadIdx.x];
     __syncthreads();
     const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t p = (uint32_t)(t / kBucketLanes);
-    const uint32_t lane = (uint32_t)(t % kBucketLanes);
+    const uint32_t p = (uint32_t)(t / kListBoundLanes);
+    const uint32_t lane = (uint32_t)(t % kListBoundLanes);
     if (p >= n) return;
     const double xi = b.x[p], yi = b.y[p], zi = b.z[p];
     const double si = sig[b.elem[p]];
     const uint32_t slot_i = b.slot[p];
     const uint32_t m = nv.cnt[p];
     if (m <= (uint32_t)nv.cap_nb) {
-        for (uint32_t e = lane; e < m; e += kBucketLanes) {
+        for (uint32_t e = lane; e < m; e += kListBoundLanes) {
             const uint32_t q = __ldg(nv.list + (size_t)e * nv.stride + p) & nv.idx_mask;
             if (q > p)
                 bound_candidate(xi, yi, zi, si, slot_i, b.x[q], b.y[q], b.z[q], sig[b.elem[q]], b.slot[q], box0, box1,
@@ -589,7 +590,7 @@ __global__ void __launch_bounds__(256) k_bound_from_list(StateBuf b, uint32_t n,
         const uint32_t c = nv.home[p];
         uint32_t cx, cy, cz;
         decode(nv.lg, c, cx, cy, cz);
-        for (uint32_t code = lane; code < 27; code += kBucketLanes) {
+        for (uint32_t code = lane; code < 27; code += kListBoundLanes) {
             const int ox = (int)(code % 3u) - 1, oy = (int)((code / 3u) % 3u) - 1, oz = (int)(code / 9u) - 1;
             const uint32_t B = encode(nv.lg, wrap_add(cx, ox, nv.lg.n[0]), wrap_add(cy, oy, nv.lg.n[1]),
                                       wrap_add(cz, oz, nv.lg.n[2]));
@@ -1066,7 +1067,7 @@ int bound_buckets_device(gx_handle* h, void** pool, double k_bind, uint32_t* buc
     if (bound_from_list(h, cutoff, g, &nv)) {
         prof_begin(h, "bound_pairs");
         if (n)
-            GX_LAUNCH(h, k_bound_from_list, nblk((size_t)n * kBucketLanes, 256), 256, h->buf[h->cur], n, nv,
+            GX_LAUNCH(h, k_bound_from_list, nblk((size_t)n * kListBoundLanes, 256), 256, h->buf[h->cur], n, nv,
                       h->p.box[0], h->p.box[1], h->p.box[2], cutoff * cutoff, v);
         prof_end(h, "bound_pairs");
         return GX_OK;
