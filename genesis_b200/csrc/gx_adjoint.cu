@@ -652,6 +652,7 @@ int gx_adjoint_forward(gx_handle* h, const gx_adjoint_spec* spec, double* potent
     int rc = GX_OK;
     if (!h->cap) return set_err(h, GX_ERR_STATE, "no state uploaded (call gx_set_state first)");
     if (h->n == 0) return set_err(h, GX_ERR_ARG, "the adjoint needs at least one atom");
+    if ((rc = settle_step_errors(h))) return rc;  // a queued step's error first: the word is cleared below
     h->nl_fresh = false;  // conservative: the passes below may reorder or move the resident state
     if (spec->nsteps < 1 || spec->checkpoint_every < 1) return set_err(h, GX_ERR_ARG, "nsteps and checkpoint_every must be >= 1");
     if (spec->gr_bins < 0 || spec->gr_bins > kAdjMaxBins) return set_err(h, GX_ERR_ARG, "gr_bins must be in [0, 512]");
@@ -720,7 +721,8 @@ int gx_adjoint_backward(gx_handle* h, const double* dl_dpotential, const double*
     AdjBuffers* A = static_cast<AdjBuffers*>(h->adj);
     if (!A || !A->ready) return set_err(h, GX_ERR_STATE, "call gx_adjoint_forward first");
     if (h->n != A->n) return set_err(h, GX_ERR_STATE, "atom count changed since gx_adjoint_forward");
-    int rc = GX_OK;
+    int rc = settle_step_errors(h);
+    if (rc) return rc;
     const uint32_t n = (uint32_t)A->n;
     const size_t cap = A->cap;
     const int T = A->T, K = A->K;

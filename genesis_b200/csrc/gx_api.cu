@@ -280,6 +280,11 @@ int take_step_errors(gx_handle* h) {
     h->step_errs_pending = false;
     return step_error(h, *h->herr);
 }
+int settle_step_errors(gx_handle* h) {
+    if (!h->step_errs_pending) return GX_OK;
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    return take_step_errors(h);
+}
 }  // namespace gx
 
 namespace {
@@ -625,6 +630,7 @@ int gx_forces(gx_handle* h, double* potential, double* bond_energy, uint64_t* pa
     int rc = require_state(h);
     if (rc) return rc;
     if ((rc = check_kinds(h))) return rc;
+    if ((rc = settle_step_errors(h))) return rc;  // the pass reads and clears the error word
     if (h->n == 0) {  // systems/forces.rs:201-203
         if (potential) *potential = 0.0;
         if (bond_energy) *bond_energy = 0.0;

@@ -323,6 +323,10 @@ void collide_free(gx_handle* h);
 void export_free(gx_handle* h);  // gx_export.cu
 // After a wait on the stream: the error word an asynchronous gx_step left.
 int take_step_errors(gx_handle* h);
+// Waits for a queued asynchronous gx_step and reports its error word.  Every
+// call that clears or consumes the device error word runs this first, so a
+// step's error is never cleared before it is reported.
+int settle_step_errors(gx_handle* h);
 
 // Read-only view of the persistent neighbour list (gx_nlist.cu) for the
 // passes that can take their candidates from it.  Entry e of atom p (sorted

@@ -670,6 +670,7 @@ int gr_common(gx_handle* h, int ta, int tb, double r_max_in, size_t nbins_in, si
     int rc = require(h);
     if (rc) return rc;
     if (!counts) return GX_ERR_ARG;
+    if ((rc = settle_step_errors(h))) return rc;  // this call clears the error word below
     size_t nbins = nbins_in < 1 ? 1 : (nbins_in > 65536 ? 65536 : nbins_in);
     const double* box = h->p.box;
     double half_min = std::fmin(std::fmin(box[0], box[1]), box[2]) * 0.5;

@@ -805,6 +805,8 @@ int nl_rebuilds(gx_handle* h, uint64_t* out) {
 // (`reps` launches each) and keeps the fastest.  The state is not touched:
 // the pass only writes the force scratch, which the next tick overwrites.
 int nl_tune_tpp(gx_handle* h, int reps) {
+    int rs = settle_step_errors(h);  // the error word is cleared after the timing below
+    if (rs) return rs;
     NlState* s = nl_of(h);
     if (!s->list || !s->cap || h->n == 0) return GX_OK;
     const uint32_t n = (uint32_t)h->n;

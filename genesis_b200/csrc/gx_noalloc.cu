@@ -22,7 +22,9 @@
 // the GPU (two host threads at once on one device) race on it.  The first
 // call on a device looks up the array's device address with
 // cudaGetSymbolAddress while that device is current; make that first call
-// before any stream capture begins.
+// before any stream capture begins.  The address is kept for the life of the
+// process (a device reset after the first call is not supported).  Each call
+// runs on the legacy default stream and waits for it.
 #include <cmath>
 #include <cstring>
 
@@ -44,8 +46,9 @@ constexpr size_t kOffAos = 0;                                      // 3 f64 per 
 constexpr size_t kOffX = kOffAos + 3 * 8 * kNaAtoms;               // sorted x, y, z
 constexpr size_t kOffKey = kOffX + 3 * 8 * kNaAtoms;               // key per sampled atom
 constexpr size_t kOffSKey = kOffKey + 4 * kNaAtoms;                // key, sorted
-constexpr size_t kOffPerm = kOffSKey + 4 * kNaAtoms;
-constexpr size_t kOffCount = kOffPerm + 4 * kNaAtoms;              // kNaCells + 1
+constexpr size_t kOffPerm = kOffSKey + 4 * kNaAtoms;               // sample index per slot, unordered in a cell
+constexpr size_t kOffOrder = kOffPerm + 4 * kNaAtoms;              // the same, ascending in each cell
+constexpr size_t kOffCount = kOffOrder + 4 * kNaAtoms;             // kNaCells + 1
 constexpr size_t kOffStart = kOffCount + 4 * (kNaCells + 64);      // kNaCells + 1
 constexpr size_t kOffFill = kOffStart + 4 * (kNaCells + 64);       // kNaCells
 constexpr size_t kOffSums = kOffFill + 4 * (kNaCells + 64);        // scan tile sums
@@ -61,7 +64,7 @@ unsigned char* g_scratch_addr[kMaxDevices] = {};
 struct NaView {
     double* aos;
     double *x, *y, *z;
-    uint32_t *key, *skey, *perm, *count, *start, *fill, *sums, *err;
+    uint32_t *key, *skey, *perm, *order, *count, *start, *fill, *sums, *err;
     unsigned long long* bins;
 };
 
@@ -74,6 +77,7 @@ NaView view(unsigned char* s) {
     v.key = (uint32_t*)(s + kOffKey);
     v.skey = (uint32_t*)(s + kOffSKey);
     v.perm = (uint32_t*)(s + kOffPerm);
+    v.order = (uint32_t*)(s + kOffOrder);
     v.count = (uint32_t*)(s + kOffCount);
     v.start = (uint32_t*)(s + kOffStart);
     v.fill = (uint32_t*)(s + kOffFill);
@@ -143,24 +147,24 @@ __global__ void na_scatter(NaView v, uint32_t m) {
     v.perm[v.start[c] + atomicAdd(&v.fill[c], 1u)] = q;
 }
 
-__global__ void na_segsort(NaView v, uint32_t ncell) {
-    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncell) return;
-    uint32_t lo = v.start[c], hi = v.start[c + 1];
-    for (uint32_t a = lo + 1; a < hi; ++a) {
-        uint32_t x = v.perm[a], b = a;
-        while (b > lo && v.perm[b - 1] > x) {
-            v.perm[b] = v.perm[b - 1];
-            --b;
-        }
-        v.perm[b] = x;
-    }
+// Makes the scatter deterministic: sample q goes to start[c] + (the number of
+// samples of its cell with a smaller index), so each cell lists its samples
+// in ascending order.  One thread per sample reads its cell's segment, which
+// keeps a cell that holds most of the sample (a droplet) parallel: the work
+// is the sum of the squared cell sizes spread over all samples.
+__global__ void na_rank(NaView v, uint32_t m) {
+    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= m) return;
+    uint32_t c = v.key[q];
+    uint32_t lo = v.start[c], hi = v.start[c + 1], r = 0;
+    for (uint32_t b = lo; b < hi; ++b) r += v.perm[b] < q ? 1u : 0u;
+    v.order[lo + r] = q;
 }
 
 __global__ void na_gather(NaView v, uint32_t m) {
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= m) return;
-    uint32_t q = v.perm[p];
+    uint32_t q = v.order[p];
     v.x[p] = v.aos[3 * q];
     v.y[p] = v.aos[3 * q + 1];
     v.z[p] = v.aos[3 * q + 2];
@@ -229,6 +233,9 @@ extern "C" int gx_radial_distribution_noalloc(size_t n, const double* pos, const
         step = n / 8192 + 1;
         m = n / step;
     }
+    // A non-sticky error an earlier, unrelated CUDA call left on this thread
+    // is dropped here, so that the checks below see only this call's errors.
+    cudaGetLastError();
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return GX_ERR_CUDA;
     if (!g_scratch_addr[dev]) {
@@ -240,15 +247,26 @@ extern "C" int gx_radial_distribution_noalloc(size_t n, const double* pos, const
     NaView v = view(g_scratch_addr[dev]);
     cudaStream_t s = 0;
     uint32_t um = (uint32_t)m, nc = g.ncell;
-    if (cudaMemsetAsync(v.count, 0, 4 * ((size_t)nc + 1), s) != cudaSuccess) return GX_ERR_CUDA;
-    cudaMemsetAsync(v.fill, 0, 4 * (size_t)nc, s);
-    cudaMemsetAsync(v.err, 0, 4, s);
-    cudaMemsetAsync(v.bins, 0, 8 * nbins, s);
+    // Every enqueue is checked; after a failed one the call waits for what it
+    // already queued on the stream before it returns.
+    bool bad = false;
+    auto chk = [&](cudaError_t e) {
+        if (e != cudaSuccess) bad = true;
+        return !bad;
+    };
+    auto fail = [&]() {
+        cudaStreamSynchronize(s);
+        cudaGetLastError();
+        return GX_ERR_CUDA;
+    };
+    chk(cudaMemsetAsync(v.count, 0, 4 * ((size_t)nc + 1), s)) && chk(cudaMemsetAsync(v.fill, 0, 4 * (size_t)nc, s)) &&
+        chk(cudaMemsetAsync(v.err, 0, 4, s)) && chk(cudaMemsetAsync(v.bins, 0, 8 * nbins, s));
+    if (bad) return fail();
     if (m) {
         // every step-th AoS record of the host array into the scratch sample
-        if (cudaMemcpy2DAsync(v.aos, 24, pos, 24 * step, 24, m, cudaMemcpyHostToDevice, s) != cudaSuccess)
-            return GX_ERR_CUDA;
+        if (!chk(cudaMemcpy2DAsync(v.aos, 24, pos, 24 * step, 24, m, cudaMemcpyHostToDevice, s))) return fail();
         na_keys<<<nb(m, 256), 256, 0, s>>>(g, v, um);
+        if (!chk(cudaGetLastError())) return fail();
     }
     uint32_t nscan = nc + 1;
     unsigned tiles = (nscan + kNaTile - 1) / kNaTile;
@@ -257,15 +275,18 @@ extern "C" int gx_radial_distribution_noalloc(size_t n, const double* pos, const
         na_scan<<<1, kNaScanThreads, 0, s>>>(v.sums, v.sums, tiles, nullptr);
         na_scan_add<<<nb(nscan, 256), 256, 0, s>>>(v.start, nscan, v.sums);
     }
+    if (!chk(cudaGetLastError())) return fail();
     if (m) {
         na_scatter<<<nb(m, 256), 256, 0, s>>>(v, um);
-        na_segsort<<<nb(nc, 128), 128, 0, s>>>(v, nc);
+        na_rank<<<nb(m, 128), 128, 0, s>>>(v, um);
         na_gather<<<nb(m, 256), 256, 0, s>>>(v, um);
         na_pairs<<<nb(m, 128), 128, 0, s>>>(g, v, um, r_max * r_max, r_max, dr, (uint32_t)nbins);
+        if (!chk(cudaGetLastError())) return fail();
     }
     uint32_t err = 0;
-    cudaMemcpyAsync(counts, v.bins, 8 * nbins, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(&err, v.err, 4, cudaMemcpyDeviceToHost, s);
+    chk(cudaMemcpyAsync(counts, v.bins, 8 * nbins, cudaMemcpyDeviceToHost, s)) &&
+        chk(cudaMemcpyAsync(&err, v.err, 4, cudaMemcpyDeviceToHost, s));
+    if (bad) return fail();
     if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) return GX_ERR_CUDA;
     if (r_max_out) *r_max_out = r_max;
     if (dr_out) *dr_out = dr;

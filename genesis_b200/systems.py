@@ -10,13 +10,12 @@ live in a :class:`World` on the host; the GPU systems share one
 :class:`GpuWorld` (one device handle) and sync columns lazily, so a tick of
 GPU systems never crosses PCIe unless a host system touches the columns.
 
-Host-only logic that is part of the path stays here: the pair tracker and the
-persistence threshold of the bond observation (src/analysis/pairs.rs:43-109,
-src/systems/bonds.rs:73-185).
+The bond observation's pair tracker and persistence threshold
+(src/analysis/pairs.rs:43-109, src/systems/bonds.rs:73-185) run on the device
+(gx_bond_observe); :class:`GpuBondObservation` only reads their summary.
 """
 from __future__ import annotations
 
-import math
 import time
 from dataclasses import dataclass, field
 
@@ -304,55 +303,6 @@ class GpuStructure(_GpuSystem):
         _, st = self.gpu.h.clusters(E.BOND_FACTOR)
         st["tick"] = ctx.time.tick
         ctx.resources["StructureStats"] = st
-
-
-class PairTracker:
-    """Episode tracking with debounce (src/analysis/pairs.rs:43-109).
-    Pairs are (a, b) entity tuples with a < b."""
-
-    def __init__(self, debounce: int):
-        self.debounce = max(int(debounce), 1)
-        self.open: dict = {}
-        self.missing: dict = {}
-        self.completed: list = []
-
-    def track_tick(self, bound):
-        current = set(bound)
-        for p in current:
-            self.missing.pop(p, None)
-            self.open[p] = self.open.get(p, 0) + 1
-        for p in [p for p in self.open if p not in current]:
-            self.missing[p] = self.missing.get(p, 0) + 1
-            if self.missing[p] >= self.debounce:
-                ticks = self.open.pop(p)
-                del self.missing[p]
-                self.completed.append((p, ticks))
-
-    def close_all(self):
-        for p, t in self.open.items():
-            self.completed.append((p, t))
-        self.open.clear()
-        self.missing.clear()
-
-    def open_count(self) -> int:
-        return len(self.open)
-
-
-def well_curvature(eps: float, sigma: float) -> float:  # physics/forces.rs:194-196
-    return 72.0 * 2.0 ** (-1.0 / 3.0) * eps / (sigma * sigma)
-
-
-def vib_period(eps: float, sigma: float, mu: float) -> float:  # physics/forces.rs:201-203
-    return 2.0 * math.pi * math.sqrt(mu / well_curvature(eps, sigma))
-
-
-def persistence_ticks(cfg, ea: int, eb: int) -> int:
-    """ceil(min_periods * vib_period / dt) for a species pair (src/systems/bonds.rs:94-99)."""
-    ma, mb = E.MASS[ea], E.MASS[eb]
-    mu = ma * mb / (ma + mb)
-    eps = cfg.thermal_constant * math.sqrt(cfg.epsilon_k[ea] * cfg.epsilon_k[eb])
-    sig = 0.5 * (cfg.sigma[ea] + cfg.sigma[eb])
-    return math.ceil(max(cfg.bond_min_periods, 0.1) * vib_period(eps, sig, mu) / cfg.dt)
 
 
 class GpuBondObservation(_GpuSystem):

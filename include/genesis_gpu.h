@@ -215,8 +215,11 @@ int gx_radial_distribution_between(gx_handle* h, uint8_t ta, uint8_t tb, double 
  * may hold at most 65536 cells (GX_ERR_CAPACITY otherwise); nbins is clamped
  * to [1, 65536] like the reference; the sample never exceeds 8192 atoms.
  * The first call on a device looks up the array's address and should come
- * before any stream capture.  Calls share the array: calls that overlap on
- * the GPU race. */
+ * before any stream capture; the address is kept for the life of the
+ * process, so a device reset (cudaDeviceReset) after that first call is not
+ * supported.  Every call runs on the legacy default stream and waits for it,
+ * so it must not run while another thread captures a graph in global mode.
+ * Calls share the array: calls that overlap on the GPU race. */
 int gx_radial_distribution_noalloc(size_t n, const double* pos, const double box[3], double r_max,
                                    size_t nbins, uint64_t* counts, double* bins, double* r_max_out,
                                    double* dr_out);

@@ -10,6 +10,7 @@ values are restated as data.  When the reference tree is present, each entry's
 from __future__ import annotations
 
 import argparse
+import os
 import json
 from pathlib import Path
 
@@ -105,13 +106,16 @@ def verify(root: Path) -> list[str]:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference-root", default="/root/reference")
+    ap.add_argument("--reference-root", default=os.environ.get("GENESIS_REFERENCE_ROOT"),
+                    help="checkout of the reference repository whose text each citation is checked "
+                         "against (or set GENESIS_REFERENCE_ROOT)")
     a = ap.parse_args()
+    if not a.reference_root:
+        raise SystemExit("give --reference-root or set GENESIS_REFERENCE_ROOT")
     root = Path(a.reference_root)
-    if root.exists():
-        bad = verify(root)
-        if bad:
-            raise SystemExit("\n".join(bad))
+    bad = verify(root)
+    if bad:
+        raise SystemExit("\n".join(bad))
     (HERE / "reference_known_answers.json").write_text(json.dumps({"cases": CASES}, indent=1) + "\n")
 
 

@@ -17,7 +17,6 @@ from genesis_b200 import config as G
 from genesis_b200 import elements as E
 from genesis_b200 import synth
 from genesis_b200 import workloads as W
-from genesis_b200.systems import PairTracker, persistence_ticks
 
 ROOT = Path(__file__).resolve().parent.parent
 CASES = {c["id"]: c for c in json.loads((ROOT / "tests/golden/reference_known_answers.json").read_text())["cases"]}
@@ -81,34 +80,6 @@ def test_element_names():
 
 
 # ---------------------------------------------------------------- tracker and persistence
-
-
-def test_tracker_debounce():
-    c = CASES["tracker_debounce"]
-    p = (1, 2)
-    t = PairTracker(1)
-    for _ in range(c["bound_ticks"]):
-        t.track_tick([p])
-    t.track_tick([])
-    assert len(t.completed) == 1 and t.completed[0][1] == c["bound_ticks"] and t.open_count() == 0
-    for _ in range(c["rebind_ticks"]):
-        t.track_tick([p])
-    t.close_all()
-    assert len(t.completed) == 2 and t.completed[1][1] == c["rebind_ticks"]
-    t2 = PairTracker(3)
-    for _ in range(c["bound_ticks"]):
-        t2.track_tick([p])
-    t2.track_tick([])
-    assert len(t2.completed) == 0 and t2.open_count() == 1
-    t2.track_tick([])
-    t2.track_tick([])
-    assert len(t2.completed) == 1 and t2.completed[0][1] == c["bound_ticks"]
-
-
-def test_persistence_threshold_is_per_pair():
-    cfg = G.default_config()
-    h, fe = E.by_name("H"), E.by_name("Fe")
-    assert persistence_ticks(cfg, h, h) < persistence_ticks(cfg, fe, fe)
 
 
 def test_bond_debounce_constant():

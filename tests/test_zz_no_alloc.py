@@ -44,6 +44,36 @@ def test_noalloc_gr_matches_allocating_entry_point_twice(gpu):
         h.close()
 
 
+def test_noalloc_gr_clustered_sample_matches_allocating_entry_point(gpu):
+    """A droplet: 6,000 of 8,000 atoms inside one cell of the g(r) grid.
+
+    Each cell lists its samples in ascending order, ranked in parallel, so a
+    cell that holds most of the sample stays fast; the counts still equal the
+    allocating entry point's on two calls in a row."""
+    from genesis_b200._lib import Handle, radial_distribution_noalloc
+    from genesis_b200 import synth
+    wl = W.C1.scaled(20)
+    cfg = wl.config()
+    u = wl.generate()
+    L = cfg.size[0]
+    rng = np.random.default_rng(5)
+    k = 6000
+    d = rng.normal(size=(k, 3))
+    d *= (rng.random(k) ** (1.0 / 3.0) * 4.0 / np.linalg.norm(d, axis=1))[:, None]
+    pos = u.pos.copy()
+    pos[:k] = 0.25 * L + d  # radius 4 around one point, inside a cell of edge L/2
+    u2 = synth.Universe(box=u.box, pos=pos, vel=u.vel, elem=u.elem, charge=u.charge, mass=u.mass,
+                        entity=u.entity)
+    with Handle(cfg, "fp64") as h:
+        h.set_universe(u2)
+        p_dev, _, _ = h.get_state()
+        c_ref, b_ref, _, _ = h.radial_distribution(0.5 * L, 128, E.G_SAMPLE_CAP)
+    for _ in range(2):
+        counts, bins, _, _ = radial_distribution_noalloc(p_dev, cfg.size, 0.5 * L, 128)
+        assert np.array_equal(counts, c_ref)
+        assert np.array_equal(bins, b_ref)
+
+
 def test_noalloc_gr_rejects_a_grid_beyond_its_limit(gpu):
     from genesis_b200._lib import GxError, radial_distribution_noalloc
     pos = np.zeros((10, 3))
