@@ -42,13 +42,30 @@ FLOP_PER_PAIR_LJC_NOV = 71
 # the arrays the kernel must touch; FP64 state, u8 element/kind, u32 ids).
 BYTES_PER_ATOM = {
     "kick": 72, "drift": 72, "wrap": 48, "cell_keys": 28, "cell_count": 4, "cell_scan": 0,
-    "cell_scatter": 16, "reorder": 220, "stage_pos4": 45, "kinetic": 32,
+    # scatter: read key, read the cell's start, write the slot; segment sort:
+    # read and write the slot
+    "cell_scatter": 12, "cell_segsort": 8, "reorder": 220, "stage_pos4": 45, "kinetic": 32,
     # list path: fused kick + drift + wrap + FP32 staging + displacement test
     # (read x v a 72, kind 1, home cell 4, reference float4 16; write x v 48,
     # float4 16), and fused F -> a + kick + K (read F 24, v 24, 1/m 8, m 8;
     # write a 24, v 24)
     "nl_advance": 157, "nl_finish": 112,
+    # list rebuild: the sorted state copied back (12 f64 columns, 2 u8, 1 u32,
+    # read and written), the staging (read x y z 24, kind 1, home 4; write
+    # the float4 and its reference copy 32); the list build's own bytes
+    # depend on the entries it writes (list_build_bytes_per_atom)
+    "nl_copy": 204, "nl_stage": 61,
 }
+# kernels that run only on ticks that rebuild the neighbour list
+REBUILD_KERNELS = ("cell_keys", "cell_count", "cell_scan", "cell_scatter", "cell_segsort", "reorder", "nl_copy",
+                   "nl_stage", "nl_build")
+
+
+def list_build_bytes_per_atom(entries_per_atom: float) -> float:
+    """k_nl_build: read the atom's float4 16 and home cell 4, write its count
+    4 and its list entries 4 each; the candidates it tests are L1/L2 hits of
+    the same float4 array."""
+    return 24.0 + 4.0 * entries_per_atom
 
 
 def parse():
@@ -64,7 +81,7 @@ def parse():
                     help="fix the mixed pair-pass variant instead of autotuning (profiling only)")
     ap.add_argument("--skin", type=float, default=-1.0,
                     help="neighbour-list skin in length units instead of 0.1 r_c (profiling only; 0 = rebuild every tick)")
-    ap.add_argument("--leg", default="", choices=["", "ionic", "accuracy", "adjoint", "xyz", "sweep"],
+    ap.add_argument("--leg", default="", choices=["", "ionic", "accuracy", "adjoint", "xyz", "sweep", "c1"],
                     help="run one extra leg alone and print its JSON (profiling only)")
     ap.add_argument("--leg-steps", type=int, default=0, help="ticks of the --leg run (0: the workload's own)")
     return ap.parse_args()
@@ -333,8 +350,13 @@ def lens_leg(h, k_bind: float) -> dict:
     return out
 
 
-def run_ticks(h, wl, cfg, steps: int, start_tick: int) -> int:
-    """steps ticks through gx_step, with the workload's g(r) every gr_every ticks."""
+def run_ticks(h, wl, cfg, steps: int, start_tick: int, record: bool = True) -> int:
+    """steps ticks through gx_step, with the workload's g(r) every gr_every
+    ticks.  With `record` every tick records K, V, lambda and the in-cutoff
+    pair count on the device (the reference computes the potential every
+    tick, src/systems/forces.rs:347, for StatsSystem,
+    src/systems/aggregate.rs:86-143); without it the pair pass leaves the
+    potential and the pair count out."""
     from genesis_b200 import elements as E
 
     t = start_tick
@@ -344,7 +366,7 @@ def run_ticks(h, wl, cfg, steps: int, start_tick: int) -> int:
         k = steps - done
         if wl.gr_every:
             k = min(k, wl.gr_every - (t % wl.gr_every))
-        h.step(k, stats=False, graph=True)
+        h.step(k, stats=record, graph=True)
         done += k
         t += k
         if wl.gr_every and t % wl.gr_every == 0:
@@ -404,6 +426,53 @@ def accuracy_leg(dev: int, steps: int = 10000) -> dict:
                          "E0": float(E[0]), "E_end": float(E[-1])}
     out["drift_ratio_mixed_over_fp64"] = abs(out["mixed"]["drift_rel"]) / max(abs(out["fp64"]["drift_rel"]), 1e-300)
     out["gr_L1_mixed_vs_fp64"] = float(np.abs(hists["mixed"] - hists["fp64"]).sum())
+    return out
+
+
+def c1_leg(dev: int, cpu: bool, steps: int = 1000, cpu_budget_s: float = 8.0) -> dict:
+    """Throughput on the C1 workload (4,096 atoms, 16^3 lattice, LJ only,
+    60 K NVE, 1,000 ticks; the configuration the reference runs on its CPU
+    today): the mixed path and the plain FP64 path through gx_step as captured
+    ticks that record K, V and pairs every tick, and with `cpu` the oracle's
+    threaded restatement of the reference tick on the host cores over a
+    bounded sample of the same run."""
+    from genesis_b200 import workloads as W
+    from genesis_b200._lib import Handle
+
+    wl = W.C1
+    cfg, u = wl.config(), wl.generate()
+    out = {"workload": f"{wl.name}: {u.n} atoms, LJ, 60 K NVE, {steps} ticks",
+           "timing": "CUDA events around gx_step(steps) of captured ticks, after 5 warm-up ticks"}
+    for prec in ("mixed", "fp64"):
+        with Handle(cfg, prec, dev) as h:
+            h.set_universe(u)
+            picked = None
+            if prec == "mixed":
+                picked, _ = h.autotune(reps=3)  # state unchanged
+            h.step(5, stats=True, graph=True)
+            h.synchronize()
+            h.mark(0)
+            h.step(steps, stats=True, graph=True)
+            h.mark(1)
+            ms = h.elapsed_ms(0, 1)
+            out[prec] = {"value": u.n * steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps,
+                         "kernel_variant": picked}
+    out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    if cpu:
+        from oracle import oracle
+
+        threads = os.cpu_count() or 1
+        p, v, a = u.pos, u.vel, None
+        ticks, el = 0, 0.0
+        while (el < cpu_budget_s or ticks == 0) and ticks < steps:
+            t0 = time.perf_counter()
+            p, v, a, _ = oracle.ticks(cfg, p, v, a, u.elem, u.charge, u.mass, 10, nthreads=threads)
+            el += time.perf_counter() - t0
+            ticks += 10
+        out["cpu_baseline"] = {"value": u.n * ticks / el, "unit": UNIT, "cores": threads, "kind": "port",
+                               "sample": f"the first {ticks} ticks of the run ({el:.1f} s): C++ restatement of the "
+                                         f"reference rayon tick on {threads} host threads"}
+        out["mixed_over_cpu"] = out["mixed"]["value"] / out["cpu_baseline"]["value"]
     return out
 
 
@@ -531,6 +600,32 @@ def ionic_leg(dev: int, cpu: bool, steps: int | None = None, cpu_budget_s: float
     out["potential_rel_err_vs_fp64"] = abs(Vm - V64) / abs(V64)
     out["bond_energy_rel_err_vs_fp64"] = abs(Vbm - Vb64) / abs(Vb64) if Vb64 else None
     out["bonds_in_accuracy_state"] = int(len(bonds))
+    # With the workload's persistence (10 vibration periods, about 3,200
+    # ticks of one uninterrupted episode) no bond forms at 300 K.  To measure
+    # the spring's error as well, the same system is observed with the
+    # reference's floor of 0.1 periods (bonds persist after ~32 ticks).
+    mp_fast = 0.1
+    with Handle(cfg, "mixed", dev) as h:
+        h.set_universe(u)
+        for t in range(1, 121):
+            h.step(1, stats=False, graph=True)
+            ob = h.bond_observe(kb, mp_fast, t)
+        (pos, vel, _), bonds = h.get_state(), h.get_bonds()
+    res = {}
+    for prec in ("mixed", "fp64"):
+        with Handle(cfg, prec, dev) as h:
+            h.set_state(pos, vel, u.elem, charge=u.charge, mass=u.mass, entity=u.entity)
+            h.set_bonds(bonds)
+            V, Vb, _ = h.forces()
+            res[prec] = (h.get_state()[2], V, Vb)
+    am, Vm, Vbm = res["mixed"]
+    a64, V64, Vb64 = res["fp64"]
+    out["with_bonds"] = {"min_periods": mp_fast, "ticks": 120, "bonds": int(len(bonds)),
+                         "bonds_formed": ob["bonds_formed"],
+                         "force_rel_rms_vs_fp64": float(np.linalg.norm(am - a64) / np.linalg.norm(a64)),
+                         "potential_rel_err_vs_fp64": abs(Vm - V64) / abs(V64),
+                         "bond_energy_rel_err_vs_fp64": abs(Vbm - Vb64) / abs(Vb64) if Vb64 else None,
+                         "bond_energy": Vb64}
     if cpu:
         from oracle import oracle
 
@@ -602,7 +697,7 @@ def ours_arm(args, dist):
     clocks.start()
     l0 = h.launches
     h.mark(0)
-    tick = run_ticks(h, wl, cfg, K, tick)
+    tick = run_ticks(h, wl, cfg, K, tick)  # the reference's full tick: K, V and pairs every tick
     h.mark(1)
     ms = h.elapsed_ms(0, 1)
     clk = clocks.stop()
@@ -612,22 +707,35 @@ def ours_arm(args, dist):
     dist.barrier()
     ms_max = dist.max(ms)
     value = dist.world * u.n * K / (ms_max * 1e-3)
+    # the same ticks with the energy-free pair pass (nothing recorded)
+    h.mark(2)
+    tick = run_ticks(h, wl, cfg, K, tick, record=False)
+    h.mark(3)
+    ms_nov = dist.max(h.elapsed_ms(2, 3))
 
-    # per-kernel device times over a profiled pass of the same (non-recording)
-    # ticks; the in-cutoff pair count from one recorded tick
+    # per-kernel device times over a profiled pass of the same (recording,
+    # eagerly launched) ticks; the in-cutoff pair count from one recorded tick
     pairs = float(h.step(1, stats=True)["pairs"][0])
     h.profile(True)
-    h.step(min(K, 50), stats=False)
+    h.step(min(K, 50), stats=True)
     prof = h.profile_read(reset=True)
+    # the rebuild kernels timed on ticks that each rebuild (setting the skin
+    # again forces one), so that no launch of them returns at the rebuild gate
+    skin_now, _ = h.list_config()
+    n_rb = 8
+    rbp0 = h.list_rebuilds()
+    for _ in range(n_rb):
+        h.set_list_skin(skin_now)
+        h.step(1, stats=True)
+    rb_ran = h.list_rebuilds() - rbp0
+    prof_rb = h.profile_read(reset=True)
     h.profile(False)
+    entries, overflowed = h.list_stats()
     force_k = "force_nl" if "force_nl" in prof else "force_mixed"
     f_launch, f_ms = prof.get(force_k, (1, float("nan")))
     force_ms = f_ms / max(f_launch, 1)
-    tot_ms = sum(v[1] for v in prof.values())
-    if force_k == "force_nl":
-        flop_pp = FLOP_PER_PAIR_LJC_NOV if cfg.enable_electrostatics else FLOP_PER_PAIR_LJ_NOV
-    else:
-        flop_pp = FLOP_PER_PAIR_LJC if cfg.enable_electrostatics else FLOP_PER_PAIR_LJ
+    tot_ms = sum(v[1] for k, v in prof.items() if k != "nl_rebuild")
+    flop_pp = FLOP_PER_PAIR_LJC if cfg.enable_electrostatics else FLOP_PER_PAIR_LJ
     achieved = pairs * flop_pp / (force_ms * 1e-3) / 1e12
     try:
         peak = _lib.measure_fp32_peak(dev)
@@ -642,23 +750,43 @@ def ours_arm(args, dist):
                 "unit": "L1/TEX throughput, fraction of peak (ncu)", "frac": l1,
                 "note": "the pass is bound by its neighbour gathers and far-end integer reductions in L1/TEX, "
                         "not by the FP32 pipe (profiles/k_nl_force__c3_262144_atoms.txt)"},
-            "flop_per_launch": pairs * flop_pp, "pairs_per_launch": pairs, "launch_ms": force_ms,
-            "share_of_step": f_ms / tot_ms if tot_ms else None}
+            "flop_per_launch": pairs * flop_pp, "flop_per_pair": flop_pp, "pairs_per_launch": pairs,
+            "launch_ms": force_ms, "share_of_step": f_ms / tot_ms if tot_ms else None,
+            "timing": "CUDA events around each launch of the profiled eager ticks (energy-carrying pass, as "
+                      "in the timed ticks)"}
     hbm, hbm_src = hbm_peak()
+    epa = entries / u.n if u.n else 0.0
     mem = {}
-    for k, (nl, kms) in prof.items():
-        if k in BYTES_PER_ATOM and nl and BYTES_PER_ATOM[k]:
-            gbs = BYTES_PER_ATOM[k] * u.n / (kms / nl * 1e-3) / 1e9
-            mem[k] = {"launch_ms": kms / nl, "GB/s": gbs, "frac": gbs / hbm if hbm else None,
-                      "share": kms / tot_ms if tot_ms else None}
-    top_mem = max(mem.items(), key=lambda kv: kv[1]["launch_ms"] * prof[kv[0]][0]) if mem else None
+    for src, keys in ((prof, ("nl_advance", "nl_finish", "kick", "drift", "wrap", "kinetic", "stage_pos4")),
+                      (prof_rb, REBUILD_KERNELS)):
+        for k in keys:
+            if k not in src or not src[k][0]:
+                continue
+            nl, kms = src[k]
+            bpa = list_build_bytes_per_atom(epa) if k == "nl_build" else BYTES_PER_ATOM.get(k, 0)
+            if not bpa:
+                continue
+            gbs = bpa * u.n / (kms / nl * 1e-3) / 1e9
+            mem[k] = {"launch_ms": kms / nl, "bytes_per_atom": bpa, "GB/s": gbs, "frac": gbs / hbm if hbm else None,
+                      "launches": "every tick" if src is prof else "rebuild ticks only (each timed launch ran)"}
+    every = {k: v for k, v in mem.items() if v["launches"] == "every tick"}
+    top_mem = max(every.items(), key=lambda kv: kv[1]["launch_ms"]) if every else None
     roof_hbm = None
     if top_mem:
         roof_hbm = {"kernel": top_mem[0], "bound": "hbm", "achieved": top_mem[1]["GB/s"], "peak": hbm,
                     "unit": "GB/s", "frac": top_mem[1]["frac"], "peak_source": hbm_src,
                     "traffic": ncu_traffic(top_mem[0])}
+    roof_rebuild = None
+    if "nl_rebuild" in prof_rb and rb_ran:
+        rb_ms = prof_rb["nl_rebuild"][1] / max(prof_rb["nl_rebuild"][0], 1)
+        rb_bytes = sum(v["bytes_per_atom"] for k, v in mem.items() if k in REBUILD_KERNELS) * u.n
+        roof_rebuild = {"kernel": "nl_rebuild (the whole rebuild: keys, sort, reorder, copy, staging, list build)",
+                        "bound": "hbm", "achieved": rb_bytes / (rb_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                        "frac": rb_bytes / (rb_ms * 1e-3) / 1e9 / hbm, "peak_source": hbm_src, "ms": rb_ms,
+                        "algorithmic_bytes": rb_bytes, "rebuilds_timed": int(rb_ran),
+                        "list_entries_per_atom": epa, "overflowed_atoms": int(overflowed)}
     kernels = {k: {"launches": v[0], "ms": v[1], "share": v[1] / tot_ms if tot_ms else None}
-               for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}
+               for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1]) if k != "nl_rebuild"}
 
     if not args.no_extras:
         # plain FP64 GPU path on the same state
@@ -794,6 +922,10 @@ def ours_arm(args, dist):
         except Exception as e:  # noqa: BLE001
             extras["adjoint_error"] = repr(e)
         try:
+            extras["c1"] = c1_leg(dev, cpu=dist.rank == 0 and dist.world == 1)
+        except Exception as e:  # noqa: BLE001
+            extras["c1_error"] = repr(e)
+        try:
             extras["ionic"] = ionic_leg(dev, cpu=dist.rank == 0 and dist.world == 1)
         except Exception as e:  # noqa: BLE001
             extras["ionic_error"] = repr(e)
@@ -821,6 +953,13 @@ def ours_arm(args, dist):
                            "neighbour_list_skin_and_threads_per_atom": list_cfg,
                            "cuda_graph": True},
                 "gpu_launches": launches, "clocks": clk, "roofline": roof, "roofline_hbm": roof_hbm,
+                "roofline_rebuild": roof_rebuild,
+                "tick": "the reference's tick: kick, drift, wrap, list check (rebuild when flagged), pair pass "
+                        "with the potential and the in-cutoff pair count, second kick, Berendsen; K, V, lambda "
+                        "and pairs recorded on the device every tick",
+                "energy_free_ticks": {"value": dist.world * u.n * K / (ms_nov * 1e-3), "ms_per_step": ms_nov / K,
+                                      "steps": K, "note": "the same ticks with a pair pass that leaves the "
+                                      "potential and pair count out (ticks that record nothing)"},
                 "kernels": kernels, "memory_kernels": mem, "pairs_per_tick": pairs}
         line.update(extras)
         if "e2e" not in line:
@@ -840,6 +979,8 @@ def main():
                 out = ionic_leg(dev, cpu=False, steps=args.leg_steps or None, variant=args.variant)
             elif args.leg == "accuracy":
                 out = accuracy_leg(dev, args.leg_steps or 10000)
+            elif args.leg == "c1":
+                out = c1_leg(dev, cpu=True, steps=args.leg_steps or 1000)
             elif args.leg == "sweep":
                 from genesis_b200 import sweep
 

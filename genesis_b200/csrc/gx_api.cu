@@ -866,7 +866,7 @@ int gx_collisions(gx_handle* h, uint64_t* collisions) {
 }
 
 int gx_set_kernel_variant(gx_handle* h, int variant) {
-    if (!h || variant < 0 || variant > 6) return GX_ERR_ARG;
+    if (!h || variant < 0 || variant > 7) return GX_ERR_ARG;
     h->kernel_variant = variant;
     invalidate_graphs(h);
     return GX_OK;
@@ -876,7 +876,7 @@ int gx_autotune(gx_handle* h, int reps, int* best, double* ms) {
     int rc = require_state(h);
     if (rc) return rc;
     if (reps < 1) reps = 1;
-    for (int v = 0; v < 7; ++v)
+    for (int v = 0; v < 8; ++v)
         if (ms) ms[v] = -1.0;
     if (h->precision != GX_MIXED || h->n == 0) {
         if (best) *best = h->kernel_variant;
@@ -924,10 +924,10 @@ int gx_autotune(gx_handle* h, int reps, int* best, double* ms) {
             GX_LAUNCH(h, k_soa_to_aos, nblk(n, 256), 256, b0.ax, b0.ay, b0.az, b0.slot, snap + 6 * (size_t)n, n);
             cudaMemcpyAsync(&lam0, h->dscal, sizeof lam0, cudaMemcpyDeviceToHost, h->stream);
             cudaStreamSynchronize(h->stream);
-            const int vs[3] = {pick, 5, 6};
-            double tt[3] = {1e300, 1e300, 1e300};
+            const int vs[4] = {pick, 5, 6, 7};
+            double tt[4] = {1e300, 1e300, 1e300, 1e300};
             const int ticks = reps < 20 ? 20 : reps;  // long enough to include list rebuilds
-            for (int q = 0; q < 3 && !rc; ++q) {
+            for (int q = 0; q < 4 && !rc; ++q) {
                 h->kernel_variant = vs[q];
                 invalidate_graphs(h);
                 double t = 0.0;
@@ -952,13 +952,15 @@ int gx_autotune(gx_handle* h, int reps, int* best, double* ms) {
                 ms[0] = tt[0] < 1e300 ? tt[0] : -1.0;
                 ms[5] = tt[1] < 1e300 ? tt[1] : -1.0;
                 ms[6] = tt[2] < 1e300 ? tt[2] : -1.0;
+                ms[7] = tt[3] < 1e300 ? tt[3] : -1.0;
             }
             if (!rc) {
-                int q = tt[1] < tt[0] ? 1 : 0;
-                if (tt[2] < tt[q]) q = 2;
+                int q = 0;
+                for (int k = 1; k < 4; ++k)
+                    if (tt[k] < tt[q]) q = k;
                 pick = vs[q];
             }
-            if (!rc && pick >= 5) {  // threads per atom of the list pass, on the list just built
+            if (!rc && pick >= 5) {  // threads per atom (stash size for 7) of the list pass, on the list just built
                 h->kernel_variant = pick;
                 rc = nl_tune_tpp(h, reps);
             }
@@ -998,6 +1000,17 @@ int gx_set_list_threads(gx_handle* h, int threads_per_atom) {
     if (!h) return GX_ERR_ARG;
     invalidate_graphs(h);
     return nl_set_tpp(h, threads_per_atom);
+}
+
+int gx_set_list_stash(gx_handle* h, int slots) {
+    if (!h) return GX_ERR_ARG;
+    invalidate_graphs(h);
+    return nl_set_slots(h, slots);
+}
+
+int gx_list_stats(gx_handle* h, uint64_t* entries, uint64_t* overflowed_atoms) {
+    if (!h || !entries || !overflowed_atoms) return GX_ERR_ARG;
+    return nl_stats(h, entries, overflowed_atoms);
 }
 
 int gx_list_rebuilds(gx_handle* h, uint64_t* rebuilds) {

@@ -340,8 +340,10 @@ int counting_sort(gx_handle* h, CellList& cl, uint32_t ncell, const uint32_t* ke
     prof_end(h, "cell_scan");
     prof_begin(h, "cell_scatter");
     if (n) GX_LAUNCH(h, k_scatter, nblk(n, 256), 256, key, n, cl.start, cl.fill, perm, gate);
-    GX_LAUNCH(h, k_segsort, nblk(ncell, 128), 128, cl.start, ncell, perm, gate);
     prof_end(h, "cell_scatter");
+    prof_begin(h, "cell_segsort");
+    GX_LAUNCH(h, k_segsort, nblk(ncell, 128), 128, cl.start, ncell, perm, gate);
+    prof_end(h, "cell_segsort");
     return GX_OK;
 }
 

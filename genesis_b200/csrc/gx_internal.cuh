@@ -311,6 +311,8 @@ int nl_set_skin(gx_handle* h, double skin);
 int nl_tune_tpp(gx_handle* h, int reps);
 int nl_config(gx_handle* h, double* skin, int* tpp);
 int nl_set_tpp(gx_handle* h, int tpp);
+int nl_set_slots(gx_handle* h, int slots);
+int nl_stats(gx_handle* h, uint64_t* entries, uint64_t* overflowed);
 void nl_free(gx_handle* h);
 void tracker_free(gx_handle* h);
 void lens_free(gx_handle* h);

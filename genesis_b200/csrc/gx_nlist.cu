@@ -47,6 +47,7 @@ struct NlState {
     double skin_used = 0.0;
     int half = -1;            // list kind built: 0 full, 1 half (variant 6)
     int tpp = 1;              // threads per atom in the list pass (1, 2, 4, 8)
+    int slots = 16;           // variant 7: stash slots per thread (8 or 16)
     int cap_nb = 0;           // list entries per atom
     size_t cap = 0;           // atoms the buffers hold
     uint32_t* list = nullptr; // entry e of atom p at list[e * cap + p]
@@ -500,12 +501,152 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force_tpp(GridGeom g, const f
     }
 }
 
+// Variant 7: the half list of variant 6, evaluated in two phases per round.
+// Each thread first walks its list and keeps the entries that lie within the
+// cutoff (their displacement and the packed partner index and kind) in a
+// shared-memory stash of S slots; then the warp runs the pair law over the
+// stashed entries together.  The lanes whose atoms have fewer pairs in range
+// wait only in the short collection loop, not in the pair law, which keeps
+// more of the warp busy in the arithmetic.  Same pairs, same per-pair
+// operations, same integer sums: the forces are bit-identical to variant 6.
+template <bool ENERGY, int S>
+__global__ void __launch_bounds__(kNlThreads) k_nl_force_cmp(GridGeom g, const float4* __restrict__ pos4,
+                                                              const uint32_t* __restrict__ home,
+                                                              const uint32_t* __restrict__ start, uint32_t n,
+                                                              LawF32 L, const PairF* __restrict__ tab,
+                                                              const uint32_t* __restrict__ list, size_t stride,
+                                                              int cap_nb, const uint32_t* __restrict__ cnt,
+                                                              long long* __restrict__ F, size_t fstride,
+                                                              unsigned long long* __restrict__ vacc,
+                                                              unsigned long long* __restrict__ npairs,
+                                                              uint32_t* __restrict__ err) {
+    __shared__ PairF st[kMaxKinds * kMaxKinds];
+    __shared__ float4 s_shift[27];
+    __shared__ unsigned long long shu[kNlThreads / 32];
+    __shared__ float4 stash[S * kNlThreads];  // slot k of thread t at [k * kNlThreads + t]
+    int nk2 = L.nkinds * L.nkinds;
+    for (int t = threadIdx.x; t < nk2; t += kNlThreads) st[t] = tab[t];
+    if (threadIdx.x < 27) {
+        float sx, sy, sz;
+        code_shift(g, threadIdx.x, sx, sy, sz);
+        s_shift[threadIdx.x] = make_float4(sx, sy, sz, 0.f);
+    }
+    __syncthreads();
+    const uint32_t p = blockIdx.x * kNlThreads + threadIdx.x;
+    PairAcc a;
+    float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
+    int ki = 0;
+    uint32_t m = 0;
+    if (p < n) {
+        pi = pos4[p];
+        ki = __float_as_int(pi.w);
+        m = cnt[p];
+        if (m > (uint32_t)cap_nb) {  // overflowed list: scan the home-grid cells directly
+            uint32_t cx, cy, cz;
+            const uint32_t c = home[p];
+            decode(g, c, cx, cy, cz);
+            for (uint32_t code = 0; code < 27; ++code) {
+                uint32_t B = cell_at(g, cx, cy, cz, code);
+                if (B < c) continue;
+                float4 sh = s_shift[code];
+                for (uint32_t q = start[B], hi = start[B + 1]; q < hi; ++q)
+                    if (q > p) nl_pair(L, st, ki, pi, pos4[q], sh.x, sh.y, sh.z, ENERGY, a, err, F, q, fstride);
+            }
+            m = 0;
+        }
+    }
+    const uint32_t* lp = list + p;
+    float4* my = stash + threadIdx.x;
+    uint32_t e = 0;
+    while (__any_sync(0xffffffffu, e < m)) {
+        // collect: up to S in-range entries, four list entries per round with every load issued first
+        int k = 0;
+        for (; e + 4 <= m && k <= S - 4; e += 4) {
+            uint32_t w[4];
+            float4 pj[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) w[u] = __ldg(lp + (size_t)(e + u) * stride);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) pj[u] = __ldg(pos4 + (w[u] & kIdxMask));
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const float4 sh = s_shift[w[u] >> 27];
+                const float dx = delta1(pi.x, pj[u].x, sh.x), dy = delta1(pi.y, pj[u].y, sh.y),
+                            dz = delta1(pi.z, pj[u].z, sh.z);
+                const float d2 = dist2(dx, dy, dz);
+                if (d2 < L.rc2 && d2 != 0.f) {
+                    my[k * kNlThreads] = make_float4(
+                        dx, dy, dz, __uint_as_float((w[u] & kIdxMask) | ((uint32_t)__float_as_int(pj[u].w) << 27)));
+                    ++k;
+                }
+            }
+        }
+        for (; e < m && k < S; ++e) {
+            const uint32_t w = __ldg(lp + (size_t)e * stride);
+            const float4 pj = __ldg(pos4 + (w & kIdxMask));
+            const float4 sh = s_shift[w >> 27];
+            const float dx = delta1(pi.x, pj.x, sh.x), dy = delta1(pi.y, pj.y, sh.y), dz = delta1(pi.z, pj.z, sh.z);
+            const float d2 = dist2(dx, dy, dz);
+            if (d2 < L.rc2 && d2 != 0.f) {
+                my[k * kNlThreads] =
+                    make_float4(dx, dy, dz, __uint_as_float((w & kIdxMask) | ((uint32_t)__float_as_int(pj.w) << 27)));
+                ++k;
+            }
+        }
+        int kmax = k;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+        // evaluate: the warp runs the pair law over the stashed entries together
+        for (int t = 0; t < kmax; ++t) {
+            if (t < k) {
+                const float4 sv = my[t * kNlThreads];
+                const uint32_t qk = __float_as_uint(sv.w);
+                const uint32_t q = qk & kIdxMask;
+                float fs, v;
+                pair_f32(L, st[ki * L.nkinds + (int)(qk >> 27)], dist2(sv.x, sv.y, sv.z), fs, v);
+                const long long qx = quant(fmul(sv.x, fs), err), qy = quant(fmul(sv.y, fs), err),
+                                qz = quant(fmul(sv.z, fs), err);
+                a.fx += qx;
+                a.fy += qy;
+                a.fz += qz;
+                atomicAdd((unsigned long long*)&F[q], (unsigned long long)(-qx));
+                atomicAdd((unsigned long long*)&F[fstride + q], (unsigned long long)(-qy));
+                atomicAdd((unsigned long long*)&F[2 * fstride + q], (unsigned long long)(-qz));
+                if (ENERGY && q > p) {
+                    a.vq += quant(v, err);
+                    ++a.np;
+                }
+            }
+        }
+    }
+    if (p < n) {
+        atomicAdd((unsigned long long*)&F[p], (unsigned long long)a.fx);
+        atomicAdd((unsigned long long*)&F[fstride + p], (unsigned long long)a.fy);
+        atomicAdd((unsigned long long*)&F[2 * fstride + p], (unsigned long long)a.fz);
+    }
+    if (ENERGY) {
+        unsigned long long s = block_sum_u<kNlThreads>((unsigned long long)a.vq, shu);
+        unsigned long long np = block_sum_u<kNlThreads>(a.np, shu);
+        if (threadIdx.x == 0) {
+            if (s) atomicAdd(vacc, s);
+            if (np) atomicAdd(npairs, np);
+        }
+    }
+}
+
 template <bool HALF>
 void launch_nl_force(gx_handle* h, int tpp, const GridGeom& g, const NlState* s, uint32_t n, const LawF32& L,
                      bool energy) {
     const float4* pos4 = h->pos4;
     const uint32_t* home = h->key_sorted;
     const uint32_t* start = s->cl.start;
+    if (HALF && h->kernel_variant == 7) {
+        auto kc = s->slots == 8 ? (energy ? k_nl_force_cmp<true, 8> : k_nl_force_cmp<false, 8>)
+                                : (energy ? k_nl_force_cmp<true, 16> : k_nl_force_cmp<false, 16>);
+        GX_LAUNCH(h, kc, nblk(n, kNlThreads), kNlThreads, g, pos4, home, start, n, L, h->d_pairf, s->list, s->cap,
+                  s->cap_nb, s->cnt, h->F, h->cap, h->dcount + 1, h->dcount + 0, h->derr);
+        return;
+    }
     if (tpp <= 1) {
         auto k1 = energy ? k_nl_force<HALF, true> : k_nl_force<HALF, false>;
         GX_LAUNCH(h, k1, nblk(n, kNlThreads), kNlThreads, g, pos4, home, start, n, L, h->d_pairf, s->list, s->cap,
@@ -735,13 +876,19 @@ int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nb_out, bool
         int r = counting_sort(h, s->cl, g.ncell, h->key, n, h->perm, s->flag);
         if (r) return r;
         launch_gather(h, b, o, h->perm, h->key, h->key_sorted, n, h->pos_of_slot, s->flag);
+        prof_begin(h, "nl_copy");
         GX_LAUNCH(h, k_nl_copy, nblk(n, 256), 256, o, b, n, s->flag);
+        prof_end(h, "nl_copy");
+        prof_begin(h, "nl_stage");
         GX_LAUNCH(h, k_nl_stage, nblk(n, 256), 256, g, b, h->key_sorted, n, h->pos4, s->ref, s->flag);
+        prof_end(h, "nl_stage");
         const float rl = (float)((h->fs.rc + s->skin_used) * (1.0 + 1e-6));
         auto build = s->half == 1 ? k_nl_build<true> : k_nl_build<false>;
+        prof_begin(h, "nl_build");
         GX_LAUNCH(h, build, nblk(n, kNlBuildThreads), kNlBuildThreads, g, h->pos4, h->key_sorted, s->cl.start, n,
                   rl * rl,
                   s->list, s->cap, s->cap_nb, s->cnt, s->flag);
+        prof_end(h, "nl_build");
         return GX_OK;
     };
     int rc = rebuild();
@@ -811,10 +958,14 @@ int nl_tune_tpp(gx_handle* h, int reps) {
     if (!s->list || !s->cap || h->n == 0) return GX_OK;
     const uint32_t n = (uint32_t)h->n;
     const LawF32 L = make_law32(h);
+    // variant 7: the stash size (8 or 16 slots per thread); else threads per atom
+    const bool stash = h->kernel_variant == 7;
     const int cand[4] = {1, 2, 4, 8};
+    const int ncand = stash ? 2 : 4;
     double best = 1e300;
-    int pick = s->tpp;
-    for (int k = 0; k < 4; ++k) {
+    int pick = stash ? s->slots : s->tpp;
+    for (int k = 0; k < ncand; ++k) {
+        if (stash) s->slots = k == 0 ? 8 : 16;
         int rc = gx_timer_mark(h, 14);
         for (int r = 0; r < reps && !rc; ++r) {
             if (s->half == 1) launch_nl_force<true>(h, cand[k], s->lg, s, n, L, false);
@@ -826,11 +977,49 @@ int nl_tune_tpp(gx_handle* h, int reps) {
         if (rc) return rc;
         if (t / reps < best) {
             best = t / reps;
-            pick = cand[k];
+            pick = stash ? s->slots : cand[k];
         }
     }
-    s->tpp = pick;
+    if (stash) s->slots = pick;
+    else s->tpp = pick;
     GX_CUDA(h, cudaMemsetAsync(h->derr, 0, sizeof(uint32_t), h->stream));
+    return GX_OK;
+}
+
+__global__ void k_nl_stats(const uint32_t* __restrict__ cnt, uint32_t n, int cap_nb,
+                           unsigned long long* __restrict__ out) {
+    unsigned long long e = 0, o = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t m = cnt[i];
+        e += m;
+        o += m > (uint32_t)cap_nb ? 1ull : 0ull;
+    }
+#pragma unroll
+    for (int k = 16; k > 0; k >>= 1) {
+        e += __shfl_down_sync(0xffffffffu, e, k);
+        o += __shfl_down_sync(0xffffffffu, o, k);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (e) atomicAdd(out, e);
+        if (o) atomicAdd(out + 1, o);
+    }
+}
+
+// Entries held by the current list (an overflowed atom counts the entries it
+// found) and atoms whose list overflowed; synchronises the stream.
+int nl_stats(gx_handle* h, uint64_t* entries, uint64_t* overflowed) {
+    *entries = 0;
+    *overflowed = 0;
+    NlState* s = h->nl ? static_cast<NlState*>(h->nl) : nullptr;
+    if (!s || !s->cnt || !h->nl_valid || !h->n) return GX_OK;
+    unsigned long long* d = h->dcount + 12;  // two scratch counters outside the tick's slots
+    GX_CUDA(h, cudaMemsetAsync(d, 0, 2 * sizeof(unsigned long long), h->stream));
+    GX_LAUNCH(h, k_nl_stats, 256, 256, s->cnt, (uint32_t)h->n, s->cap_nb, d);
+    unsigned long long v[2] = {0, 0};
+    GX_CUDA(h, cudaMemcpyAsync(v, d, sizeof v, cudaMemcpyDeviceToHost, h->stream));
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    *entries = v[0];
+    *overflowed = v[1];
     return GX_OK;
 }
 
@@ -838,6 +1027,12 @@ int nl_config(gx_handle* h, double* skin, int* tpp) {
     NlState* s = nl_of(h);
     if (skin) *skin = skin_of(h, s);
     if (tpp) *tpp = s->tpp;
+    return GX_OK;
+}
+
+int nl_set_slots(gx_handle* h, int slots) {
+    if (slots != 8 && slots != 16) return set_err(h, GX_ERR_ARG, "stash slots must be 8 or 16");
+    nl_of(h)->slots = slots;
     return GX_OK;
 }
 

@@ -113,22 +113,25 @@ int gx_set_precision(gx_handle* h, int precision);
  * neighbour list: pairs within r_c + skin on a grid of cells >= r_c + skin,
  * rebuilt (re-sort included) only when an atom has moved more than skin/2,
  * one thread per atom over its full list, no atomics; 6 = the same with a
- * half list (each pair once, the far end's force through integer atomics).
- * 5 and 6 need >= 3 list-grid cells per axis, else they fall back to 4.  Variants 2 and 3 need >= 3 force-grid
+ * half list (each pair once, the far end's force through integer atomics);
+ * 7 = the half list of 6 with each thread's in-cutoff entries first
+ * collected in shared memory, so that the warp evaluates the pair law on
+ * them together (fewer idle lanes; same forces as 6, bit for bit).
+ * 5, 6 and 7 need >= 3 list-grid cells per axis, else they fall back to 4.  Variants 2 and 3 need >= 3 force-grid
  * cells per axis and fall back to 1 otherwise.  Variants 1-4 give
- * bit-identical forces, and so do 5 and 6 (fixed-point sums); 5 and 6
+ * bit-identical forces, and so do 5, 6 and 7 (fixed-point sums); 5-7
  * evaluate the same pair set in a cell-local frame whose origin is the
  * atom's cell at the last rebuild, so their FP32 forces can differ from 1-4
  * in the last bits (same error bound). */
 int gx_set_kernel_variant(gx_handle* h, int variant);
 /* Autotuner: times `reps` mixed pair passes of variants 1-4 on the resident
  * state (left bit-identical: they give the same fixed-point sums) and, where
- * variants 5 and 6 apply, full ticks of the best of them against full ticks
- * of 5 and of 6, each from a snapshot of (x, v, a) restored afterwards.
+ * variants 5-7 apply, full ticks of the best of them against full ticks
+ * of 5, 6 and 7, each from a snapshot of (x, v, a) restored afterwards.
  * Selects the fastest and returns it in *best.  ms[1..4], when given,
- * receive the per-pass milliseconds, ms[0], ms[5], ms[6] the per-tick
- * milliseconds of the best pass variant, of 5 and of 6 (-1 = not run);
- * ms has 7 entries. */
+ * receive the per-pass milliseconds, ms[0], ms[5], ms[6], ms[7] the
+ * per-tick milliseconds of the best pass variant, of 5, 6 and 7 (-1 = not
+ * run); ms has 8 entries. */
 int gx_autotune(gx_handle* h, int reps, int* best, double* ms);
 /* No counterpart in the reference.  Skin of the variant-5/6 neighbour list
  * (default 0.1 r_c); 0 rebuilds every tick. */
@@ -138,8 +141,19 @@ int gx_set_list_skin(gx_handle* h, double skin);
  * choice gives the same bits (integer sums).  No counterpart in the
  * reference. */
 int gx_set_list_threads(gx_handle* h, int threads_per_atom);
+/* Stash size of the variant-7 list pass: 8 or 16 in-cutoff entries per
+ * thread are collected in shared memory before the warp evaluates them
+ * (default 16; the autotuner picks the faster).  Both give the same bits.
+ * No counterpart in the reference. */
+int gx_set_list_stash(gx_handle* h, int slots);
 /* Skin and threads per atom of the variant-5/6 list pass. */
 int gx_get_list_config(gx_handle* h, double* skin, int* threads_per_atom);
+/* Occupancy of the current neighbour list: the entries it holds (pairs
+ * within r_c + skin, each once on a half list) and the atoms whose list
+ * overflowed its per-atom capacity (they scan their cells directly).  Zeros
+ * when no list is built.  Synchronises the stream.  No counterpart in the
+ * reference. */
+int gx_list_stats(gx_handle* h, uint64_t* entries, uint64_t* overflowed_atoms);
 /* Number of variant-5/6 list rebuilds so far (synchronises the stream). */
 int gx_list_rebuilds(gx_handle* h, uint64_t* rebuilds);
 

@@ -1,8 +1,9 @@
 """The persistent neighbour-list passes (kernel variants 5: full list, 6:
-half list with far-end atomics) against the oracle, each other and the
-per-tick re-sort variants.
+half list with far-end atomics, 7: the half list with in-cutoff entries
+collected in shared memory before the pair law) against the oracle, each
+other and the per-tick re-sort variants.
 
-Variants 5 and 6 evaluate the same pair set {d < r_c} as every other variant, in a
+Variants 5-7 evaluate the same pair set {d < r_c} as every other variant, in a
 cell-local frame anchored at the last rebuild, so its FP32 forces can differ
 from variants 1-4 in the last bits: the checks are the mixed path's error
 bound against the FP64 oracle (force rel-RMS <= 1e-5), agreement of whole
@@ -40,7 +41,7 @@ def _relnorm(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
-@pytest.mark.parametrize("coul,variant", [(False, 5), (True, 5), (False, 6), (True, 6)])
+@pytest.mark.parametrize("coul,variant", [(False, 5), (True, 5), (False, 6), (True, 6), (True, 7)])
 def test_first_tick_forces_match_fp64_oracle(gpu, orc, coul, variant):
     cfg, u = _lattice(18, coul=coul)
     h = _handle(cfg, variant)
@@ -60,15 +61,18 @@ def test_full_and_half_lists_are_bit_identical(gpu, thermo):
         cfg.enable_thermostat = True
         cfg.thermostat_temperature = 40.0
     out = []
-    for variant in (5, 6):
+    for variant, slots in ((5, 0), (6, 0), (7, 16), (7, 8)):
         h = _handle(cfg, variant)
+        if slots:
+            h.set_list_stash(slots)
         h.set_universe(u)
         st = h.step(25, graph=True)
         out.append((h.get_state(), st, h.list_rebuilds()))
-    for x, y in zip(out[0][0], out[1][0]):
-        assert np.array_equal(x, y)
-    assert np.array_equal(out[0][1], out[1][1])
-    assert out[0][2] == out[1][2]
+    for o in out[1:]:
+        for x, y in zip(out[0][0], o[0]):
+            assert np.array_equal(x, y)
+        assert np.array_equal(out[0][1], o[1])
+        assert out[0][2] == o[2]
 
 
 @pytest.mark.parametrize("thermo", [False, True])
@@ -144,7 +148,7 @@ def test_list_path_is_deterministic_and_graph_invariant(gpu):
         assert np.array_equal(runs[0][1], r[1])
 
 
-@pytest.mark.parametrize("variant", [5, 6])
+@pytest.mark.parametrize("variant", [5, 6, 7])
 def test_overflowing_lists_fall_back_to_cell_scans(gpu, orc, variant):
     # a dense clump far above the average density overflows the per-atom lists
     cfg, u = _lattice(12, temperature=10.0)
@@ -177,7 +181,7 @@ def test_state_round_trip_after_list_ticks(gpu):
     assert np.array_equal(pos, p2) and np.array_equal(vel, v2) and np.array_equal(acc, a2)
 
 
-@pytest.mark.parametrize("variant", [5, 6])
+@pytest.mark.parametrize("variant", [5, 6, 7])
 def test_captured_rebuilds_run_only_when_flagged(gpu, variant):
     # a captured tick holds the rebuild in a conditional graph node set from
     # the displacement flag: the same ticks and rebuilds as eager execution,

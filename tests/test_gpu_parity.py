@@ -440,3 +440,32 @@ def test_async_steps_give_the_same_ticks(gpu):
         out.append(h.get_state())
     for a, b in zip(*out):
         assert np.array_equal(a, b)
+
+
+def test_async_step_error_is_not_lost_to_a_lens_call(gpu):
+    """A queued tick that saturates the fixed-point sums, then g(r): the lens
+    clears the device error word for its own use, so it must report the
+    queued tick's error first; a clean queued tick afterwards reports none."""
+    from genesis_b200._lib import GxError
+    import dataclasses
+    wl, cfg, u = _small_ionic(n_side=8)
+    cfg = dataclasses.replace(cfg, coulomb_constant=1e12, enable_bond_observation=False,
+                              enable_bond_interaction=False, enable_thermostat=False)
+    hot = synth.Universe(box=u.box, pos=u.pos.copy(), vel=u.vel, elem=u.elem, charge=u.charge.copy(),
+                         mass=u.mass, entity=u.entity)
+    hot.charge[:] = 0.0
+    hot.charge[:2] = 1.0
+    hot.pos[1] = hot.pos[0] + np.array([0.3, 0.0, 0.0])  # k_e q^2 / 0.5^2 = 4e12 >> 2^31
+    clean = synth.Universe(box=u.box, pos=u.pos, vel=u.vel, elem=u.elem, charge=np.zeros_like(u.charge),
+                           mass=u.mass, entity=u.entity)
+    h = _handle(cfg, "mixed")
+    h.set_universe(hot)
+    h.set_step_async(True)
+    h.step(1, stats=False)  # queued
+    with pytest.raises(GxError) as e:
+        h.radial_distribution(10.0, 64)
+    assert e.value.status == -5
+    h.set_universe(clean)
+    h.step(1, stats=False)
+    h.synchronize()  # the earlier error was reported once, this tick has none
+    h.close()
