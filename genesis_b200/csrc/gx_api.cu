@@ -905,9 +905,10 @@ int gx_autotune(gx_handle* h, int reps, int* best, double* ms) {
             pick = v;
         }
     }
-    // The neighbour-list path (variant 5) changes the whole tick, so it is
-    // compared with the best single-pass variant over full ticks, each run
-    // from the same snapshot of (x, v, a, pending lambda) restored afterwards.
+    // The neighbour-list paths (variants 5-7) change the whole tick, so they
+    // are compared with the best single-pass variant over full ticks, each
+    // run from the same snapshot of (x, v, a, pending lambda) restored
+    // afterwards.  The list skin is then chosen the same way.
     if (!rc && nl_eligible(h)) {
         const uint32_t n = (uint32_t)h->n;
         double* snap = nullptr;
@@ -924,17 +925,16 @@ int gx_autotune(gx_handle* h, int reps, int* best, double* ms) {
             GX_LAUNCH(h, k_soa_to_aos, nblk(n, 256), 256, b0.ax, b0.ay, b0.az, b0.slot, snap + 6 * (size_t)n, n);
             cudaMemcpyAsync(&lam0, h->dscal, sizeof lam0, cudaMemcpyDeviceToHost, h->stream);
             cudaStreamSynchronize(h->stream);
-            const int vs[4] = {pick, 5, 6, 7};
-            double tt[4] = {1e300, 1e300, 1e300, 1e300};
             const int ticks = reps < 20 ? 20 : reps;  // long enough to include list rebuilds
-            for (int q = 0; q < 4 && !rc; ++q) {
-                h->kernel_variant = vs[q];
+            // ms per tick of the current configuration, state restored afterwards
+            auto tick_ms = [&](double* out) -> int {
                 invalidate_graphs(h);
                 double t = 0.0;
-                if (!(rc = gx_step(h, 2, nullptr, 1)) && !(rc = gx_timer_mark(h, 14)) &&
-                    !(rc = gx_step(h, ticks, nullptr, 1)) && !(rc = gx_timer_mark(h, 15)) &&
-                    !(rc = gx_timer_elapsed(h, 14, 15, &t)))
-                    tt[q] = t / ticks;
+                int r = GX_OK;
+                if (!(r = gx_step(h, 2, nullptr, 1)) && !(r = gx_timer_mark(h, 14)) &&
+                    !(r = gx_step(h, ticks, nullptr, 1)) && !(r = gx_timer_mark(h, 15)) &&
+                    !(r = gx_timer_elapsed(h, 14, 15, &t)))
+                    *out = t / ticks;
                 StateBuf& b = h->buf[h->cur];
                 GX_LAUNCH(h, k_aos_to_sorted, nblk(n, 256), 256, snap, h->pos_of_slot, b.x, b.y, b.z, n);
                 GX_LAUNCH(h, k_aos_to_sorted, nblk(n, 256), 256, snap + 3 * (size_t)n, h->pos_of_slot, b.vx, b.vy,
@@ -946,8 +946,14 @@ int gx_autotune(gx_handle* h, int reps, int* best, double* ms) {
                 h->lambda_pending = pend0;
                 h->sorted = false;
                 h->nl_fresh = false;  // positions restored behind the list's back
+                return r;
+            };
+            const int vs[4] = {pick, 5, 6, 7};
+            double tt[4] = {1e300, 1e300, 1e300, 1e300};
+            for (int q = 0; q < 4 && !rc; ++q) {
+                h->kernel_variant = vs[q];
+                rc = tick_ms(&tt[q]);
             }
-            cudaFree(snap);
             if (ms) {
                 ms[0] = tt[0] < 1e300 ? tt[0] : -1.0;
                 ms[5] = tt[1] < 1e300 ? tt[1] : -1.0;
@@ -960,10 +966,34 @@ int gx_autotune(gx_handle* h, int reps, int* best, double* ms) {
                     if (tt[k] < tt[q]) q = k;
                 pick = vs[q];
             }
-            if (!rc && pick >= 5) {  // threads per atom (stash size for 7) of the list pass, on the list just built
+            if (!rc && pick >= 5) {
                 h->kernel_variant = pick;
-                rc = nl_tune_tpp(h, reps);
+                // the skin: 0.05, 0.1, 0.15 and 0.2 r_c (cell size r_c + skin)
+                // over whole ticks, rebuilds included
+                double skin0 = 0.0;
+                nl_config(h, &skin0, nullptr);
+                double best_t = 1e300, best_skin = skin0;
+                const double fr[4] = {0.05, 0.1, 0.15, 0.2};
+                for (int k = 0; k < 4 && !rc; ++k) {
+                    const double sk = fr[k] * h->fs.rc;
+                    nl_set_skin(h, sk);
+                    double t = 1e300;
+                    if ((rc = tick_ms(&t))) break;
+                    if (t < best_t) {
+                        best_t = t;
+                        best_skin = sk;
+                    }
+                }
+                nl_set_skin(h, rc ? skin0 : best_skin);
+                invalidate_graphs(h);
+                // threads per atom (stash size for 7) of the list pass, on a list of the chosen skin
+                if (!rc && !(rc = gx_step(h, 1, nullptr, 0))) {
+                    rc = nl_tune_tpp(h, reps);
+                    int r2 = tick_ms(&best_t);  // restores the snapshot after the tick above
+                    if (!rc) rc = r2;
+                }
             }
+            cudaFree(snap);
         }
     }
     h->kernel_variant = rc ? saved : pick;

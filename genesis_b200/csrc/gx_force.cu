@@ -303,7 +303,11 @@ inline unsigned nblk(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 }  // namespace
 
 // Device copies of the FP64 pair table (the mixed table is built in gx_api.cu).
-static double* d_psig(gx_handle* h) { return h->red + 6 * (size_t)h->cap / 64 + 6 * kRedCap; }
+double* d_psig(gx_handle* h) { return h->red + 6 * (size_t)h->cap / 64 + 6 * kRedCap; }
+
+void launch_sum_rows(gx_handle* h, const double* part, int nb, double* out) {
+    GX_LAUNCH(h, k_sum_rows, 1, 256, part, nb, out);
+}
 
 int bond_spring(gx_handle* h, bool unit_mult) {
     if (!bonds_on(h)) {

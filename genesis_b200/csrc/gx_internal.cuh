@@ -298,6 +298,10 @@ int force_pass(gx_handle* h, bool finalize_acc, double* V, double* Vb, uint64_t*
 // `unit_mult`: every pair within the cutoff occurs once in the reference's
 // pair list (a cell grid of at least 3 cells per axis).
 int bond_spring(gx_handle* h, bool unit_mult);
+// FP64 pair table on the device: sigma_ij then eps_ij, kNElem^2 each (gx_force.cu).
+double* d_psig(gx_handle* h);
+// out = the sum of part[0..nb) in a fixed order, one block (gx_force.cu).
+void launch_sum_rows(gx_handle* h, const double* part, int nb, double* out);
 inline bool bonds_on(const gx_handle* h) { return h->p.enable_bond_interaction && h->bonds_cap > 0; }
 inline unsigned long long* dnbonds(gx_handle* h) { return h->dcount + 8; }
 void adjoint_free(gx_handle* h);

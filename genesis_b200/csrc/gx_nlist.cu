@@ -37,6 +37,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "gx_law64.cuh"
 #include "gx_pair_f32.cuh"
 
 namespace gx {
@@ -725,6 +726,105 @@ __global__ void __launch_bounds__(kRedThreads) k_nl_finish(StateBuf b, const lon
     }
 }
 
+// Plain FP64 pass over the full list: one thread per atom visits every
+// neighbour of its list (within r_c + skin at the last rebuild) in the
+// build's order with the reference's exact per-pair arithmetic (the
+// minimum image of the FP64 positions, pair_f64) and sums its acceleration
+// in that order: no atomics, deterministic.  The list build used the FP32
+// staging; its radius exceeds r_c + skin by 1e-6 relative and the staging
+// error is ~1e-6 absolute, both far inside the skin/2 margin, so every pair
+// with d < r_c in FP64 is in the list.  V and the pair count take each
+// unordered pair once (q > p).
+__global__ void __launch_bounds__(kNlThreads) k_nl_force64(GridGeom g, StateBuf b, const uint32_t* __restrict__ home,
+                                                            const uint32_t* __restrict__ start, uint32_t n, LawF64 L,
+                                                            const double* __restrict__ psig,
+                                                            const double* __restrict__ peps,
+                                                            const uint32_t* __restrict__ list, size_t stride,
+                                                            int cap_nb, const uint32_t* __restrict__ cnt,
+                                                            double* __restrict__ vpart,
+                                                            unsigned long long* __restrict__ npairs) {
+    __shared__ double shd[kNlThreads / 32];
+    __shared__ unsigned long long shu[kNlThreads / 32];
+    const uint32_t i = blockIdx.x * kNlThreads + threadIdx.x;
+    double V = 0.0;
+    unsigned long long np = 0;
+    if (i < n) {
+        const double xi = b.x[i], yi = b.y[i], zi = b.z[i];
+        const int ti = b.elem[i];
+        const double qi = b.charge[i], mi = b.mass[i], inv_mi = b.inv_mass[i];
+        double ax = 0.0, ay = 0.0, az = 0.0;
+        auto visit = [&](uint32_t j) {
+            const double dx = min_image1(xsub(xi, b.x[j]), L.box[0]);
+            const double dy = min_image1(xsub(yi, b.y[j]), L.box[1]);
+            const double dz = min_image1(xsub(zi, b.z[j]), L.box[2]);
+            const double d2 = xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
+            if (d2 >= L.rc2) return;
+            const double d = xsqrt(d2);
+            if (d <= kEpsF64) return;
+            const int tj = b.elem[j];
+            double fmag, Vij = 0.0;
+            pair_f64(L, d, psig[ti * kNElem + tj], peps[ti * kNElem + tj], qi, b.charge[j], mi, b.mass[j], fmag, Vij);
+            if (j > i) {
+                V = xadd(V, Vij);
+                ++np;
+            }
+            if (fmag != 0.0) {
+                const double inv = xdiv(1.0, d);
+                ax = xadd(ax, xmul(xmul(xmul(dx, inv), fmag), inv_mi));
+                ay = xadd(ay, xmul(xmul(xmul(dy, inv), fmag), inv_mi));
+                az = xadd(az, xmul(xmul(xmul(dz, inv), fmag), inv_mi));
+            }
+        };
+        const uint32_t m = cnt[i];
+        if (m <= (uint32_t)cap_nb) {
+            const uint32_t* lp = list + i;
+            for (uint32_t e = 0; e < m; ++e) visit(__ldg(lp + (size_t)e * stride) & kIdxMask);
+        } else {  // overflowed list: every atom of the 27 home-grid cells
+            uint32_t cx, cy, cz;
+            decode(g, home[i], cx, cy, cz);
+            for (uint32_t code = 0; code < 27; ++code) {
+                const uint32_t B = cell_at(g, cx, cy, cz, code);
+                for (uint32_t q = start[B], hi = start[B + 1]; q < hi; ++q)
+                    if (q != i) visit(q);
+            }
+        }
+        b.ax[i] = ax;
+        b.ay[i] = ay;
+        b.az[i] = az;
+    }
+    V = block_sum_d<kNlThreads>(V, shd);
+    np = block_sum_u<kNlThreads>(np, shu);
+    if (threadIdx.x == 0) {
+        vpart[blockIdx.x] = V;
+        if (np) atomicAdd(npairs, np);
+    }
+}
+
+// FP64 second kick (as k_kick) and, with THERMO, the kinetic-energy partials
+// with k_nl_finish's block mapping and operation order.
+template <bool THERMO>
+__global__ void __launch_bounds__(kRedThreads) k_nl_finish64(StateBuf b, uint32_t n, double half_dt,
+                                                             double* __restrict__ kpart) {
+    __shared__ double sh[kRedThreads / 32];
+    double ks = 0.0;
+    for (uint32_t i = blockIdx.x * kRedThreads + threadIdx.x; i < n; i += gridDim.x * kRedThreads) {
+        const double vx = xadd(b.vx[i], xmul(b.ax[i], half_dt));
+        const double vy = xadd(b.vy[i], xmul(b.ay[i], half_dt));
+        const double vz = xadd(b.vz[i], xmul(b.az[i], half_dt));
+        b.vx[i] = vx;
+        b.vy[i] = vy;
+        b.vz[i] = vz;
+        if (THERMO) {
+            double l2 = xadd(xadd(xmul(vx, vx), xmul(vy, vy)), xmul(vz, vz));
+            ks = xadd(ks, xmul(xmul(0.5, b.mass[i]), l2));
+        }
+    }
+    if (THERMO) {
+        ks = block_sum_d<kRedThreads>(ks, sh);
+        if (threadIdx.x == 0) kpart[blockIdx.x] = ks;
+    }
+}
+
 NlState* nl_of(gx_handle* h) {
     if (!h->nl) h->nl = new NlState();
     return static_cast<NlState*>(h->nl);
@@ -750,12 +850,11 @@ void nl_free(gx_handle* h) {
     h->nl = nullptr;
 }
 
-// The list path applies to the mixed pass with at least 3 list-grid cells
-// per axis (so the force grid has at least 3 too, and every pair within the
-// cutoff occurs once in the reference's pair list) and atom indices below
-// 2^27.
+// The list path applies to both precisions (mixed: variants 5-7; FP64: the
+// full-list pass k_nl_force64) with at least 3 list-grid cells per axis (so
+// the force grid has at least 3 too, and every pair within the cutoff occurs
+// once in the reference's pair list) and atom indices below 2^27.
 bool nl_eligible(gx_handle* h) {
-    if (h->precision != GX_MIXED) return false;
     if (h->n == 0 || h->n >= (1u << 27)) return false;
     NlState* s = nl_of(h);
     double rl = h->fs.rc + skin_of(h, s);
@@ -802,7 +901,8 @@ int nl_prepare(gx_handle* h, bool* stale) {
         h->nl_valid = false;
         *stale = true;
     }
-    const int half = h->kernel_variant == 5 ? 0 : 1;  // 6 and automatic: half list
+    // 6, 7 and automatic: half list; 5 and the FP64 pass: full list
+    const int half = (h->kernel_variant == 5 || h->precision != GX_MIXED) ? 0 : 1;
     if (half != s->half) {
         s->half = half;
         h->nl_valid = false;
@@ -905,15 +1005,24 @@ int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nb_out, bool
     GX_LAUNCH(h, k_nl_end, 1, 1, s->flag, h->p.enable_boundaries ? 1 : 0, h->dcount);
     prof_end(h, "nl_rebuild");
     const bool halfl = s->half == 1;
+    const bool f64 = h->precision != GX_MIXED;
     LawF32 L = make_law32(h);
     prof_begin(h, "force_nl");
-    if (halfl)
+    if (f64) {
+        double* vpart = h->red;  // row 0 of the block partials
+        const double* psig = d_psig(h);
+        const unsigned fb = nblk(n, kNlThreads);
+        GX_LAUNCH(h, k_nl_force64, fb, kNlThreads, g, b, h->key_sorted, s->cl.start, n, make_law64(h), psig,
+                  psig + kNElem * kNElem, s->list, s->cap, s->cap_nb, s->cnt, vpart, h->dcount + 0);
+        launch_sum_rows(h, vpart, (int)fb, h->dscal + 2);
+    } else if (halfl) {
         launch_nl_force<true>(h, s->tpp, g, s, n, L, energy);
-    else
+    } else {
         launch_nl_force<false>(h, s->tpp, g, s, n, L, energy);
+    }
     prof_end(h, "force_nl");
     const bool spring = bonds_on(h);
-    if (spring) GX_LAUNCH(h, k_nl_fix_to_double, 1, 1, h->dcount + 1, h->dscal + 2, h->dscal + 3);
+    if (spring && !f64) GX_LAUNCH(h, k_nl_fix_to_double, 1, 1, h->dcount + 1, h->dscal + 2, h->dscal + 3);
     if (spring && (rc = bond_spring(h, true))) return rc;  // into F before it becomes a
     if (h->p.enable_collisions && (rc = collide_pass(h))) return rc;  // CollisionSystem, before the second kick
     int nb = (int)nblk(n, kRedThreads);
@@ -921,7 +1030,13 @@ int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nb_out, bool
     if (nb < 1) nb = 1;
     prof_begin(h, "nl_finish");
     const unsigned long long* vsum = spring ? nullptr : h->dcount + 1;
-    if (kpart)
+    if (f64) {
+        if (kpart)
+            GX_LAUNCH(h, k_nl_finish64<true>, nb, kRedThreads, b, n, half_dt, kpart);
+        else
+            GX_LAUNCH(h, k_nl_finish64<false>, nb, kRedThreads, b, n, half_dt, nullptr);
+        if (!spring) GX_CUDA(h, cudaMemsetAsync(h->dscal + 3, 0, sizeof(double), h->stream));
+    } else if (kpart)
         GX_LAUNCH(h, k_nl_finish<true>, nb, kRedThreads, b, h->F, h->cap, n, half_dt, kpart, vsum, h->dscal + 2,
                   h->dscal + 3);
     else

@@ -131,7 +131,11 @@ int gx_set_kernel_variant(gx_handle* h, int variant);
  * Selects the fastest and returns it in *best.  ms[1..4], when given,
  * receive the per-pass milliseconds, ms[0], ms[5], ms[6], ms[7] the
  * per-tick milliseconds of the best pass variant, of 5, 6 and 7 (-1 = not
- * run); ms has 8 entries. */
+ * run); ms has 8 entries.  Where a list variant wins, the list skin is
+ * then chosen the same way over whole ticks among 0.05, 0.1, 0.15 and
+ * 0.2 r_c (the list-grid cell is r_c + skin; gx_get_list_config reports
+ * the choice), and the lanes per atom (or the stash size of 7) over passes
+ * on a list of that skin.  The state is left as it was. */
 int gx_autotune(gx_handle* h, int reps, int* best, double* ms);
 /* No counterpart in the reference.  Skin of the variant-5/6 neighbour list
  * (default 0.1 r_c); 0 rebuilds every tick. */

@@ -210,11 +210,56 @@ def test_ticks_fp64(gpu, orc, nticks):
     assert np.allclose(st["lambda"], st_ref[:, 3], rtol=tol, atol=0)
 
 
+@pytest.mark.parametrize("nticks", [1, 25])
+def test_fp64_list_path_matches_oracle(gpu, orc, nticks):
+    # the plain FP64 path's default tick runs on the persistent full list
+    # (k_nl_force64): the reference's per-pair arithmetic, sums in list order
+    wl, cfg, u = _c1(n_side=14)
+    cfg.enable_thermostat = True
+    cfg.thermostat_temperature = 30.0
+    cfg.enable_electrostatics = True
+    h = _handle(cfg)
+    h.set_universe(u)
+    st = h.step(nticks, graph=True)
+    assert h.list_rebuilds() >= 1
+    pos, vel, acc = h.get_state()
+    p_ref, v_ref, a_ref, st_ref = orc.ticks(cfg, u.pos, u.vel, None, u.elem, u.charge, u.mass, nticks)
+    tol = FP64_REL if nticks == 1 else 1e-9
+    assert _relnorm(pos, p_ref) <= tol
+    assert _relnorm(vel, v_ref) <= tol
+    assert _relnorm(acc, a_ref) <= tol
+    assert np.all(st["pairs"] == st_ref[:, 4].astype(np.uint64))
+    assert np.allclose(st["potential"], st_ref[:, 1], rtol=tol, atol=0)
+    assert np.allclose(st["lambda"], st_ref[:, 3], rtol=tol, atol=0)
+
+
+def test_fp64_list_overflow_scans_cells(gpu, orc):
+    # a dense clump overflows the per-atom lists; those atoms scan their cells
+    wl, cfg, u = _c1(n_side=12)
+    rng = np.random.default_rng(4)
+    pos = u.pos.copy()
+    k = 300
+    d = rng.normal(size=(k, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    pos[:k] = d * (4.0 * rng.random(k) ** (1.0 / 3.0) + 0.3)[:, None]
+    u2 = synth.Universe(box=u.box, pos=pos, vel=u.vel, elem=u.elem, charge=u.charge, mass=u.mass, entity=u.entity)
+    h = _handle(cfg)
+    h.set_universe(u2)
+    st = h.step(1)
+    assert h.list_stats()[1] > 0  # some lists overflowed
+    _, _, acc = h.get_state()
+    _, _, a_ref, st_ref = orc.ticks(cfg, u2.pos, u2.vel, None, u2.elem, u2.charge, u2.mass, 1)
+    assert _relnorm(acc, a_ref) <= FP64_REL
+    assert int(st["pairs"][0]) == int(st_ref[0, 4])
+
+
 def test_step_matches_granular_calls(gpu):
+    # the per-tick re-sort path (variant 1) runs the same force pass as gx_forces
     wl, cfg, u = _c1(n_side=10)
     cfg.enable_thermostat = True
     cfg.thermostat_temperature = 30.0
     a = _handle(cfg)
+    a.set_kernel_variant(1)
     a.set_universe(u)
     a.step(3)
     b = _handle(cfg)
@@ -295,8 +340,12 @@ def test_autotune_leaves_state_unchanged(gpu):
     a.step(2)
     before = a.get_state()
     best, ms = a.autotune(reps=2)
-    assert best in ms and best in (1, 2, 3, 4, 5, 6)
-    assert 5 in ms and 6 in ms and 0 in ms  # the list paths were timed against the best single-pass tick
+    assert best in ms and best in (1, 2, 3, 4, 5, 6, 7)
+    assert 5 in ms and 6 in ms and 7 in ms and 0 in ms  # the list paths were timed against the best pass tick
+    if best >= 5:  # the skin was chosen among 0.05, 0.1, 0.15, 0.2 r_c
+        skin, _ = a.list_config()
+        rc = E.LJ_CUTOFF_FACTOR * max(cfg.sigma)
+        assert min(abs(skin - f * rc) for f in (0.05, 0.1, 0.15, 0.2)) <= 1e-12 * rc
     after = a.get_state()
     for x, y in zip(before, after):
         assert np.array_equal(x, y)
