@@ -69,7 +69,7 @@ EXPORTS = (
     "gx_batch_step", "gx_batch_get_state", "gx_adjoint_forward", "gx_adjoint_backward",
     "gx_set_list_skin", "gx_list_rebuilds", "gx_list_stats", "gx_batch_set_mode", "gx_batch_get_mode", "gx_batch_autotune",
     "gx_get_list_config", "gx_set_list_threads", "gx_set_list_stash", "gx_bond_observe", "gx_bond_tracker_reset", "gx_get_bonds",
-    "gx_bond_components", "gx_collisions", "gx_collision_count", "gx_xyz_frame",
+    "gx_bond_components", "gx_collisions", "gx_collision_count", "gx_xyz_frame", "gx_snapshot_world",
     "gx_set_step_async",
 )
 
@@ -136,6 +136,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
         "gx_collisions": (C.c_int, [vp, u64p]),
         "gx_collision_count": (C.c_int, [vp, u64p]),
         "gx_xyz_frame": (C.c_int, [vp, C.c_uint64, C.c_char_p, sz, C.POINTER(sz)]),
+        "gx_snapshot_world": (C.c_int, [vp, u32p, C.c_void_p, sz, C.POINTER(sz)]),
         "gx_set_step_async": (C.c_int, [vp, C.c_int]),
         "gx_adjoint_backward": (C.c_int, [vp, dp, dp, dp, dp, dp, dp, dp]),
     }
@@ -505,6 +506,24 @@ class Handle:
         buf = C.create_string_buffer(n.value)
         self._check(self.lib.gx_xyz_frame(self.h, int(tick), buf, n.value, C.byref(n)))
         return buf.raw[: n.value]
+
+    def snapshot_world(self, generation=None) -> bytes:
+        """The bincode encoding of the snapshot's Vec<EntitySnapshot>
+        (src/serialization/mod.rs:38-56) for the resident atoms, encoded on
+        the device (gx_snapshot_world)."""
+        gen = None
+        if generation is not None:
+            gen = np.ascontiguousarray(generation, dtype=np.uint32)
+            if gen.shape != (self.n,):
+                raise ValueError("one generation per atom")
+        n = C.c_size_t()
+        gp = _ptr(gen, C.c_uint32) if gen is not None else None
+        rc = self.lib.gx_snapshot_world(self.h, gp, None, 0, C.byref(n))
+        if rc != -4:
+            self._check(rc)
+        buf = np.empty(n.value, dtype=np.uint8)
+        self._check(self.lib.gx_snapshot_world(self.h, gp, buf.ctypes.data_as(C.c_void_p), n.value, C.byref(n)))
+        return buf.tobytes()
 
     # -- profiling ----------------------------------------------------------
     def profile(self, on: bool = True):

@@ -275,6 +275,7 @@ int step_error(gx_handle* h, uint32_t e) {
 }  // namespace
 
 namespace gx {
+int commit_pending_lambda(gx_handle* h) { return commit_lambda(h); }
 int take_step_errors(gx_handle* h) {
     if (!h->step_errs_pending) return GX_OK;
     h->step_errs_pending = false;
@@ -431,6 +432,7 @@ void gx_destroy(gx_handle* h) {
     lens_free(h);
     collide_free(h);
     export_free(h);
+    snapshot_free(h);
     if (h->herr) cudaFreeHost(h->herr);
     free_buf(h->buf[0]);
     free_buf(h->buf[1]);

@@ -249,6 +249,7 @@ struct gx_handle {
     void* lens = nullptr;     // analysis staging pool (gx_lens.cu)
     void* coll = nullptr;     // collision pass state (gx_lens.cu)
     void* xport = nullptr;    // XYZ frame buffers (gx_export.cu)
+    void* snap = nullptr;     // snapshot encoder buffers (gx_snapshot.cu)
 };
 
 // Every kernel launch of the library goes through this macro so the
@@ -327,6 +328,9 @@ int collide_pass(gx_handle* h);
 int collide_read(gx_handle* h, unsigned long long* pass, unsigned long long* total);
 void collide_free(gx_handle* h);
 void export_free(gx_handle* h);  // gx_export.cu
+void snapshot_free(gx_handle* h);  // gx_snapshot.cu
+// Applies a pending Berendsen scale to v (any call that reads v commits it).
+int commit_pending_lambda(gx_handle* h);
 // After a wait on the stream: the error word an asynchronous gx_step left.
 int take_step_errors(gx_handle* h);
 // Waits for a queued asynchronous gx_step and reports its error word.  Every

@@ -251,6 +251,21 @@ int gx_clusters(gx_handle* h, double bond_factor, uint32_t* labels, uint64_t sta
  * order. */
 int gx_bound_pairs(gx_handle* h, double k_bind, uint32_t* pairs, size_t cap, size_t* npairs);
 
+/* ---- snapshot ------------------------------------------------------- */
+
+/* The world section of Universe::save (src/serialization/mod.rs:38-56,
+ * 85-104): the bincode 1 encoding of Vec<EntitySnapshot> for the resident
+ * atoms in ECS slot order, every record with all seven components (position,
+ * velocity, mass, charge, atom type, bonds, acceleration), encoded on the
+ * device.  Entity indices are the ones given to gx_set_state (else the slot);
+ * generation[slot] (may be null: 0) gives each id's generation.  Bonds are
+ * the handle's bond list, each slot's partners in ascending slot order.
+ * *len receives the byte count (8 + 115 n + 16 bonds); GX_ERR_CAPACITY when
+ * cap is smaller (out may be null to ask for the size).  The format number,
+ * configuration, clock, RNG and statistics that precede the world in a
+ * snapshot file come from the caller's own encoder. */
+int gx_snapshot_world(gx_handle* h, const uint32_t* generation, uint8_t* out, size_t cap, size_t* len);
+
 /* ---- bond observation ----------------------------------------------- */
 
 /* One tick of BondObservationSystem::run (src/systems/bonds.rs:73-185) with
