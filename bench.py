@@ -887,22 +887,27 @@ def ours_arm(args, dist):
             sweep_steps = 2000
             _, stb, msb = sweep.run_batched(mine, sweep_steps, dev, mode=2)
             _, _, msp = sweep.run_batched(mine, sweep_steps, dev, mode=1)
+            _, stc, msc = sweep.run_batched(mine, sweep_steps, dev, mode=3)
             seq_steps = 50
             _, mss = sweep.run_sequential(mine, seq_steps, dev)
-            msb, msp, mss = dist.max(msb), dist.max(msp), dist.max(mss)
+            msb, msp, msc, mss = dist.max(msb), dist.max(msp), dist.max(msc), dist.max(mss)
             vb = len(wls) * sweep_steps / (msb * 1e-3)
             vp = len(wls) * sweep_steps / (msp * 1e-3)
+            vc = len(wls) * sweep_steps / (msc * 1e-3)
             vs = len(wls) * seq_steps / (mss * 1e-3)
             stats = sweep.assemble(parts, dist.all_gather_object(np.asarray(stb).tolist()))
-            best = max(vb, vp)
+            best = max(vb, vp, vc)
+            mode_name = {vb: "all-replica graph", vp: "persistent launch, a CTA per replica",
+                         vc: "persistent cooperative launch"}[best]
             extras["replica_sweep"] = {
                 "metric": "replica-steps/s", "replicas": len(wls), "atoms": sweep.atoms(wls),
                 "scaling": "strong: one sweep shared over the ranks",
                 "atoms_per_rank": [int(sum(sizes[i] for i in p)) for p in parts],
-                "batched": {"value": best, "steps": sweep_steps,
-                            "mode": "all-replica graph" if vb >= vp else "persistent launch",
+                "batched": {"value": best, "steps": sweep_steps, "mode": mode_name,
                             "all_replica_graph": {"value": vb, "ms": msb},
-                            "persistent_launch": {"value": vp, "ms": msp}},
+                            "persistent_launch": {"value": vp, "ms": msp},
+                            "persistent_cooperative_launch": {"value": vc, "ms": msc,
+                                                              "same_bits_as_graph": bool(np.array_equal(stb, stc))}},
                 "sequential": {"value": vs, "steps_per_replica": seq_steps, "ms": mss},
                 "batched_over_sequential": best / vs,
                 "final_kinetic_sum": float(stats[:, 0].sum()), "final_pairs_sum": float(stats[:, 3].sum()),
@@ -986,8 +991,9 @@ def main():
 
                 wls = sweep.make_replicas(256, seed=0)
                 steps = args.leg_steps or 2000
-                _, _, ms = sweep.run_batched(wls, steps, dev, mode=2)
-                out = {"workload": "256 replicas, all-replica graph", "steps": steps, "ms": ms,
+                mode = args.variant if args.variant in (1, 2, 3) else 2
+                _, _, ms = sweep.run_batched(wls, steps, dev, mode=mode)
+                out = {"workload": f"256 replicas, batch mode {mode}", "steps": steps, "ms": ms,
                        "replica_steps_per_s": len(wls) * steps / (ms * 1e-3), "atoms": sweep.atoms(wls)}
             elif args.leg == "xyz":
                 import dataclasses

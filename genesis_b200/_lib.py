@@ -620,7 +620,8 @@ class Batch:
         return st, ms.value
 
     def set_mode(self, mode: int):
-        """1 = persistent launch (one CTA per replica), 2 = all-replica graph."""
+        """1 = persistent launch (one CTA per replica), 2 = all-replica graph,
+        3 = the all-replica phases in one persistent cooperative launch."""
         self._check(self.lib.gx_batch_set_mode(self.b, mode))
 
     @property
@@ -630,11 +631,11 @@ class Batch:
         return m.value
 
     def autotune(self, ticks: int = 10):
-        """Times both modes from a snapshot, keeps the faster: (mode, {mode: ms per tick})."""
+        """Times the three modes from a snapshot, keeps the fastest: (mode, {mode: ms per tick})."""
         m = C.c_int()
-        ms = np.zeros(2)
+        ms = np.zeros(3)
         self._check(self.lib.gx_batch_autotune(self.b, ticks, C.byref(m), _ptr(ms, C.c_double)))
-        return m.value, {1: float(ms[0]), 2: float(ms[1])}
+        return m.value, {k + 1: float(t) for k, t in enumerate(ms) if t >= 0}
 
     def get_state(self):
         n = int(self.natoms.sum())

@@ -513,6 +513,9 @@ int gx_batch_step(gx_batch* b, int nsteps, double* stats, double* device_ms) {
             k_batch<<<b->nrep, kBThreads, 0, b->stream>>>(b->d_reps, b->d_order, b->A, b->L, b->d_tab, P, b->d_out,
                                                           b->d_err);
         GXB_CUDA(b, cudaGetLastError());
+    } else if (b->mode == 3) {
+        int rc = batch_coop_step(b, nsteps, nullptr);
+        if (rc) return rc;
     } else {
         int rc = batch_flat_step(b, nsteps, nullptr);
         if (rc) return rc;
@@ -532,12 +535,13 @@ int gx_batch_step(gx_batch* b, int nsteps, double* stats, double* device_ms) {
         cudaMemset(b->d_err, 0, sizeof(uint32_t));
         if (e & kErrNonFinite) return berr(b, GX_ERR_NONFINITE, "non-finite position or force in a replica");
         if (e & kErrSaturation) return berr(b, GX_ERR_SATURATION, "fixed-point force saturated");
+        if (e & kErrTimeout) return berr(b, GX_ERR_TIMEOUT, "a grid barrier of the cooperative launch timed out");
     }
     return GX_OK;
 }
 
 int gx_batch_set_mode(gx_batch* b, int mode) {
-    if (!b || mode < 0 || mode > 2) return GX_ERR_ARG;
+    if (!b || mode < 0 || mode > 3) return GX_ERR_ARG;
     b->mode = mode == 0 ? 2 : mode;
     return GX_OK;
 }
@@ -557,9 +561,12 @@ int gx_batch_autotune(gx_batch* b, int ticks, int* mode, double* ms) {
     // x y z vx vy vz ax ay az are the first nine columns of one allocation
     GXB_CUDA(b, cudaMemcpyAsync(snap, b->A.x, n9 * sizeof(double), cudaMemcpyDeviceToDevice, b->stream));
     const int saved = b->mode;
-    double t[2] = {0.0, 0.0};
+    double t[3] = {-1.0, -1.0, -1.0};
     int rc = GX_OK;
-    for (int m = 1; m <= 2 && !rc; ++m) {
+    bool fits1 = true;  // mode 1 keeps each replica's cells in shared memory
+    for (const RepDesc& d : b->reps) fits1 = fits1 && d.g.ncell <= kBMaxCells;
+    for (int m = 1; m <= 3 && !rc; ++m) {
+        if (m == 1 && !fits1) continue;
         b->mode = m;
         double w = 0.0;
         if (!(rc = gx_batch_step(b, 1, nullptr, &w)) && !(rc = gx_batch_step(b, ticks, nullptr, &w))) t[m - 1] = w;
@@ -567,12 +574,13 @@ int gx_batch_autotune(gx_batch* b, int ticks, int* mode, double* ms) {
     }
     cudaStreamSynchronize(b->stream);
     cudaFree(snap);
-    b->mode = rc ? saved : (t[1] <= t[0] ? 2 : 1);
+    int pick = 2;
+    for (int m = 1; m <= 3; ++m)
+        if (t[m - 1] >= 0.0 && t[m - 1] < t[pick - 1]) pick = m;
+    b->mode = rc ? saved : pick;
     if (mode) *mode = b->mode;
-    if (ms) {
-        ms[0] = t[0] / ticks;
-        ms[1] = t[1] / ticks;
-    }
+    if (ms)
+        for (int m = 0; m < 3; ++m) ms[m] = t[m] >= 0.0 ? t[m] / ticks : -1.0;
     return rc;
 }
 

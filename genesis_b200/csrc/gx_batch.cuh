@@ -59,10 +59,12 @@ struct gx_batch {
     std::string err;
     double pair_sigma[gx::kNElem * gx::kNElem], pair_eps[gx::kNElem * gx::kNElem];
     bool has_state = false;
-    int mode = 2;                  // 1 persistent launch, 2 all-replica graph
+    int mode = 2;                  // 1 persistent launch (a CTA per replica), 2 all-replica graph,
+                                   // 3 persistent cooperative launch of the all-replica phases
     gx::BatchFlat* flat = nullptr;  // state of mode 2
 };
 
 namespace gx {
 int batch_flat_step(gx_batch* b, int nsteps, uint64_t* launches);
+int batch_coop_step(gx_batch* b, int nsteps, uint64_t* launches);
 }

@@ -63,6 +63,9 @@ struct BatchFlat {
     gx_handle* ctx = nullptr;           // launch context of the shared counting sort
     cudaGraphExec_t graph[2] = {};      // tick without / with the potential and pair count
     uint64_t graph_kernels = 0;
+    unsigned* coop_bar = nullptr;       // mode 3: grid barrier (arrivals, generation)
+    uint32_t* coop_tile = nullptr;      // mode 3: scan tile totals
+    int coop_grid = 0;
 };
 
 void batch_flat_free(BatchFlat* f) {
@@ -75,6 +78,8 @@ void batch_flat_free(BatchFlat* f) {
     cudaFree(f->srep);
     cudaFree(f->lam);
     cudaFree(f->acc);
+    cudaFree(f->coop_bar);
+    cudaFree(f->coop_tile);
     if (f->ctx) {
         cudaFree(f->ctx->cl.count);
         cudaFree(f->ctx->cl.start);
@@ -102,11 +107,10 @@ __device__ __forceinline__ uint32_t cell_of_rep(const RepGeo& G, double x, doubl
 
 // Kick (k_kick with the replica's scale), drift (k_drift), wrap (k_wrap),
 // global cell key.
-__global__ void k_fb_advance(const RepGeo* __restrict__ geo, const uint32_t* __restrict__ rep_of, BatchArrays A,
-                             const double* __restrict__ lam, double half_dt, double dt, int wrap, uint32_t total,
-                             uint32_t* __restrict__ key, uint32_t* __restrict__ err) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= total) return;
+__device__ __forceinline__ void fb_advance_one(uint32_t i, const RepGeo* __restrict__ geo,
+                                               const uint32_t* __restrict__ rep_of, const BatchArrays& A,
+                                               const double* __restrict__ lam, double half_dt, double dt, int wrap,
+                                               uint32_t* __restrict__ key, uint32_t* __restrict__ err) {
     const uint32_t r = rep_of[i];
     const RepGeo& G = geo[r];
     const double l = lam[r];
@@ -129,13 +133,19 @@ __global__ void k_fb_advance(const RepGeo* __restrict__ geo, const uint32_t* __r
     key[i] = G.cell_base + cell_of_rep(G, x, y, z);
 }
 
+__global__ void k_fb_advance(const RepGeo* __restrict__ geo, const uint32_t* __restrict__ rep_of, BatchArrays A,
+                             const double* __restrict__ lam, double half_dt, double dt, int wrap, uint32_t total,
+                             uint32_t* __restrict__ key, uint32_t* __restrict__ err) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < total) fb_advance_one(i, geo, rep_of, A, lam, half_dt, dt, wrap, key, err);
+}
+
 // Sorted staging: cell-local FP32 position + kind (as k_build_pos4), the
 // local cell and replica of each sorted position, zeroed forces.
-__global__ void k_fb_stage(const RepGeo* __restrict__ geo, const uint32_t* __restrict__ rep_of, BatchArrays A,
-                           const uint32_t* __restrict__ perm, const uint32_t* __restrict__ key, uint32_t total,
-                           uint32_t* __restrict__ srep, size_t fstride) {
-    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= total) return;
+__device__ __forceinline__ void fb_stage_one(uint32_t s, const RepGeo* __restrict__ geo,
+                                             const uint32_t* __restrict__ rep_of, const BatchArrays& A,
+                                             const uint32_t* __restrict__ perm, const uint32_t* __restrict__ key,
+                                             uint32_t* __restrict__ srep, size_t fstride) {
     const uint32_t i = perm[s], r = rep_of[i];
     const RepGeo& G = geo[r];
     const uint32_t c = key[i] - G.cell_base;
@@ -152,21 +162,23 @@ __global__ void k_fb_stage(const RepGeo* __restrict__ geo, const uint32_t* __res
     A.F[2 * fstride + s] = 0;
 }
 
+__global__ void k_fb_stage(const RepGeo* __restrict__ geo, const uint32_t* __restrict__ rep_of, BatchArrays A,
+                           const uint32_t* __restrict__ perm, const uint32_t* __restrict__ key, uint32_t total,
+                           uint32_t* __restrict__ srep, size_t fstride) {
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < total) fb_stage_one(s, geo, rep_of, A, perm, key, srep, fstride);
+}
+
 // k_force_mixed on the atom's own replica grid (canonical half shell, the
-// same shifts, minimum image on axes with fewer than 3 cells).
+// same shifts, minimum image on axes with fewer than 3 cells).  Every lane of
+// the warp calls it (s >= total: no atom), for the warp-level sums.
 template <bool ENERGY>
-__global__ void __launch_bounds__(kFbThreads) k_fb_force(const RepGeo* __restrict__ geo, const float4* __restrict__ pos4,
-                                                          const uint32_t* __restrict__ skey,
-                                                          const uint32_t* __restrict__ srep,
-                                                          const uint32_t* __restrict__ start, uint32_t total, LawF32 L,
-                                                          const PairF* __restrict__ tab, long long* __restrict__ F,
-                                                          size_t fstride, unsigned long long* __restrict__ racc,
-                                                          uint32_t* __restrict__ err) {
-    __shared__ PairF st[kMaxKinds * kMaxKinds];
-    const int nk2 = L.nkinds * L.nkinds;
-    for (int t = threadIdx.x; t < nk2; t += kFbThreads) st[t] = tab[t];
-    __syncthreads();
-    const uint32_t s = blockIdx.x * kFbThreads + threadIdx.x;
+__device__ __forceinline__ void fb_force_one(uint32_t s, const RepGeo* __restrict__ geo,
+                                             const float4* __restrict__ pos4, const uint32_t* __restrict__ skey,
+                                             const uint32_t* __restrict__ srep, const uint32_t* __restrict__ start,
+                                             uint32_t total, const LawF32& L, const PairF* st,
+                                             long long* __restrict__ F, size_t fstride,
+                                             unsigned long long* __restrict__ racc, uint32_t* __restrict__ err) {
     long long vq = 0;
     unsigned long long np = 0;
     uint32_t r = 0xFFFFFFFFu;
@@ -245,11 +257,25 @@ __global__ void __launch_bounds__(kFbThreads) k_fb_force(const RepGeo* __restric
     }
 }
 
+template <bool ENERGY>
+__global__ void __launch_bounds__(kFbThreads) k_fb_force(const RepGeo* __restrict__ geo, const float4* __restrict__ pos4,
+                                                          const uint32_t* __restrict__ skey,
+                                                          const uint32_t* __restrict__ srep,
+                                                          const uint32_t* __restrict__ start, uint32_t total, LawF32 L,
+                                                          const PairF* __restrict__ tab, long long* __restrict__ F,
+                                                          size_t fstride, unsigned long long* __restrict__ racc,
+                                                          uint32_t* __restrict__ err) {
+    __shared__ PairF st[kMaxKinds * kMaxKinds];
+    const int nk2 = L.nkinds * L.nkinds;
+    for (int t = threadIdx.x; t < nk2; t += kFbThreads) st[t] = tab[t];
+    __syncthreads();
+    fb_force_one<ENERGY>(blockIdx.x * kFbThreads + threadIdx.x, geo, pos4, skey, srep, start, total, L, st, F, fstride,
+                         racc, err);
+}
+
 // a = F 2^-32 (1/m) (k_fix_to_acc), v += a dt/2 (k_kick).
-__global__ void k_fb_finish(BatchArrays A, const uint32_t* __restrict__ perm, uint32_t total, double half_dt,
-                            size_t fstride) {
-    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= total) return;
+__device__ __forceinline__ void fb_finish_one(uint32_t s, const BatchArrays& A, const uint32_t* __restrict__ perm,
+                                              double half_dt, size_t fstride) {
     const uint32_t i = perm[s];
     const double im = A.inv_mass[i];
     double ax = xmul(xmul(__ll2double_rn(A.F[s]), kFixInv), im);
@@ -261,6 +287,12 @@ __global__ void k_fb_finish(BatchArrays A, const uint32_t* __restrict__ perm, ui
     A.vx[i] = xadd(A.vx[i], xmul(ax, half_dt));
     A.vy[i] = xadd(A.vy[i], xmul(ay, half_dt));
     A.vz[i] = xadd(A.vz[i], xmul(az, half_dt));
+}
+
+__global__ void k_fb_finish(BatchArrays A, const uint32_t* __restrict__ perm, uint32_t total, double half_dt,
+                            size_t fstride) {
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < total) fb_finish_one(s, A, perm, half_dt, fstride);
 }
 
 __device__ __forceinline__ double block_sum_fb(double v, double* sh) {
@@ -279,11 +311,9 @@ __device__ __forceinline__ double block_sum_fb(double v, double* sh) {
 // One block per replica: kinetic energy of its atoms in a fixed order and
 // the Berendsen scale of ThermostatSystem::run (thermostat.rs:52-71), kept
 // pending for the next kick; the tick's V, lambda and pair count to out.
-__global__ void __launch_bounds__(kFbRed) k_fb_thermo(const RepThermo* __restrict__ th, BatchArrays A,
-                                                      double* __restrict__ lam, unsigned long long* __restrict__ racc,
-                                                      double k_thermal, double* __restrict__ out) {
-    __shared__ double sh[kFbRed / 32];
-    const int r = blockIdx.x;
+__device__ __forceinline__ void fb_thermo_one(int r, const RepThermo* __restrict__ th, const BatchArrays& A,
+                                              double* __restrict__ lam, unsigned long long* __restrict__ racc,
+                                              double k_thermal, double* __restrict__ out, double* sh) {
     const RepThermo T = th[r];
     double ks = 0.0;
     for (uint32_t i = T.base + threadIdx.x; i < T.base + T.n; i += kFbRed) {
@@ -310,11 +340,16 @@ __global__ void __launch_bounds__(kFbRed) k_fb_thermo(const RepThermo* __restric
     }
 }
 
-// End of a step call: apply the pending scales, kinetic energy after them.
-__global__ void __launch_bounds__(kFbRed) k_fb_commit(const RepThermo* __restrict__ th, BatchArrays A,
-                                                      double* __restrict__ lam, double* __restrict__ out) {
+__global__ void __launch_bounds__(kFbRed) k_fb_thermo(const RepThermo* __restrict__ th, BatchArrays A,
+                                                      double* __restrict__ lam, unsigned long long* __restrict__ racc,
+                                                      double k_thermal, double* __restrict__ out) {
     __shared__ double sh[kFbRed / 32];
-    const int r = blockIdx.x;
+    fb_thermo_one(blockIdx.x, th, A, lam, racc, k_thermal, out, sh);
+}
+
+// End of a step call: apply the pending scales, kinetic energy after them.
+__device__ __forceinline__ void fb_commit_one(int r, const RepThermo* __restrict__ th, const BatchArrays& A,
+                                              double* __restrict__ lam, double* __restrict__ out, double* sh) {
     const RepThermo T = th[r];
     const double l = lam[r];
     double ks = 0.0;
@@ -331,6 +366,216 @@ __global__ void __launch_bounds__(kFbRed) k_fb_commit(const RepThermo* __restric
         out[4 * r + 0] = ks;
         lam[r] = 1.0;
     }
+}
+
+__global__ void __launch_bounds__(kFbRed) k_fb_commit(const RepThermo* __restrict__ th, BatchArrays A,
+                                                      double* __restrict__ lam, double* __restrict__ out) {
+    __shared__ double sh[kFbRed / 32];
+    fb_commit_one(blockIdx.x, th, A, lam, out, sh);
+}
+
+// ---------------------------------------------------------------------------
+// Batch mode 3: the same phases inside ONE persistent cooperative launch for
+// all the ticks of a step call.  Every block of the grid is resident (the
+// grid is sized from the occupancy and launched cooperatively), and the
+// phases are separated by a grid barrier with a bounded wait: a block that
+// waits longer than about two seconds sets kErrTimeout and every block
+// leaves at its next barrier.  The counting sort is done in place (cell
+// counts fused into the advance phase, a tiled scan, the scatter and the
+// per-cell index sort of the shared counting_sort), and the other phases
+// call the functions of the kernels above, so a tick is the same bits as a
+// mode-2 tick.  The block size is kFbRed, as the per-replica reductions of
+// k_fb_thermo and k_fb_commit need the same thread mapping.
+constexpr int kCoopThreads = kFbRed;
+constexpr int kCoopItems = 16;
+constexpr uint32_t kCoopTile = kCoopThreads * kCoopItems;  // counters per scan tile
+constexpr unsigned long long kCoopSpins = 20000000ull;     // x ~100 ns sleeps: the barrier's wait limit
+
+struct CoopArgs {
+    const RepGeo* geo;
+    const RepThermo* th;
+    const uint32_t* rep_of;
+    uint32_t* srep;
+    double* lam;
+    unsigned long long* racc;
+    BatchArrays A;
+    LawF32 L;
+    const PairF* tab;
+    double* out;
+    uint32_t* err;
+    uint32_t *count, *start, *fill, *tile;
+    unsigned* bar;  // [0] arrivals, [1] generation
+    uint32_t ncell, total;
+    int nrep;
+    BatchParams P;
+};
+
+// Grid barrier: arrive, then wait (bounded) for the last arrival to advance
+// the generation.  Returns false on every block once any block timed out.
+__device__ __forceinline__ bool coop_sync(const CoopArgs& a, int* s_ok) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* gen = a.bar + 1;
+        const unsigned g = *gen;
+        __threadfence();
+        if (atomicAdd(a.bar, 1u) == gridDim.x - 1) {
+            atomicExch(a.bar, 0u);
+            __threadfence();
+            atomicAdd(a.bar + 1, 1u);
+        } else {
+            unsigned long long spins = 0;
+            while (*gen == g) {
+                if (++spins > kCoopSpins || (*(volatile uint32_t*)a.err & kErrTimeout)) {
+                    atomicOr(a.err, kErrTimeout);
+                    break;
+                }
+                __nanosleep(100);
+            }
+        }
+        __threadfence();
+        *s_ok = (*(volatile uint32_t*)a.err & kErrTimeout) == 0u;
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+
+// Exclusive scan of one tile of cell counts into start; the tile's total to tile[t].
+__device__ __forceinline__ void coop_scan_tile(const CoopArgs& a, uint32_t t, uint32_t m, uint32_t* s_warp) {
+    const uint32_t base = t * kCoopTile + threadIdx.x * kCoopItems;
+    uint32_t v[kCoopItems];
+    uint32_t local = 0;
+#pragma unroll
+    for (int k = 0; k < kCoopItems; ++k) {
+        v[k] = base + k < m ? a.count[base + k] : 0u;
+        local += v[k];
+    }
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t inc = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t u = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= (uint32_t)o) inc += u;
+    }
+    if (lane == 31) s_warp[w] = inc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int k = 0; k < kCoopThreads / 32; ++k) {
+            const uint32_t x = s_warp[k];
+            s_warp[k] = run;
+            run += x;
+        }
+        a.tile[t] = run;
+    }
+    __syncthreads();
+    uint32_t run = s_warp[w] + inc - local;
+#pragma unroll
+    for (int k = 0; k < kCoopItems; ++k) {
+        if (base + k < m) a.start[base + k] = run;
+        run += v[k];
+    }
+    __syncthreads();  // s_warp is reused by the next tile
+}
+
+// Exclusive scan of the tile totals in place (block 0), 256 at a time.
+__device__ __forceinline__ void coop_scan_tiles(const CoopArgs& a, uint32_t ntiles, uint32_t* s_warp) {
+    uint32_t carry = 0;
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (uint32_t c0 = 0; c0 < ntiles; c0 += kCoopThreads) {
+        const uint32_t t = c0 + threadIdx.x;
+        const uint32_t x = t < ntiles ? a.tile[t] : 0u;
+        uint32_t inc = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t u = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= (uint32_t)o) inc += u;
+        }
+        if (lane == 31) s_warp[w] = inc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t run = 0;
+            for (int k = 0; k < kCoopThreads / 32; ++k) {
+                const uint32_t y = s_warp[k];
+                s_warp[k] = run;
+                run += y;
+            }
+            s_warp[kCoopThreads / 32] = run;
+        }
+        __syncthreads();
+        if (t < ntiles) a.tile[t] = carry + s_warp[w] + inc - x;
+        carry += s_warp[kCoopThreads / 32];
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kCoopThreads) k_fb_coop(CoopArgs a) {
+    __shared__ PairF st[kMaxKinds * kMaxKinds];
+    __shared__ double sh[kCoopThreads / 32];
+    __shared__ uint32_t s_warp[kCoopThreads / 32 + 1];
+    __shared__ int s_ok;
+    const int nk2 = a.L.nkinds * a.L.nkinds;
+    for (int t = threadIdx.x; t < nk2; t += kCoopThreads) st[t] = a.tab[t];
+    const uint32_t gt = blockIdx.x * kCoopThreads + threadIdx.x, gs = gridDim.x * kCoopThreads;
+    const uint32_t n = a.total, m = a.ncell + 1;
+    const uint32_t ntiles = (m + kCoopTile - 1) / kCoopTile;
+    const uint32_t npad = (n + 31u) & ~31u;
+    const size_t fs = a.A.total;
+    const BatchArrays& A = a.A;
+    for (uint32_t c = gt; c < m; c += gs) {
+        a.count[c] = 0u;
+        a.fill[c] = 0u;
+    }
+    if (!coop_sync(a, &s_ok)) return;
+    for (int step = 0; step < a.P.nsteps; ++step) {
+        const bool energy = step == a.P.nsteps - 1;  // only the last tick reports V and the pair count
+        for (uint32_t i = gt; i < n; i += gs) {      // k_fb_advance + k_count
+            fb_advance_one(i, a.geo, a.rep_of, A, a.lam, a.P.half_dt, a.P.dt, a.P.boundaries, A.key, a.err);
+            atomicAdd(&a.count[A.key[i]], 1u);
+        }
+        if (!coop_sync(a, &s_ok)) return;
+        for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) coop_scan_tile(a, t, m, s_warp);
+        if (!coop_sync(a, &s_ok)) return;
+        if (blockIdx.x == 0) coop_scan_tiles(a, ntiles, s_warp);
+        if (!coop_sync(a, &s_ok)) return;
+        for (uint32_t c = gt; c < m; c += gs) a.start[c] += a.tile[c / kCoopTile];
+        if (!coop_sync(a, &s_ok)) return;
+        for (uint32_t i = gt; i < n; i += gs) {  // k_scatter
+            const uint32_t c = A.key[i];
+            A.idx[a.start[c] + atomicAdd(&a.fill[c], 1u)] = i;
+        }
+        if (!coop_sync(a, &s_ok)) return;
+        for (uint32_t c = gt; c < a.ncell; c += gs) {  // k_segsort
+            const uint32_t lo = a.start[c], hi = a.start[c + 1];
+            for (uint32_t q = lo + 1; q < hi; ++q) {
+                const uint32_t v = A.idx[q];
+                uint32_t b = q;
+                while (b > lo && A.idx[b - 1] > v) {
+                    A.idx[b] = A.idx[b - 1];
+                    --b;
+                }
+                A.idx[b] = v;
+            }
+        }
+        if (!coop_sync(a, &s_ok)) return;
+        for (uint32_t s2 = gt; s2 < n; s2 += gs) fb_stage_one(s2, a.geo, a.rep_of, A, A.idx, A.key, a.srep, fs);
+        if (!coop_sync(a, &s_ok)) return;
+        for (uint32_t s2 = gt; s2 < npad; s2 += gs) {
+            if (energy)
+                fb_force_one<true>(s2, a.geo, A.pos4, A.skey, a.srep, a.start, n, a.L, st, A.F, fs, a.racc, a.err);
+            else
+                fb_force_one<false>(s2, a.geo, A.pos4, A.skey, a.srep, a.start, n, a.L, st, A.F, fs, a.racc, a.err);
+        }
+        if (!coop_sync(a, &s_ok)) return;
+        for (uint32_t s2 = gt; s2 < n; s2 += gs) fb_finish_one(s2, A, A.idx, a.P.half_dt, fs);
+        if (!coop_sync(a, &s_ok)) return;
+        for (int r = blockIdx.x; r < a.nrep; r += gridDim.x) fb_thermo_one(r, a.th, A, a.lam, a.racc, a.P.k_thermal, a.out, sh);
+        for (uint32_t c = gt; c < m; c += gs) {  // the next tick's counters
+            a.count[c] = 0u;
+            a.fill[c] = 0u;
+        }
+        if (!coop_sync(a, &s_ok)) return;
+    }
+    for (int r = blockIdx.x; r < a.nrep; r += gridDim.x) fb_commit_one(r, a.th, A, a.lam, a.out, sh);
 }
 
 int ferr(gx_batch* b, int code, const std::string& m) {
@@ -424,6 +669,60 @@ int flat_tick(gx_batch* b, BatchParams P, bool energy) {
 }
 
 }  // namespace
+
+// Mode 3: nsteps ticks of every replica in one cooperative launch.
+int batch_coop_step(gx_batch* b, int nsteps, uint64_t* launches) {
+    int rc = flat_prepare(b);
+    if (rc) return rc;
+    if (launches) *launches = 0;
+    if (!b->total || nsteps <= 0) return GX_OK;
+    BatchFlat* f = b->flat;
+    if (!f->coop_bar) {
+        const uint32_t m = f->ncell + 1;
+        const size_t ntiles = (m + kCoopTile - 1) / kCoopTile;
+        GXF_CUDA(b, cudaMalloc(&f->coop_bar, 2 * sizeof(unsigned)));
+        GXF_CUDA(b, cudaMalloc(&f->coop_tile, ntiles * sizeof(uint32_t)));
+        int dev = 0, sms = 0, per_sm = 0, coop = 0;
+        GXF_CUDA(b, cudaGetDevice(&dev));
+        GXF_CUDA(b, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        GXF_CUDA(b, cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+        if (!coop) return ferr(b, GX_ERR_UNSUPPORTED, "the device does not support cooperative launches");
+        GXF_CUDA(b, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fb_coop, kCoopThreads, 0));
+        if (per_sm < 1) return ferr(b, GX_ERR_UNSUPPORTED, "the cooperative batch kernel does not fit on an SM");
+        f->coop_grid = sms * per_sm;
+    }
+    GXF_CUDA(b, cudaMemsetAsync(f->coop_bar, 0, 2 * sizeof(unsigned), b->stream));
+    CoopArgs a;
+    a.geo = f->geo;
+    a.th = f->th;
+    a.rep_of = f->rep_of;
+    a.srep = f->srep;
+    a.lam = f->lam;
+    a.racc = f->acc;
+    a.A = b->A;
+    a.L = b->L;
+    a.tab = b->d_tab;
+    a.out = b->d_out;
+    a.err = b->d_err;
+    a.count = f->ctx->cl.count;
+    a.start = f->ctx->cl.start;
+    a.fill = f->ctx->cl.fill;
+    a.tile = f->coop_tile;
+    a.bar = f->coop_bar;
+    a.ncell = f->ncell;
+    a.total = (uint32_t)b->total;
+    a.nrep = b->nrep;
+    a.P.dt = b->p.dt;
+    a.P.half_dt = 0.5 * b->p.dt;
+    a.P.k_thermal = b->p.thermal_constant;
+    a.P.boundaries = b->p.enable_boundaries ? 1 : 0;
+    a.P.nsteps = nsteps;
+    void* args[] = {&a};
+    GXF_CUDA(b, cudaLaunchCooperativeKernel((const void*)k_fb_coop, dim3(f->coop_grid), dim3(kCoopThreads), args, 0,
+                                            b->stream));
+    if (launches) *launches = 1;
+    return GX_OK;
+}
 
 // nsteps ticks of every replica as one system; device time between the
 // events b->ev[0], b->ev[1] (recorded by the caller).

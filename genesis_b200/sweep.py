@@ -23,7 +23,8 @@ def make_replicas(count: int = 256, seed: int = 0):
 def run_batched(wls, steps: int, device: int = 0, mode: int = 2):
     """Returns (replica-steps/s from the step call's CUDA-event time, stats,
     ms).  mode 1: one persistent launch, one CTA per replica; mode 2: every
-    phase as one kernel over all replicas, CUDA-graph replay."""
+    phase as one kernel over all replicas, CUDA-graph replay; mode 3: mode
+    2's phases in one persistent cooperative launch."""
     base = wls[0].config()
     b = Batch(base, [wl.config().size for wl in wls], [wl.thermostat_temperature for wl in wls], device)
     b.set_mode(mode)

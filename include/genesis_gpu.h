@@ -348,8 +348,9 @@ int gx_set_dynamic(gx_handle* h, const double* pos, const double* vel, const dou
  * after another (examples/temperature_sweep.rs:70-113).  A gx_batch holds
  * nrep independent universes of uneven sizes that share the laws in `base`
  * (mixed precision) and advances all of them together: as one captured
- * graph of all-replica kernels, or in one persistent launch with one CTA per
- * replica (gx_batch_set_mode).  box: 3 doubles per replica; target_T: Berendsen target
+ * graph of all-replica kernels, in one persistent launch with one CTA per
+ * replica, or in one persistent cooperative launch that runs the
+ * all-replica phases for every tick (gx_batch_set_mode).  box: 3 doubles per replica; target_T: Berendsen target
  * per replica (<= 0 or base->enable_thermostat == 0: NVE); NULL uses
  * base->thermostat_temperature.  Each replica's force grid must have >= 1
  * and <= 4096 cells. */
@@ -374,13 +375,18 @@ int gx_batch_get_state(gx_batch* b, double* pos, double* vel, double* acc);
  * replica grid <= 4096 force cells, else GX_ERR_CAPACITY at the step);
  * 2 = every phase of the tick as one kernel over the atoms of all
  * replicas (a global cell index, per-replica geometry), captured once as a
- * CUDA graph; 0 = the default (2).  Both give each NVE replica the same bits
- * as a gx_handle on pair-pass variants 1-4. */
+ * CUDA graph; 3 = the phases of mode 2 inside one persistent cooperative
+ * launch for all the ticks of a step call, separated by grid barriers
+ * whose waits are bounded (GX_ERR_TIMEOUT if one gives up); 0 = the default
+ * (2).  All give each NVE replica the same bits as a gx_handle on pair-pass
+ * variants 1-4, and modes 2 and 3 give each other the same bits with the
+ * thermostat on. */
 int gx_batch_set_mode(gx_batch* b, int mode);
 int gx_batch_get_mode(gx_batch* b, int* mode);
 /* Times `ticks` ticks in each mode from a snapshot of the state (restored
- * afterwards), keeps the faster; ms[0], ms[1] (may be NULL) receive the
- * per-tick device milliseconds of modes 1 and 2. */
+ * afterwards), keeps the fastest; ms[0], ms[1], ms[2] (may be NULL) receive
+ * the per-tick device milliseconds of modes 1, 2 and 3 (-1: mode 1 skipped
+ * because a replica grid exceeds its limit). */
 int gx_batch_autotune(gx_batch* b, int ticks, int* mode, double* ms);
 
 /* ---- adjoint: derivatives of short NVE horizons ----------------------- */

@@ -1,4 +1,5 @@
-"""Batched replicas (one persistent launch) against one gx_handle per replica."""
+"""Batched replicas (persistent launches and the all-replica graph) against
+one gx_handle per replica."""
 from __future__ import annotations
 
 import numpy as np
@@ -44,7 +45,7 @@ def _batch(wls, steps, mode=2):
     return out, st, ms
 
 
-@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("mode", [1, 2, 3])
 def test_batch_nve_matches_single_universes_bit_for_bit(gpu, mode):
     wls = _replicas(thermo=False)
     out, st, ms = _batch(wls, 6, mode)
@@ -57,7 +58,7 @@ def test_batch_nve_matches_single_universes_bit_for_bit(gpu, mode):
         assert st[k, 1] == rst["potential"][-1]
 
 
-@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("mode", [1, 2, 3])
 def test_batch_nvt_matches_single_universes(gpu, mode):
     wls = _replicas(thermo=True)
     out, st, _ = _batch(wls, 5, mode)
@@ -99,9 +100,31 @@ def test_batch_modes_agree_and_autotune_restores_state(gpu):
     b.set_universes([wl.generate() for wl in wls])
     before = b.get_state()
     mode, ms = b.autotune(ticks=3)
-    assert mode in (1, 2) and ms[1] > 0 and ms[2] > 0
+    assert mode in (1, 2, 3) and ms[1] > 0 and ms[2] > 0 and ms[3] > 0
     after = b.get_state()
     for x, y in zip(before, after):
         for p, q in zip(x, y):
             assert np.array_equal(p, q)
     b.close()
+
+
+def test_cooperative_launch_matches_the_graph_bit_for_bit(gpu):
+    # mode 3 runs mode 2's phases inside one launch: the same bits, thermostat
+    # on, over step calls of several lengths (the last tick of each reports)
+    wls = _replicas(thermo=True)
+    runs = []
+    for mode in (2, 3):
+        from genesis_b200._lib import Batch
+        base = wls[0].config()
+        base.enable_thermostat = True
+        b = Batch(base, [wl.config().size for wl in wls], [wl.thermostat_temperature for wl in wls])
+        b.set_mode(mode)
+        b.set_universes([wl.generate() for wl in wls])
+        sts = [b.step(k)[0] for k in (1, 7, 30)]
+        runs.append((b.get_state(), sts))
+        b.close()
+    for x, y in zip(runs[0][0], runs[1][0]):
+        for p, q in zip(x, y):
+            assert np.array_equal(p, q)
+    for a, c in zip(runs[0][1], runs[1][1]):
+        assert np.array_equal(a, c)
