@@ -813,8 +813,31 @@ def ours_arm(args, dist):
             am = hm.get_state()[2]
             a64 = h64.get_state()[2]
             rel = float(np.linalg.norm(am - a64) / np.linalg.norm(a64))
+            # the FP64 pair pass against the FP64 pipe: each unique in-cutoff
+            # pair's algorithmic FLOPs (the same count as the mixed pass) over
+            # the pass time (the full list visits every pair from both ends)
+            h64.set_state(pos, vel, u.elem, acc=acc, charge=u.charge, mass=u.mass, entity=u.entity)
+            h64.step(2, stats=True)
+            h64.profile(True)
+            pairs64 = float(h64.step(10, stats=True)["pairs"].mean())
+            p64 = h64.profile_read(reset=True)
+            h64.profile(False)
+            k64 = "force_nl" if "force_nl" in p64 else "force_f64"
+            nl64, t64 = p64.get(k64, (1, float("nan")))
+            pass64_ms = t64 / max(nl64, 1)
+            try:
+                peak64 = _lib.measure_fp64_peak(dev)
+                peak64_src = "measured: FP64 FMA loop on all SMs (gx_measure_fp64_peak)"
+            except Exception as e:  # noqa: BLE001
+                peak64, peak64_src = 37.0, f"nominal ({e})"
+            ach64 = pairs64 * flop_pp / (pass64_ms * 1e-3) / 1e12
             extras["fp64"] = {"value": v64, "ms_per_step": ms64 / K64, "steps": K64,
-                              "mixed_over_fp64": value / v64}
+                              "mixed_over_fp64": value / v64,
+                              "tick": "the same tick on the plain FP64 path: the persistent full neighbour list, "
+                                      "the reference's FP64 per-pair arithmetic (k_nl_force64)",
+                              "roofline": {"kernel": k64, "bound": "fp64", "achieved": ach64, "peak": peak64,
+                                           "unit": "TFLOP/s", "frac": ach64 / peak64, "peak_source": peak64_src,
+                                           "launch_ms": pass64_ms, "flop_per_pair": flop_pp}}
             extras["force_rel_rms_vs_fp64"] = rel
             extras["potential_rel_err_vs_fp64"] = abs(Vm - V64) / abs(V64)
             hm.close()

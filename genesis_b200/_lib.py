@@ -63,7 +63,7 @@ EXPORTS = (
     "gx_cell_assign", "gx_neighbors", "gx_radial_distribution",
     "gx_radial_distribution_between", "gx_clusters", "gx_bound_pairs",
     "gx_synchronize", "gx_profile_enable", "gx_profile_read", "gx_set_dynamic",
-    "gx_timer_mark", "gx_timer_elapsed", "gx_launch_count", "gx_measure_fp32_peak",
+    "gx_timer_mark", "gx_timer_elapsed", "gx_launch_count", "gx_measure_fp32_peak", "gx_measure_fp64_peak",
     "gx_radial_distribution_noalloc", "gx_set_kernel_variant", "gx_autotune",
     "gx_batch_create", "gx_batch_destroy", "gx_batch_last_error", "gx_batch_set_state",
     "gx_batch_step", "gx_batch_get_state", "gx_adjoint_forward", "gx_adjoint_backward",
@@ -119,6 +119,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
         "gx_timer_elapsed": (C.c_int, [vp, C.c_int, C.c_int, dp]),
         "gx_launch_count": (C.c_uint64, [vp]),
         "gx_measure_fp32_peak": (C.c_int, [C.c_int, dp]),
+        "gx_measure_fp64_peak": (C.c_int, [C.c_int, dp]),
         "gx_radial_distribution_noalloc": (C.c_int, [sz, dp, dp, _D, sz, u64p, dp, dp, dp]),
         "gx_set_kernel_variant": (C.c_int, [vp, C.c_int]),
         "gx_autotune": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), dp]),
@@ -548,6 +549,16 @@ def measure_fp32_peak(device: int = 0) -> float:
     rc = lib.gx_measure_fp32_peak(device, C.byref(t))
     if rc != 0:
         raise GxError(rc, "gx_measure_fp32_peak failed")
+    return t.value
+
+
+def measure_fp64_peak(device: int = 0) -> float:
+    """Measured FP64 FMA throughput (TFLOP/s) of the device."""
+    lib = load()
+    t = C.c_double()
+    rc = lib.gx_measure_fp64_peak(device, C.byref(t))
+    if rc != 0:
+        raise GxError(rc, "gx_measure_fp64_peak failed")
     return t.value
 
 

@@ -218,6 +218,20 @@ __global__ void k_fma_peak(float* out, int iters, float seed) {
     for (int k = 0; k < 8; ++k) s += a[k];
     if (s == 12345.678f) out[threadIdx.x] = s;  // keeps the chains live
 }
+__global__ void k_fma_peak_f64(double* out, int iters, double seed) {
+    double a[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = seed + 1e-3 * (threadIdx.x + k);
+    const double m = 0.9999999999, c = 1e-12;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a[k] = fma(a[k], m, c);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += a[k];
+    if (s == 12345.678) out[threadIdx.x] = s;  // keeps the chains live
+}
 __global__ void k_init_slots(StateBuf b, uint32_t* pos_of_slot, uint32_t n) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -1135,6 +1149,39 @@ int gx_measure_fp32_peak(int device, double* tflops) {
         cudaEventElapsedTime(&t, a, b);
         // 8 independent FMA chains x iters per thread, 2 FLOP per FMA
         double flop = 2.0 * 8.0 * iters * (double)threads * blocks;
+        double tf = flop / (t * 1e-3) / 1e12;
+        if (tf > best) best = tf;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaError_t e = cudaGetLastError();
+    cudaFree(out);
+    if (e != cudaSuccess) return GX_ERR_CUDA;
+    *tflops = best;
+    return GX_OK;
+}
+
+int gx_measure_fp64_peak(int device, double* tflops) {
+    if (!tflops) return GX_ERR_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return GX_ERR_CUDA;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    double* out = nullptr;
+    if (cudaMalloc(&out, 1024 * sizeof(double)) != cudaSuccess) return GX_ERR_OOM;
+    const int iters = 2048, threads = 512, blocks = sms * 8;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    k_fma_peak_f64<<<blocks, threads>>>(out, iters, 1.0);  // warm-up
+    double best = 0.0;
+    for (int rep = 0; rep < 5; ++rep) {
+        cudaEventRecord(a);
+        k_fma_peak_f64<<<blocks, threads>>>(out, iters, 1.0 + rep * 1e-9);
+        cudaEventRecord(b);
+        cudaEventSynchronize(b);
+        float t = 0.f;
+        cudaEventElapsedTime(&t, a, b);
+        double flop = 2.0 * 8.0 * iters * (double)threads * blocks;  // 8 FMA chains, 2 FLOP per FMA
         double tf = flop / (t * 1e-3) / 1e12;
         if (tf > best) best = tf;
     }

@@ -454,6 +454,10 @@ uint64_t gx_launch_count(const gx_handle* h);
 /* Diagnostic: measured FP32 FMA throughput of this GPU in TFLOP/s (a
  * dependent-FMA loop on every SM; roofline denominator for the pair pass). */
 int gx_measure_fp32_peak(int device, double* tflops);
+/* The same measurement for the FP64 pipe (independent FP64 FMA chains on every
+ * SM): the denominator of the plain FP64 pair pass's roofline.  No
+ * counterpart in the reference. */
+int gx_measure_fp64_peak(int device, double* tflops);
 /* Per-kernel CUDA-event timing of gx_step/gx_forces launches (on the
  * handle's stream).  When enabled, each launch is bracketed by events. */
 int gx_profile_enable(gx_handle* h, int on);
