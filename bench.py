@@ -81,7 +81,8 @@ def parse():
                     help="fix the mixed pair-pass variant instead of autotuning (profiling only)")
     ap.add_argument("--skin", type=float, default=-1.0,
                     help="neighbour-list skin in length units instead of 0.1 r_c (profiling only; 0 = rebuild every tick)")
-    ap.add_argument("--leg", default="", choices=["", "ionic", "accuracy", "adjoint", "xyz", "sweep", "c1"],
+    ap.add_argument("--leg", default="",
+                    choices=["", "ionic", "accuracy", "adjoint", "xyz", "sweep", "c1", "rebuild", "gr", "fp64"],
                     help="run one extra leg alone and print its JSON (profiling only)")
     ap.add_argument("--leg-steps", type=int, default=0, help="ticks of the --leg run (0: the workload's own)")
     return ap.parse_args()
@@ -649,6 +650,46 @@ def ionic_leg(dev: int, cpu: bool, steps: int | None = None, cpu_budget_s: float
     return out
 
 
+def kernel_leg(args, dev: int) -> dict:
+    """Profiling legs on the quench workload (scaled by --n-side): `rebuild`
+    runs eager ticks that each rebuild the neighbour list (setting the skin
+    again forces one), so every launch of the rebuild kernels does its work;
+    `gr` runs g(r) of the whole state (no subsample); `fp64` runs eager
+    ticks of the plain FP64 path.  Prints per-kernel device times."""
+    import dataclasses
+
+    from genesis_b200 import workloads as W
+    from genesis_b200._lib import Handle
+
+    wl = W.C3 if args.n_side <= 0 else dataclasses.replace(W.C3, n_side=args.n_side)
+    cfg, u = wl.config(), wl.generate()
+    reps = args.leg_steps or 5
+    prec = "fp64" if args.leg == "fp64" else "mixed"
+    with Handle(cfg, prec, dev) as h:
+        if args.variant >= 0:
+            h.set_kernel_variant(args.variant)
+        h.set_universe(u)
+        h.step(2, stats=True)
+        h.profile(True)
+        if args.leg == "rebuild":
+            skin, _ = h.list_config()
+            for _ in range(reps):
+                h.set_list_skin(skin)
+                h.step(1, stats=True)
+        elif args.leg == "gr":
+            for _ in range(reps):
+                h.radial_distribution(17.25, 256, sample_cap=u.n)
+        else:
+            h.step(reps, stats=True)
+        prof = h.profile_read(reset=True)
+        h.profile(False)
+        entries, overflowed = h.list_stats()
+    return {"workload": f"{wl.name} at {u.n} atoms, {prec}", "reps": reps, "list_entries": entries,
+            "overflowed_atoms": overflowed,
+            "kernels_ms_per_launch": {k: v[1] / max(v[0], 1) for k, v in prof.items()},
+            "launches": {k: v[0] for k, v in prof.items()}}
+
+
 def reference_arm(args, dist):
     if dist.rank != 0:
         return
@@ -1031,6 +1072,8 @@ def main():
                 h.step(2)
                 out = xyz_leg(h, u.elem, 2, cpu=True)
                 h.close()
+            elif args.leg in ("rebuild", "gr", "fp64"):
+                out = kernel_leg(args, dev)
             else:
                 out = adjoint_leg(dev)
             if dist.rank == 0:
