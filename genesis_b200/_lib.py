@@ -68,7 +68,7 @@ EXPORTS = (
     "gx_batch_create", "gx_batch_destroy", "gx_batch_last_error", "gx_batch_set_state",
     "gx_batch_step", "gx_batch_get_state", "gx_adjoint_forward", "gx_adjoint_backward",
     "gx_set_list_skin", "gx_list_rebuilds", "gx_list_stats", "gx_batch_set_mode", "gx_batch_get_mode", "gx_batch_autotune",
-    "gx_get_list_config", "gx_set_list_threads", "gx_set_list_stash", "gx_bond_observe", "gx_bond_tracker_reset", "gx_get_bonds",
+    "gx_get_list_config", "gx_set_list_threads", "gx_set_list_stash", "gx_set_list_brick", "gx_bond_observe", "gx_bond_tracker_reset", "gx_get_bonds",
     "gx_bond_components", "gx_collisions", "gx_collision_count", "gx_xyz_frame", "gx_snapshot_world",
     "gx_set_step_async",
 )
@@ -130,6 +130,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
         "gx_get_list_config": (C.c_int, [vp, dp, C.POINTER(C.c_int)]),
         "gx_set_list_threads": (C.c_int, [vp, C.c_int]),
         "gx_set_list_stash": (C.c_int, [vp, C.c_int]),
+        "gx_set_list_brick": (C.c_int, [vp, C.c_int]),
         "gx_bond_observe": (C.c_int, [vp, _D, _D, C.c_int, C.c_uint64, C.c_int, C.POINTER(GxBondObservation)]),
         "gx_bond_tracker_reset": (C.c_int, [vp]),
         "gx_get_bonds": (C.c_int, [vp, u32p, sz, C.POINTER(sz)]),
@@ -265,15 +266,17 @@ class Handle:
         3 staged rows, 4 per-thread candidate lists, 5 persistent full
         neighbour list, 6 persistent half list with far-end atomics, 7 the
         half list with each thread's in-cutoff entries collected in shared
-        memory before the warp evaluates them (same forces as 6)."""
+        memory before the warp evaluates them (same forces as 6), 8 the half
+        list brick by brick with the brick's neighbourhood staged in shared
+        memory (same forces as 6)."""
         self._check(self.lib.gx_set_kernel_variant(self.h, variant))
 
     def autotune(self, reps: int = 5):
         """Times every applicable pair-pass variant and keeps the fastest;
         returns (variant, {variant: ms}) -- ms per pass for 1-4, ms per tick
-        for 5, 6, 7 and 0 (the tick of the best of 1-4)."""
+        for 5-8 and 0 (the tick of the best of 1-4)."""
         best = C.c_int()
-        ms = np.full(8, -1.0)
+        ms = np.full(9, -1.0)
         self._check(self.lib.gx_autotune(self.h, reps, C.byref(best), _ptr(ms, C.c_double)))
         return best.value, {v: float(t) for v, t in enumerate(ms) if t >= 0}
 
@@ -293,6 +296,10 @@ class Handle:
     def set_list_stash(self, slots: int):
         """Stash slots per thread of the variant-7 list pass (8 or 16)."""
         self._check(self.lib.gx_set_list_stash(self.h, slots))
+
+    def set_list_brick(self, cells: int):
+        """Brick length of the variant-8 list pass (4 or 8 cells)."""
+        self._check(self.lib.gx_set_list_brick(self.h, cells))
 
     def list_stats(self) -> tuple[int, int]:
         """(entries held by the neighbour list, atoms whose list overflowed)."""

@@ -49,6 +49,7 @@ struct NlState {
     int half = -1;            // list kind built: 0 full, 1 half (variant 6)
     int tpp = 1;              // threads per atom in the list pass (1, 2, 4, 8)
     int slots = 16;           // variant 7: stash slots per thread (8 or 16)
+    int brick = 1;            // variant 8: 0 = bricks of 4 cells (1024 staged atoms), 1 = 8 cells (2048)
     int cap_nb = 0;           // list entries per atom
     size_t cap = 0;           // atoms the buffers hold
     uint32_t* list = nullptr; // entry e of atom p at list[e * cap + p]
@@ -635,12 +636,181 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force_cmp(GridGeom g, const f
     }
 }
 
+// Variant 8: the half list of variant 6, evaluated brick by brick with the
+// brick's neighbourhood staged in shared memory.  A brick is K consecutive
+// list-grid cells of one x-row; atoms are sorted by cell, so its home atoms
+// are one contiguous range, and the neighbour cells of every home cell lie
+// in the 9 rows (y +- 1, z +- 1) over x0 - 1 .. x0 + K, each at most two
+// contiguous ranges of sorted atoms (two where the x-range wraps).  The block
+// copies those ranges of staged positions into shared memory once; each
+// thread then walks a home atom's list and reads its partners from there: a
+// partner in neighbour-cell code c lies in row c / 3, whose ranges give its
+// shared-memory slot.  Same pairs and per-pair operations as variant 6:
+// bit-identical forces.  A brick whose neighbourhood exceeds CAP atoms reads
+// its partners from global memory instead.
+// The staged position of list entry w: its row is code / 3 (code = (ox+1) +
+// 3 (oy+1) + 9 (oz+1)); piece A when the partner lies in its range, else
+// piece B.  A slot outside the staged range (not expected) reads global memory.
+__device__ __forceinline__ float4 brick_pos(uint32_t w, bool staged, const float4* s_pos, uint32_t total,
+                                            const uint32_t* gA, const uint32_t* eA, const uint32_t* oA,
+                                            const uint32_t* gB, const uint32_t* oB, const float4* __restrict__ pos4) {
+    const uint32_t q = w & kIdxMask;
+    if (!staged) return __ldg(pos4 + q);
+    const uint32_t r = (w >> 27) / 3u;
+    const uint32_t idx = q - gA[r] < eA[r] - gA[r] ? oA[r] + (q - gA[r]) : oB[r] + (q - gB[r]);
+    return idx < total ? s_pos[idx] : __ldg(pos4 + q);
+}
+
+template <bool ENERGY, int CAP>
+__global__ void __launch_bounds__(kNlThreads) k_nl_force_brick(GridGeom g, const float4* __restrict__ pos4,
+                                                                const uint32_t* __restrict__ home,
+                                                                const uint32_t* __restrict__ start, uint32_t n,
+                                                                LawF32 L, const PairF* __restrict__ tab,
+                                                                const uint32_t* __restrict__ list, size_t stride,
+                                                                int cap_nb, const uint32_t* __restrict__ cnt,
+                                                                long long* __restrict__ F, size_t fstride,
+                                                                unsigned long long* __restrict__ vacc,
+                                                                unsigned long long* __restrict__ npairs,
+                                                                uint32_t* __restrict__ err, uint32_t K,
+                                                                uint32_t nchunks) {
+    __shared__ PairF st[kMaxKinds * kMaxKinds];
+    __shared__ float4 s_shift[27];
+    __shared__ unsigned long long shu[kNlThreads / 32];
+    __shared__ float4 s_pos[CAP];
+    __shared__ uint32_t s_gA[9], s_eA[9], s_oA[9], s_gB[9], s_eB[9], s_oB[9];
+    __shared__ uint32_t s_total;
+    const int nk2 = L.nkinds * L.nkinds;
+    for (int t = threadIdx.x; t < nk2; t += kNlThreads) st[t] = tab[t];
+    if (threadIdx.x < 27) {
+        float sx, sy, sz;
+        code_shift(g, threadIdx.x, sx, sy, sz);
+        s_shift[threadIdx.x] = make_float4(sx, sy, sz, 0.f);
+    }
+    const uint32_t nx = g.n[0], ny = g.n[1], nz = g.n[2];
+    const uint32_t row = blockIdx.x / nchunks, chunk = blockIdx.x - row * nchunks;
+    const uint32_t cy = row % ny, cz = row / ny;
+    const uint32_t x0 = chunk * K, x1 = min(x0 + K, nx);  // home cells x0 .. x1 - 1
+    if (threadIdx.x < 9) {
+        const int dy = (int)(threadIdx.x % 3) - 1, dz = (int)(threadIdx.x / 3) - 1;
+        const uint32_t rb = nx * (wrap_add(cy, dy, ny) + ny * wrap_add(cz, dz, nz));  // cell x = 0 of the row
+        uint32_t gA, eA, gB = 0, eB = 0;
+        if (x1 - x0 + 2 >= nx) {  // cells x0 - 1 .. x1 cover the whole row
+            gA = start[rb];
+            eA = start[rb + nx];
+        } else if (x0 == 0) {  // cell nx - 1, then 0 .. x1
+            gA = start[rb + nx - 1];
+            eA = start[rb + nx];
+            gB = start[rb];
+            eB = start[rb + x1 + 1];
+        } else if (x1 == nx) {  // x0 - 1 .. nx - 1, then cell 0
+            gA = start[rb + x0 - 1];
+            eA = start[rb + nx];
+            gB = start[rb];
+            eB = start[rb + 1];
+        } else {
+            gA = start[rb + x0 - 1];
+            eA = start[rb + x1 + 1];
+        }
+        s_gA[threadIdx.x] = gA;
+        s_eA[threadIdx.x] = eA;
+        s_gB[threadIdx.x] = gB;
+        s_eB[threadIdx.x] = eB;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t off = 0;
+        for (int r = 0; r < 9; ++r) {
+            s_oA[r] = off;
+            off += s_eA[r] - s_gA[r];
+            s_oB[r] = off;
+            off += s_eB[r] - s_gB[r];
+        }
+        s_total = off;
+    }
+    __syncthreads();
+    const bool staged = s_total <= (uint32_t)CAP;
+    if (staged) {
+        for (int r = 0; r < 9; ++r) {
+            const uint32_t la = s_eA[r] - s_gA[r], lb = s_eB[r] - s_gB[r];
+            for (uint32_t k = threadIdx.x; k < la; k += kNlThreads) s_pos[s_oA[r] + k] = pos4[s_gA[r] + k];
+            for (uint32_t k = threadIdx.x; k < lb; k += kNlThreads) s_pos[s_oB[r] + k] = pos4[s_gB[r] + k];
+        }
+    }
+    __syncthreads();
+    const uint32_t hb = nx * (cy + ny * cz);
+    const uint32_t hlo = start[hb + x0], hhi = start[hb + x1];
+    PairAcc a;
+    for (uint32_t p = hlo + threadIdx.x; p < hhi; p += kNlThreads) {
+        const float4 pi = pos4[p];
+        const int ki = __float_as_int(pi.w);
+        const uint32_t m = cnt[p];
+        a.fx = a.fy = a.fz = 0;  // this atom's own sums (the potential and pair count run on)
+        if (m <= (uint32_t)cap_nb) {
+            const uint32_t* lp = list + p;
+            uint32_t e = 0;
+            for (; e + 4 <= m; e += 4) {
+                uint32_t w[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) w[u] = __ldg(lp + (size_t)(e + u) * stride);
+                float4 pj[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) pj[u] = brick_pos(w[u], staged, s_pos, s_total, s_gA, s_eA, s_oA, s_gB, s_oB, pos4);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const float4 sh = s_shift[w[u] >> 27];
+                    const uint32_t q = w[u] & kIdxMask;
+                    nl_pair(L, st, ki, pi, pj[u], sh.x, sh.y, sh.z, ENERGY && q > p, a, err, F, q, fstride);
+                }
+            }
+            for (; e < m; ++e) {
+                const uint32_t w = __ldg(lp + (size_t)e * stride);
+                const uint32_t q = w & kIdxMask;
+                const float4 pj = brick_pos(w, staged, s_pos, s_total, s_gA, s_eA, s_oA, s_gB, s_oB, pos4);
+                const float4 sh = s_shift[w >> 27];
+                nl_pair(L, st, ki, pi, pj, sh.x, sh.y, sh.z, ENERGY && q > p, a, err, F, q, fstride);
+            }
+        } else {  // overflowed list: scan the home-grid cells directly
+            uint32_t cx, ccy, ccz;
+            const uint32_t c = home[p];
+            decode(g, c, cx, ccy, ccz);
+            for (uint32_t code = 0; code < 27; ++code) {
+                const uint32_t B = cell_at(g, cx, ccy, ccz, code);
+                if (B < c) continue;
+                const float4 sh = s_shift[code];
+                for (uint32_t q = start[B], hi = start[B + 1]; q < hi; ++q)
+                    if (q > p) nl_pair(L, st, ki, pi, pos4[q], sh.x, sh.y, sh.z, ENERGY, a, err, F, q, fstride);
+            }
+        }
+        atomicAdd((unsigned long long*)&F[p], (unsigned long long)a.fx);
+        atomicAdd((unsigned long long*)&F[fstride + p], (unsigned long long)a.fy);
+        atomicAdd((unsigned long long*)&F[2 * fstride + p], (unsigned long long)a.fz);
+    }
+    if (ENERGY) {
+        unsigned long long sv = block_sum_u<kNlThreads>((unsigned long long)a.vq, shu);
+        unsigned long long np = block_sum_u<kNlThreads>(a.np, shu);
+        if (threadIdx.x == 0) {
+            if (sv) atomicAdd(vacc, sv);
+            if (np) atomicAdd(npairs, np);
+        }
+    }
+}
+
 template <bool HALF>
 void launch_nl_force(gx_handle* h, int tpp, const GridGeom& g, const NlState* s, uint32_t n, const LawF32& L,
                      bool energy) {
     const float4* pos4 = h->pos4;
     const uint32_t* home = h->key_sorted;
     const uint32_t* start = s->cl.start;
+    if (HALF && h->kernel_variant == 8) {
+        const uint32_t K = s->brick == 0 ? 4u : 8u;
+        const uint32_t nchunks = (g.n[0] + K - 1) / K;
+        const unsigned nb = nchunks * g.n[1] * g.n[2];
+        auto kb = s->brick == 0 ? (energy ? k_nl_force_brick<true, 1024> : k_nl_force_brick<false, 1024>)
+                                : (energy ? k_nl_force_brick<true, 2048> : k_nl_force_brick<false, 2048>);
+        GX_LAUNCH(h, kb, nb, kNlThreads, g, pos4, home, start, n, L, h->d_pairf, s->list, s->cap, s->cap_nb, s->cnt,
+                  h->F, h->cap, h->dcount + 1, h->dcount + 0, h->derr, K, nchunks);
+        return;
+    }
     if (HALF && h->kernel_variant == 7) {
         auto kc = s->slots == 8 ? (energy ? k_nl_force_cmp<true, 8> : k_nl_force_cmp<false, 8>)
                                 : (energy ? k_nl_force_cmp<true, 16> : k_nl_force_cmp<false, 16>);
@@ -1073,14 +1243,16 @@ int nl_tune_tpp(gx_handle* h, int reps) {
     if (!s->list || !s->cap || h->n == 0) return GX_OK;
     const uint32_t n = (uint32_t)h->n;
     const LawF32 L = make_law32(h);
-    // variant 7: the stash size (8 or 16 slots per thread); else threads per atom
-    const bool stash = h->kernel_variant == 7;
+    // variant 7: the stash size (8 or 16 slots per thread); variant 8: the
+    // brick length (4 or 8 cells); else threads per atom
+    const bool stash = h->kernel_variant == 7, brick = h->kernel_variant == 8;
     const int cand[4] = {1, 2, 4, 8};
-    const int ncand = stash ? 2 : 4;
+    const int ncand = (stash || brick) ? 2 : 4;
     double best = 1e300;
-    int pick = stash ? s->slots : s->tpp;
+    int pick = stash ? s->slots : (brick ? s->brick : s->tpp);
     for (int k = 0; k < ncand; ++k) {
         if (stash) s->slots = k == 0 ? 8 : 16;
+        if (brick) s->brick = k;
         int rc = gx_timer_mark(h, 14);
         for (int r = 0; r < reps && !rc; ++r) {
             if (s->half == 1) launch_nl_force<true>(h, cand[k], s->lg, s, n, L, false);
@@ -1092,10 +1264,11 @@ int nl_tune_tpp(gx_handle* h, int reps) {
         if (rc) return rc;
         if (t / reps < best) {
             best = t / reps;
-            pick = stash ? s->slots : cand[k];
+            pick = stash ? s->slots : (brick ? k : cand[k]);
         }
     }
     if (stash) s->slots = pick;
+    else if (brick) s->brick = pick;
     else s->tpp = pick;
     GX_CUDA(h, cudaMemsetAsync(h->derr, 0, sizeof(uint32_t), h->stream));
     return GX_OK;
@@ -1142,6 +1315,12 @@ int nl_config(gx_handle* h, double* skin, int* tpp) {
     NlState* s = nl_of(h);
     if (skin) *skin = skin_of(h, s);
     if (tpp) *tpp = s->tpp;
+    return GX_OK;
+}
+
+int nl_set_brick(gx_handle* h, int cells) {
+    if (cells != 4 && cells != 8) return set_err(h, GX_ERR_ARG, "brick length must be 4 or 8 cells");
+    nl_of(h)->brick = cells == 4 ? 0 : 1;
     return GX_OK;
 }
 

@@ -116,25 +116,29 @@ int gx_set_precision(gx_handle* h, int precision);
  * half list (each pair once, the far end's force through integer atomics);
  * 7 = the half list of 6 with each thread's in-cutoff entries first
  * collected in shared memory, so that the warp evaluates the pair law on
- * them together (fewer idle lanes; same forces as 6, bit for bit).
- * 5, 6 and 7 need >= 3 list-grid cells per axis, else they fall back to 4.  Variants 2 and 3 need >= 3 force-grid
+ * them together (fewer idle lanes; same forces as 6, bit for bit);
+ * 8 = the half list of 6 evaluated brick by brick (4 or 8 list-grid cells of
+ * one x-row), the brick's neighbour rows staged in shared memory once and
+ * read from there (same forces as 6, bit for bit).
+ * 5-8 need >= 3 list-grid cells per axis, else they fall back to 4.  Variants 2 and 3 need >= 3 force-grid
  * cells per axis and fall back to 1 otherwise.  Variants 1-4 give
- * bit-identical forces, and so do 5, 6 and 7 (fixed-point sums); 5-7
+ * bit-identical forces, and so do 5-8 (fixed-point sums); 5-8
  * evaluate the same pair set in a cell-local frame whose origin is the
  * atom's cell at the last rebuild, so their FP32 forces can differ from 1-4
  * in the last bits (same error bound). */
 int gx_set_kernel_variant(gx_handle* h, int variant);
 /* Autotuner: times `reps` mixed pair passes of variants 1-4 on the resident
  * state (left bit-identical: they give the same fixed-point sums) and, where
- * variants 5-7 apply, full ticks of the best of them against full ticks
- * of 5, 6 and 7, each from a snapshot of (x, v, a) restored afterwards.
+ * variants 5-8 apply, full ticks of the best of them against full ticks
+ * of 5, 6, 7 and 8, each from a snapshot of (x, v, a) restored afterwards.
  * Selects the fastest and returns it in *best.  ms[1..4], when given,
- * receive the per-pass milliseconds, ms[0], ms[5], ms[6], ms[7] the
- * per-tick milliseconds of the best pass variant, of 5, 6 and 7 (-1 = not
- * run); ms has 8 entries.  Where a list variant wins, the list skin is
+ * receive the per-pass milliseconds, ms[0], ms[5..8] the per-tick
+ * milliseconds of the best pass variant and of 5-8 (-1 = not run); ms has
+ * 9 entries.  Where a list variant wins, the list skin is
  * then chosen the same way over whole ticks among 0.05, 0.1, 0.15 and
  * 0.2 r_c (the list-grid cell is r_c + skin; gx_get_list_config reports
- * the choice), and the lanes per atom (or the stash size of 7) over passes
+ * the choice), and the lanes per atom (the stash size of 7, the brick
+ * length of 8) over passes
  * on a list of that skin.  The state is left as it was. */
 int gx_autotune(gx_handle* h, int reps, int* best, double* ms);
 /* No counterpart in the reference.  Skin of the variant-5/6 neighbour list
@@ -150,6 +154,11 @@ int gx_set_list_threads(gx_handle* h, int threads_per_atom);
  * (default 16; the autotuner picks the faster).  Both give the same bits.
  * No counterpart in the reference. */
 int gx_set_list_stash(gx_handle* h, int slots);
+/* Brick length of the variant-8 list pass: 4 or 8 list-grid cells per brick
+ * (at most 1024 or 2048 staged atoms; a brick with more reads global
+ * memory).  Default 8; the autotuner picks the faster.  Both give the same
+ * bits.  No counterpart in the reference. */
+int gx_set_list_brick(gx_handle* h, int cells);
 /* Skin and threads per atom of the variant-5/6 list pass. */
 int gx_get_list_config(gx_handle* h, double* skin, int* threads_per_atom);
 /* Occupancy of the current neighbour list: the entries it holds (pairs
