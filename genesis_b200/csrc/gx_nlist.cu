@@ -642,7 +642,8 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force_cmp(GridGeom g, const f
 // are one contiguous range, and the neighbour cells of every home cell lie
 // in the 9 rows (y +- 1, z +- 1) over x0 - 1 .. x0 + K, each at most two
 // contiguous ranges of sorted atoms (two where the x-range wraps).  The block
-// copies those ranges of staged positions into shared memory once; each
+// copies those ranges of staged positions into shared memory once, as TMA
+// bulk copies (cp.async.bulk, completing on an mbarrier); each
 // thread then walks a home atom's list and reads its partners from there: a
 // partner in neighbour-cell code c lies in row c / 3, whose ranges give its
 // shared-memory slot.  Same pairs and per-pair operations as variant 6:
@@ -661,6 +662,8 @@ __device__ __forceinline__ float4 brick_pos(uint32_t w, bool staged, const float
     return idx < total ? s_pos[idx] : __ldg(pos4 + q);
 }
 
+constexpr uint32_t kBrickWaitLimit = 1u << 20;  // polls of the staging mbarrier before giving up
+
 template <bool ENERGY, int CAP>
 __global__ void __launch_bounds__(kNlThreads) k_nl_force_brick(GridGeom g, const float4* __restrict__ pos4,
                                                                 const uint32_t* __restrict__ home,
@@ -676,9 +679,10 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force_brick(GridGeom g, const
     __shared__ PairF st[kMaxKinds * kMaxKinds];
     __shared__ float4 s_shift[27];
     __shared__ unsigned long long shu[kNlThreads / 32];
-    __shared__ float4 s_pos[CAP];
+    __shared__ __align__(16) float4 s_pos[CAP];
     __shared__ uint32_t s_gA[9], s_eA[9], s_oA[9], s_gB[9], s_eB[9], s_oB[9];
     __shared__ uint32_t s_total;
+    __shared__ __align__(8) unsigned long long s_mbar;
     const int nk2 = L.nkinds * L.nkinds;
     for (int t = threadIdx.x; t < nk2; t += kNlThreads) st[t] = tab[t];
     if (threadIdx.x < 27) {
@@ -729,14 +733,51 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force_brick(GridGeom g, const
     }
     __syncthreads();
     const bool staged = s_total <= (uint32_t)CAP;
-    if (staged) {
+    // The staged ranges are contiguous runs of float4 (16-byte aligned, whole
+    // 16-byte items), so one thread issues them as TMA bulk copies that
+    // complete on one mbarrier; every thread then waits, a bounded number of
+    // polls, for the bytes to land.
+    const uint32_t mbar = (uint32_t)__cvta_generic_to_shared(&s_mbar);
+    if (staged && s_total && threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(s_total * 16u)
+                     : "memory");
         for (int r = 0; r < 9; ++r) {
-            const uint32_t la = s_eA[r] - s_gA[r], lb = s_eB[r] - s_gB[r];
-            for (uint32_t k = threadIdx.x; k < la; k += kNlThreads) s_pos[s_oA[r] + k] = pos4[s_gA[r] + k];
-            for (uint32_t k = threadIdx.x; k < lb; k += kNlThreads) s_pos[s_oB[r] + k] = pos4[s_gB[r] + k];
+            const uint32_t gs[2] = {s_gA[r], s_gB[r]}, ln[2] = {s_eA[r] - s_gA[r], s_eB[r] - s_gB[r]},
+                           os[2] = {s_oA[r], s_oB[r]};
+            for (int k = 0; k < 2; ++k) {
+                if (!ln[k]) continue;
+                const uint32_t dst = (uint32_t)__cvta_generic_to_shared(s_pos + os[k]);
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                    "l"(pos4 + gs[k]), "r"(ln[k] * 16u), "r"(mbar)
+                    : "memory");
+            }
         }
     }
     __syncthreads();
+    if (staged && s_total) {
+        auto wait = [&](uint32_t limit) -> bool {
+            for (uint32_t it = 0; it < limit; ++it) {
+                uint32_t done = 0;
+                asm volatile(
+                    "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                    : "=r"(done)
+                    : "r"(mbar), "r"(0u)
+                    : "memory");
+                if (done) return true;
+            }
+            return false;
+        };
+        const bool ok = wait(kBrickWaitLimit);
+        if (__syncthreads_or(!ok)) {  // every thread leaves together
+            if (!ok) wait(kBrickWaitLimit);  // let copies still in flight land before the block exits
+            if (threadIdx.x == 0) atomicOr(err, kErrTimeout);
+            return;
+        }
+    }
     const uint32_t hb = nx * (cy + ny * cz);
     const uint32_t hlo = start[hb + x0], hhi = start[hb + x1];
     PairAcc a;
