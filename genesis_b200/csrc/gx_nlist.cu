@@ -636,60 +636,35 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force_cmp(GridGeom g, const f
     }
 }
 
-// Variant 8: the half list of variant 6, evaluated brick by brick with the
-// brick's neighbourhood staged in shared memory.  A brick is K consecutive
-// list-grid cells of one x-row; atoms are sorted by cell, so its home atoms
-// are one contiguous range, and the neighbour cells of every home cell lie
-// in the 9 rows (y +- 1, z +- 1) over x0 - 1 .. x0 + K, each at most two
-// contiguous ranges of sorted atoms (two where the x-range wraps).  The block
-// copies those ranges of staged positions into shared memory once, as TMA
-// bulk copies (cp.async.bulk, completing on an mbarrier); each
-// thread then walks a home atom's list and reads its partners from there: a
-// partner in neighbour-cell code c lies in row c / 3, whose ranges give its
-// shared-memory slot.  Same pairs and per-pair operations as variant 6:
-// bit-identical forces.  A brick whose neighbourhood exceeds CAP atoms reads
-// its partners from global memory instead.
-// The staged position of list entry w: its row is code / 3 (code = (ox+1) +
-// 3 (oy+1) + 9 (oz+1)); piece A when the partner lies in its range, else
-// piece B.  A slot outside the staged range (not expected) reads global memory.
-__device__ __forceinline__ float4 brick_pos(uint32_t w, bool staged, const float4* s_pos, uint32_t total,
-                                            const uint32_t* gA, const uint32_t* eA, const uint32_t* oA,
-                                            const uint32_t* gB, const uint32_t* oB, const float4* __restrict__ pos4) {
-    const uint32_t q = w & kIdxMask;
-    if (!staged) return __ldg(pos4 + q);
-    const uint32_t r = (w >> 27) / 3u;
-    const uint32_t idx = q - gA[r] < eA[r] - gA[r] ? oA[r] + (q - gA[r]) : oB[r] + (q - gB[r]);
-    return idx < total ? s_pos[idx] : __ldg(pos4 + q);
-}
-
+// Bricks.  A brick is K consecutive list-grid cells of one x-row; atoms are
+// sorted by cell, so its home atoms are one contiguous range, and the
+// neighbour cells of every home cell lie in the 9 rows (y +- 1, z +- 1) over
+// x0 - 1 .. x0 + K, each at most two contiguous ranges of sorted atoms (two
+// where the x-range wraps).  brick_stage copies those ranges of the float4
+// staging into shared memory as TMA bulk copies (cp.async.bulk: every range
+// starts on a 16-byte boundary and is a whole number of float4s; no
+// multicast, the source is this GPU's memory) completing on one mbarrier,
+// and every thread polls it a bounded number of times.  A partner in
+// neighbour-cell code c lies in row c / 3 (code = (ox+1) + 3 (oy+1) +
+// 9 (oz+1)), whose ranges give its shared-memory slot.  A brick whose
+// neighbourhood exceeds CAP atoms reads global memory instead.
 constexpr uint32_t kBrickWaitLimit = 1u << 20;  // polls of the staging mbarrier before giving up
 
-template <bool ENERGY, int CAP>
-__global__ void __launch_bounds__(kNlThreads) k_nl_force_brick(GridGeom g, const float4* __restrict__ pos4,
-                                                                const uint32_t* __restrict__ home,
-                                                                const uint32_t* __restrict__ start, uint32_t n,
-                                                                LawF32 L, const PairF* __restrict__ tab,
-                                                                const uint32_t* __restrict__ list, size_t stride,
-                                                                int cap_nb, const uint32_t* __restrict__ cnt,
-                                                                long long* __restrict__ F, size_t fstride,
-                                                                unsigned long long* __restrict__ vacc,
-                                                                unsigned long long* __restrict__ npairs,
-                                                                uint32_t* __restrict__ err, uint32_t K,
-                                                                uint32_t nchunks) {
-    __shared__ PairF st[kMaxKinds * kMaxKinds];
-    __shared__ float4 s_shift[27];
-    __shared__ unsigned long long shu[kNlThreads / 32];
-    __shared__ __align__(16) float4 s_pos[CAP];
-    __shared__ uint32_t s_gA[9], s_eA[9], s_oA[9], s_gB[9], s_eB[9], s_oB[9];
-    __shared__ uint32_t s_total;
-    __shared__ __align__(8) unsigned long long s_mbar;
-    const int nk2 = L.nkinds * L.nkinds;
-    for (int t = threadIdx.x; t < nk2; t += kNlThreads) st[t] = tab[t];
-    if (threadIdx.x < 27) {
-        float sx, sy, sz;
-        code_shift(g, threadIdx.x, sx, sy, sz);
-        s_shift[threadIdx.x] = make_float4(sx, sy, sz, 0.f);
-    }
+template <int CAP>
+struct BrickSmem {
+    float4 pos[CAP];
+    uint32_t gA[9], eA[9], oA[9], gB[9], eB[9], oB[9];
+    uint32_t total;
+    unsigned long long mbar;
+};
+
+// Stages the brick's neighbourhood; [hlo, hhi) = its home atoms.  Returns
+// false (on every thread, after the copies in flight have landed and
+// kErrTimeout is set) when the staging wait gave up.
+template <int CAP>
+__device__ bool brick_stage(const GridGeom& g, const uint32_t* __restrict__ start, const float4* __restrict__ pos4,
+                            uint32_t K, uint32_t nchunks, BrickSmem<CAP>& S, uint32_t* __restrict__ err,
+                            uint32_t& hlo, uint32_t& hhi) {
     const uint32_t nx = g.n[0], ny = g.n[1], nz = g.n[2];
     const uint32_t row = blockIdx.x / nchunks, chunk = blockIdx.x - row * nchunks;
     const uint32_t cy = row % ny, cz = row / ny;
@@ -715,50 +690,48 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force_brick(GridGeom g, const
             gA = start[rb + x0 - 1];
             eA = start[rb + x1 + 1];
         }
-        s_gA[threadIdx.x] = gA;
-        s_eA[threadIdx.x] = eA;
-        s_gB[threadIdx.x] = gB;
-        s_eB[threadIdx.x] = eB;
+        S.gA[threadIdx.x] = gA;
+        S.eA[threadIdx.x] = eA;
+        S.gB[threadIdx.x] = gB;
+        S.eB[threadIdx.x] = eB;
     }
+    const uint32_t hb = nx * (cy + ny * cz);
+    hlo = start[hb + x0];
+    hhi = start[hb + x1];
     __syncthreads();
+    const uint32_t mbar = (uint32_t)__cvta_generic_to_shared(&S.mbar);
     if (threadIdx.x == 0) {
         uint32_t off = 0;
         for (int r = 0; r < 9; ++r) {
-            s_oA[r] = off;
-            off += s_eA[r] - s_gA[r];
-            s_oB[r] = off;
-            off += s_eB[r] - s_gB[r];
+            S.oA[r] = off;
+            off += S.eA[r] - S.gA[r];
+            S.oB[r] = off;
+            off += S.eB[r] - S.gB[r];
         }
-        s_total = off;
-    }
-    __syncthreads();
-    const bool staged = s_total <= (uint32_t)CAP;
-    // The staged ranges are contiguous runs of float4 (16-byte aligned, whole
-    // 16-byte items), so one thread issues them as TMA bulk copies that
-    // complete on one mbarrier; every thread then waits, a bounded number of
-    // polls, for the bytes to land.
-    const uint32_t mbar = (uint32_t)__cvta_generic_to_shared(&s_mbar);
-    if (staged && s_total && threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(s_total * 16u)
-                     : "memory");
-        for (int r = 0; r < 9; ++r) {
-            const uint32_t gs[2] = {s_gA[r], s_gB[r]}, ln[2] = {s_eA[r] - s_gA[r], s_eB[r] - s_gB[r]},
-                           os[2] = {s_oA[r], s_oB[r]};
-            for (int k = 0; k < 2; ++k) {
-                if (!ln[k]) continue;
-                const uint32_t dst = (uint32_t)__cvta_generic_to_shared(s_pos + os[k]);
-                asm volatile(
-                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                    "l"(pos4 + gs[k]), "r"(ln[k] * 16u), "r"(mbar)
-                    : "memory");
+        S.total = off;
+        if (off && off <= (uint32_t)CAP) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(off * 16u)
+                         : "memory");
+            for (int r = 0; r < 9; ++r) {
+                const uint32_t gs[2] = {S.gA[r], S.gB[r]}, ln[2] = {S.eA[r] - S.gA[r], S.eB[r] - S.gB[r]},
+                               os[2] = {S.oA[r], S.oB[r]};
+                for (int k = 0; k < 2; ++k) {
+                    if (!ln[k]) continue;
+                    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(S.pos + os[k]);
+                    asm volatile(
+                        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                            dst),
+                        "l"(pos4 + gs[k]), "r"(ln[k] * 16u), "r"(mbar)
+                        : "memory");
+                }
             }
         }
     }
     __syncthreads();
-    if (staged && s_total) {
+    if (S.total && S.total <= (uint32_t)CAP) {
         auto wait = [&](uint32_t limit) -> bool {
             for (uint32_t it = 0; it < limit; ++it) {
                 uint32_t done = 0;
@@ -775,11 +748,59 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force_brick(GridGeom g, const
         if (__syncthreads_or(!ok)) {  // every thread leaves together
             if (!ok) wait(kBrickWaitLimit);  // let copies still in flight land before the block exits
             if (threadIdx.x == 0) atomicOr(err, kErrTimeout);
-            return;
+            return false;
         }
     }
-    const uint32_t hb = nx * (cy + ny * cz);
-    const uint32_t hlo = start[hb + x0], hhi = start[hb + x1];
+    return true;
+}
+
+// Shared-memory slot of the atom at sorted position q seen through
+// neighbour-cell code `code`; >= S.total when not staged (not expected for a
+// list partner; the caller then reads global memory).
+template <int CAP>
+__device__ __forceinline__ uint32_t brick_slot(const BrickSmem<CAP>& S, uint32_t q, uint32_t code) {
+    const uint32_t r = code / 3u;
+    return q - S.gA[r] < S.eA[r] - S.gA[r] ? S.oA[r] + (q - S.gA[r]) : S.oB[r] + (q - S.gB[r]);
+}
+
+template <int CAP>
+__device__ __forceinline__ float4 brick_pos(const BrickSmem<CAP>& S, bool staged, uint32_t w,
+                                            const float4* __restrict__ pos4) {
+    const uint32_t q = w & kIdxMask;
+    if (!staged) return __ldg(pos4 + q);
+    const uint32_t idx = brick_slot(S, q, w >> 27);
+    return idx < S.total ? S.pos[idx] : __ldg(pos4 + q);
+}
+
+// Variant 8: the half list of variant 6, evaluated brick by brick, each
+// partner read from the staged neighbourhood.  Same pairs and per-pair
+// operations as variant 6: bit-identical forces.
+template <bool ENERGY, int CAP>
+__global__ void __launch_bounds__(kNlThreads) k_nl_force_brick(GridGeom g, const float4* __restrict__ pos4,
+                                                                const uint32_t* __restrict__ home,
+                                                                const uint32_t* __restrict__ start, uint32_t n,
+                                                                LawF32 L, const PairF* __restrict__ tab,
+                                                                const uint32_t* __restrict__ list, size_t stride,
+                                                                int cap_nb, const uint32_t* __restrict__ cnt,
+                                                                long long* __restrict__ F, size_t fstride,
+                                                                unsigned long long* __restrict__ vacc,
+                                                                unsigned long long* __restrict__ npairs,
+                                                                uint32_t* __restrict__ err, uint32_t K,
+                                                                uint32_t nchunks) {
+    __shared__ PairF st[kMaxKinds * kMaxKinds];
+    __shared__ float4 s_shift[27];
+    __shared__ unsigned long long shu[kNlThreads / 32];
+    __shared__ __align__(16) BrickSmem<CAP> S;
+    const int nk2 = L.nkinds * L.nkinds;
+    for (int t = threadIdx.x; t < nk2; t += kNlThreads) st[t] = tab[t];
+    if (threadIdx.x < 27) {
+        float sx, sy, sz;
+        code_shift(g, threadIdx.x, sx, sy, sz);
+        s_shift[threadIdx.x] = make_float4(sx, sy, sz, 0.f);
+    }
+    uint32_t hlo, hhi;
+    if (!brick_stage<CAP>(g, start, pos4, K, nchunks, S, err, hlo, hhi)) return;
+    const bool staged = S.total <= (uint32_t)CAP;
     PairAcc a;
     for (uint32_t p = hlo + threadIdx.x; p < hhi; p += kNlThreads) {
         const float4 pi = pos4[p];
@@ -795,7 +816,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force_brick(GridGeom g, const
                 for (int u = 0; u < 4; ++u) w[u] = __ldg(lp + (size_t)(e + u) * stride);
                 float4 pj[4];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) pj[u] = brick_pos(w[u], staged, s_pos, s_total, s_gA, s_eA, s_oA, s_gB, s_oB, pos4);
+                for (int u = 0; u < 4; ++u) pj[u] = brick_pos(S, staged, w[u], pos4);
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const float4 sh = s_shift[w[u] >> 27];
@@ -806,7 +827,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force_brick(GridGeom g, const
             for (; e < m; ++e) {
                 const uint32_t w = __ldg(lp + (size_t)e * stride);
                 const uint32_t q = w & kIdxMask;
-                const float4 pj = brick_pos(w, staged, s_pos, s_total, s_gA, s_eA, s_oA, s_gB, s_oB, pos4);
+                const float4 pj = brick_pos(S, staged, w, pos4);
                 const float4 sh = s_shift[w >> 27];
                 nl_pair(L, st, ki, pi, pj, sh.x, sh.y, sh.z, ENERGY && q > p, a, err, F, q, fstride);
             }
@@ -833,6 +854,61 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force_brick(GridGeom g, const
             if (sv) atomicAdd(vacc, sv);
             if (np) atomicAdd(npairs, np);
         }
+    }
+}
+
+// The list build of k_nl_build brick by brick: the candidates are read from
+// the staged neighbourhood; the cells, the reach test, the candidate order
+// and the distance test are k_nl_build's, so the lists are the same words.
+template <bool HALF, int CAP>
+__global__ void __launch_bounds__(kNlBuildThreads) k_nl_build_brick(GridGeom g, const float4* __restrict__ pos4,
+                                                                    const uint32_t* __restrict__ home,
+                                                                    const uint32_t* __restrict__ start, float rl2,
+                                                                    uint32_t* __restrict__ list, size_t stride,
+                                                                    int cap_nb, uint32_t* __restrict__ cnt,
+                                                                    uint32_t* __restrict__ err, uint32_t K,
+                                                                    uint32_t nchunks,
+                                                                    const uint32_t* __restrict__ gate) {
+    __shared__ __align__(16) BrickSmem<CAP> S;
+    if (gated_off(gate)) return;
+    uint32_t hlo, hhi;
+    if (!brick_stage<CAP>(g, start, pos4, K, nchunks, S, err, hlo, hhi)) return;
+    const bool staged = S.total <= (uint32_t)CAP;
+    const float slack = 1e-3f;  // atoms of a cell sit within [0, cell) of its frame up to staging rounding
+    for (uint32_t p = hlo + threadIdx.x; p < hhi; p += kNlBuildThreads) {
+        const float4 pi = pos4[p];
+        const uint32_t c = home[p];
+        uint32_t cx, cy, cz;
+        decode(g, c, cx, cy, cz);
+        uint32_t m = 0;
+        for (uint32_t code = 0; code < 27; ++code) {
+            const int ox = (int)(code % 3u) - 1, oy = (int)((code / 3u) % 3u) - 1, oz = (int)(code / 9u) - 1;
+            const uint32_t B = cell_at(g, cx, cy, cz, code);
+            if (HALF && B < c) continue;  // atoms are sorted by cell: a lower cell index means every q < p
+            const float mx = fmaxf((ox > 0 ? g.cellf[0] - pi.x : (ox < 0 ? pi.x : 0.f)) - slack, 0.f);
+            const float my = fmaxf((oy > 0 ? g.cellf[1] - pi.y : (oy < 0 ? pi.y : 0.f)) - slack, 0.f);
+            const float mz = fmaxf((oz > 0 ? g.cellf[2] - pi.z : (oz < 0 ? pi.z : 0.f)) - slack, 0.f);
+            if (dist2(mx, my, mz) >= rl2) continue;  // the whole cell is out of reach
+            float sx, sy, sz;
+            code_shift(g, code, sx, sy, sz);
+            const float qx = fadd(pi.x, sx), qy = fadd(pi.y, sy), qz = fadd(pi.z, sz);
+            uint32_t lo = start[B];
+            const uint32_t hi = start[B + 1];
+            if (HALF && B == c) lo = p + 1;  // HALF: every candidate lies after p
+            // the cell is one contiguous run of its row's staged range
+            const uint32_t s0 = staged ? brick_slot(S, lo, code) : 0u;
+            const bool in_smem = staged && lo < hi && s0 + (hi - lo) <= S.total;
+#pragma unroll(kNlBuildUnroll)
+            for (uint32_t q = lo; q < hi; ++q) {
+                if (!HALF && q == p) continue;
+                const float4 pj = in_smem ? S.pos[s0 + (q - lo)] : pos4[q];
+                if (dist2(fsub(qx, pj.x), fsub(qy, pj.y), fsub(qz, pj.z)) < rl2) {
+                    if (m < (uint32_t)cap_nb) list[(size_t)m * stride + p] = q | (code << 27);
+                    ++m;
+                }
+            }
+        }
+        cnt[p] = m;
     }
 }
 
@@ -1194,11 +1270,17 @@ int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nb_out, bool
         GX_LAUNCH(h, k_nl_stage, nblk(n, 256), 256, g, b, h->key_sorted, n, h->pos4, s->ref, s->flag);
         prof_end(h, "nl_stage");
         const float rl = (float)((h->fs.rc + s->skin_used) * (1.0 + 1e-6));
-        auto build = s->half == 1 ? k_nl_build<true> : k_nl_build<false>;
         prof_begin(h, "nl_build");
-        GX_LAUNCH(h, build, nblk(n, kNlBuildThreads), kNlBuildThreads, g, h->pos4, h->key_sorted, s->cl.start, n,
-                  rl * rl,
-                  s->list, s->cap, s->cap_nb, s->cnt, s->flag);
+        if (h->kernel_variant == 8) {  // the brick build: candidates from the staged neighbourhood
+            const uint32_t K = 8, nchunks = (g.n[0] + K - 1) / K;
+            auto bb = s->half == 1 ? k_nl_build_brick<true, 2048> : k_nl_build_brick<false, 2048>;
+            GX_LAUNCH(h, bb, nchunks * g.n[1] * g.n[2], kNlBuildThreads, g, h->pos4, h->key_sorted, s->cl.start,
+                      rl * rl, s->list, s->cap, s->cap_nb, s->cnt, h->derr, K, nchunks, s->flag);
+        } else {
+            auto build = s->half == 1 ? k_nl_build<true> : k_nl_build<false>;
+            GX_LAUNCH(h, build, nblk(n, kNlBuildThreads), kNlBuildThreads, g, h->pos4, h->key_sorted, s->cl.start,
+                      n, rl * rl, s->list, s->cap, s->cap_nb, s->cnt, s->flag);
+        }
         prof_end(h, "nl_build");
         return GX_OK;
     };

@@ -78,6 +78,26 @@ def test_full_and_half_lists_are_bit_identical(gpu, thermo):
         assert out[0][2] == o[2]
 
 
+def test_brick_list_build_writes_the_same_lists(gpu):
+    # variant 8 builds its half lists brick by brick from shared memory;
+    # the entry counts equal variant 6's after every tick of a run with
+    # rebuilds, and the trajectories are the same bits
+    cfg, u = _lattice(14, temperature=200.0, coul=True)
+    hs = []
+    for variant in (6, 8):
+        h = _handle(cfg, variant)
+        h.set_universe(u)
+        hs.append(h)
+    for _ in range(12):
+        st = [h.step(2) for h in hs]
+        e6, e8 = hs[0].list_stats(), hs[1].list_stats()
+        assert e6 == e8 and e6[0] > 0
+        assert np.array_equal(st[0], st[1])
+    assert hs[1].list_rebuilds() >= 2
+    for x, y in zip(hs[0].get_state(), hs[1].get_state()):
+        assert np.array_equal(x, y)
+
+
 @pytest.mark.parametrize("thermo", [False, True])
 def test_trajectory_follows_per_tick_variant(gpu, thermo):
     cfg, u = _lattice(16, temperature=120.0, coul=True)
