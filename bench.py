@@ -79,6 +79,9 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip fp64/e2e/cpu legs (testing only)")
     ap.add_argument("--variant", type=int, default=-1,
                     help="fix the mixed pair-pass variant instead of autotuning (profiling only)")
+    ap.add_argument("--list-block", type=int, default=-1,
+                    help="block of the shared far-end sums of the one-lane half-list pass: 256, 128 or 0 "
+                         "(profiling only)")
     ap.add_argument("--skin", type=float, default=-1.0,
                     help="neighbour-list skin in length units instead of 0.1 r_c (profiling only; 0 = rebuild every tick)")
     ap.add_argument("--leg", default="",
@@ -724,6 +727,8 @@ def ours_arm(args, dist):
     h = Handle(cfg, "mixed", dev)
     if args.skin >= 0:
         h.set_list_skin(args.skin)
+    if args.list_block >= 0:
+        h.set_list_block(args.list_block)
     h.set_universe(u)
     if args.variant >= 0:
         h.set_kernel_variant(args.variant)

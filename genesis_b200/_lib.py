@@ -68,7 +68,7 @@ EXPORTS = (
     "gx_batch_create", "gx_batch_destroy", "gx_batch_last_error", "gx_batch_set_state",
     "gx_batch_step", "gx_batch_get_state", "gx_adjoint_forward", "gx_adjoint_backward",
     "gx_set_list_skin", "gx_list_rebuilds", "gx_list_stats", "gx_batch_set_mode", "gx_batch_get_mode", "gx_batch_autotune",
-    "gx_get_list_config", "gx_set_list_threads", "gx_set_list_stash", "gx_set_list_brick", "gx_bond_observe", "gx_bond_tracker_reset", "gx_get_bonds",
+    "gx_get_list_config", "gx_set_list_threads", "gx_set_list_stash", "gx_set_list_brick", "gx_set_list_block", "gx_bond_observe", "gx_bond_tracker_reset", "gx_get_bonds",
     "gx_bond_components", "gx_collisions", "gx_collision_count", "gx_xyz_frame", "gx_snapshot_world",
     "gx_set_step_async",
 )
@@ -131,6 +131,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
         "gx_set_list_threads": (C.c_int, [vp, C.c_int]),
         "gx_set_list_stash": (C.c_int, [vp, C.c_int]),
         "gx_set_list_brick": (C.c_int, [vp, C.c_int]),
+        "gx_set_list_block": (C.c_int, [vp, C.c_int]),
         "gx_bond_observe": (C.c_int, [vp, _D, _D, C.c_int, C.c_uint64, C.c_int, C.POINTER(GxBondObservation)]),
         "gx_bond_tracker_reset": (C.c_int, [vp]),
         "gx_get_bonds": (C.c_int, [vp, u32p, sz, C.POINTER(sz)]),
@@ -296,6 +297,11 @@ class Handle:
     def set_list_stash(self, slots: int):
         """Stash slots per thread of the variant-7 list pass (8 or 16)."""
         self._check(self.lib.gx_set_list_stash(self.h, slots))
+
+    def set_list_block(self, threads: int):
+        """Block of the shared far-end sums of the one-lane half-list pass
+        (256, 128, or 0 for every far end in global memory)."""
+        self._check(self.lib.gx_set_list_block(self.h, threads))
 
     def set_list_brick(self, cells: int):
         """Brick length of the variant-8 list pass (4 or 8 cells)."""

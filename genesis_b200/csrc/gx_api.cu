@@ -1056,6 +1056,12 @@ int gx_set_list_stash(gx_handle* h, int slots) {
     return nl_set_slots(h, slots);
 }
 
+int gx_set_list_block(gx_handle* h, int threads) {
+    if (!h) return GX_ERR_ARG;
+    invalidate_graphs(h);
+    return nl_set_block(h, threads);
+}
+
 int gx_set_list_brick(gx_handle* h, int cells) {
     if (!h) return GX_ERR_ARG;
     invalidate_graphs(h);

@@ -318,6 +318,7 @@ int nl_config(gx_handle* h, double* skin, int* tpp);
 int nl_set_tpp(gx_handle* h, int tpp);
 int nl_set_slots(gx_handle* h, int slots);
 int nl_set_brick(gx_handle* h, int cells);
+int nl_set_block(gx_handle* h, int block);
 int nl_stats(gx_handle* h, uint64_t* entries, uint64_t* overflowed);
 void nl_free(gx_handle* h);
 void tracker_free(gx_handle* h);

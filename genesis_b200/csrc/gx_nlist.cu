@@ -50,6 +50,8 @@ struct NlState {
     int tpp = 1;              // threads per atom in the list pass (1, 2, 4, 8)
     int slots = 16;           // variant 7: stash slots per thread (8 or 16)
     int brick = 1;            // variant 8: 0 = bricks of 4 cells (1024 staged atoms), 1 = 8 cells (2048)
+    int block = 256;          // variant 6, one lane per atom: 0 = far ends always global, 128 or 256 = far
+                              // ends inside a block of that many atoms summed in shared memory
     int cap_nb = 0;           // list entries per atom
     size_t cap = 0;           // atoms the buffers hold
     uint32_t* list = nullptr; // entry e of atom p at list[e * cap + p]
@@ -313,6 +315,133 @@ __device__ __forceinline__ void nl_pair(const LawF32& L, const PairF* st, int ki
     if (once) {
         a.vq += quant(v, err);
         ++a.np;
+    }
+}
+
+// The half-list pass with one lane per atom and the far end's force kept in
+// the block where it can be.  Atoms are sorted by cell, so a block of BS
+// consecutive atoms covers whole runs of cells along x, and for about half
+// of the pairs within r_c the far end q lies in the same block (a numpy
+// count on the quench lattice: 47 % at 128 atoms, 56 % at 256).  Those far
+// ends go into 64-bit sums in shared memory, each kept as two 32-bit words
+// added with the low word's carry (two native 32-bit shared atomics, where a
+// 64-bit shared atomic is several times slower); the others go to global
+// memory as in k_nl_force.  At the end each thread adds its atom's shared
+// sum to its own and writes one global atomic per component.  Integer sums
+// modulo 2^64, so the forces are the same bits as k_nl_force's.
+template <bool ENERGY, int BS>
+__global__ void __launch_bounds__(BS) k_nl_force_local(GridGeom g, const float4* __restrict__ pos4,
+                                                        const uint32_t* __restrict__ home,
+                                                        const uint32_t* __restrict__ start, uint32_t n, LawF32 L,
+                                                        const PairF* __restrict__ tab,
+                                                        const uint32_t* __restrict__ list, size_t stride,
+                                                        int cap_nb, const uint32_t* __restrict__ cnt,
+                                                        long long* __restrict__ F, size_t fstride,
+                                                        unsigned long long* __restrict__ vacc,
+                                                        unsigned long long* __restrict__ npairs,
+                                                        uint32_t* __restrict__ err) {
+    __shared__ PairF st[kMaxKinds * kMaxKinds];
+    __shared__ float4 s_shift[27];
+    __shared__ unsigned long long shu[BS / 32];
+    __shared__ uint32_t s_lo[3][BS], s_hi[3][BS];
+    const int nk2 = L.nkinds * L.nkinds;
+    for (int t = threadIdx.x; t < nk2; t += BS) st[t] = tab[t];
+    if (threadIdx.x < 27) {
+        float sx, sy, sz;
+        code_shift(g, threadIdx.x, sx, sy, sz);
+        s_shift[threadIdx.x] = make_float4(sx, sy, sz, 0.f);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        s_lo[c][threadIdx.x] = 0u;
+        s_hi[c][threadIdx.x] = 0u;
+    }
+    __syncthreads();
+    const uint32_t b0 = blockIdx.x * BS;
+    const uint32_t p = b0 + threadIdx.x;
+    PairAcc a;
+    // the far end's share of one pair: shared memory inside the block, else global
+    auto far = [&](uint32_t q, long long fx, long long fy, long long fz) {
+        const uint32_t lq = q - b0;
+        if (lq < (uint32_t)BS) {
+            const long long v[3] = {-fx, -fy, -fz};
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const unsigned long long u = (unsigned long long)v[c];
+                const uint32_t lo = (uint32_t)u, old = atomicAdd(&s_lo[c][lq], lo);
+                atomicAdd(&s_hi[c][lq], (uint32_t)(u >> 32) + (old + lo < old ? 1u : 0u));
+            }
+        } else {
+            atomicAdd((unsigned long long*)&F[q], (unsigned long long)(-fx));
+            atomicAdd((unsigned long long*)&F[fstride + q], (unsigned long long)(-fy));
+            atomicAdd((unsigned long long*)&F[2 * fstride + q], (unsigned long long)(-fz));
+        }
+    };
+    auto pair = [&](const float4& pi, int ki, const float4& pj, const float4& sh, uint32_t q) {
+        const float dx = delta1(pi.x, pj.x, sh.x), dy = delta1(pi.y, pj.y, sh.y), dz = delta1(pi.z, pj.z, sh.z);
+        const float d2 = dist2(dx, dy, dz);
+        if (!(d2 < L.rc2) || d2 == 0.f) return;
+        float fs, v;
+        pair_f32(L, st[ki * L.nkinds + __float_as_int(pj.w)], d2, fs, v);
+        const long long qx = quant(fmul(dx, fs), err), qy = quant(fmul(dy, fs), err), qz = quant(fmul(dz, fs), err);
+        a.fx += qx;
+        a.fy += qy;
+        a.fz += qz;
+        far(q, qx, qy, qz);
+        if (ENERGY && q > p) {
+            a.vq += quant(v, err);
+            ++a.np;
+        }
+    };
+    if (p < n) {
+        const float4 pi = pos4[p];
+        const int ki = __float_as_int(pi.w);
+        const uint32_t m = cnt[p];
+        if (m <= (uint32_t)cap_nb) {
+            const uint32_t* lp = list + p;
+            uint32_t e = 0;
+            for (; e + 4 <= m; e += 4) {  // four entries per round, every load issued before any pair math
+                uint32_t w[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) w[k] = __ldg(lp + (size_t)(e + k) * stride);
+                float4 pj[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) pj[k] = __ldg(pos4 + (w[k] & kIdxMask));
+#pragma unroll
+                for (int k = 0; k < 4; ++k) pair(pi, ki, pj[k], s_shift[w[k] >> 27], w[k] & kIdxMask);
+            }
+            for (; e < m; ++e) {
+                const uint32_t w = __ldg(lp + (size_t)e * stride);
+                pair(pi, ki, __ldg(pos4 + (w & kIdxMask)), s_shift[w >> 27], w & kIdxMask);
+            }
+        } else {  // overflowed list: scan the home-grid cells directly
+            uint32_t cx, cy, cz;
+            const uint32_t c = home[p];
+            decode(g, c, cx, cy, cz);
+            for (uint32_t code = 0; code < 27; ++code) {
+                const uint32_t B = cell_at(g, cx, cy, cz, code);
+                if (B < c) continue;
+                for (uint32_t q = start[B], hi = start[B + 1]; q < hi; ++q)
+                    if (q > p) pair(pi, ki, pos4[q], s_shift[code], q);
+            }
+        }
+    }
+    __syncthreads();
+    if (p < n) {
+        const long long sx = (long long)(((unsigned long long)s_hi[0][threadIdx.x] << 32) | s_lo[0][threadIdx.x]);
+        const long long sy = (long long)(((unsigned long long)s_hi[1][threadIdx.x] << 32) | s_lo[1][threadIdx.x]);
+        const long long sz = (long long)(((unsigned long long)s_hi[2][threadIdx.x] << 32) | s_lo[2][threadIdx.x]);
+        atomicAdd((unsigned long long*)&F[p], (unsigned long long)(a.fx + sx));
+        atomicAdd((unsigned long long*)&F[fstride + p], (unsigned long long)(a.fy + sy));
+        atomicAdd((unsigned long long*)&F[2 * fstride + p], (unsigned long long)(a.fz + sz));
+    }
+    if (ENERGY) {
+        unsigned long long sv = block_sum_u<BS>((unsigned long long)a.vq, shu);
+        unsigned long long np = block_sum_u<BS>(a.np, shu);
+        if (threadIdx.x == 0) {
+            if (sv) atomicAdd(vacc, sv);
+            if (np) atomicAdd(npairs, np);
+        }
     }
 }
 
@@ -1070,6 +1199,18 @@ void launch_nl_force(gx_handle* h, int tpp, const GridGeom& g, const NlState* s,
                   s->cap_nb, s->cnt, h->F, h->cap, h->dcount + 1, h->dcount + 0, h->derr);
         return;
     }
+    if (HALF && tpp <= 1 && s->block > 0) {  // far ends inside the block summed in shared memory
+        if (s->block == 256) {
+            auto kl = energy ? k_nl_force_local<true, 256> : k_nl_force_local<false, 256>;
+            GX_LAUNCH(h, kl, nblk(n, 256), 256, g, pos4, home, start, n, L, h->d_pairf, s->list, s->cap, s->cap_nb,
+                      s->cnt, h->F, h->cap, h->dcount + 1, h->dcount + 0, h->derr);
+        } else {
+            auto kl = energy ? k_nl_force_local<true, 128> : k_nl_force_local<false, 128>;
+            GX_LAUNCH(h, kl, nblk(n, 128), 128, g, pos4, home, start, n, L, h->d_pairf, s->list, s->cap, s->cap_nb,
+                      s->cnt, h->F, h->cap, h->dcount + 1, h->dcount + 0, h->derr);
+        }
+        return;
+    }
     if (tpp <= 1) {
         auto k1 = energy ? k_nl_force<HALF, true> : k_nl_force<HALF, false>;
         GX_LAUNCH(h, k1, nblk(n, kNlThreads), kNlThreads, g, pos4, home, start, n, L, h->d_pairf, s->list, s->cap,
@@ -1502,32 +1643,55 @@ int nl_tune_tpp(gx_handle* h, int reps) {
     const uint32_t n = (uint32_t)h->n;
     const LawF32 L = make_law32(h);
     // variant 7: the stash size (8 or 16 slots per thread); variant 8: the
-    // brick length (4 or 8 cells); else threads per atom
+    // brick length (4 or 8 cells); else threads per atom, and with one lane
+    // per atom on the half list the block of the shared far-end sums (256,
+    // 128 or none)
     const bool stash = h->kernel_variant == 7, brick = h->kernel_variant == 8;
-    const int cand[4] = {1, 2, 4, 8};
-    const int ncand = (stash || brick) ? 2 : 4;
+    struct Cand {
+        int tpp, block;
+    };
+    const Cand lanes[6] = {{1, 256}, {1, 128}, {1, 0}, {2, 0}, {4, 0}, {8, 0}};
+    const int ncand = (stash || brick) ? 2 : (s->half == 1 ? 6 : 4);
     double best = 1e300;
-    int pick = stash ? s->slots : (brick ? s->brick : s->tpp);
+    const int tpp0 = s->tpp, block0 = s->block;
+    int pick = 0;
     for (int k = 0; k < ncand; ++k) {
+        int tpp = s->tpp;
         if (stash) s->slots = k == 0 ? 8 : 16;
-        if (brick) s->brick = k;
+        else if (brick) s->brick = k;
+        else if (s->half == 1) {
+            tpp = lanes[k].tpp;
+            s->block = lanes[k].block;
+        } else {
+            tpp = lanes[k + 2].tpp;
+        }
         int rc = gx_timer_mark(h, 14);
         for (int r = 0; r < reps && !rc; ++r) {
-            if (s->half == 1) launch_nl_force<true>(h, cand[k], s->lg, s, n, L, false);
-            else launch_nl_force<false>(h, cand[k], s->lg, s, n, L, false);
+            if (s->half == 1) launch_nl_force<true>(h, tpp, s->lg, s, n, L, false);
+            else launch_nl_force<false>(h, tpp, s->lg, s, n, L, false);
         }
         double t = 0.0;
         if (!rc) rc = gx_timer_mark(h, 15);
         if (!rc) rc = gx_timer_elapsed(h, 14, 15, &t);
-        if (rc) return rc;
+        if (rc) {
+            s->tpp = tpp0;
+            s->block = block0;
+            return rc;
+        }
         if (t / reps < best) {
             best = t / reps;
-            pick = stash ? s->slots : (brick ? k : cand[k]);
+            pick = k;
         }
     }
-    if (stash) s->slots = pick;
+    if (stash) s->slots = pick == 0 ? 8 : 16;
     else if (brick) s->brick = pick;
-    else s->tpp = pick;
+    else if (s->half == 1) {
+        s->tpp = lanes[pick].tpp;
+        s->block = lanes[pick].block;
+    } else {
+        s->tpp = lanes[pick + 2].tpp;
+        s->block = block0;
+    }
     GX_CUDA(h, cudaMemsetAsync(h->derr, 0, sizeof(uint32_t), h->stream));
     return GX_OK;
 }
@@ -1579,6 +1743,13 @@ int nl_config(gx_handle* h, double* skin, int* tpp) {
 int nl_set_brick(gx_handle* h, int cells) {
     if (cells != 4 && cells != 8) return set_err(h, GX_ERR_ARG, "brick length must be 4 or 8 cells");
     nl_of(h)->brick = cells == 4 ? 0 : 1;
+    return GX_OK;
+}
+
+int nl_set_block(gx_handle* h, int block) {
+    if (block != 0 && block != 128 && block != 256)
+        return set_err(h, GX_ERR_ARG, "list block must be 0 (far ends in global memory), 128 or 256");
+    nl_of(h)->block = block;
     return GX_OK;
 }
 

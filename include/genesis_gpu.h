@@ -157,6 +157,14 @@ int gx_set_list_threads(gx_handle* h, int threads_per_atom);
  * (default 16; the autotuner picks the faster).  Both give the same bits.
  * No counterpart in the reference. */
 int gx_set_list_stash(gx_handle* h, int slots);
+/* The half-list pass with one lane per atom (variant 6): 128 or 256 atoms
+ * per block with the far end of every pair inside the block summed in
+ * shared memory (two 32-bit words with the carry), so that only the other
+ * pairs send their far end's force to global memory; 0 = every far end to
+ * global memory.  Default 256; the autotuner picks among 256, 128, 0 and the
+ * wider lanes per atom.  All give the same bits.  No counterpart in the
+ * reference. */
+int gx_set_list_block(gx_handle* h, int threads);
 /* Brick length of the variant-8 list pass: 4 or 8 list-grid cells per brick
  * (at most 1024 or 2048 staged atoms; a brick with more reads global
  * memory).  Default 8; the autotuner picks the faster.  Both give the same

@@ -124,12 +124,14 @@ def test_trajectory_follows_per_tick_variant(gpu, thermo):
 
 @pytest.mark.parametrize("variant", [5, 6])
 def test_threads_per_atom_are_bit_identical(gpu, variant):
+    # lanes per atom, and for one lane the block of the shared far-end sums
     cfg, u = _lattice(14, temperature=150.0, coul=True)
     cfg.enable_thermostat = True
     cfg.thermostat_temperature = 40.0
     out = []
-    for tpp in (1, 2, 4, 8):
+    for tpp, block in ((1, 0), (1, 128), (1, 256), (2, 0), (4, 0), (8, 0)):
         h = _handle(cfg, variant)
+        h.set_list_block(block)
         h.set_list_threads(tpp)
         h.set_universe(u)
         st = h.step(12, graph=True)
