@@ -269,15 +269,15 @@ class Handle:
         half list with each thread's in-cutoff entries collected in shared
         memory before the warp evaluates them (same forces as 6), 8 the half
         list brick by brick with the brick's neighbourhood staged in shared
-        memory (same forces as 6), 9 the bricks of 8 with the stash of 7."""
+        memory (same forces as 6)."""
         self._check(self.lib.gx_set_kernel_variant(self.h, variant))
 
     def autotune(self, reps: int = 5):
         """Times every applicable pair-pass variant and keeps the fastest;
         returns (variant, {variant: ms}) -- ms per pass for 1-4, ms per tick
-        for 5-9 and 0 (the tick of the best of 1-4)."""
+        for 5-8 and 0 (the tick of the best of 1-4)."""
         best = C.c_int()
-        ms = np.full(10, -1.0)
+        ms = np.full(9, -1.0)
         self._check(self.lib.gx_autotune(self.h, reps, C.byref(best), _ptr(ms, C.c_double)))
         return best.value, {v: float(t) for v, t in enumerate(ms) if t >= 0}
 

@@ -882,7 +882,7 @@ int gx_collisions(gx_handle* h, uint64_t* collisions) {
 }
 
 int gx_set_kernel_variant(gx_handle* h, int variant) {
-    if (!h || variant < 0 || variant > 9) return GX_ERR_ARG;
+    if (!h || variant < 0 || variant > 8) return GX_ERR_ARG;
     h->kernel_variant = variant;
     invalidate_graphs(h);
     return GX_OK;
@@ -892,7 +892,7 @@ int gx_autotune(gx_handle* h, int reps, int* best, double* ms) {
     int rc = require_state(h);
     if (rc) return rc;
     if (reps < 1) reps = 1;
-    for (int v = 0; v < 10; ++v)
+    for (int v = 0; v < 9; ++v)
         if (ms) ms[v] = -1.0;
     if (h->precision != GX_MIXED || h->n == 0) {
         if (best) *best = h->kernel_variant;
@@ -964,9 +964,9 @@ int gx_autotune(gx_handle* h, int reps, int* best, double* ms) {
                 h->nl_fresh = false;  // positions restored behind the list's back
                 return r;
             };
-            const int vs[6] = {pick, 5, 6, 7, 8, 9};
-            double tt[6] = {1e300, 1e300, 1e300, 1e300, 1e300, 1e300};
-            for (int q = 0; q < 6 && !rc; ++q) {
+            const int vs[5] = {pick, 5, 6, 7, 8};
+            double tt[5] = {1e300, 1e300, 1e300, 1e300, 1e300};
+            for (int q = 0; q < 5 && !rc; ++q) {
                 h->kernel_variant = vs[q];
                 rc = tick_ms(&tt[q]);
             }
@@ -976,11 +976,10 @@ int gx_autotune(gx_handle* h, int reps, int* best, double* ms) {
                 ms[6] = tt[2] < 1e300 ? tt[2] : -1.0;
                 ms[7] = tt[3] < 1e300 ? tt[3] : -1.0;
                 ms[8] = tt[4] < 1e300 ? tt[4] : -1.0;
-                ms[9] = tt[5] < 1e300 ? tt[5] : -1.0;
             }
             if (!rc) {
                 int q = 0;
-                for (int k = 1; k < 6; ++k)
+                for (int k = 1; k < 5; ++k)
                     if (tt[k] < tt[q]) q = k;
                 pick = vs[q];
             }

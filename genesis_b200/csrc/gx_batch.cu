@@ -191,8 +191,8 @@ __global__ void __launch_bounds__(kBThreads, 2)
                     ++np;
                     float fs, v;
                     pair_f32(L, s_tab[ki * nk + __float_as_int(pj.w)], d2, fs, v);
-                    long long qx = quant(fmul(dx, fs), err), qy = quant(fmul(dy, fs), err),
-                              qz = quant(fmul(dz, fs), err);
+                    long long qx, qy, qz;
+                quant3(fmul(dx, fs), fmul(dy, fs), fmul(dz, fs), qx, qy, qz, err);
                     fx += qx;
                     fy += qy;
                     fz += qz;

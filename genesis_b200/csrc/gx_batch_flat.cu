@@ -219,7 +219,8 @@ __device__ __forceinline__ void fb_force_one(uint32_t s, const RepGeo* __restric
                 if (!(d2 < L.rc2) || d2 == 0.f) continue;
                 float fs, v;
                 pair_f32(L, st[ki * L.nkinds + __float_as_int(pj.w)], d2, fs, v);
-                long long qx = quant(fmul(dx, fs), err), qy = quant(fmul(dy, fs), err), qz = quant(fmul(dz, fs), err);
+                long long qx, qy, qz;
+                quant3(fmul(dx, fs), fmul(dy, fs), fmul(dz, fs), qx, qy, qz, err);
                 fx += qx;
                 fy += qy;
                 fz += qz;

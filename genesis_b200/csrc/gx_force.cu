@@ -179,7 +179,8 @@ __global__ void __launch_bounds__(kForceThreads) k_force_mixed(GridGeom g, const
                 ++np;
                 float fs, v;
                 pair_f32(L, st[ki * L.nkinds + __float_as_int(pj.w)], d2, fs, v);
-                long long qx = quant(fmul(dx, fs), err), qy = quant(fmul(dy, fs), err), qz = quant(fmul(dz, fs), err);
+                long long qx, qy, qz;
+                quant3(fmul(dx, fs), fmul(dy, fs), fmul(dz, fs), qx, qy, qz, err);
                 fx += qx;
                 fy += qy;
                 fz += qz;

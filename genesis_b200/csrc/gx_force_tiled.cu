@@ -221,7 +221,8 @@ __global__ void __launch_bounds__(kTThreads, 4)
             float d2 = dist2(dx, dy, dz);
             float fs, v;
             pair_f32(L, s_tab[__float_as_int(pi.w) * nk + __float_as_int(pj.w)], d2, fs, v);
-            long long qx = quant(fmul(dx, fs), err), qy = quant(fmul(dy, fs), err), qz = quant(fmul(dz, fs), err);
+            long long qx, qy, qz;
+                quant3(fmul(dx, fs), fmul(dy, fs), fmul(dz, fs), qx, qy, qz, err);
             if (shared_i) {
                 atomicAdd(&s_acc[w][3 * i], (unsigned long long)qx);
                 atomicAdd(&s_acc[w][3 * i + 1], (unsigned long long)qy);
@@ -386,7 +387,8 @@ __global__ void __launch_bounds__(kRThreads, 4)
                     float d2 = dist2(dx, dy, dz);
                     float fs, v;
                     pair_f32(L, s_tab[ki * nk + __float_as_int(pj.w)], d2, fs, v);
-                    long long qx = quant(fmul(dx, fs), err), qy = quant(fmul(dy, fs), err), qz = quant(fmul(dz, fs), err);
+                    long long qx, qy, qz;
+                quant3(fmul(dx, fs), fmul(dy, fs), fmul(dz, fs), qx, qy, qz, err);
                     fx += qx;
                     fy += qy;
                     fz += qz;
@@ -521,7 +523,8 @@ __global__ void __launch_bounds__(kLThreads, 8)
                 float d2 = dist2(dx, dy, dz);
                 float fs, v;
                 pair_f32(L, s_tab[ki * nk + __float_as_int(pj.w)], d2, fs, v);
-                long long qx = quant(fmul(dx, fs), err), qy = quant(fmul(dy, fs), err), qz = quant(fmul(dz, fs), err);
+                long long qx, qy, qz;
+                quant3(fmul(dx, fs), fmul(dy, fs), fmul(dz, fs), qx, qy, qz, err);
                 fx += qx;
                 fy += qy;
                 fz += qz;

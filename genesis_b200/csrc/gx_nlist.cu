@@ -50,7 +50,7 @@ struct NlState {
     int tpp = 1;              // threads per atom in the list pass (1, 2, 4, 8)
     int slots = 16;           // variant 7: stash slots per thread (8 or 16)
     int brick = 1;            // variant 8: 0 = bricks of 4 cells (1024 staged atoms), 1 = 8 cells (2048)
-    int block = 256;          // variant 6, one lane per atom: 0 = far ends always global, 128 or 256 = far
+    int block = 0;            // variant 6, one lane per atom: 0 = far ends always global, 128 or 256 = far
                               // ends inside a block of that many atoms summed in shared memory
     int cap_nb = 0;           // list entries per atom
     size_t cap = 0;           // atoms the buffers hold
@@ -303,7 +303,8 @@ __device__ __forceinline__ void nl_pair(const LawF32& L, const PairF* st, int ki
     if (!(d2 < L.rc2) || d2 == 0.f) return;
     float fs, v;
     pair_f32(L, st[ki * L.nkinds + __float_as_int(pj.w)], d2, fs, v);
-    long long qx = quant(fmul(dx, fs), err), qy = quant(fmul(dy, fs), err), qz = quant(fmul(dz, fs), err);
+    long long qx, qy, qz;
+    quant3(fmul(dx, fs), fmul(dy, fs), fmul(dz, fs), qx, qy, qz, err);
     a.fx += qx;
     a.fy += qy;
     a.fz += qz;
@@ -383,7 +384,8 @@ __global__ void __launch_bounds__(BS) k_nl_force_local(GridGeom g, const float4*
         if (!(d2 < L.rc2) || d2 == 0.f) return;
         float fs, v;
         pair_f32(L, st[ki * L.nkinds + __float_as_int(pj.w)], d2, fs, v);
-        const long long qx = quant(fmul(dx, fs), err), qy = quant(fmul(dy, fs), err), qz = quant(fmul(dz, fs), err);
+        long long qx, qy, qz;
+                quant3(fmul(dx, fs), fmul(dy, fs), fmul(dz, fs), qx, qy, qz, err);
         a.fx += qx;
         a.fy += qy;
         a.fz += qz;
@@ -735,8 +737,8 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force_cmp(GridGeom g, const f
                 const uint32_t q = qk & kIdxMask;
                 float fs, v;
                 pair_f32(L, st[ki * L.nkinds + (int)(qk >> 27)], dist2(sv.x, sv.y, sv.z), fs, v);
-                const long long qx = quant(fmul(sv.x, fs), err), qy = quant(fmul(sv.y, fs), err),
-                                qz = quant(fmul(sv.z, fs), err);
+                long long qx, qy, qz;
+                    quant3(fmul(sv.x, fs), fmul(sv.y, fs), fmul(sv.z, fs), qx, qy, qz, err);
                 a.fx += qx;
                 a.fy += qy;
                 a.fz += qz;
@@ -986,134 +988,6 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force_brick(GridGeom g, const
     }
 }
 
-// Variant 9: variant 8's staged bricks with variant 7's two phases: each
-// thread collects up to S in-cutoff entries of its home atom's list (partner
-// positions read from the staged neighbourhood) into a shared-memory stash,
-// then the warp runs the pair law over the stash together.  The home atoms of
-// a brick are taken 128 at a time, one per thread, so the warp-level loops
-// see every lane.  Same pairs and per-pair operations as variant 6:
-// bit-identical forces.
-template <bool ENERGY, int CAP, int S>
-__global__ void __launch_bounds__(kNlThreads) k_nl_force_brick_cmp(
-    GridGeom g, const float4* __restrict__ pos4, const uint32_t* __restrict__ home, const uint32_t* __restrict__ start,
-    uint32_t n, LawF32 L, const PairF* __restrict__ tab, const uint32_t* __restrict__ list, size_t stride, int cap_nb,
-    const uint32_t* __restrict__ cnt, long long* __restrict__ F, size_t fstride, unsigned long long* __restrict__ vacc,
-    unsigned long long* __restrict__ npairs, uint32_t* __restrict__ err, uint32_t K, uint32_t nchunks) {
-    __shared__ PairF st[kMaxKinds * kMaxKinds];
-    __shared__ float4 s_shift[27];
-    __shared__ unsigned long long shu[kNlThreads / 32];
-    __shared__ __align__(16) BrickSmem<CAP> B;
-    __shared__ float4 stash[S * kNlThreads];  // slot k of thread t at [k * kNlThreads + t]
-    const int nk2 = L.nkinds * L.nkinds;
-    for (int t = threadIdx.x; t < nk2; t += kNlThreads) st[t] = tab[t];
-    if (threadIdx.x < 27) {
-        float sx, sy, sz;
-        code_shift(g, threadIdx.x, sx, sy, sz);
-        s_shift[threadIdx.x] = make_float4(sx, sy, sz, 0.f);
-    }
-    uint32_t hlo, hhi;
-    if (!brick_stage<CAP>(g, start, pos4, K, nchunks, B, err, hlo, hhi)) return;
-    const bool staged = B.total <= (uint32_t)CAP;
-    PairAcc a;
-    float4* my = stash + threadIdx.x;
-    for (uint32_t base = hlo; base < hhi; base += kNlThreads) {  // uniform over the block
-        const uint32_t p = base + threadIdx.x;
-        a.fx = a.fy = a.fz = 0;
-        float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
-        int ki = 0;
-        uint32_t m = 0;
-        if (p < hhi) {
-            pi = pos4[p];
-            ki = __float_as_int(pi.w);
-            m = cnt[p];
-            if (m > (uint32_t)cap_nb) {  // overflowed list: scan the home-grid cells directly
-                uint32_t cx, cy, cz;
-                const uint32_t c = home[p];
-                decode(g, c, cx, cy, cz);
-                for (uint32_t code = 0; code < 27; ++code) {
-                    const uint32_t Bc = cell_at(g, cx, cy, cz, code);
-                    if (Bc < c) continue;
-                    const float4 sh = s_shift[code];
-                    for (uint32_t q = start[Bc], hi = start[Bc + 1]; q < hi; ++q)
-                        if (q > p) nl_pair(L, st, ki, pi, pos4[q], sh.x, sh.y, sh.z, ENERGY, a, err, F, q, fstride);
-                }
-                m = 0;
-            }
-        }
-        const uint32_t* lp = list + p;
-        uint32_t e = 0;
-        while (__any_sync(0xffffffffu, e < m)) {
-            int k = 0;
-            for (; e + 4 <= m && k <= S - 4; e += 4) {
-                uint32_t w[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) w[u] = __ldg(lp + (size_t)(e + u) * stride);
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const float4 pj = brick_pos(B, staged, w[u], pos4);
-                    const float4 sh = s_shift[w[u] >> 27];
-                    const float dx = delta1(pi.x, pj.x, sh.x), dy = delta1(pi.y, pj.y, sh.y), dz = delta1(pi.z, pj.z, sh.z);
-                    const float d2 = dist2(dx, dy, dz);
-                    if (d2 < L.rc2 && d2 != 0.f) {
-                        my[k * kNlThreads] = make_float4(
-                            dx, dy, dz, __uint_as_float((w[u] & kIdxMask) | ((uint32_t)__float_as_int(pj.w) << 27)));
-                        ++k;
-                    }
-                }
-            }
-            for (; e < m && k < S; ++e) {
-                const uint32_t w = __ldg(lp + (size_t)e * stride);
-                const float4 pj = brick_pos(B, staged, w, pos4);
-                const float4 sh = s_shift[w >> 27];
-                const float dx = delta1(pi.x, pj.x, sh.x), dy = delta1(pi.y, pj.y, sh.y), dz = delta1(pi.z, pj.z, sh.z);
-                const float d2 = dist2(dx, dy, dz);
-                if (d2 < L.rc2 && d2 != 0.f) {
-                    my[k * kNlThreads] =
-                        make_float4(dx, dy, dz, __uint_as_float((w & kIdxMask) | ((uint32_t)__float_as_int(pj.w) << 27)));
-                    ++k;
-                }
-            }
-            int kmax = k;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
-            for (int t = 0; t < kmax; ++t) {
-                if (t < k) {
-                    const float4 sv = my[t * kNlThreads];
-                    const uint32_t qk = __float_as_uint(sv.w);
-                    const uint32_t q = qk & kIdxMask;
-                    float fs, v;
-                    pair_f32(L, st[ki * L.nkinds + (int)(qk >> 27)], dist2(sv.x, sv.y, sv.z), fs, v);
-                    const long long qx = quant(fmul(sv.x, fs), err), qy = quant(fmul(sv.y, fs), err),
-                                    qz = quant(fmul(sv.z, fs), err);
-                    a.fx += qx;
-                    a.fy += qy;
-                    a.fz += qz;
-                    atomicAdd((unsigned long long*)&F[q], (unsigned long long)(-qx));
-                    atomicAdd((unsigned long long*)&F[fstride + q], (unsigned long long)(-qy));
-                    atomicAdd((unsigned long long*)&F[2 * fstride + q], (unsigned long long)(-qz));
-                    if (ENERGY && q > p) {
-                        a.vq += quant(v, err);
-                        ++a.np;
-                    }
-                }
-            }
-        }
-        if (p < hhi) {
-            atomicAdd((unsigned long long*)&F[p], (unsigned long long)a.fx);
-            atomicAdd((unsigned long long*)&F[fstride + p], (unsigned long long)a.fy);
-            atomicAdd((unsigned long long*)&F[2 * fstride + p], (unsigned long long)a.fz);
-        }
-    }
-    if (ENERGY) {
-        unsigned long long sv = block_sum_u<kNlThreads>((unsigned long long)a.vq, shu);
-        unsigned long long np = block_sum_u<kNlThreads>(a.np, shu);
-        if (threadIdx.x == 0) {
-            if (sv) atomicAdd(vacc, sv);
-            if (np) atomicAdd(npairs, np);
-        }
-    }
-}
-
 // The list build of k_nl_build brick by brick: the candidates are read from
 // the staged neighbourhood; the cells, the reach test, the candidate order
 // and the distance test are k_nl_build's, so the lists are the same words.
@@ -1175,13 +1049,6 @@ void launch_nl_force(gx_handle* h, int tpp, const GridGeom& g, const NlState* s,
     const float4* pos4 = h->pos4;
     const uint32_t* home = h->key_sorted;
     const uint32_t* start = s->cl.start;
-    if (HALF && h->kernel_variant == 9) {  // bricks of 4 cells, an 8-slot stash
-        const uint32_t K = 4u, nchunks = (g.n[0] + K - 1) / K;
-        auto kb = energy ? k_nl_force_brick_cmp<true, 1024, 8> : k_nl_force_brick_cmp<false, 1024, 8>;
-        GX_LAUNCH(h, kb, nchunks * g.n[1] * g.n[2], kNlThreads, g, pos4, home, start, n, L, h->d_pairf, s->list,
-                  s->cap, s->cap_nb, s->cnt, h->F, h->cap, h->dcount + 1, h->dcount + 0, h->derr, K, nchunks);
-        return;
-    }
     if (HALF && h->kernel_variant == 8) {
         const uint32_t K = s->brick == 0 ? 4u : 8u;
         const uint32_t nchunks = (g.n[0] + K - 1) / K;
@@ -1547,7 +1414,7 @@ int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nb_out, bool
         prof_end(h, "nl_stage");
         const float rl = (float)((h->fs.rc + s->skin_used) * (1.0 + 1e-6));
         prof_begin(h, "nl_build");
-        if (h->kernel_variant >= 8) {  // the brick build: candidates from the staged neighbourhood
+        if (h->kernel_variant == 8) {  // the brick build: candidates from the staged neighbourhood
             const uint32_t K = 8, nchunks = (g.n[0] + K - 1) / K;
             auto bb = s->half == 1 ? k_nl_build_brick<true, 2048> : k_nl_build_brick<false, 2048>;
             GX_LAUNCH(h, bb, nchunks * g.n[1] * g.n[2], kNlBuildThreads, g, h->pos4, h->key_sorted, s->cl.start,

@@ -107,6 +107,23 @@ __device__ __forceinline__ long long quant(float v, uint32_t* err) {
     return __float2ll_rn(s);
 }
 
+// The three components of one pair force: quant of each, with one range
+// check on the fast path (the same integers and flags as three quant calls;
+// a NaN fails the check and takes the per-component path, which flags it).
+__device__ __forceinline__ void quant3(float fx, float fy, float fz, long long& qx, long long& qy, long long& qz,
+                                       uint32_t* err) {
+    const float ux = fmul(fx, kFixScaleF), uy = fmul(fy, kFixScaleF), uz = fmul(fz, kFixScaleF);
+    if (fabsf(ux) < 9.0e18f && fabsf(uy) < 9.0e18f && fabsf(uz) < 9.0e18f) {
+        qx = __float2ll_rn(ux);
+        qy = __float2ll_rn(uy);
+        qz = __float2ll_rn(uz);
+    } else {
+        qx = quant(fx, err);
+        qy = quant(fy, err);
+        qz = quant(fz, err);
+    }
+}
+
 LawF32 make_law32(const gx_handle* h);
 
 // Thread-per-atom pair pass with per-thread candidate lists (gx_force_tiled.cu);

@@ -119,25 +119,23 @@ int gx_set_precision(gx_handle* h, int precision);
  * them together (fewer idle lanes; same forces as 6, bit for bit);
  * 8 = the half list of 6 evaluated brick by brick (4 or 8 list-grid cells of
  * one x-row), the brick's neighbour rows staged in shared memory once and
- * read from there (same forces as 6, bit for bit); 9 = the bricks of 8
- * (4 cells) with the in-cutoff entries of 7 collected in an 8-slot stash
- * first (same forces as 6, bit for bit).  8 and 9 also build their lists
+ * read from there (same forces as 6, bit for bit); 8 also builds its lists
  * brick by brick from shared memory (the same lists).
- * 5-9 need >= 3 list-grid cells per axis, else they fall back to 4.  Variants 2 and 3 need >= 3 force-grid
+ * 5-8 need >= 3 list-grid cells per axis, else they fall back to 4.  Variants 2 and 3 need >= 3 force-grid
  * cells per axis and fall back to 1 otherwise.  Variants 1-4 give
- * bit-identical forces, and so do 5-9 (fixed-point sums); 5-9
+ * bit-identical forces, and so do 5-8 (fixed-point sums); 5-8
  * evaluate the same pair set in a cell-local frame whose origin is the
  * atom's cell at the last rebuild, so their FP32 forces can differ from 1-4
  * in the last bits (same error bound). */
 int gx_set_kernel_variant(gx_handle* h, int variant);
 /* Autotuner: times `reps` mixed pair passes of variants 1-4 on the resident
  * state (left bit-identical: they give the same fixed-point sums) and, where
- * variants 5-9 apply, full ticks of the best of them against full ticks
- * of 5-9, each from a snapshot of (x, v, a) restored afterwards.
+ * variants 5-8 apply, full ticks of the best of them against full ticks
+ * of 5-8, each from a snapshot of (x, v, a) restored afterwards.
  * Selects the fastest and returns it in *best.  ms[1..4], when given,
- * receive the per-pass milliseconds, ms[0], ms[5..9] the per-tick
- * milliseconds of the best pass variant and of 5-9 (-1 = not run); ms has
- * 10 entries.  Where a list variant wins, the list skin is
+ * receive the per-pass milliseconds, ms[0], ms[5..8] the per-tick
+ * milliseconds of the best pass variant and of 5-8 (-1 = not run); ms has
+ * 9 entries.  Where a list variant wins, the list skin is
  * then chosen the same way over whole ticks among 0.05, 0.1, 0.15 and
  * 0.2 r_c (the list-grid cell is r_c + skin; gx_get_list_config reports
  * the choice), and the lanes per atom (the stash size of 7, the brick
@@ -161,7 +159,7 @@ int gx_set_list_stash(gx_handle* h, int slots);
  * per block with the far end of every pair inside the block summed in
  * shared memory (two 32-bit words with the carry), so that only the other
  * pairs send their far end's force to global memory; 0 = every far end to
- * global memory.  Default 256; the autotuner picks among 256, 128, 0 and the
+ * global memory.  Default 0; the autotuner picks among 256, 128, 0 and the
  * wider lanes per atom.  All give the same bits.  No counterpart in the
  * reference. */
 int gx_set_list_block(gx_handle* h, int threads);

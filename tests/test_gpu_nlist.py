@@ -1,11 +1,10 @@
 """The persistent neighbour-list passes (kernel variants 5: full list, 6:
 half list with far-end atomics, 7: the half list with in-cutoff entries
 collected in shared memory before the pair law, 8: the half list brick by
-brick with the brick's neighbourhood staged in shared memory, 9: 8 with
-7's stash) against the
+brick with the brick's neighbourhood staged in shared memory) against the
 oracle, each other and the per-tick re-sort variants.
 
-Variants 5-9 evaluate the same pair set {d < r_c} as every other variant, in a
+Variants 5-8 evaluate the same pair set {d < r_c} as every other variant, in a
 cell-local frame anchored at the last rebuild, so its FP32 forces can differ
 from variants 1-4 in the last bits: the checks are the mixed path's error
 bound against the FP64 oracle (force rel-RMS <= 1e-5), agreement of whole
@@ -43,7 +42,7 @@ def _relnorm(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
-@pytest.mark.parametrize("coul,variant", [(False, 5), (True, 5), (False, 6), (True, 6), (True, 7), (True, 8), (True, 9)])
+@pytest.mark.parametrize("coul,variant", [(False, 5), (True, 5), (False, 6), (True, 6), (True, 7), (True, 8)])
 def test_first_tick_forces_match_fp64_oracle(gpu, orc, coul, variant):
     cfg, u = _lattice(18, coul=coul)
     h = _handle(cfg, variant)
@@ -63,7 +62,7 @@ def test_full_and_half_lists_are_bit_identical(gpu, thermo):
         cfg.enable_thermostat = True
         cfg.thermostat_temperature = 40.0
     out = []
-    for variant, opt in ((5, 0), (6, 0), (7, 16), (7, 8), (8, 4), (8, 8), (9, 0)):
+    for variant, opt in ((5, 0), (6, 0), (7, 16), (7, 8), (8, 4), (8, 8)):
         h = _handle(cfg, variant)
         if variant == 7:
             h.set_list_stash(opt)
@@ -174,7 +173,7 @@ def test_list_path_is_deterministic_and_graph_invariant(gpu):
         assert np.array_equal(runs[0][1], r[1])
 
 
-@pytest.mark.parametrize("variant", [5, 6, 7, 8, 9])
+@pytest.mark.parametrize("variant", [5, 6, 7, 8])
 def test_overflowing_lists_fall_back_to_cell_scans(gpu, orc, variant):
     # a dense clump far above the average density overflows the per-atom lists
     cfg, u = _lattice(12, temperature=10.0)
@@ -207,7 +206,7 @@ def test_state_round_trip_after_list_ticks(gpu):
     assert np.array_equal(pos, p2) and np.array_equal(vel, v2) and np.array_equal(acc, a2)
 
 
-@pytest.mark.parametrize("variant", [5, 6, 7, 8, 9])
+@pytest.mark.parametrize("variant", [5, 6, 7, 8])
 def test_captured_rebuilds_run_only_when_flagged(gpu, variant):
     # a captured tick holds the rebuild in a conditional graph node set from
     # the displacement flag: the same ticks and rebuilds as eager execution,
@@ -268,7 +267,7 @@ def test_bricks_beyond_the_staging_capacity_read_global_memory(gpu):
     pos[:k] = d * (6.0 * rng.random(k) ** (1.0 / 3.0) + 0.2)[:, None]
     u2 = dataclasses.replace(u, pos=pos)
     out = []
-    for variant, brick in ((6, 0), (8, 4), (8, 8), (9, 0)):
+    for variant, brick in ((6, 0), (8, 4), (8, 8)):
         h = _handle(cfg, variant)
         if brick:
             h.set_list_brick(brick)

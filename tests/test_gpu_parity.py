@@ -340,8 +340,8 @@ def test_autotune_leaves_state_unchanged(gpu):
     a.step(2)
     before = a.get_state()
     best, ms = a.autotune(reps=2)
-    assert best in ms and best in (1, 2, 3, 4, 5, 6, 7, 8, 9)
-    assert all(v in ms for v in (0, 5, 6, 7, 8, 9))  # the list paths were timed against the best pass tick
+    assert best in ms and best in (1, 2, 3, 4, 5, 6, 7, 8)
+    assert all(v in ms for v in (0, 5, 6, 7, 8))  # the list paths were timed against the best pass tick
     if best >= 5:  # the skin was chosen among 0.05, 0.1, 0.15, 0.2 r_c
         skin, _ = a.list_config()
         rc = E.LJ_CUTOFF_FACTOR * max(cfg.sigma)
