@@ -36,9 +36,12 @@ __device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a,
 __device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
 __device__ __forceinline__ double xsqrt(double a) { return __dsqrt_rn(a); }
 
-// f64::rem_euclid: r = a % b (fmod, exact); r < 0 ? r + |b| : r.
+// f64::rem_euclid: r = a % b (fmod, exact); r < 0 ? r + |b| : r.  When
+// |a| < |b|, fmod(a, b) is a itself (the quotient truncates to 0), so the
+// division is skipped: every coordinate that is already inside the box takes
+// that path, with the same bits.
 __device__ __forceinline__ double rem_euclid(double a, double b) {
-    double r = fmod(a, b);
+    double r = fabs(a) < fabs(b) ? a : fmod(a, b);
     return r < 0.0 ? xadd(r, fabs(b)) : r;
 }
 // min_image, src/physics/grid.rs:300-306 (round = half away from zero).
