@@ -42,9 +42,10 @@ FLOP_PER_PAIR_LJC_NOV = 71
 # the arrays the kernel must touch; FP64 state, u8 element/kind, u32 ids).
 BYTES_PER_ATOM = {
     "kick": 72, "drift": 72, "wrap": 48, "cell_keys": 28, "cell_count": 4, "cell_scan": 0,
-    # scatter: read key, read the cell's start, write the slot; segment sort:
-    # read and write the slot
-    "cell_scatter": 12, "cell_segsort": 8, "reorder": 220, "stage_pos4": 45, "kinetic": 32,
+    # scatter: read key, read the cell's start, write the slot; the per-cell
+    # ranking: read key, the cell's start and end, write the slot (the cell's
+    # segment it scans is an L1/L2 hit)
+    "cell_scatter": 12, "cell_rank": 16, "reorder": 220, "stage_pos4": 45, "kinetic": 32,
     # list path: fused kick + drift + wrap + FP32 staging + displacement test
     # (read x v a 72, kind 1, home cell 4, reference float4 16; write x v 48,
     # float4 16), and fused F -> a + kick + K (read F 24, v 24, 1/m 8, m 8;
@@ -57,7 +58,7 @@ BYTES_PER_ATOM = {
     "nl_copy": 204, "nl_stage": 61,
 }
 # kernels that run only on ticks that rebuild the neighbour list
-REBUILD_KERNELS = ("cell_keys", "cell_count", "cell_scan", "cell_scatter", "cell_segsort", "reorder", "nl_copy",
+REBUILD_KERNELS = ("cell_keys", "cell_count", "cell_scan", "cell_scatter", "cell_rank", "reorder", "nl_copy",
                    "nl_stage", "nl_build")
 
 

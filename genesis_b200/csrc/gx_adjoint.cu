@@ -503,10 +503,7 @@ struct AdjBuffers {
 static void adj_release(AdjBuffers* A) {
     for (void* p : A->owned) cudaFree(p);
     A->owned.clear();
-    cudaFree(A->cl.count);
-    cudaFree(A->cl.start);
-    cudaFree(A->cl.fill);
-    for (auto q : A->cl.scan_levels) cudaFree(q);
+    cells_free(A->cl);
     A->cl = CellList();
 }
 

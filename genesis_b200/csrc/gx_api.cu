@@ -460,10 +460,7 @@ void gx_destroy(gx_handle* h) {
     cudaFree(h->derr);
     cudaFree(h->d_pairf);
     cudaFree(h->bonds);
-    cudaFree(h->cl.count);
-    cudaFree(h->cl.start);
-    cudaFree(h->cl.fill);
-    for (auto q : h->cl.scan_levels) cudaFree(q);
+    cells_free(h->cl);
     for (auto& s : h->prof)
         for (auto ev : s.ev) cudaEventDestroy(ev);
     for (auto ev : h->ev_pool) cudaEventDestroy(ev);
@@ -738,6 +735,7 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
     // state, so it can be captured: the first kick always applies the lambda
     // slot (1.0 unless a Berendsen scale is pending; v * 1.0 == v) and resets it.
     const bool use_nl = n && (h->kernel_variant >= 5 || h->kernel_variant == 0) && nl_eligible(h);
+    if (n && (rc = ensure_sort_tmp(h, h->cl, h->cap))) return rc;  // a captured re-sort must not allocate
     if (n && h->p.enable_collisions && (rc = collide_prepare(h))) return rc;  // CollisionSystem: allocate first
     if (use_nl) {
         bool stale = false;

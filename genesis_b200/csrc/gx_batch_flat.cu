@@ -81,10 +81,7 @@ void batch_flat_free(BatchFlat* f) {
     cudaFree(f->coop_bar);
     cudaFree(f->coop_tile);
     if (f->ctx) {
-        cudaFree(f->ctx->cl.count);
-        cudaFree(f->ctx->cl.start);
-        cudaFree(f->ctx->cl.fill);
-        for (auto q : f->ctx->cl.scan_levels) cudaFree(q);
+        cells_free(f->ctx->cl);
         f->ctx->stream = nullptr;  // owned by the batch
         delete f->ctx;
     }
@@ -383,7 +380,7 @@ __global__ void __launch_bounds__(kFbRed) k_fb_commit(const RepThermo* __restric
 // waits longer than about two seconds sets kErrTimeout and every block
 // leaves at its next barrier.  The counting sort is done in place (cell
 // counts fused into the advance phase, a tiled scan, the scatter and the
-// per-cell index sort of the shared counting_sort), and the other phases
+// per-cell ranking of the shared counting_sort), and the other phases
 // call the functions of the kernels above, so a tick is the same bits as a
 // mode-2 tick.  The block size is kFbRed, as the per-replica reductions of
 // k_fb_thermo and k_fb_commit need the same thread mapping.
@@ -404,7 +401,7 @@ struct CoopArgs {
     const PairF* tab;
     double* out;
     uint32_t* err;
-    uint32_t *count, *start, *fill, *tile;
+    uint32_t *count, *start, *fill, *tile, *tmp;
     unsigned* bar;  // [0] arrivals, [1] generation
     uint32_t ncell, total;
     int nrep;
@@ -542,20 +539,15 @@ __global__ void __launch_bounds__(kCoopThreads) k_fb_coop(CoopArgs a) {
         if (!coop_sync(a, &s_ok)) return;
         for (uint32_t i = gt; i < n; i += gs) {  // k_scatter
             const uint32_t c = A.key[i];
-            A.idx[a.start[c] + atomicAdd(&a.fill[c], 1u)] = i;
+            a.tmp[a.start[c] + atomicAdd(&a.fill[c], 1u)] = i;
         }
         if (!coop_sync(a, &s_ok)) return;
-        for (uint32_t c = gt; c < a.ncell; c += gs) {  // k_segsort
+        for (uint32_t i = gt; i < n; i += gs) {  // k_rank: ascending source order within each cell
+            const uint32_t c = A.key[i];
             const uint32_t lo = a.start[c], hi = a.start[c + 1];
-            for (uint32_t q = lo + 1; q < hi; ++q) {
-                const uint32_t v = A.idx[q];
-                uint32_t b = q;
-                while (b > lo && A.idx[b - 1] > v) {
-                    A.idx[b] = A.idx[b - 1];
-                    --b;
-                }
-                A.idx[b] = v;
-            }
+            uint32_t r = 0;
+            for (uint32_t q = lo; q < hi; ++q) r += a.tmp[q] < i ? 1u : 0u;
+            A.idx[lo + r] = i;
         }
         if (!coop_sync(a, &s_ok)) return;
         for (uint32_t s2 = gt; s2 < n; s2 += gs) fb_stage_one(s2, a.geo, a.rep_of, A, A.idx, A.key, a.srep, fs);
@@ -641,6 +633,7 @@ int flat_prepare(gx_batch* b) {
     f->ctx = new gx_handle();
     f->ctx->stream = b->stream;
     if (ensure_cells(f->ctx, f->ctx->cl, f->ncell)) return ferr(b, GX_ERR_OOM, f->ctx->err);
+    if (ensure_sort_tmp(f->ctx, f->ctx->cl, b->total)) return ferr(b, GX_ERR_OOM, f->ctx->err);  // before capture
     return GX_OK;
 }
 
@@ -708,6 +701,7 @@ int batch_coop_step(gx_batch* b, int nsteps, uint64_t* launches) {
     a.count = f->ctx->cl.count;
     a.start = f->ctx->cl.start;
     a.fill = f->ctx->cl.fill;
+    a.tmp = f->ctx->cl.tmp;
     a.tile = f->coop_tile;
     a.bar = f->coop_bar;
     a.ncell = f->ncell;

@@ -86,22 +86,22 @@ __global__ void k_scatter(const uint32_t* __restrict__ key, uint32_t n, const ui
     perm[start[c] + atomicAdd(&fill[c], 1u)] = i;
 }
 
-// Makes the scatter deterministic: each cell's segment sorted by source index.
-__global__ void k_segsort(const uint32_t* __restrict__ start, uint32_t ncell, uint32_t* __restrict__ perm,
-                          const uint32_t* __restrict__ gate) {
+// Makes the scatter deterministic: atom i goes to start[c] + (the number of
+// atoms of its cell with a smaller index), so each cell lists its atoms in
+// ascending source order.  One thread per atom reads its cell's segment of
+// the scatter's order: a cell of k atoms costs k^2 reads spread over its k
+// atoms, where a per-cell insertion sort ran them on one thread.
+__global__ void k_rank(const uint32_t* __restrict__ key, uint32_t n, const uint32_t* __restrict__ start,
+                       const uint32_t* __restrict__ scattered, uint32_t* __restrict__ perm,
+                       const uint32_t* __restrict__ gate) {
     if (gated_off(gate)) return;
-    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncell) return;
-    uint32_t lo = start[c], hi = start[c + 1];
-    for (uint32_t a = lo + 1; a < hi; ++a) {
-        uint32_t v = perm[a];
-        uint32_t b = a;
-        while (b > lo && perm[b - 1] > v) {
-            perm[b] = perm[b - 1];
-            --b;
-        }
-        perm[b] = v;
-    }
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t c = key[i];
+    const uint32_t lo = start[c], hi = start[c + 1];
+    uint32_t r = 0;
+    for (uint32_t b = lo; b < hi; ++b) r += __ldg(scattered + b) < i ? 1u : 0u;
+    perm[lo + r] = i;
 }
 
 __global__ void k_cell_keys(GridGeom g, const double* __restrict__ x, const double* __restrict__ y,
@@ -280,6 +280,30 @@ inline unsigned nblk(uint32_t n, int bs) { return (n + bs - 1) / bs; }
 
 }  // namespace
 
+void cells_free(CellList& cl) {
+    cudaFree(cl.count);
+    cudaFree(cl.start);
+    cudaFree(cl.fill);
+    cudaFree(cl.tmp);
+    for (auto p : cl.scan_levels) cudaFree(p);
+    cl.count = cl.start = cl.fill = cl.tmp = nullptr;
+    cl.scan_levels.clear();
+    cl.scan_sizes.clear();
+    cl.cap_cells = 0;
+    cl.cap_tmp = 0;
+}
+
+int ensure_sort_tmp(gx_handle* h, CellList& cl, size_t n) {
+    if (n <= cl.cap_tmp) return GX_OK;
+    cudaFree(cl.tmp);
+    cl.tmp = nullptr;
+    cl.cap_tmp = 0;
+    const size_t cap = n + n / 8 + 64;
+    GX_CUDA(h, cudaMalloc(&cl.tmp, cap * sizeof(uint32_t)));
+    cl.cap_tmp = cap;
+    return GX_OK;
+}
+
 int ensure_cells(gx_handle* h, CellList& cl, uint32_t ncell) {
     if (ncell + 1 > cl.cap_cells) {
         cudaFree(cl.count);
@@ -338,12 +362,13 @@ int counting_sort(gx_handle* h, CellList& cl, uint32_t ncell, const uint32_t* ke
     prof_begin(h, "cell_scan");
     scan_rec(h, cl, cl.count, cl.start, ncell + 1, 0, gate);
     prof_end(h, "cell_scan");
+    if ((rc = ensure_sort_tmp(h, cl, n))) return rc;  // allocated before any capture by the callers that capture
     prof_begin(h, "cell_scatter");
-    if (n) GX_LAUNCH(h, k_scatter, nblk(n, 256), 256, key, n, cl.start, cl.fill, perm, gate);
+    if (n) GX_LAUNCH(h, k_scatter, nblk(n, 256), 256, key, n, cl.start, cl.fill, cl.tmp, gate);
     prof_end(h, "cell_scatter");
-    prof_begin(h, "cell_segsort");
-    GX_LAUNCH(h, k_segsort, nblk(ncell, 128), 128, cl.start, ncell, perm, gate);
-    prof_end(h, "cell_segsort");
+    prof_begin(h, "cell_rank");
+    if (n) GX_LAUNCH(h, k_rank, nblk(n, 256), 256, key, n, cl.start, cl.tmp, perm, gate);
+    prof_end(h, "cell_rank");
     return GX_OK;
 }
 

@@ -157,7 +157,10 @@ struct CellList {
     size_t cap_cells = 0;
     std::vector<uint32_t*> scan_levels;  // block sums per scan level
     std::vector<size_t> scan_sizes;
+    uint32_t* tmp = nullptr;     // n: the scatter's order before the per-cell ranking
+    size_t cap_tmp = 0;
 };
+void cells_free(CellList& cl);
 
 struct ProfSlot {
     const char* name;
@@ -282,6 +285,8 @@ void prof_end(gx_handle* h, const char* name);
 
 // Launchers implemented in the .cu files.
 int ensure_cells(gx_handle* h, CellList& cl, uint32_t ncell);
+// The counting sort's per-atom scratch (outside any stream capture).
+int ensure_sort_tmp(gx_handle* h, CellList& cl, size_t n);
 void cell_scan(gx_handle* h, CellList& cl, uint32_t ncell);
 // Counting sort of atoms [0,n) by key into perm (sorted pos -> source index),
 // deterministic (ties keep ascending source index).  cl.start gets cell starts.

@@ -52,9 +52,9 @@ struct AuxPool {
 
 void pool_release(AuxPool* P) {
     if (!P) return;
-    void* ps[] = {P->xyz, P->elem, P->u32, P->parent, P->cnt, P->counts, P->cl.count, P->cl.start, P->cl.fill};
+    void* ps[] = {P->xyz, P->elem, P->u32, P->parent, P->cnt, P->counts};
     for (void* q : ps) cudaFree(q);
-    for (auto q : P->cl.scan_levels) cudaFree(q);
+    cells_free(P->cl);
     delete P;
 }
 

@@ -1271,10 +1271,7 @@ void nl_free(gx_handle* h) {
     cudaFree(s->cnt);
     cudaFree(s->ref);
     cudaFree(s->flag);
-    cudaFree(s->cl.count);
-    cudaFree(s->cl.start);
-    cudaFree(s->cl.fill);
-    for (auto q : s->cl.scan_levels) cudaFree(q);
+    cells_free(s->cl);
     if (s->side) cudaStreamDestroy(s->side);
     delete s;
     h->nl = nullptr;
@@ -1347,6 +1344,7 @@ int nl_prepare(gx_handle* h, bool* stale) {
     const size_t cl_cap = s->cl.cap_cells;
     int rc = ensure_cells(h, s->cl, g.ncell);
     if (rc) return rc;
+    if ((rc = ensure_sort_tmp(h, s->cl, h->cap))) return rc;  // the captured rebuild must not allocate
     if (s->cl.cap_cells != cl_cap) *stale = true;
     if (!h->nl_valid) {
         const uint32_t one = 1u;
