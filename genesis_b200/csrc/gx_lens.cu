@@ -963,6 +963,7 @@ int collide_prepare(gx_handle* h) {
     if (!c->pool) c->pool = new AuxPool();
     int rc = ensure_pool(h, *c->pool, h->n, h->n);
     if (!rc) rc = ensure_cells(h, c->pool->cl, g.ncell);
+    if (!rc) rc = ensure_sort_tmp(h, c->pool->cl, h->cap);  // the pass runs inside captured ticks
     if (rc) return rc;
     if (c->cap < h->cap) {
         cudaFree(c->dv);
