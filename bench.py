@@ -69,6 +69,7 @@ def list_build_bytes_per_atom(entries_per_atom: float) -> float:
     return 24.0 + 4.0 * entries_per_atom
 
 
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1013,6 +1014,7 @@ def ours_arm(args, dist):
                 extras["cpu_baseline_error"] = repr(e)
 
     list_cfg = h.list_config()
+    list_shape = h.list_shape()
     h.close()
     if dist.rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": K, "warmup": Wm,
@@ -1026,6 +1028,7 @@ def ours_arm(args, dist):
                            "pair_pass_variant": variant, "autotune_ms": tune_ms,
                            "neighbour_list_rebuilds_in_timed_ticks": rebuilds,
                            "neighbour_list_skin_and_threads_per_atom": list_cfg,
+                           "list_pass_shape": list_shape,
                            "cuda_graph": True},
                 "gpu_launches": launches, "clocks": clk, "roofline": roof, "roofline_hbm": roof_hbm,
                 "roofline_rebuild": roof_rebuild,

@@ -68,7 +68,7 @@ EXPORTS = (
     "gx_batch_create", "gx_batch_destroy", "gx_batch_last_error", "gx_batch_set_state",
     "gx_batch_step", "gx_batch_get_state", "gx_adjoint_forward", "gx_adjoint_backward",
     "gx_set_list_skin", "gx_list_rebuilds", "gx_list_stats", "gx_batch_set_mode", "gx_batch_get_mode", "gx_batch_autotune",
-    "gx_get_list_config", "gx_set_list_threads", "gx_set_list_stash", "gx_set_list_brick", "gx_set_list_block", "gx_bond_observe", "gx_bond_tracker_reset", "gx_get_bonds",
+    "gx_get_list_config", "gx_set_list_threads", "gx_set_list_stash", "gx_set_list_brick", "gx_set_list_block", "gx_get_list_shape", "gx_bond_observe", "gx_bond_tracker_reset", "gx_get_bonds",
     "gx_bond_components", "gx_collisions", "gx_collision_count", "gx_xyz_frame", "gx_snapshot_world",
     "gx_set_step_async",
 )
@@ -132,6 +132,8 @@ def load(path: str | Path | None = None) -> C.CDLL:
         "gx_set_list_stash": (C.c_int, [vp, C.c_int]),
         "gx_set_list_brick": (C.c_int, [vp, C.c_int]),
         "gx_set_list_block": (C.c_int, [vp, C.c_int]),
+        "gx_get_list_shape": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                      C.POINTER(C.c_int)]),
         "gx_bond_observe": (C.c_int, [vp, _D, _D, C.c_int, C.c_uint64, C.c_int, C.POINTER(GxBondObservation)]),
         "gx_bond_tracker_reset": (C.c_int, [vp]),
         "gx_get_bonds": (C.c_int, [vp, u32p, sz, C.POINTER(sz)]),
@@ -290,6 +292,13 @@ class Handle:
         skin, tpp = C.c_double(), C.c_int()
         self._check(self.lib.gx_get_list_config(self.h, C.byref(skin), C.byref(tpp)))
         return skin.value, tpp.value
+
+    def list_shape(self) -> dict:
+        """The list pass's work shape: threads per atom, far-end block,
+        variant-7 stash slots, variant-8 brick cells."""
+        v = [C.c_int() for _ in range(4)]
+        self._check(self.lib.gx_get_list_shape(self.h, *[C.byref(x) for x in v]))
+        return dict(zip(("threads_per_atom", "block", "stash_slots", "brick_cells"), (x.value for x in v)))
 
     def set_list_threads(self, threads_per_atom: int):
         self._check(self.lib.gx_set_list_threads(self.h, threads_per_atom))

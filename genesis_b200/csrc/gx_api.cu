@@ -1059,6 +1059,11 @@ int gx_set_list_block(gx_handle* h, int threads) {
     return nl_set_block(h, threads);
 }
 
+int gx_get_list_shape(gx_handle* h, int* threads_per_atom, int* block, int* stash_slots, int* brick_cells) {
+    if (!h || !threads_per_atom || !block || !stash_slots || !brick_cells) return GX_ERR_ARG;
+    return nl_shape(h, threads_per_atom, block, stash_slots, brick_cells);
+}
+
 int gx_set_list_brick(gx_handle* h, int cells) {
     if (!h) return GX_ERR_ARG;
     invalidate_graphs(h);

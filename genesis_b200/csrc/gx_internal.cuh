@@ -327,6 +327,7 @@ int nl_set_tpp(gx_handle* h, int tpp);
 int nl_set_slots(gx_handle* h, int slots);
 int nl_set_brick(gx_handle* h, int cells);
 int nl_set_block(gx_handle* h, int block);
+int nl_shape(gx_handle* h, int* tpp, int* block, int* stash, int* brick);
 int nl_stats(gx_handle* h, uint64_t* entries, uint64_t* overflowed);
 void nl_free(gx_handle* h);
 void tracker_free(gx_handle* h);

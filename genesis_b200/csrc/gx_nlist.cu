@@ -1605,6 +1605,15 @@ int nl_config(gx_handle* h, double* skin, int* tpp) {
     return GX_OK;
 }
 
+int nl_shape(gx_handle* h, int* tpp, int* block, int* stash, int* brick) {
+    const NlState* s = nl_of(h);
+    *tpp = s->tpp;
+    *block = s->block;
+    *stash = s->slots;
+    *brick = s->brick == 0 ? 4 : 8;
+    return GX_OK;
+}
+
 int nl_set_brick(gx_handle* h, int cells) {
     if (cells != 4 && cells != 8) return set_err(h, GX_ERR_ARG, "brick length must be 4 or 8 cells");
     nl_of(h)->brick = cells == 4 ? 0 : 1;

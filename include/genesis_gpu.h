@@ -163,6 +163,10 @@ int gx_set_list_stash(gx_handle* h, int slots);
  * wider lanes per atom.  All give the same bits.  No counterpart in the
  * reference. */
 int gx_set_list_block(gx_handle* h, int threads);
+/* The list pass's work shape as set or tuned: threads per atom, far-end
+ * block (0, 128, 256), variant-7 stash slots (8, 16) and variant-8 brick
+ * length (4, 8 cells). */
+int gx_get_list_shape(gx_handle* h, int* threads_per_atom, int* block, int* stash_slots, int* brick_cells);
 /* Brick length of the variant-8 list pass: 4 or 8 list-grid cells per brick
  * (at most 1024 or 2048 staged atoms; a brick with more reads global
  * memory).  Default 8; the autotuner picks the faster.  Both give the same

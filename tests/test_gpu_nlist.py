@@ -135,6 +135,8 @@ def test_threads_per_atom_are_bit_identical(gpu, variant):
         h.set_universe(u)
         st = h.step(12, graph=True)
         assert h.list_config()[1] == tpp
+        shape = h.list_shape()
+        assert (shape["threads_per_atom"], shape["block"]) == (tpp, block)
         out.append((h.get_state(), st))
     for o in out[1:]:
         for x, y in zip(out[0][0], o[0]):
