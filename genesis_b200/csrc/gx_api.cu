@@ -245,10 +245,16 @@ __global__ void k_fill_d(double* p, uint32_t n, double v) {
 }
 // Appends this tick's observables at record index dcount[5] (a device-side
 // cursor, so the same launch sequence can be replayed from a CUDA graph).
-__global__ void k_record(gx_tick_stats* rec, const double* dscal, unsigned long long* dcount, int thermo) {
+// One tick's record.  `scale`: dscal[1] and dscal[4] hold K and the speed
+// sum before the thermostat's scale lambda = dscal[0]; the record takes
+// those of lambda v, lambda^2 K and lambda S (equal to the sums over the
+// scaled components up to the rounding of the products, ~1e-16 relative).
+__global__ void k_record(gx_tick_stats* rec, const double* dscal, unsigned long long* dcount, int thermo,
+                         int scale) {
     unsigned long long k = dcount[5];
-    rec[k].kinetic = dscal[1];
-    rec[k].speed_sum = dscal[4];
+    const double l = scale ? dscal[0] : 1.0;
+    rec[k].kinetic = scale ? xmul(xmul(dscal[1], l), l) : dscal[1];
+    rec[k].speed_sum = scale ? xmul(dscal[4], l) : dscal[4];
     rec[k].potential = dscal[2];
     rec[k].bond_energy = dscal[3];
     rec[k].lambda = thermo ? dscal[0] : 1.0;
@@ -746,8 +752,10 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
     auto tick_nl = [&](bool uniform) -> int {
         const bool pend = uniform || h->lambda_pending;
         int nb = 0;
-        // the potential and pair count only where a record takes them
-        int r = nl_tick(h, pend ? h->dscal + 0 : nullptr, thermo ? kpart : nullptr, &nb, drec != nullptr);
+        // the potential and pair count only where a record takes them; the
+        // record's K and speed sum come from the finish kernel's partials
+        int r = nl_tick(h, pend ? h->dscal + 0 : nullptr, (thermo || drec) ? kpart : nullptr, drec ? spart : nullptr,
+                        &nb, drec != nullptr);
         if (r) return r;
         // the scale slot back to 1 once applied; with the thermostat on, its
         // kernel below overwrites the slot anyway
@@ -758,11 +766,10 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
                                      h->dscal + 0, nullptr);
             h->lambda_pending = true;
         }
-        if (drec) {
-            launch_kinetic(h, h->buf[h->cur], n, h->lambda_pending ? h->dscal + 0 : nullptr, kpart, spart, &nb);
+        if (drec) {  // K and the speed sum of the scaled v: lambda^2 K and lambda S of the kicked v
             launch_finalize_sum(h, kpart, nb, h->dscal + 1);
             launch_finalize_sum(h, spart, nb, h->dscal + 4);
-            GX_LAUNCH(h, k_record, 1, 1, drec, h->dscal, h->dcount, thermo ? 1 : 0);
+            GX_LAUNCH(h, k_record, 1, 1, drec, h->dscal, h->dcount, thermo ? 1 : 0, thermo ? 1 : 0);
         }
         return GX_OK;
     };
@@ -794,7 +801,7 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
             launch_kinetic(h, h->buf[h->cur], n, h->lambda_pending ? h->dscal + 0 : nullptr, kpart, spart, &nb);
             launch_finalize_sum(h, kpart, nb, h->dscal + 1);
             launch_finalize_sum(h, spart, nb, h->dscal + 4);
-            GX_LAUNCH(h, k_record, 1, 1, drec, h->dscal, h->dcount, thermo ? 1 : 0);
+            GX_LAUNCH(h, k_record, 1, 1, drec, h->dscal, h->dcount, thermo ? 1 : 0, 0);
         }
         return GX_OK;
     };

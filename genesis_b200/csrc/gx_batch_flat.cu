@@ -63,7 +63,7 @@ struct BatchFlat {
     gx_handle* ctx = nullptr;           // launch context of the shared counting sort
     cudaGraphExec_t graph[2] = {};      // tick without / with the potential and pair count
     uint64_t graph_kernels = 0;
-    unsigned* coop_bar = nullptr;       // mode 3: grid barrier (arrivals, generation)
+    unsigned* coop_bar = nullptr;       // mode 3: grid barrier (arrivals, generation), force chunk counters (2)
     uint32_t* coop_tile = nullptr;      // mode 3: scan tile totals
     int coop_grid = 0;
 };
@@ -402,7 +402,7 @@ struct CoopArgs {
     double* out;
     uint32_t* err;
     uint32_t *count, *start, *fill, *tile, *tmp;
-    unsigned* bar;  // [0] arrivals, [1] generation
+    unsigned* bar;  // [0] arrivals, [1] generation, [2 + tick parity] next force chunk
     uint32_t ncell, total;
     int nrep;
     BatchParams P;
@@ -552,11 +552,21 @@ __global__ void __launch_bounds__(kCoopThreads) k_fb_coop(CoopArgs a) {
         if (!coop_sync(a, &s_ok)) return;
         for (uint32_t s2 = gt; s2 < n; s2 += gs) fb_stage_one(s2, a.geo, a.rep_of, A, A.idx, A.key, a.srep, fs);
         if (!coop_sync(a, &s_ok)) return;
-        for (uint32_t s2 = gt; s2 < npad; s2 += gs) {
-            if (energy)
-                fb_force_one<true>(s2, a.geo, A.pos4, A.skey, a.srep, a.start, n, a.L, st, A.F, fs, a.racc, a.err);
-            else
-                fb_force_one<false>(s2, a.geo, A.pos4, A.skey, a.srep, a.start, n, a.L, st, A.F, fs, a.racc, a.err);
+        {  // the pair pass: warps take 32-atom chunks from a counter, as a chunk's
+           // cost follows the local density (a static split waits for the densest)
+            unsigned* next = a.bar + 2 + (step & 1);
+            for (;;) {
+                uint32_t base = 0;
+                if ((threadIdx.x & 31) == 0) base = atomicAdd(next, 32u);
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (base >= npad) break;
+                const uint32_t s2 = base + (threadIdx.x & 31);
+                if (energy)
+                    fb_force_one<true>(s2, a.geo, A.pos4, A.skey, a.srep, a.start, n, a.L, st, A.F, fs, a.racc, a.err);
+                else
+                    fb_force_one<false>(s2, a.geo, A.pos4, A.skey, a.srep, a.start, n, a.L, st, A.F, fs, a.racc,
+                                        a.err);
+            }
         }
         if (!coop_sync(a, &s_ok)) return;
         for (uint32_t s2 = gt; s2 < n; s2 += gs) fb_finish_one(s2, A, A.idx, a.P.half_dt, fs);
@@ -566,6 +576,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_fb_coop(CoopArgs a) {
             a.count[c] = 0u;
             a.fill[c] = 0u;
         }
+        if (gt == 0) a.bar[2 + ((step + 1) & 1)] = 0u;  // last taken two ticks back, before several barriers
         if (!coop_sync(a, &s_ok)) return;
     }
     for (int r = blockIdx.x; r < a.nrep; r += gridDim.x) fb_commit_one(r, a.th, A, a.lam, a.out, sh);
@@ -674,7 +685,7 @@ int batch_coop_step(gx_batch* b, int nsteps, uint64_t* launches) {
     if (!f->coop_bar) {
         const uint32_t m = f->ncell + 1;
         const size_t ntiles = (m + kCoopTile - 1) / kCoopTile;
-        GXF_CUDA(b, cudaMalloc(&f->coop_bar, 2 * sizeof(unsigned)));
+        GXF_CUDA(b, cudaMalloc(&f->coop_bar, 4 * sizeof(unsigned)));
         GXF_CUDA(b, cudaMalloc(&f->coop_tile, ntiles * sizeof(uint32_t)));
         int dev = 0, sms = 0, per_sm = 0, coop = 0;
         GXF_CUDA(b, cudaGetDevice(&dev));
@@ -685,7 +696,7 @@ int batch_coop_step(gx_batch* b, int nsteps, uint64_t* launches) {
         if (per_sm < 1) return ferr(b, GX_ERR_UNSUPPORTED, "the cooperative batch kernel does not fit on an SM");
         f->coop_grid = sms * per_sm;
     }
-    GXF_CUDA(b, cudaMemsetAsync(f->coop_bar, 0, 2 * sizeof(unsigned), b->stream));
+    GXF_CUDA(b, cudaMemsetAsync(f->coop_bar, 0, 4 * sizeof(unsigned), b->stream));
     CoopArgs a;
     a.geo = f->geo;
     a.th = f->th;

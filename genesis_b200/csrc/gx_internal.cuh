@@ -48,6 +48,16 @@ __device__ __forceinline__ double rem_euclid(double a, double b) {
 __device__ __forceinline__ double min_image1(double d, double L) {
     return xsub(d, xmul(L, round(xdiv(d, L))));
 }
+// min_image1 without the division, for the separation d of two wrapped
+// positions (|d| < L): round(d / L) is then 0 or +-1, and the sign test
+// below gives the same value except for |d| within rounding of L/2; the
+// subtraction is min_image1's, so elsewhere the bits are the same.  Near
+// |d| = L/2 both images lie about L/2 from the atom, beyond the cutoff of
+// any grid with >= 3 cells per axis (cutoff <= cell <= L/3).
+__device__ __forceinline__ double min_image_near(double d, double L, double half_L) {
+    const double k = d > half_L ? 1.0 : (d < -half_L ? -1.0 : 0.0);
+    return xsub(d, xmul(L, k));
+}
 
 // Geometry of one SpatialGrid (src/physics/grid.rs:67-86).
 struct GridGeom {
@@ -318,7 +328,7 @@ void adjoint_free(gx_handle* h);
 // Neighbour-list path of the mixed pass (gx_nlist.cu).
 bool nl_eligible(gx_handle* h);
 int nl_prepare(gx_handle* h, bool* graphs_stale);
-int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nblocks, bool energy);
+int nl_tick(gx_handle* h, const double* lambda, double* kpart, double* spart, int* nblocks, bool energy);
 int nl_rebuilds(gx_handle* h, uint64_t* out);
 int nl_set_skin(gx_handle* h, double skin);
 int nl_tune_tpp(gx_handle* h, int reps);

@@ -1115,14 +1115,15 @@ __device__ __forceinline__ double block_sum_d(double v, double* sh) {
 }
 
 // a = F 2^-32 (1/m) (as k_fix_to_acc), v += a dt/2 (as k_kick), and with
-// THERMO the kinetic-energy partials of the new v with k_kinetic's block
-// mapping and operation order, so lambda is bit-identical to the unfused tick.
+// THERMO >= 1 the kinetic-energy partials of the new v with k_kinetic's block
+// mapping and operation order, so lambda is bit-identical to the unfused tick;
+// THERMO = 2 also the speed partials (sum of |v|) for the tick's record.
 // With vsum: also k_nl_fix_to_double's conversion of the potential (ticks
 // without a bond spring, which would write the bond-energy slot after it).
-template <bool THERMO>
+template <int THERMO>
 __global__ void __launch_bounds__(kRedThreads) k_nl_finish(StateBuf b, const long long* __restrict__ F,
                                                            size_t fstride, uint32_t n, double half_dt,
-                                                           double* __restrict__ kpart,
+                                                           double* __restrict__ kpart, double* __restrict__ spart,
                                                            const unsigned long long* __restrict__ vsum,
                                                            double* __restrict__ vout, double* __restrict__ bzero) {
     __shared__ double sh[kRedThreads / 32];
@@ -1130,7 +1131,7 @@ __global__ void __launch_bounds__(kRedThreads) k_nl_finish(StateBuf b, const lon
         *vout = xmul(__ll2double_rn((long long)*vsum), kFixInv);
         *bzero = 0.0;
     }
-    double ks = 0.0;
+    double ks = 0.0, ss = 0.0;
     for (uint32_t i = blockIdx.x * kRedThreads + threadIdx.x; i < n; i += gridDim.x * kRedThreads) {
         double im = b.inv_mass[i];
         double ax = xmul(xmul(__ll2double_rn(F[i]), kFixInv), im);
@@ -1148,11 +1149,16 @@ __global__ void __launch_bounds__(kRedThreads) k_nl_finish(StateBuf b, const lon
         if (THERMO) {
             double l2 = xadd(xadd(xmul(vx, vx), xmul(vy, vy)), xmul(vz, vz));
             ks = xadd(ks, xmul(xmul(0.5, b.mass[i]), l2));
+            if (THERMO == 2) ss = xadd(ss, xsqrt(l2));
         }
     }
     if (THERMO) {
         ks = block_sum_d<kRedThreads>(ks, sh);
         if (threadIdx.x == 0) kpart[blockIdx.x] = ks;
+    }
+    if (THERMO == 2) {
+        ss = block_sum_d<kRedThreads>(ss, sh);
+        if (threadIdx.x == 0) spart[blockIdx.x] = ss;
     }
 }
 
@@ -1183,10 +1189,12 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force64(GridGeom g, StateBuf 
         const int ti = b.elem[i];
         const double qi = b.charge[i], mi = b.mass[i], inv_mi = b.inv_mass[i];
         double ax = 0.0, ay = 0.0, az = 0.0;
+        // the list grid has >= 3 cells per axis (min_image_near)
+        const double hx = xmul(0.5, L.box[0]), hy = xmul(0.5, L.box[1]), hz = xmul(0.5, L.box[2]);
         auto visit = [&](uint32_t j) {
-            const double dx = min_image1(xsub(xi, b.x[j]), L.box[0]);
-            const double dy = min_image1(xsub(yi, b.y[j]), L.box[1]);
-            const double dz = min_image1(xsub(zi, b.z[j]), L.box[2]);
+            const double dx = min_image_near(xsub(xi, b.x[j]), L.box[0], hx);
+            const double dy = min_image_near(xsub(yi, b.y[j]), L.box[1], hy);
+            const double dz = min_image_near(xsub(zi, b.z[j]), L.box[2], hz);
             const double d2 = xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
             if (d2 >= L.rc2) return;
             const double d = xsqrt(d2);
@@ -1232,11 +1240,11 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force64(GridGeom g, StateBuf 
 
 // FP64 second kick (as k_kick) and, with THERMO, the kinetic-energy partials
 // with k_nl_finish's block mapping and operation order.
-template <bool THERMO>
+template <int THERMO>
 __global__ void __launch_bounds__(kRedThreads) k_nl_finish64(StateBuf b, uint32_t n, double half_dt,
-                                                             double* __restrict__ kpart) {
+                                                             double* __restrict__ kpart, double* __restrict__ spart) {
     __shared__ double sh[kRedThreads / 32];
-    double ks = 0.0;
+    double ks = 0.0, ss = 0.0;
     for (uint32_t i = blockIdx.x * kRedThreads + threadIdx.x; i < n; i += gridDim.x * kRedThreads) {
         const double vx = xadd(b.vx[i], xmul(b.ax[i], half_dt));
         const double vy = xadd(b.vy[i], xmul(b.ay[i], half_dt));
@@ -1247,11 +1255,16 @@ __global__ void __launch_bounds__(kRedThreads) k_nl_finish64(StateBuf b, uint32_
         if (THERMO) {
             double l2 = xadd(xadd(xmul(vx, vx), xmul(vy, vy)), xmul(vz, vz));
             ks = xadd(ks, xmul(xmul(0.5, b.mass[i]), l2));
+            if (THERMO == 2) ss = xadd(ss, xsqrt(l2));
         }
     }
     if (THERMO) {
         ks = block_sum_d<kRedThreads>(ks, sh);
         if (threadIdx.x == 0) kpart[blockIdx.x] = ks;
+    }
+    if (THERMO == 2) {
+        ss = block_sum_d<kRedThreads>(ss, sh);
+        if (threadIdx.x == 0) spart[blockIdx.x] = ss;
     }
 }
 
@@ -1355,8 +1368,9 @@ int nl_prepare(gx_handle* h, bool* stale) {
 }
 
 // One tick of the list path up to and including the second kick; with
-// `kpart` also the kinetic-energy partials (nb blocks) for the thermostat.
-int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nb_out, bool energy) {
+// `kpart` also the kinetic-energy partials (nb blocks) of the kicked v, and
+// with `spart` (which needs kpart) its speed partials.
+int nl_tick(gx_handle* h, const double* lambda, double* kpart, double* spart, int* nb_out, bool energy) {
     NlState* s = nl_of(h);
     const uint32_t n = (uint32_t)h->n;
     const GridGeom& g = s->lg;
@@ -1464,18 +1478,15 @@ int nl_tick(gx_handle* h, const double* lambda, double* kpart, int* nb_out, bool
     if (nb < 1) nb = 1;
     prof_begin(h, "nl_finish");
     const unsigned long long* vsum = spring ? nullptr : h->dcount + 1;
+    const int mode = kpart ? (spart ? 2 : 1) : 0;
     if (f64) {
-        if (kpart)
-            GX_LAUNCH(h, k_nl_finish64<true>, nb, kRedThreads, b, n, half_dt, kpart);
-        else
-            GX_LAUNCH(h, k_nl_finish64<false>, nb, kRedThreads, b, n, half_dt, nullptr);
+        auto k = mode == 2 ? k_nl_finish64<2> : (mode == 1 ? k_nl_finish64<1> : k_nl_finish64<0>);
+        GX_LAUNCH(h, k, nb, kRedThreads, b, n, half_dt, kpart, spart);
         if (!spring) GX_CUDA(h, cudaMemsetAsync(h->dscal + 3, 0, sizeof(double), h->stream));
-    } else if (kpart)
-        GX_LAUNCH(h, k_nl_finish<true>, nb, kRedThreads, b, h->F, h->cap, n, half_dt, kpart, vsum, h->dscal + 2,
-                  h->dscal + 3);
-    else
-        GX_LAUNCH(h, k_nl_finish<false>, nb, kRedThreads, b, h->F, h->cap, n, half_dt, nullptr, vsum, h->dscal + 2,
-                  h->dscal + 3);
+    } else {
+        auto k = mode == 2 ? k_nl_finish<2> : (mode == 1 ? k_nl_finish<1> : k_nl_finish<0>);
+        GX_LAUNCH(h, k, nb, kRedThreads, b, h->F, h->cap, n, half_dt, kpart, spart, vsum, h->dscal + 2, h->dscal + 3);
+    }
     prof_end(h, "nl_finish");
     if (nb_out) *nb_out = nb;
     return GX_OK;
