@@ -969,11 +969,22 @@ int gx_autotune(gx_handle* h, int reps, int* best, double* ms) {
                 h->nl_fresh = false;  // positions restored behind the list's back
                 return r;
             };
+            // each list variant with its own work shape (lanes and far-end
+            // block for 5 and 6, stash for 7, brick for 8) tuned on a list
+            // built for it; at small sizes the shape decides more than the
+            // variant does
             const int vs[5] = {pick, 5, 6, 7, 8};
             double tt[5] = {1e300, 1e300, 1e300, 1e300, 1e300};
+            int shape[5][4] = {};
             for (int q = 0; q < 5 && !rc; ++q) {
                 h->kernel_variant = vs[q];
-                rc = tick_ms(&tt[q]);
+                if (vs[q] >= 5) {
+                    invalidate_graphs(h);
+                    if (!(rc = gx_step(h, 1, nullptr, 0))) rc = nl_tune_tpp(h, reps);
+                    if (!rc) nl_shape(h, &shape[q][0], &shape[q][1], &shape[q][2], &shape[q][3]);
+                }
+                int r2 = tick_ms(&tt[q]);  // restores the snapshot, the tuning tick's too
+                if (!rc) rc = r2;
             }
             if (ms) {
                 ms[0] = tt[0] < 1e300 ? tt[0] : -1.0;
@@ -982,14 +993,18 @@ int gx_autotune(gx_handle* h, int reps, int* best, double* ms) {
                 ms[7] = tt[3] < 1e300 ? tt[3] : -1.0;
                 ms[8] = tt[4] < 1e300 ? tt[4] : -1.0;
             }
+            int qpick = 0;
             if (!rc) {
-                int q = 0;
                 for (int k = 1; k < 5; ++k)
-                    if (tt[k] < tt[q]) q = k;
-                pick = vs[q];
+                    if (tt[k] < tt[qpick]) qpick = k;
+                pick = vs[qpick];
             }
             if (!rc && pick >= 5) {
                 h->kernel_variant = pick;
+                nl_set_tpp(h, shape[qpick][0]);
+                nl_set_block(h, shape[qpick][1]);
+                nl_set_slots(h, shape[qpick][2]);
+                nl_set_brick(h, shape[qpick][3]);
                 // the skin: 0.05, 0.1, 0.15 and 0.2 r_c (cell size r_c + skin)
                 // over whole ticks, rebuilds included
                 double skin0 = 0.0;

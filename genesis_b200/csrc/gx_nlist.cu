@@ -34,6 +34,7 @@
 //   k_nl_finish    a = F 2^-32 / m, second kick, kinetic-energy partials
 // An atom whose list overflowed scans its 27 home-grid cells directly, so
 // the pair set stays exact whatever the local density.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -1509,7 +1510,8 @@ int nl_rebuilds(gx_handle* h, uint64_t* out) {
 }
 
 // Times the list pass at 1, 2, 4 and 8 threads per atom on the current list
-// (`reps` launches each) and keeps the fastest.  The state is not touched:
+// (the best of three rounds of at least `reps` launches each) and keeps the
+// fastest.  The state is not touched:
 // the pass only writes the force scratch, which the next tick overwrites.
 int nl_tune_tpp(gx_handle* h, int reps) {
     int rs = settle_step_errors(h);  // the error word is cleared after the timing below
@@ -1531,6 +1533,7 @@ int nl_tune_tpp(gx_handle* h, int reps) {
     double best = 1e300;
     const int tpp0 = s->tpp, block0 = s->block;
     int pick = 0;
+    int launches = reps;
     for (int k = 0; k < ncand; ++k) {
         int tpp = s->tpp;
         if (stash) s->slots = k == 0 ? 8 : 16;
@@ -1541,21 +1544,32 @@ int nl_tune_tpp(gx_handle* h, int reps) {
         } else {
             tpp = lanes[k + 2].tpp;
         }
-        int rc = gx_timer_mark(h, 14);
-        for (int r = 0; r < reps && !rc; ++r) {
-            if (s->half == 1) launch_nl_force<true>(h, tpp, s->lg, s, n, L, false);
-            else launch_nl_force<false>(h, tpp, s->lg, s, n, L, false);
+        // the best of three rounds of `launches` passes; a short pass (a
+        // small system) gets enough launches for ~1 ms per round, so that
+        // the event resolution and launch jitter do not decide the pick
+        double t_min = 1e300;
+        int rc = 0;
+        for (int round = 0; round < 3 && !rc; ++round) {
+            rc = gx_timer_mark(h, 14);
+            for (int r = 0; r < launches && !rc; ++r) {
+                if (s->half == 1) launch_nl_force<true>(h, tpp, s->lg, s, n, L, false);
+                else launch_nl_force<false>(h, tpp, s->lg, s, n, L, false);
+            }
+            double t = 0.0;
+            if (!rc) rc = gx_timer_mark(h, 15);
+            if (!rc) rc = gx_timer_elapsed(h, 14, 15, &t);
+            if (!rc && launches == reps && k == 0 && round == 0 && t < 1.0)
+                launches = (int)std::min(200.0, std::ceil(reps * 1.0 / std::max(t, 1e-3)));
+            else if (!rc)
+                t_min = std::min(t_min, t / launches);
         }
-        double t = 0.0;
-        if (!rc) rc = gx_timer_mark(h, 15);
-        if (!rc) rc = gx_timer_elapsed(h, 14, 15, &t);
         if (rc) {
             s->tpp = tpp0;
             s->block = block0;
             return rc;
         }
-        if (t / reps < best) {
-            best = t / reps;
+        if (t_min < best) {
+            best = t_min;
             pick = k;
         }
     }

@@ -131,7 +131,9 @@ int gx_set_kernel_variant(gx_handle* h, int variant);
 /* Autotuner: times `reps` mixed pair passes of variants 1-4 on the resident
  * state (left bit-identical: they give the same fixed-point sums) and, where
  * variants 5-8 apply, full ticks of the best of them against full ticks
- * of 5-8, each from a snapshot of (x, v, a) restored afterwards.
+ * of 5-8, each list variant with its own work shape (lanes per atom and
+ * far-end block, stash size, brick length) tuned first on a list built for
+ * it, each from a snapshot of (x, v, a) restored afterwards.
  * Selects the fastest and returns it in *best.  ms[1..4], when given,
  * receive the per-pass milliseconds, ms[0], ms[5..8] the per-tick
  * milliseconds of the best pass variant and of 5-8 (-1 = not run); ms has
