@@ -422,9 +422,17 @@ int upload_pair_table_f64(gx_handle* h) {
     double* psig = d_psig(h);
     GX_CUDA(h, cudaMemcpy(psig, h->fs.pair_sigma, sizeof(h->fs.pair_sigma), cudaMemcpyHostToDevice));
     GX_CUDA(h, cudaMemcpy(psig + kNElem * kNElem, h->fs.pair_eps, sizeof(h->fs.pair_eps), cudaMemcpyHostToDevice));
+    // third table: (24 eps) / sigma per element pair, the two IEEE operations
+    // of the law (lj_raw, src/physics/forces.rs:346-353) done once on the host
+    double e24s[kNElem * kNElem];
+    for (int k = 0; k < kNElem * kNElem; ++k) {
+        volatile double t = 24.0 * h->fs.pair_eps[k];  // rounded before the division
+        e24s[k] = t / h->fs.pair_sigma[k];
+    }
+    GX_CUDA(h, cudaMemcpy(psig + 2 * kNElem * kNElem, e24s, sizeof e24s, cudaMemcpyHostToDevice));
     return GX_OK;
 }
 
-size_t red_doubles(size_t cap) { return 6 * (cap / 64) + 6 * kRedCap + 2 * kNElem * kNElem + 64; }
+size_t red_doubles(size_t cap) { return 6 * (cap / 64) + 6 * kRedCap + 3 * kNElem * kNElem + 64; }
 
 }  // namespace gx

@@ -32,8 +32,11 @@ __device__ __forceinline__ void smooth_f64(double r, double ron, double rc, doub
 }
 
 // One pair's LJ + Coulomb + gravity scalar (systems/forces.rs:270-299), exact.
-__device__ __forceinline__ void pair_f64(const LawF64& L, double d, double sg, double ep, double qa, double qb,
-                                         double ma, double mb, double& fmag, double& V) {
+// e24s = (24 ep) / sg, which depends on the element pair only: a caller may
+// pass it from a table computed with the same two IEEE operations (the same
+// bits) instead of dividing per pair.
+__device__ __forceinline__ void pair_f64_e24(const LawF64& L, double d, double sg, double ep, double e24s, double qa,
+                                             double qb, double ma, double mb, double& fmag, double& V) {
     fmag = 0.0;
     double sw, dsw;
     if (d < L.lj_rc) {  // force_switched_scalar, forces.rs:270-275; lj_raw :346-353
@@ -42,7 +45,7 @@ __device__ __forceinline__ void pair_f64(const LawF64& L, double d, double sg, d
         double s6 = xmul(xmul(xmul(xmul(xmul(s, s), s), s), s), s);
         double s12 = xmul(s6, s6);
         double v = xmul(xmul(4.0, ep), xsub(s12, s6));
-        double m = xmul(xmul(xdiv(xmul(24.0, ep), sg), s), xsub(xmul(2.0, s12), s6));
+        double m = xmul(xmul(e24s, s), xsub(xmul(2.0, s12), s6));
         smooth_f64(r, L.lj_ron, L.lj_rc, sw, dsw);
         fmag = xadd(fmag, xsub(xmul(m, sw), xmul(v, dsw)));
         V = xadd(V, xmul(v, sw));
@@ -65,6 +68,11 @@ __device__ __forceinline__ void pair_f64(const LawF64& L, double d, double sg, d
         fmag = xadd(fmag, xsub(xmul(m, sw), xmul(v, dsw)));
         V = xadd(V, xmul(v, sw));
     }
+}
+
+__device__ __forceinline__ void pair_f64(const LawF64& L, double d, double sg, double ep, double qa, double qb,
+                                         double ma, double mb, double& fmag, double& V) {
+    pair_f64_e24(L, d, sg, ep, xdiv(xmul(24.0, ep), sg), qa, qb, ma, mb, fmag, V);
 }
 
 inline LawF64 make_law64(const gx_handle* h) {

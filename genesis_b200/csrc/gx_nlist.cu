@@ -1202,7 +1202,9 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force64(GridGeom g, StateBuf 
             if (d <= kEpsF64) return;
             const int tj = b.elem[j];
             double fmag, Vij = 0.0;
-            pair_f64(L, d, psig[ti * kNElem + tj], peps[ti * kNElem + tj], qi, b.charge[j], mi, b.mass[j], fmag, Vij);
+            const int tt = ti * kNElem + tj;  // psig, then peps, then (24 eps) / sigma, each kNElem^2
+            pair_f64_e24(L, d, psig[tt], peps[tt], peps[kNElem * kNElem + tt], qi, b.charge[j], mi, b.mass[j], fmag,
+                         Vij);
             if (j > i) {
                 V = xadd(V, Vij);
                 ++np;
