@@ -67,7 +67,7 @@ EXPORTS = (
     "gx_radial_distribution_noalloc", "gx_set_kernel_variant", "gx_autotune",
     "gx_batch_create", "gx_batch_destroy", "gx_batch_last_error", "gx_batch_set_state",
     "gx_batch_step", "gx_batch_get_state", "gx_adjoint_forward", "gx_adjoint_backward",
-    "gx_set_list_skin", "gx_list_rebuilds", "gx_list_stats", "gx_batch_set_mode", "gx_batch_get_mode", "gx_batch_autotune",
+    "gx_set_list_skin", "gx_list_rebuilds", "gx_list_stats", "gx_batch_set_mode", "gx_batch_get_mode", "gx_batch_autotune", "gx_batch_set_list_skin", "gx_batch_list_rebuilds",
     "gx_get_list_config", "gx_set_list_threads", "gx_set_list_stash", "gx_set_list_brick", "gx_set_list_block", "gx_get_list_shape", "gx_bond_observe", "gx_bond_tracker_reset", "gx_get_bonds",
     "gx_bond_components", "gx_collisions", "gx_collision_count", "gx_xyz_frame", "gx_snapshot_world",
     "gx_set_step_async",
@@ -654,7 +654,8 @@ class Batch:
 
     def set_mode(self, mode: int):
         """1 = persistent launch (one CTA per replica), 2 = all-replica graph,
-        3 = the all-replica phases in one persistent cooperative launch."""
+        3 = the all-replica phases in one persistent cooperative launch,
+        4 = the all-replica graph over persistent neighbour lists."""
         self._check(self.lib.gx_batch_set_mode(self.b, mode))
 
     @property
@@ -663,10 +664,20 @@ class Batch:
         self._check(self.lib.gx_batch_get_mode(self.b, C.byref(m)))
         return m.value
 
+    def set_list_skin(self, skin: float):
+        """Skin of mode 4's neighbour lists (default 0.1 r_c)."""
+        self._check(self.lib.gx_batch_set_list_skin(self.b, skin))
+
+    def list_rebuilds(self) -> int:
+        """Mode 4's list rebuilds so far."""
+        v = C.c_uint64()
+        self._check(self.lib.gx_batch_list_rebuilds(self.b, C.byref(v)))
+        return v.value
+
     def autotune(self, ticks: int = 10):
-        """Times the three modes from a snapshot, keeps the fastest: (mode, {mode: ms per tick})."""
+        """Times the four modes from a snapshot, keeps the fastest: (mode, {mode: ms per tick})."""
         m = C.c_int()
-        ms = np.zeros(3)
+        ms = np.zeros(4)
         self._check(self.lib.gx_batch_autotune(self.b, ticks, C.byref(m), _ptr(ms, C.c_double)))
         return m.value, {k + 1: float(t) for k, t in enumerate(ms) if t >= 0}
 
@@ -697,6 +708,8 @@ def _declare_batch(lib):
         "gx_batch_set_mode": (C.c_int, [vp, C.c_int]),
         "gx_batch_get_mode": (C.c_int, [vp, C.POINTER(C.c_int)]),
         "gx_batch_autotune": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), dp]),
+        "gx_batch_set_list_skin": (C.c_int, [vp, C.c_double]),
+        "gx_batch_list_rebuilds": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
     }
     for name, (res, args) in proto.items():
         f = getattr(lib, name)

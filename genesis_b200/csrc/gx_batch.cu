@@ -338,6 +338,7 @@ int gx_batch_create(const gx_params* p, int nrep, const double* box, const doubl
     double lj_rc = std::fmax(p->lj_cutoff_factor, 1.0) * max_pair;
     double coul_rc = p->enable_electrostatics ? std::fmax(p->coulomb_cutoff, 1.0) * max_sigma : 0.0;
     double rc = std::fmax(lj_rc, coul_rc);
+    b->rc = rc;
     LawF32& L = b->L;
     L.rc2 = (float)(rc * rc);
     L.lj_rc = (float)lj_rc;
@@ -379,6 +380,8 @@ int gx_batch_create(const gx_params* p, int nrep, const double* box, const doubl
 void gx_batch_destroy(gx_batch* b) {
     if (!b) return;
     if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_nl_free(b->nl);
+    b->nl = nullptr;
     batch_flat_free(b->flat);
     b->flat = nullptr;
     free_arrays(b);
@@ -490,6 +493,9 @@ int gx_batch_set_state(gx_batch* b, const uint32_t* natoms, const double* pos, c
     std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return b->reps[a].n > b->reps[c].n; });
     GXB_CUDA(b, cudaMemcpy(b->d_order, order.data(), b->nrep * sizeof(int), cudaMemcpyHostToDevice));
     b->has_state = true;
+    ++b->version;
+    batch_nl_free(b->nl);  // sized for the old atom counts
+    b->nl = nullptr;
     return GX_OK;
 }
 
@@ -516,10 +522,14 @@ int gx_batch_step(gx_batch* b, int nsteps, double* stats, double* device_ms) {
     } else if (b->mode == 3) {
         int rc = batch_coop_step(b, nsteps, nullptr);
         if (rc) return rc;
+    } else if (b->mode == 4) {
+        int rc = batch_nl_step(b, nsteps, nullptr);
+        if (rc) return rc;
     } else {
         int rc = batch_flat_step(b, nsteps, nullptr);
         if (rc) return rc;
     }
+    if (b->mode != 4) ++b->version;  // a mode-4 list no longer matches the state
     GXB_CUDA(b, cudaEventRecord(b->ev[1], b->stream));
     uint32_t e = 0;
     GXB_CUDA(b, cudaMemcpyAsync(&e, b->d_err, sizeof e, cudaMemcpyDeviceToHost, b->stream));
@@ -541,9 +551,20 @@ int gx_batch_step(gx_batch* b, int nsteps, double* stats, double* device_ms) {
 }
 
 int gx_batch_set_mode(gx_batch* b, int mode) {
-    if (!b || mode < 0 || mode > 3) return GX_ERR_ARG;
+    if (!b || mode < 0 || mode > 4) return GX_ERR_ARG;
     b->mode = mode == 0 ? 2 : mode;
     return GX_OK;
+}
+
+int gx_batch_set_list_skin(gx_batch* b, double skin) {
+    if (!b || !(skin >= 0.0) || !std::isfinite(skin)) return GX_ERR_ARG;
+    b->nl_skin = skin;  // the next mode-4 step rebuilds its lists on the new grid
+    return GX_OK;
+}
+
+int gx_batch_list_rebuilds(gx_batch* b, uint64_t* rebuilds) {
+    if (!b || !rebuilds) return GX_ERR_ARG;
+    return batch_nl_rebuilds(b, rebuilds);
 }
 
 int gx_batch_get_mode(gx_batch* b, int* mode) {
@@ -561,26 +582,28 @@ int gx_batch_autotune(gx_batch* b, int ticks, int* mode, double* ms) {
     // x y z vx vy vz ax ay az are the first nine columns of one allocation
     GXB_CUDA(b, cudaMemcpyAsync(snap, b->A.x, n9 * sizeof(double), cudaMemcpyDeviceToDevice, b->stream));
     const int saved = b->mode;
-    double t[3] = {-1.0, -1.0, -1.0};
+    double t[4] = {-1.0, -1.0, -1.0, -1.0};
     int rc = GX_OK;
     bool fits1 = true;  // mode 1 keeps each replica's cells in shared memory
     for (const RepDesc& d : b->reps) fits1 = fits1 && d.g.ncell <= kBMaxCells;
-    for (int m = 1; m <= 3 && !rc; ++m) {
+    for (int m = 1; m <= 4 && !rc; ++m) {
         if (m == 1 && !fits1) continue;
+        if (m == 4 && !batch_nl_eligible(b)) continue;
         b->mode = m;
         double w = 0.0;
         if (!(rc = gx_batch_step(b, 1, nullptr, &w)) && !(rc = gx_batch_step(b, ticks, nullptr, &w))) t[m - 1] = w;
         cudaMemcpyAsync(b->A.x, snap, n9 * sizeof(double), cudaMemcpyDeviceToDevice, b->stream);
+        ++b->version;
     }
     cudaStreamSynchronize(b->stream);
     cudaFree(snap);
     int pick = 2;
-    for (int m = 1; m <= 3; ++m)
+    for (int m = 1; m <= 4; ++m)
         if (t[m - 1] >= 0.0 && t[m - 1] < t[pick - 1]) pick = m;
     b->mode = rc ? saved : pick;
     if (mode) *mode = b->mode;
     if (ms)
-        for (int m = 0; m < 3; ++m) ms[m] = t[m] >= 0.0 ? t[m] / ticks : -1.0;
+        for (int m = 0; m < 4; ++m) ms[m] = t[m] >= 0.0 ? t[m] / ticks : -1.0;
     return rc;
 }
 

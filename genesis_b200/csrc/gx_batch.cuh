@@ -39,6 +39,9 @@ LawF32 make_law32(const gx_handle* h);
 
 struct BatchFlat;  // gx_batch_flat.cu
 void batch_flat_free(BatchFlat* f);
+struct BatchNl;  // gx_batch_nl.cu
+void batch_nl_free(BatchNl* n);
+struct RepThermo;  // gx_batch_flat.cu
 
 }  // namespace gx
 
@@ -60,11 +63,31 @@ struct gx_batch {
     double pair_sigma[gx::kNElem * gx::kNElem], pair_eps[gx::kNElem * gx::kNElem];
     bool has_state = false;
     int mode = 2;                  // 1 persistent launch (a CTA per replica), 2 all-replica graph,
-                                   // 3 persistent cooperative launch of the all-replica phases
-    gx::BatchFlat* flat = nullptr;  // state of mode 2
+                                   // 3 persistent cooperative launch of the all-replica phases,
+                                   // 4 all-replica graph over persistent neighbour lists
+    gx::BatchFlat* flat = nullptr;  // state of modes 2-4
+    gx::BatchNl* nl = nullptr;      // lists of mode 4
+    double rc = 0.0;                // pair cutoff
+    double nl_skin = -1.0;          // mode 4 list skin (< 0: 0.1 rc)
+    uint64_t version = 0;           // bumped whenever the state changes other than by a mode-4 step
 };
 
 namespace gx {
 int batch_flat_step(gx_batch* b, int nsteps, uint64_t* launches);
 int batch_coop_step(gx_batch* b, int nsteps, uint64_t* launches);
+int batch_nl_step(gx_batch* b, int nsteps, uint64_t* launches);
+bool batch_nl_eligible(const gx_batch* b);  // every replica: >= 3 list cells per axis, >= 128 atoms
+int batch_nl_rebuilds(gx_batch* b, uint64_t* out);
+// shared with mode 4 (gx_batch_flat.cu): prepares the all-replica tables and
+// returns them; launches of the finishing kick and the thermostat over a
+// given slot-to-atom permutation
+struct FlatShared {
+    const uint32_t* rep_of;
+    const RepThermo* th;
+    double* lam;
+    unsigned long long* acc;
+};
+int flat_shared(gx_batch* b, FlatShared* out);
+void flat_finish_thermo(gx_batch* b, gx_handle* h, const uint32_t* perm);
+void flat_commit(gx_batch* b, gx_handle* h);
 }

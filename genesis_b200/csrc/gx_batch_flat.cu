@@ -675,6 +675,27 @@ int flat_tick(gx_batch* b, BatchParams P, bool energy) {
 
 }  // namespace
 
+int flat_shared(gx_batch* b, FlatShared* out) {
+    int rc = flat_prepare(b);
+    if (rc) return rc;
+    out->rep_of = b->flat->rep_of;
+    out->th = b->flat->th;
+    out->lam = b->flat->lam;
+    out->acc = b->flat->acc;
+    return GX_OK;
+}
+
+void flat_finish_thermo(gx_batch* b, gx_handle* h, const uint32_t* perm) {
+    BatchFlat* f = b->flat;
+    const uint32_t n = (uint32_t)b->total;
+    GX_LAUNCH(h, k_fb_finish, nblk(n, 256), 256, b->A, perm, n, 0.5 * b->p.dt, b->A.total);
+    GX_LAUNCH(h, k_fb_thermo, b->nrep, kFbRed, f->th, b->A, f->lam, f->acc, b->p.thermal_constant, b->d_out);
+}
+
+void flat_commit(gx_batch* b, gx_handle* h) {
+    GX_LAUNCH(h, k_fb_commit, b->nrep, kFbRed, b->flat->th, b->A, b->flat->lam, b->d_out);
+}
+
 // Mode 3: nsteps ticks of every replica in one cooperative launch.
 int batch_coop_step(gx_batch* b, int nsteps, uint64_t* launches) {
     int rc = flat_prepare(b);

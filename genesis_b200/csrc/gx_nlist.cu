@@ -290,36 +290,6 @@ __device__ __forceinline__ unsigned long long block_sum_u(unsigned long long v, 
     return v;
 }
 
-struct PairAcc {
-    long long fx = 0, fy = 0, fz = 0, vq = 0;
-    unsigned long long np = 0;
-};
-
-// far != null: also subtract the pair force from the far end q (HALF lists).
-__device__ __forceinline__ void nl_pair(const LawF32& L, const PairF* st, int ki, float4 pi, float4 pj, float sx,
-                                        float sy, float sz, bool once, PairAcc& a, uint32_t* err,
-                                        long long* far = nullptr, uint32_t q = 0, size_t fstride = 0) {
-    float dx = delta1(pi.x, pj.x, sx), dy = delta1(pi.y, pj.y, sy), dz = delta1(pi.z, pj.z, sz);
-    float d2 = dist2(dx, dy, dz);
-    if (!(d2 < L.rc2) || d2 == 0.f) return;
-    float fs, v;
-    pair_f32(L, st[ki * L.nkinds + __float_as_int(pj.w)], d2, fs, v);
-    long long qx, qy, qz;
-    quant3(fmul(dx, fs), fmul(dy, fs), fmul(dz, fs), qx, qy, qz, err);
-    a.fx += qx;
-    a.fy += qy;
-    a.fz += qz;
-    if (far) {
-        atomicAdd((unsigned long long*)&far[q], (unsigned long long)(-qx));
-        atomicAdd((unsigned long long*)&far[fstride + q], (unsigned long long)(-qy));
-        atomicAdd((unsigned long long*)&far[2 * fstride + q], (unsigned long long)(-qz));
-    }
-    if (once) {
-        a.vq += quant(v, err);
-        ++a.np;
-    }
-}
-
 // The half-list pass with one lane per atom and the far end's force kept in
 // the block where it can be.  Atoms are sorted by cell, so a block of BS
 // consecutive atoms covers whole runs of cells along x, and for about half

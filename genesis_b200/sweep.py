@@ -24,7 +24,8 @@ def run_batched(wls, steps: int, device: int = 0, mode: int = 2):
     """Returns (replica-steps/s from the step call's CUDA-event time, stats,
     ms).  mode 1: one persistent launch, one CTA per replica; mode 2: every
     phase as one kernel over all replicas, CUDA-graph replay; mode 3: mode
-    2's phases in one persistent cooperative launch."""
+    2's phases in one persistent cooperative launch; mode 4: mode 2 over
+    persistent neighbour lists."""
     base = wls[0].config()
     b = Batch(base, [wl.config().size for wl in wls], [wl.thermostat_temperature for wl in wls], device)
     b.set_mode(mode)

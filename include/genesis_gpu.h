@@ -373,8 +373,9 @@ int gx_set_dynamic(gx_handle* h, const double* pos, const double* vel, const dou
  * nrep independent universes of uneven sizes that share the laws in `base`
  * (mixed precision) and advances all of them together: as one captured
  * graph of all-replica kernels, in one persistent launch with one CTA per
- * replica, or in one persistent cooperative launch that runs the
- * all-replica phases for every tick (gx_batch_set_mode).  box: 3 doubles per replica; target_T: Berendsen target
+ * replica, in one persistent cooperative launch that runs the
+ * all-replica phases for every tick, or as the captured all-replica graph
+ * over persistent neighbour lists (gx_batch_set_mode).  box: 3 doubles per replica; target_T: Berendsen target
  * per replica (<= 0 or base->enable_thermostat == 0: NVE); NULL uses
  * base->thermostat_temperature.  Each replica's force grid must have >= 1
  * and <= 4096 cells. */
@@ -401,17 +402,28 @@ int gx_batch_get_state(gx_batch* b, double* pos, double* vel, double* acc);
  * replicas (a global cell index, per-replica geometry), captured once as a
  * CUDA graph; 3 = the phases of mode 2 inside one persistent cooperative
  * launch for all the ticks of a step call, separated by grid barriers
- * whose waits are bounded (GX_ERR_TIMEOUT if one gives up); 0 = the default
- * (2).  All give each NVE replica the same bits as a gx_handle on pair-pass
- * variants 1-4, and modes 2 and 3 give each other the same bits with the
- * thermostat on. */
+ * whose waits are bounded (GX_ERR_TIMEOUT if one gives up); 4 = the
+ * all-replica graph of mode 2 over persistent half neighbour lists (a list
+ * grid of cells >= r_c + skin per replica, a rebuild only after some atom
+ * moved more than skin/2, as the single-universe variant 6; every replica
+ * must hold >= 128 atoms and >= 3 list-grid cells per axis, else the step
+ * returns GX_ERR_UNSUPPORTED); 0 = the default (2).  Modes 1-3 give each
+ * NVE replica the same bits as a gx_handle on pair-pass variants 1-4, and
+ * modes 2 and 3 give each other the same bits with the thermostat on; mode
+ * 4 evaluates the same pairs in the list grid's cell-local frame, so its
+ * forces differ from mode 2's in the last FP32 bits (same error bound). */
 int gx_batch_set_mode(gx_batch* b, int mode);
 int gx_batch_get_mode(gx_batch* b, int* mode);
 /* Times `ticks` ticks in each mode from a snapshot of the state (restored
- * afterwards), keeps the fastest; ms[0], ms[1], ms[2] (may be NULL) receive
- * the per-tick device milliseconds of modes 1, 2 and 3 (-1: mode 1 skipped
- * because a replica grid exceeds its limit). */
+ * afterwards), keeps the fastest; ms[0..3] (may be NULL) receive the
+ * per-tick device milliseconds of modes 1-4 (-1: mode skipped, 1 because a
+ * replica grid exceeds its limit, 4 because a replica is too small). */
 int gx_batch_autotune(gx_batch* b, int ticks, int* mode, double* ms);
+/* Mode 4's list skin (default 0.1 r_c; the list grid's cells are >= r_c +
+ * skin).  No counterpart in the reference. */
+int gx_batch_set_list_skin(gx_batch* b, double skin);
+/* Mode 4's list rebuilds so far (synchronises the batch's stream). */
+int gx_batch_list_rebuilds(gx_batch* b, uint64_t* rebuilds);
 
 /* ---- adjoint: derivatives of short NVE horizons ----------------------- */
 

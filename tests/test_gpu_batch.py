@@ -19,11 +19,11 @@ def _replicas(thermo: bool):
     return wls
 
 
-def _single(wl, steps):
+def _single(wl, steps, variant=1):
     from genesis_b200._lib import Handle
     cfg = wl.config()
     h = Handle(cfg, "mixed")
-    h.set_kernel_variant(1)  # the batch re-sorts every tick, like variants 1-4
+    h.set_kernel_variant(variant)  # modes 1-3 re-sort every tick, like variants 1-4; mode 4 keeps lists, like 6
     u = wl.generate()
     h.set_universe(u)
     st = h.step(steps)
@@ -100,7 +100,7 @@ def test_batch_modes_agree_and_autotune_restores_state(gpu):
     b.set_universes([wl.generate() for wl in wls])
     before = b.get_state()
     mode, ms = b.autotune(ticks=3)
-    assert mode in (1, 2, 3) and ms[1] > 0 and ms[2] > 0 and ms[3] > 0
+    assert mode in (1, 2, 3, 4) and ms[1] > 0 and ms[2] > 0 and ms[3] > 0 and ms[4] > 0
     after = b.get_state()
     for x, y in zip(before, after):
         for p, q in zip(x, y):
@@ -128,3 +128,98 @@ def test_cooperative_launch_matches_the_graph_bit_for_bit(gpu):
             assert np.array_equal(p, q)
     for a, c in zip(runs[0][1], runs[1][1]):
         assert np.array_equal(a, c)
+
+
+# ---------------------------------------------------------------- mode 4: neighbour lists
+
+
+def test_list_mode_single_replica_matches_list_handle_bit_for_bit(gpu):
+    # one replica rebuilds on the handle's own schedule, in the same frames,
+    # with the same per-pair operations and integer sums
+    wl = W.replica_workload(W.Replica(n_side=12, temperature=150.0, seed=5))
+    wl.thermostat = False
+    out, st, _ = _batch([wl], 25, mode=4)
+    ref, rst = _single(wl, 25, variant=6)
+    for x, y in zip(out[0], ref):
+        assert np.array_equal(x, y)
+    assert st[0, 3] == rst["pairs"][-1]
+    assert st[0, 1] == rst["potential"][-1]
+
+
+def test_list_mode_follows_the_graph_mode_and_rebuilds(gpu):
+    from genesis_b200._lib import Batch
+    wls = _replicas(thermo=True)
+    runs = []
+    for mode in (2, 4):
+        base = wls[0].config()
+        base.enable_thermostat = True
+        b = Batch(base, [wl.config().size for wl in wls], [wl.thermostat_temperature for wl in wls])
+        b.set_mode(mode)
+        b.set_universes([wl.generate() for wl in wls])
+        sts = [b.step(k)[0] for k in (1, 9, 30)]
+        runs.append((b.get_state(), sts, b.list_rebuilds() if mode == 4 else None))
+        b.close()
+    assert runs[1][2] >= 2  # the first tick and at least one displacement-triggered rebuild
+    # the two frames differ in the last FP32 bits of each pair's displacement:
+    # forces by ~3e-6 relative (the mixed path's error against FP64 is of the
+    # same size), positions far less over 40 ticks
+    for x, y in zip(runs[0][0], runs[1][0]):
+        for p, q, tol in zip(x, y, (1e-7, 1e-5, 1e-5)):
+            assert np.linalg.norm(p - q) <= tol * max(np.linalg.norm(q), 1e-300)
+    for a, c in zip(runs[0][1], runs[1][1]):
+        assert np.allclose(a[:, 0], c[:, 0], rtol=1e-6, atol=0)  # K
+        assert np.allclose(a[:, 1], c[:, 1], rtol=1e-5, atol=0)  # V
+        assert np.all(np.abs(a[:, 3] - c[:, 3]) <= 2)            # pairs
+
+
+def test_list_mode_forces_match_the_oracle(gpu, orc):
+    from genesis_b200._lib import Batch
+    wls = _replicas(thermo=True)
+    base = wls[0].config()
+    base.enable_thermostat = True
+    b = Batch(base, [wl.config().size for wl in wls], [wl.thermostat_temperature for wl in wls])
+    b.set_mode(4)
+    us = [wl.generate() for wl in wls]
+    b.set_universes(us)
+    b.step(12)
+    out = b.get_state()
+    b.close()
+    for (pos, _, acc), wl, u in zip(out, wls, us):
+        acc_ref, _, _, _ = orc.forces(wl.config(), pos, u.elem, u.charge, u.mass)
+        assert np.linalg.norm(acc - acc_ref) <= 1e-5 * np.linalg.norm(acc_ref)
+
+
+def test_list_mode_rebuilds_after_a_new_state_and_is_deterministic(gpu):
+    from genesis_b200._lib import Batch
+    wls = _replicas(thermo=True)
+    base = wls[0].config()
+    base.enable_thermostat = True
+    b = Batch(base, [wl.config().size for wl in wls], [wl.thermostat_temperature for wl in wls])
+    b.set_mode(4)
+    first = None
+    for _ in range(2):  # the same state uploaded again: the lists restart from it
+        b.set_universes([wl.generate() for wl in wls])
+        r0 = b.list_rebuilds()
+        b.step(6)
+        assert b.list_rebuilds() > r0
+        got = b.get_state()
+        if first is None:
+            first = got
+    for x, y in zip(first, got):
+        for p, q in zip(x, y):
+            assert np.array_equal(p, q)
+    mode, ms = b.autotune(ticks=3)
+    assert mode in (1, 2, 3, 4) and ms[4] > 0
+    b.close()
+
+
+def test_list_mode_rejects_small_replicas(gpu):
+    from genesis_b200._lib import Batch, GxError
+    wl = W.replica_workload(W.Replica(n_side=4, temperature=40.0, seed=3))  # 64 atoms
+    base = wl.config()
+    b = Batch(base, [wl.config().size], [40.0])
+    b.set_universes([wl.generate()])
+    b.set_mode(4)
+    with pytest.raises(GxError):
+        b.step(1)
+    b.close()
