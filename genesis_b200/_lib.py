@@ -665,7 +665,7 @@ class Batch:
         return m.value
 
     def set_list_skin(self, skin: float):
-        """Skin of mode 4's neighbour lists (default 0.1 r_c)."""
+        """Skin of mode 4's neighbour lists (default 0.15 r_c)."""
         self._check(self.lib.gx_batch_set_list_skin(self.b, skin))
 
     def list_rebuilds(self) -> int:

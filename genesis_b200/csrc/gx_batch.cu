@@ -586,14 +586,25 @@ int gx_batch_autotune(gx_batch* b, int ticks, int* mode, double* ms) {
     int rc = GX_OK;
     bool fits1 = true;  // mode 1 keeps each replica's cells in shared memory
     for (const RepDesc& d : b->reps) fits1 = fits1 && d.g.ncell <= kBMaxCells;
+    const double skin0 = b->nl_skin;
+    double best_skin = skin0;
     for (int m = 1; m <= 4 && !rc; ++m) {
         if (m == 1 && !fits1) continue;
         if (m == 4 && !batch_nl_eligible(b)) continue;
         b->mode = m;
-        double w = 0.0;
-        if (!(rc = gx_batch_step(b, 1, nullptr, &w)) && !(rc = gx_batch_step(b, ticks, nullptr, &w))) t[m - 1] = w;
-        cudaMemcpyAsync(b->A.x, snap, n9 * sizeof(double), cudaMemcpyDeviceToDevice, b->stream);
-        ++b->version;
+        // mode 4 also over its list skin: 0.1, 0.15 and 0.2 r_c
+        const double fr[3] = {0.1, 0.15, 0.2};
+        for (int k = 0; k < (m == 4 ? 3 : 1) && !rc; ++k) {
+            if (m == 4) b->nl_skin = fr[k] * b->rc;
+            double w = 0.0;
+            if (!(rc = gx_batch_step(b, 1, nullptr, &w)) && !(rc = gx_batch_step(b, ticks, nullptr, &w)) &&
+                (t[m - 1] < 0.0 || w < t[m - 1])) {
+                t[m - 1] = w;
+                if (m == 4) best_skin = b->nl_skin;
+            }
+            cudaMemcpyAsync(b->A.x, snap, n9 * sizeof(double), cudaMemcpyDeviceToDevice, b->stream);
+            ++b->version;
+        }
     }
     cudaStreamSynchronize(b->stream);
     cudaFree(snap);
@@ -601,6 +612,7 @@ int gx_batch_autotune(gx_batch* b, int ticks, int* mode, double* ms) {
     for (int m = 1; m <= 4; ++m)
         if (t[m - 1] >= 0.0 && t[m - 1] < t[pick - 1]) pick = m;
     b->mode = rc ? saved : pick;
+    b->nl_skin = (!rc && pick == 4) ? best_skin : skin0;
     if (mode) *mode = b->mode;
     if (ms)
         for (int m = 0; m < 4; ++m) ms[m] = t[m] >= 0.0 ? t[m] / ticks : -1.0;

@@ -419,8 +419,9 @@ int gx_batch_get_mode(gx_batch* b, int* mode);
  * per-tick device milliseconds of modes 1-4 (-1: mode skipped, 1 because a
  * replica grid exceeds its limit, 4 because a replica is too small). */
 int gx_batch_autotune(gx_batch* b, int ticks, int* mode, double* ms);
-/* Mode 4's list skin (default 0.1 r_c; the list grid's cells are >= r_c +
- * skin).  No counterpart in the reference. */
+/* Mode 4's list skin (default 0.15 r_c; the list grid's cells are >= r_c +
+ * skin; gx_batch_autotune picks among 0.1, 0.15 and 0.2 r_c when it times
+ * mode 4).  No counterpart in the reference. */
 int gx_batch_set_list_skin(gx_batch* b, double skin);
 /* Mode 4's list rebuilds so far (synchronises the batch's stream). */
 int gx_batch_list_rebuilds(gx_batch* b, uint64_t* rebuilds);

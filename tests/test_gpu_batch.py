@@ -136,10 +136,25 @@ def test_cooperative_launch_matches_the_graph_bit_for_bit(gpu):
 def test_list_mode_single_replica_matches_list_handle_bit_for_bit(gpu):
     # one replica rebuilds on the handle's own schedule, in the same frames,
     # with the same per-pair operations and integer sums
+    from genesis_b200._lib import Batch, Handle
     wl = W.replica_workload(W.Replica(n_side=12, temperature=150.0, seed=5))
     wl.thermostat = False
-    out, st, _ = _batch([wl], 25, mode=4)
-    ref, rst = _single(wl, 25, variant=6)
+    cfg = wl.config()
+    skin = 0.15 * 5.75
+    b = Batch(cfg, [cfg.size], [wl.thermostat_temperature])
+    b.set_mode(4)
+    b.set_list_skin(skin)
+    b.set_universes([wl.generate()])
+    st, _ = b.step(25)
+    out = b.get_state()
+    b.close()
+    h = Handle(cfg, "mixed")
+    h.set_kernel_variant(6)
+    h.set_list_skin(skin)
+    h.set_universe(wl.generate())
+    rst = h.step(25)
+    ref = h.get_state()
+    h.close()
     for x, y in zip(out[0], ref):
         assert np.array_equal(x, y)
     assert st[0, 3] == rst["pairs"][-1]
