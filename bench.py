@@ -48,9 +48,10 @@ BYTES_PER_ATOM = {
     "cell_scatter": 12, "cell_rank": 16, "reorder": 220, "stage_pos4": 45, "kinetic": 32,
     # list path: fused kick + drift + wrap + FP32 staging + displacement test
     # (read x v a 72, kind 1, home cell 4, reference float4 16; write x v 48,
-    # float4 16), and fused F -> a + kick + K (read F 24, v 24, 1/m 8, m 8;
-    # write a 24, v 24)
-    "nl_advance": 157, "nl_finish": 112,
+    # float4 16, and zero the int64 force sums 24 for the half-list pass),
+    # and fused F -> a + kick + K (read F 24, v 24, 1/m 8, m 8; write a 24,
+    # v 24)
+    "nl_advance": 181, "nl_finish": 112,
     # list rebuild: the sorted state copied back (12 f64 columns, 2 u8, 1 u32,
     # read and written), the staging (read x y z 24, kind 1, home 4; write
     # the float4 and its reference copy 32); the list build's own bytes
