@@ -41,7 +41,12 @@ struct BatchFlat;  // gx_batch_flat.cu
 void batch_flat_free(BatchFlat* f);
 struct BatchNl;  // gx_batch_nl.cu
 void batch_nl_free(BatchNl* n);
-struct RepThermo;  // gx_batch_flat.cu
+// A replica's atom range (concatenated order) and its Berendsen thermostat.
+struct RepThermo {
+    uint32_t base, n;
+    double target, tau;
+    int thermo;
+};
 
 }  // namespace gx
 
@@ -79,8 +84,7 @@ int batch_nl_step(gx_batch* b, int nsteps, uint64_t* launches);
 bool batch_nl_eligible(const gx_batch* b);  // every replica: >= 3 list cells per axis, >= 128 atoms
 int batch_nl_rebuilds(gx_batch* b, uint64_t* out);
 // shared with mode 4 (gx_batch_flat.cu): prepares the all-replica tables and
-// returns them; launches of the finishing kick and the thermostat over a
-// given slot-to-atom permutation
+// returns them; the end-of-step commit of the pending scales
 struct FlatShared {
     const uint32_t* rep_of;
     const RepThermo* th;
@@ -88,6 +92,5 @@ struct FlatShared {
     unsigned long long* acc;
 };
 int flat_shared(gx_batch* b, FlatShared* out);
-void flat_finish_thermo(gx_batch* b, gx_handle* h, const uint32_t* perm);
 void flat_commit(gx_batch* b, gx_handle* h);
 }

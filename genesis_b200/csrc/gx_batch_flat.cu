@@ -44,12 +44,6 @@ struct RepGeo {
     int8_t half[13][3];
 };
 
-struct RepThermo {
-    uint32_t base, n;
-    double target, tau;
-    int thermo;
-};
-
 struct BatchFlat {
     size_t cap = 0;
     int nrep = 0;
@@ -683,13 +677,6 @@ int flat_shared(gx_batch* b, FlatShared* out) {
     out->lam = b->flat->lam;
     out->acc = b->flat->acc;
     return GX_OK;
-}
-
-void flat_finish_thermo(gx_batch* b, gx_handle* h, const uint32_t* perm) {
-    BatchFlat* f = b->flat;
-    const uint32_t n = (uint32_t)b->total;
-    GX_LAUNCH(h, k_fb_finish, nblk(n, 256), 256, b->A, perm, n, 0.5 * b->p.dt, b->A.total);
-    GX_LAUNCH(h, k_fb_thermo, b->nrep, kFbRed, f->th, b->A, f->lam, f->acc, b->p.thermal_constant, b->d_out);
 }
 
 void flat_commit(gx_batch* b, gx_handle* h) {

@@ -23,7 +23,10 @@
 //                 single-universe list pass's per-pair operations), far ends
 //                 through 64-bit integer atomics, potential and pair count
 //                 per replica on the tick that reports them
-//   k_fb_finish, k_fb_thermo (mode 2's kernels, over this mode's slots)
+//   k_bn_finish   a = F 2^-32 / m and the second kick per slot (k_fb_finish's
+//                 steps) with the kinetic energy summed per block
+//   k_bn_thermo   per replica: the kinetic energy from its blocks' sums, in
+//                 block order, and the Berendsen scale (k_fb_thermo's)
 //
 // The wrap of the reference (boundary.rs:28-34) translates each replica by
 // half its box every tick; as in the single-universe path, a parity of those
@@ -63,6 +66,7 @@ struct BatchNl {
     uint32_t* list = nullptr;   // entry e of slot s at list[e * cap + s], partner | code << 27
     uint32_t* cnt = nullptr;    // entries per slot (> cap_nb: overflowed, scans its cells)
     uint32_t* flag = nullptr;   // [0] rebuild requested, [1] rebuilds, [2] half-box parity, [3] body runs
+    double* kpart = nullptr;    // per finishing block: kinetic energy of its (at most two) replicas
     uint64_t version = ~0ull;   // the batch's state version the lists follow
     gx_handle* ctx = nullptr;   // launch context: stream, counter, the list grid's counting sort
     cudaStream_t side = nullptr;
@@ -85,6 +89,7 @@ void batch_nl_free(BatchNl* s) {
     cudaFree(s->list);
     cudaFree(s->cnt);
     cudaFree(s->flag);
+    cudaFree(s->kpart);
     if (s->side) cudaStreamDestroy(s->side);
     if (s->ctx) {
         cells_free(s->ctx->cl);
@@ -373,6 +378,96 @@ __global__ void __launch_bounds__(kBnThreads) k_bn_force(const BnGeo* __restrict
     }
 }
 
+// a = F 2^-32 / m and the second kick (k_fb_finish's FP64 steps) per slot,
+// with the new kinetic energy summed per block in a fixed order.  A
+// replica's atoms hold exactly the slots [base, base + n) (the slots are
+// sorted by a global cell index grouped by replica), and every replica holds
+// at least kBnThreads >= kBnRed atoms, so a block of kBnRed slots holds at
+// most two replicas: kpart[2b] is the sum over the block's first replica,
+// kpart[2b + 1] over its second.
+constexpr int kBnRed = 128;
+static_assert(kBnRed <= kBnThreads, "two replicas per reduction block at most");
+
+__global__ void __launch_bounds__(kBnRed) k_bn_finish(BatchArrays A, const uint32_t* __restrict__ perm,
+                                                       const uint32_t* __restrict__ srep, uint32_t total,
+                                                       double half_dt, double* __restrict__ kpart) {
+    __shared__ double sh[2][kBnRed / 32];
+    const uint32_t first = blockIdx.x * kBnRed, s = first + threadIdx.x;
+    const uint32_t r0 = srep[first];
+    double k0 = 0.0, k1 = 0.0;
+    if (s < total) {
+        const size_t fs = A.total;
+        const uint32_t i = perm[s];
+        const double im = A.inv_mass[i];
+        const double ax = xmul(xmul(__ll2double_rn(A.F[s]), kFixInv), im);
+        const double ay = xmul(xmul(__ll2double_rn(A.F[fs + s]), kFixInv), im);
+        const double az = xmul(xmul(__ll2double_rn(A.F[2 * fs + s]), kFixInv), im);
+        A.ax[i] = ax;
+        A.ay[i] = ay;
+        A.az[i] = az;
+        const double vx = xadd(A.vx[i], xmul(ax, half_dt));
+        const double vy = xadd(A.vy[i], xmul(ay, half_dt));
+        const double vz = xadd(A.vz[i], xmul(az, half_dt));
+        A.vx[i] = vx;
+        A.vy[i] = vy;
+        A.vz[i] = vz;
+        const double ke = xmul(xmul(0.5, A.mass[i]), xadd(xadd(xmul(vx, vx), xmul(vy, vy)), xmul(vz, vz)));
+        if (srep[s] == r0) k0 = ke;
+        else k1 = ke;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        k0 = xadd(k0, __shfl_down_sync(0xffffffffu, k0, o));
+        k1 = xadd(k1, __shfl_down_sync(0xffffffffu, k1, o));
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) {
+        sh[0][w] = k0;
+        sh[1][w] = k1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t0 = 0.0, t1 = 0.0;
+        for (int k = 0; k < kBnRed / 32; ++k) {
+            t0 = xadd(t0, sh[0][k]);
+            t1 = xadd(t1, sh[1][k]);
+        }
+        kpart[2 * blockIdx.x] = t0;
+        kpart[2 * blockIdx.x + 1] = t1;
+    }
+}
+
+// One warp per replica: its kinetic energy from the partials of the blocks
+// over its slots, in block order, and the Berendsen scale of
+// ThermostatSystem::run (thermostat.rs:52-71) as fb_thermo_one computes it;
+// the potential and pair count of the reporting tick to `out`.
+__global__ void k_bn_thermo(const RepThermo* __restrict__ th, const uint32_t* __restrict__ srep,
+                            const double* __restrict__ kpart, double* __restrict__ lam,
+                            unsigned long long* __restrict__ racc, double k_thermal, double* __restrict__ out) {
+    const int r = blockIdx.x;
+    const RepThermo T = th[r];
+    if (threadIdx.x != 0) return;
+    double ks = 0.0;
+    if (T.n) {
+        const uint32_t b0 = T.base / kBnRed, b1 = (T.base + T.n - 1) / kBnRed;
+        for (uint32_t b = b0; b <= b1; ++b) ks = xadd(ks, kpart[2 * b + (srep[b * kBnRed] == (uint32_t)r ? 0 : 1)]);
+    }
+    double l = 1.0;
+    if (T.thermo && T.n > 0) {
+        const double t = xdiv(xmul(2.0 / 3.0, xdiv(ks, (double)T.n)), k_thermal);
+        if (isfinite(t) && t > 0.0) {
+            const double l2 = xadd(1.0, xmul(xdiv(1.0, T.tau), xsub(xdiv(T.target, t), 1.0)));
+            l = xsqrt(fmax(l2, 0.0));
+        }
+    }
+    lam[r] = l;
+    out[4 * r + 1] = xmul(__ll2double_rn((long long)racc[2 * r]), kFixInv);
+    out[4 * r + 2] = l;
+    out[4 * r + 3] = (double)racc[2 * r + 1];
+    racc[2 * r] = 0;
+    racc[2 * r + 1] = 0;
+}
+
 __global__ void k_bn_body_done(uint32_t* flag) { flag[3] += 1u; }
 
 // After the (conditional) rebuild: count it and restart the parity, or
@@ -448,6 +543,7 @@ int bn_prepare(gx_batch* b, const FlatShared& fsh) {
     GXN_CUDA(b, cudaMalloc(&s->list, (size_t)cap_nb * n * sizeof(uint32_t)));
     GXN_CUDA(b, cudaMalloc(&s->cnt, n * sizeof(uint32_t)));
     GXN_CUDA(b, cudaMalloc(&s->flag, 4 * sizeof(uint32_t)));
+    GXN_CUDA(b, cudaMalloc(&s->kpart, 2 * (size_t)nblk(n, kBnRed) * sizeof(double)));
     GXN_CUDA(b, cudaMemcpy(s->geo, geo.data(), b->nrep * sizeof(BnGeo), cudaMemcpyHostToDevice));
     GXN_CUDA(b, cudaMemsetAsync(s->home, 0, n * sizeof(uint32_t), b->stream));
     GXN_CUDA(b, cudaMemsetAsync(s->srep, 0, n * sizeof(uint32_t), b->stream));
@@ -522,7 +618,9 @@ int bn_tick(gx_batch* b, const FlatShared& fsh, bool energy) {
     auto kf = energy ? k_bn_force<true> : k_bn_force<false>;
     GX_LAUNCH(h, kf, nblk(n, kBnThreads), kBnThreads, s->geo, s->shift, A.pos4, s->home, s->srep, h->cl.start, n, b->L,
               b->d_tab, s->list, s->cap, s->cap_nb, s->cnt, A.F, A.total, fsh.acc, b->d_err);
-    flat_finish_thermo(b, h, s->perm);
+    GX_LAUNCH(h, k_bn_finish, nblk(n, kBnRed), kBnRed, A, s->perm, s->srep, n, 0.5 * b->p.dt, s->kpart);
+    GX_LAUNCH(h, k_bn_thermo, b->nrep, 32, fsh.th, s->srep, s->kpart, fsh.lam, fsh.acc, b->p.thermal_constant,
+              b->d_out);
     return GX_OK;
 }
 
