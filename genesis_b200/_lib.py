@@ -67,7 +67,7 @@ EXPORTS = (
     "gx_radial_distribution_noalloc", "gx_set_kernel_variant", "gx_autotune",
     "gx_batch_create", "gx_batch_destroy", "gx_batch_last_error", "gx_batch_set_state",
     "gx_batch_step", "gx_batch_get_state", "gx_adjoint_forward", "gx_adjoint_backward",
-    "gx_set_list_skin", "gx_list_rebuilds", "gx_list_stats", "gx_batch_set_mode", "gx_batch_get_mode", "gx_batch_autotune", "gx_batch_set_list_skin", "gx_batch_list_rebuilds",
+    "gx_set_list_skin", "gx_list_rebuilds", "gx_list_stats", "gx_batch_set_mode", "gx_batch_get_mode", "gx_batch_autotune", "gx_batch_set_list_skin", "gx_batch_list_rebuilds", "gx_batch_list_stats",
     "gx_get_list_config", "gx_set_list_threads", "gx_set_list_stash", "gx_set_list_brick", "gx_set_list_block", "gx_get_list_shape", "gx_bond_observe", "gx_bond_tracker_reset", "gx_get_bonds",
     "gx_bond_components", "gx_collisions", "gx_collision_count", "gx_xyz_frame", "gx_snapshot_world",
     "gx_set_step_async",
@@ -674,6 +674,12 @@ class Batch:
         self._check(self.lib.gx_batch_list_rebuilds(self.b, C.byref(v)))
         return v.value
 
+    def list_stats(self):
+        """(entries, overflowed slots) of mode 4's current lists."""
+        e, o = C.c_uint64(), C.c_uint64()
+        self._check(self.lib.gx_batch_list_stats(self.b, C.byref(e), C.byref(o)))
+        return e.value, o.value
+
     def autotune(self, ticks: int = 10):
         """Times the four modes from a snapshot, keeps the fastest: (mode, {mode: ms per tick})."""
         m = C.c_int()
@@ -710,6 +716,7 @@ def _declare_batch(lib):
         "gx_batch_autotune": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), dp]),
         "gx_batch_set_list_skin": (C.c_int, [vp, C.c_double]),
         "gx_batch_list_rebuilds": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
+        "gx_batch_list_stats": (C.c_int, [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     }
     for name, (res, args) in proto.items():
         f = getattr(lib, name)

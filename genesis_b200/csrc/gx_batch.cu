@@ -567,6 +567,11 @@ int gx_batch_list_rebuilds(gx_batch* b, uint64_t* rebuilds) {
     return batch_nl_rebuilds(b, rebuilds);
 }
 
+int gx_batch_list_stats(gx_batch* b, uint64_t* entries, uint64_t* overflowed_slots) {
+    if (!b || !entries || !overflowed_slots) return GX_ERR_ARG;
+    return batch_nl_stats(b, entries, overflowed_slots);
+}
+
 int gx_batch_get_mode(gx_batch* b, int* mode) {
     if (!b || !mode) return GX_ERR_ARG;
     *mode = b->mode;

@@ -83,6 +83,7 @@ int batch_coop_step(gx_batch* b, int nsteps, uint64_t* launches);
 int batch_nl_step(gx_batch* b, int nsteps, uint64_t* launches);
 bool batch_nl_eligible(const gx_batch* b);  // every replica: >= 3 list cells per axis, >= 128 atoms
 int batch_nl_rebuilds(gx_batch* b, uint64_t* out);
+int batch_nl_stats(gx_batch* b, uint64_t* entries, uint64_t* overflowed);
 // shared with mode 4 (gx_batch_flat.cu): prepares the all-replica tables and
 // returns them; the end-of-step commit of the pending scales
 struct FlatShared {

@@ -482,6 +482,24 @@ __global__ void k_bn_end(uint32_t* flag, int wrap) {
     }
 }
 
+__global__ void k_bn_stats(const uint32_t* __restrict__ cnt, uint32_t n, int cap_nb, unsigned long long* __restrict__ out) {
+    unsigned long long e = 0, o = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t m = cnt[i];
+        e += m;
+        o += m > (uint32_t)cap_nb ? 1ull : 0ull;
+    }
+#pragma unroll
+    for (int k = 16; k > 0; k >>= 1) {
+        e += __shfl_down_sync(0xffffffffu, e, k);
+        o += __shfl_down_sync(0xffffffffu, o, k);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (e) atomicAdd(out, e);
+        if (o) atomicAdd(out + 1, o);
+    }
+}
+
 __global__ void k_bn_init_slots(uint32_t* __restrict__ slot_of, uint32_t* __restrict__ perm, uint32_t total) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < total) slot_of[i] = perm[i] = i;
@@ -684,6 +702,29 @@ int batch_nl_step(gx_batch* b, int nsteps, uint64_t* launches) {
     flat_commit(b, h);
     GXN_CUDA(b, cudaGetLastError());
     if (launches) *launches = h->launches - l0;
+    return GX_OK;
+}
+
+// Entries of mode 4's current lists (an overflowed slot counts the entries
+// it found) and the slots whose list overflowed (synchronises).
+int batch_nl_stats(gx_batch* b, uint64_t* entries, uint64_t* overflowed) {
+    *entries = *overflowed = 0;
+    BatchNl* s = b->nl;
+    if (!s || !s->cnt || !b->total) return GX_OK;
+    unsigned long long* d = nullptr;
+    GXN_CUDA(b, cudaMalloc(&d, 2 * sizeof(unsigned long long)));
+    unsigned long long v[2] = {0, 0};
+    cudaError_t e = cudaMemsetAsync(d, 0, sizeof v, b->stream);
+    if (e == cudaSuccess) {
+        k_bn_stats<<<256, 256, 0, b->stream>>>(s->cnt, (uint32_t)b->total, s->cap_nb, d);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(v, d, sizeof v, cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    cudaFree(d);
+    if (e != cudaSuccess) return bnerr(b, GX_ERR_CUDA, cudaGetErrorString(e));
+    *entries = v[0];
+    *overflowed = v[1];
     return GX_OK;
 }
 

@@ -425,6 +425,10 @@ int gx_batch_autotune(gx_batch* b, int ticks, int* mode, double* ms);
 int gx_batch_set_list_skin(gx_batch* b, double skin);
 /* Mode 4's list rebuilds so far (synchronises the batch's stream). */
 int gx_batch_list_rebuilds(gx_batch* b, uint64_t* rebuilds);
+/* Mode 4's current lists: entries held (an overflowed slot counts those it
+ * found) and slots whose list overflowed (they scan their 27 home-grid
+ * cells directly, the same pairs).  Synchronises. */
+int gx_batch_list_stats(gx_batch* b, uint64_t* entries, uint64_t* overflowed_slots);
 
 /* ---- adjoint: derivatives of short NVE horizons ----------------------- */
 

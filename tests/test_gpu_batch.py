@@ -238,3 +238,31 @@ def test_list_mode_rejects_small_replicas(gpu):
     with pytest.raises(GxError):
         b.step(1)
     b.close()
+
+
+def test_list_mode_overflowing_lists_scan_their_cells(gpu, orc):
+    # a dense clump in one replica overflows the per-slot lists (sized for the
+    # densest replica on average); those slots scan their cells directly
+    import dataclasses
+    from genesis_b200._lib import Batch
+    wls = _replicas(thermo=False)
+    us = [wl.generate() for wl in wls]
+    rng = np.random.default_rng(4)
+    pos = us[3].pos.copy()
+    k = 300
+    d = rng.normal(size=(k, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    pos[:k] = d * (4.0 * rng.random(k) ** (1.0 / 3.0) + 0.3)[:, None]
+    us[3] = dataclasses.replace(us[3], pos=pos, vel=us[3].vel * 0.0)
+    base = wls[0].config()
+    b = Batch(base, [wl.config().size for wl in wls], [wl.thermostat_temperature for wl in wls])
+    b.set_mode(4)
+    b.set_universes(us)
+    b.step(1)
+    entries, overflowed = b.list_stats()
+    assert entries > 0 and overflowed > 0
+    out = b.get_state()
+    b.close()
+    for (p_, _, acc), wl, u in zip(out, wls, us):
+        acc_ref, _, _, _ = orc.forces(wl.config(), p_, u.elem, u.charge, u.mass)
+        assert np.linalg.norm(acc - acc_ref) <= 1e-5 * np.linalg.norm(acc_ref)
