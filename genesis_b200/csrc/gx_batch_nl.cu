@@ -522,7 +522,7 @@ int bnerr(gx_batch* b, int code, const std::string& m) {
 double skin_of(const gx_batch* b) { return b->nl_skin >= 0.0 ? b->nl_skin : 0.15 * b->rc; }
 
 // Allocates the lists (outside any capture) for the batch's current atoms.
-int bn_prepare(gx_batch* b, const FlatShared& fsh) {
+int bn_prepare(gx_batch* b) {
     const double skin = skin_of(b);
     BatchNl* s = b->nl;
     if (s && s->cap == b->total && s->nrep == b->nrep && s->skin == skin) return GX_OK;
@@ -577,7 +577,6 @@ int bn_prepare(gx_batch* b, const FlatShared& fsh) {
     s->ctx->stream = b->stream;
     if (ensure_cells(s->ctx, s->ctx->cl, s->ncell)) return bnerr(b, GX_ERR_OOM, s->ctx->err);
     if (ensure_sort_tmp(s->ctx, s->ctx->cl, n)) return bnerr(b, GX_ERR_OOM, s->ctx->err);  // before capture
-    (void)fsh;
     return GX_OK;
 }
 
@@ -669,7 +668,7 @@ int batch_nl_step(gx_batch* b, int nsteps, uint64_t* launches) {
     FlatShared fsh;
     int rc = flat_shared(b, &fsh);
     if (rc) return rc;
-    if ((rc = bn_prepare(b, fsh))) return rc;
+    if ((rc = bn_prepare(b))) return rc;
     BatchNl* s = b->nl;
     gx_handle* h = s->ctx;
     if (s->version != b->version) {
