@@ -68,7 +68,7 @@ EXPORTS = (
     "gx_batch_create", "gx_batch_destroy", "gx_batch_last_error", "gx_batch_set_state",
     "gx_batch_step", "gx_batch_get_state", "gx_adjoint_forward", "gx_adjoint_backward",
     "gx_set_list_skin", "gx_list_rebuilds", "gx_list_stats", "gx_batch_set_mode", "gx_batch_get_mode", "gx_batch_autotune", "gx_batch_set_list_skin", "gx_batch_list_rebuilds", "gx_batch_list_stats",
-    "gx_get_list_config", "gx_set_list_threads", "gx_set_list_stash", "gx_set_list_brick", "gx_set_list_block", "gx_get_list_shape", "gx_bond_observe", "gx_bond_tracker_reset", "gx_get_bonds",
+    "gx_get_list_config", "gx_set_list_threads", "gx_set_list_stash", "gx_set_list_brick", "gx_set_list_block", "gx_get_list_shape", "gx_set_pass_timing", "gx_pass_ms", "gx_bond_observe", "gx_bond_tracker_reset", "gx_get_bonds",
     "gx_bond_components", "gx_collisions", "gx_collision_count", "gx_xyz_frame", "gx_snapshot_world",
     "gx_set_step_async",
 )
@@ -134,6 +134,8 @@ def load(path: str | Path | None = None) -> C.CDLL:
         "gx_set_list_block": (C.c_int, [vp, C.c_int]),
         "gx_get_list_shape": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                       C.POINTER(C.c_int)]),
+        "gx_set_pass_timing": (C.c_int, [vp, C.c_int]),
+        "gx_pass_ms": (C.c_int, [vp, C.POINTER(C.c_double)]),
         "gx_bond_observe": (C.c_int, [vp, _D, _D, C.c_int, C.c_uint64, C.c_int, C.POINTER(GxBondObservation)]),
         "gx_bond_tracker_reset": (C.c_int, [vp]),
         "gx_get_bonds": (C.c_int, [vp, u32p, sz, C.POINTER(sz)]),
@@ -292,6 +294,16 @@ class Handle:
         skin, tpp = C.c_double(), C.c_int()
         self._check(self.lib.gx_get_list_config(self.h, C.byref(skin), C.byref(tpp)))
         return skin.value, tpp.value
+
+    def set_pass_timing(self, on: bool):
+        """CUDA events around every tick's pair pass, inside captured ticks too."""
+        self._check(self.lib.gx_set_pass_timing(self.h, 1 if on else 0))
+
+    def pass_ms(self) -> float:
+        """Device time of the last tick's pair pass (pass timing on)."""
+        v = C.c_double()
+        self._check(self.lib.gx_pass_ms(self.h, C.byref(v)))
+        return v.value
 
     def list_shape(self) -> dict:
         """The list pass's work shape: threads per atom, far-end block,

@@ -76,7 +76,19 @@ GridGeom make_grid(const double box[3], double min_cell, int* ok) {
     return g;
 }
 
+// The pair pass's events of gx_set_pass_timing ("force_*" slots): recorded
+// in eager ticks, and inside a capture as external event nodes of the
+// tick's graph, so that a replayed tick times its own pass.
+void pass_mark(gx_handle* h, const char* name, int k) {
+    if (!h->pass_timing || std::strncmp(name, "force_", 6) != 0) return;
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(h->stream, &st) != cudaSuccess) return;
+    cudaEventRecordWithFlags(h->pass_ev[k], h->stream,
+                             st == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault);
+}
+
 void prof_begin(gx_handle* h, const char* name) {
+    pass_mark(h, name, 0);
     if (!h->prof_on) return;
     ProfSlot* s = nullptr;
     for (auto& p : h->prof)
@@ -100,6 +112,7 @@ void prof_begin(gx_handle* h, const char* name) {
     s->ev.push_back(b);
 }
 void prof_end(gx_handle* h, const char* name) {
+    pass_mark(h, name, 1);
     if (!h->prof_on) return;
     for (auto& p : h->prof)
         if (p.name == name || std::strcmp(p.name, name) == 0) {
@@ -453,6 +466,8 @@ void gx_destroy(gx_handle* h) {
     collide_free(h);
     export_free(h);
     snapshot_free(h);
+    for (cudaEvent_t e : h->pass_ev)
+        if (e) cudaEventDestroy(e);
     if (h->herr) cudaFreeHost(h->herr);
     free_buf(h->buf[0]);
     free_buf(h->buf[1]);
@@ -1095,6 +1110,27 @@ int gx_set_list_brick(gx_handle* h, int cells) {
 int gx_list_stats(gx_handle* h, uint64_t* entries, uint64_t* overflowed_atoms) {
     if (!h || !entries || !overflowed_atoms) return GX_ERR_ARG;
     return nl_stats(h, entries, overflowed_atoms);
+}
+
+int gx_set_pass_timing(gx_handle* h, int on) {
+    if (!h) return GX_ERR_ARG;
+    if (on && !h->pass_ev[0]) {
+        GX_CUDA(h, cudaEventCreate(&h->pass_ev[0]));
+        GX_CUDA(h, cudaEventCreate(&h->pass_ev[1]));
+    }
+    h->pass_timing = on != 0;
+    invalidate_graphs(h);  // the captured ticks gain or lose the event nodes
+    return GX_OK;
+}
+
+int gx_pass_ms(gx_handle* h, double* ms) {
+    if (!h || !ms) return GX_ERR_ARG;
+    if (!h->pass_ev[0]) return set_err(h, GX_ERR_STATE, "pass timing was never switched on");
+    GX_CUDA(h, cudaStreamSynchronize(h->stream));
+    float t = 0.f;
+    GX_CUDA(h, cudaEventElapsedTime(&t, h->pass_ev[0], h->pass_ev[1]));
+    *ms = t;
+    return GX_OK;
 }
 
 int gx_list_rebuilds(gx_handle* h, uint64_t* rebuilds) {

@@ -233,6 +233,8 @@ struct gx_handle {
     size_t nbonds = 0, bonds_cap = 0;
 
     // profiling
+    bool pass_timing = false;      // events around the pair pass, in captured ticks too
+    cudaEvent_t pass_ev[2] = {};
     bool prof_on = false;
     std::vector<gx::ProfSlot> prof;
     std::vector<cudaEvent_t> ev_pool;

@@ -184,6 +184,13 @@ int gx_get_list_config(gx_handle* h, double* skin, int* threads_per_atom);
 int gx_list_stats(gx_handle* h, uint64_t* entries, uint64_t* overflowed_atoms);
 /* Number of variant-5/6 list rebuilds so far (synchronises the stream). */
 int gx_list_rebuilds(gx_handle* h, uint64_t* rebuilds);
+/* Pair-pass timing: with `on`, every tick records two CUDA events around
+ * its pair pass, also inside the captured tick (external event nodes of
+ * the graph), so that gx_pass_ms gives the device time of the last tick's
+ * pass as the replayed graph runs it.  Re-captures the ticks.  No
+ * counterpart in the reference. */
+int gx_set_pass_timing(gx_handle* h, int on);
+int gx_pass_ms(gx_handle* h, double* ms);
 
 /* ---- state ----------------------------------------------------------- */
 

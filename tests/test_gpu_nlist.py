@@ -280,3 +280,20 @@ def test_bricks_beyond_the_staging_capacity_read_global_memory(gpu):
         for x, y in zip(out[0][0], o[0]):
             assert np.array_equal(x, y)
         assert np.array_equal(out[0][1], o[1])
+
+
+def test_pass_timing_inside_captured_ticks(gpu):
+    # events captured around the pair pass time the replayed tick's own pass
+    cfg, u = _lattice(14, temperature=150.0, coul=True)
+    h = _handle(cfg)
+    h.set_universe(u)
+    h.step(3, graph=True)
+    h.set_pass_timing(True)
+    h.step(2, graph=True)
+    t_graph = h.pass_ms()
+    h.step(1, graph=False)
+    t_eager = h.pass_ms()
+    h.set_pass_timing(False)
+    assert 0.0 < t_graph < 50.0 and 0.0 < t_eager < 50.0
+    st = h.step(2, graph=True)  # timing off again: the ticks re-capture without the events
+    assert len(st["pairs"]) == 2
