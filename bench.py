@@ -786,13 +786,21 @@ def ours_arm(args, dist):
     tot_ms = sum(v[1] for k, v in prof.items() if k != "nl_rebuild")
     # the pair pass as the timed ticks run it: two events captured into the
     # replayed tick around the pass (external event nodes), 40 recording ticks
+    # (the state keeps condensing, so the tick time, the pair count and the
+    # pass time are all taken on these ticks, the pairs from their records)
+    h.step(5, stats=True, graph=True)
+    h.mark(4)
+    h.step(40, stats=True, graph=True)
+    h.mark(5)
+    tick_ms_here = h.elapsed_ms(4, 5) / 40
     h.set_pass_timing(True)
-    pass_ms = []
+    pass_ms, pass_pairs = [], []
     for _ in range(40):
-        h.step(1, stats=True, graph=True)
+        pass_pairs.append(float(h.step(1, stats=True, graph=True)["pairs"][0]))
         pass_ms.append(h.pass_ms())
     h.set_pass_timing(False)
     force_ms = float(np.median(pass_ms))
+    pairs = float(np.mean(pass_pairs))
     flop_pp = FLOP_PER_PAIR_LJC if cfg.enable_electrostatics else FLOP_PER_PAIR_LJ
     achieved = pairs * flop_pp / (force_ms * 1e-3) / 1e12
     try:
@@ -809,12 +817,14 @@ def ours_arm(args, dist):
                 "note": "the pass is bound by its neighbour gathers and far-end integer reductions in L1/TEX, "
                         "not by the FP32 pipe (profiles/k_nl_force__c3_262144_atoms.txt)"},
             "flop_per_launch": pairs * flop_pp, "flop_per_pair": flop_pp, "pairs_per_launch": pairs,
-            "launch_ms": force_ms, "share_of_step": force_ms / (ms_max / K),
+            "launch_ms": force_ms, "share_of_step": force_ms / tick_ms_here, "tick_ms_at_these_ticks": tick_ms_here,
             "launch_ms_min_max": [float(np.min(pass_ms)), float(np.max(pass_ms))],
             "launch_ms_eager": force_ms_eager, "share_of_eager_step": f_ms / tot_ms if tot_ms else None,
             "timing": "median over 40 recording graph ticks of CUDA events captured into the tick around the "
-                      "energy-carrying pass (gx_set_pass_timing); launch_ms_eager: events around each launch "
-                      "of the profiled eager ticks"}
+                      "energy-carrying pass (gx_set_pass_timing), after the timed, energy-free and profiled "
+                      "ticks (the quench has condensed further by then: more pairs than in the timed ticks), "
+                      "pairs from those ticks' records, share against 40 graph ticks just before them; "
+                      "launch_ms_eager: events around each launch of the profiled eager ticks"}
     hbm, hbm_src = hbm_peak()
     epa = entries / u.n if u.n else 0.0
     mem = {}

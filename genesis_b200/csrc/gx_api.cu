@@ -275,6 +275,39 @@ __global__ void k_record(gx_tick_stats* rec, const double* dscal, unsigned long 
     dcount[5] = k + 1;
 }
 
+// The speed partials summed as k_finalize_sum sums them (the same order, so
+// the same value) into dscal[4], then the record of k_record: one launch for
+// both on the list path's recorded ticks.
+constexpr int kRecThreads = 256;
+__global__ void __launch_bounds__(kRecThreads) k_record_sum(const double* __restrict__ spart, int nb,
+                                                            gx_tick_stats* rec, double* dscal,
+                                                            unsigned long long* dcount, int thermo, int scale) {
+    __shared__ double sh[kRecThreads / 32];
+    double v = 0.0;
+    for (int i = threadIdx.x; i < nb; i += kRecThreads) v = xadd(v, spart[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    v = (threadIdx.x < kRecThreads / 32) ? sh[threadIdx.x] : 0.0;
+    if (wid == 0) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    if (threadIdx.x != 0) return;
+    dscal[4] = v;
+    unsigned long long k = dcount[5];
+    const double l = scale ? dscal[0] : 1.0;
+    rec[k].kinetic = scale ? xmul(xmul(dscal[1], l), l) : dscal[1];
+    rec[k].speed_sum = scale ? xmul(v, l) : v;
+    rec[k].potential = dscal[2];
+    rec[k].bond_energy = dscal[3];
+    rec[k].lambda = thermo ? dscal[0] : 1.0;
+    rec[k].pairs = dcount[0];
+    dcount[5] = k + 1;
+}
+
 inline unsigned nblk(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
 void invalidate_graphs(gx_handle* h) {
@@ -776,15 +809,15 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
         // kernel below overwrites the slot anyway
         if (pend && !thermo) GX_LAUNCH(h, k_fill_d, 1, 32, h->dscal, 1, 1.0);
         h->lambda_pending = false;
-        if (thermo) {
+        if (thermo) {  // on a recorded tick its sum of the partials is also the record's K
             launch_thermostat_lambda(h, kpart, nb, h->p.thermal_constant, h->p.thermostat_temperature, tau, n,
-                                     h->dscal + 0, nullptr);
+                                     h->dscal + 0, drec ? h->dscal + 1 : nullptr);
             h->lambda_pending = true;
         }
         if (drec) {  // K and the speed sum of the scaled v: lambda^2 K and lambda S of the kicked v
-            launch_finalize_sum(h, kpart, nb, h->dscal + 1);
-            launch_finalize_sum(h, spart, nb, h->dscal + 4);
-            GX_LAUNCH(h, k_record, 1, 1, drec, h->dscal, h->dcount, thermo ? 1 : 0, thermo ? 1 : 0);
+            if (!thermo) launch_finalize_sum(h, kpart, nb, h->dscal + 1);
+            GX_LAUNCH(h, k_record_sum, 1, kRecThreads, spart, nb, drec, h->dscal, h->dcount, thermo ? 1 : 0,
+                      thermo ? 1 : 0);
         }
         return GX_OK;
     };
