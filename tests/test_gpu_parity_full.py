@@ -11,7 +11,9 @@ workloads at their full size against the same CPU oracle:
 * the ionic Na/O system, 32^3 = 32,768 atoms, with bond observation every
   tick for 40 ticks (persistence after 0.1 vibration periods, so bonds form
   and the spring runs), tick by tick against the oracle's tracker in both
-  precisions, then the forces with the observed bonds.
+  precisions, then the forces with the observed bonds;
+* the 256-replica temperature sweep (1.13M atoms) in batch mode 4, every
+  replica's forces after 30 ticks of persistent neighbour lists.
 """
 from __future__ import annotations
 
@@ -173,3 +175,31 @@ def test_ionic_observation_tick_by_tick(gpu, orc, precision):
     assert _rel(acc, acc_ref) <= tol
     assert Vb_ref != 0.0 and abs(Vb - Vb_ref) <= tol * abs(Vb_ref)
     h.close()
+
+
+# ---------------------------------------------------------------- 256 sweep replicas
+
+
+def test_sweep_replicas_on_neighbour_lists_match_the_oracle(gpu, orc):
+    """The benchmarked sweep (256 replicas, 1.13M atoms) in batch mode 4:
+    after 30 ticks (the first rebuilds every list, later ones as atoms move)
+    every replica's accelerations against the oracle's forces at its own
+    positions."""
+    from genesis_b200 import sweep
+    from genesis_b200._lib import Batch
+    wls = sweep.make_replicas(256, seed=0)
+    assert sweep.atoms(wls) > 1_000_000
+    base = wls[0].config()
+    b = Batch(base, [wl.config().size for wl in wls], [wl.thermostat_temperature for wl in wls])
+    b.set_mode(4)
+    us = [wl.generate() for wl in wls]
+    b.set_universes(us)
+    b.step(30)
+    assert b.list_rebuilds() >= 2
+    out = b.get_state()
+    b.close()
+    worst = 0.0
+    for (pos, _, acc), wl, u in zip(out, wls, us):
+        acc_ref, _, _, _ = orc.forces(wl.config(), pos, u.elem, u.charge, u.mass, nthreads=THREADS)
+        worst = max(worst, _rel(acc, acc_ref))
+    assert worst <= MIXED_RMS, worst
