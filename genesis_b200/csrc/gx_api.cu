@@ -311,13 +311,22 @@ __global__ void __launch_bounds__(kRecThreads) k_record_sum(const double* __rest
 inline unsigned nblk(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
 void invalidate_graphs(gx_handle* h) {
-    for (int a = 0; a < 2; ++a)
+    for (int a = 0; a < 2; ++a) {
         for (int b = 0; b < 2; ++b) {
             if (h->graph_exec[a][b]) cudaGraphExecDestroy(h->graph_exec[a][b]);
             h->graph_exec[a][b] = nullptr;
             h->graph_key[a][b] = 0;
         }
+        if (h->graph_multi[a]) cudaGraphExecDestroy(h->graph_multi[a]);
+        h->graph_multi[a] = nullptr;
+        h->graph_multi_key[a] = 0;
+    }
 }
+
+// Ticks of the list path captured into one graph when a step call has that
+// many left: fewer graph launches for small systems, whose ticks last only
+// tens of microseconds.
+constexpr int kTicksPerGraph = 8;
 
 // The pending Berendsen scale is folded into the next kernel that reads v;
 // anything else that reads v first commits it.
@@ -858,12 +867,48 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
     const uint64_t key = ((uint64_t)n << 20) ^ ((uint64_t)h->precision << 1) ^ ((uint64_t)h->kernel_variant << 3) ^
                          ((uint64_t)bonds_on(h) << 6) ^ ((uint64_t)thermo << 7) ^ ((uint64_t)h->cap << 8) ^
                          ((uint64_t)use_nl << 62) ^ 1u;
+    // kTicksPerGraph list ticks as one graph (capture only: nothing runs);
+    // the host-side pending-scale flag is left as a captured run leaves it
+    auto capture_multi = [&](int rs) -> int {
+        if (h->graph_multi[rs]) cudaGraphExecDestroy(h->graph_multi[rs]);
+        h->graph_multi[rs] = nullptr;
+        const uint64_t l0 = h->launches;
+        const bool pend0 = h->lambda_pending;
+        GX_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        int trc = GX_OK;
+        for (int k = 0; k < kTicksPerGraph && !trc; ++k) trc = tick(true);
+        cudaGraph_t gr = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(h->stream, &gr);
+        if (trc || ce != cudaSuccess) {
+            if (gr) cudaGraphDestroy(gr);
+            h->lambda_pending = pend0;
+            h->launches = l0;
+            return trc ? trc : cuda_err(h, ce, "cudaStreamEndCapture");
+        }
+        cudaGraphExec_t ex = nullptr;
+        ce = cudaGraphInstantiate(&ex, gr, 0);
+        cudaGraphDestroy(gr);
+        if (ce != cudaSuccess) return cuda_err(h, ce, "cudaGraphInstantiate");
+        h->graph_multi[rs] = ex;
+        h->graph_multi_key[rs] = key;
+        h->graph_multi_kernels[rs] = h->launches - l0;
+        h->launches = l0;
+        return GX_OK;
+    };
     for (int s = 0; s < nsteps; ++s) {
         if (!graph) {
             if ((rc = tick(false))) return rc;
             continue;
         }
         const int par = h->cur, rs = drec ? 1 : 0;
+        if (use_nl && nsteps - s >= kTicksPerGraph) {  // the list path keeps one buffer: ticks chain as captured
+            if (!(h->graph_multi[rs] && h->graph_multi_key[rs] == key) && (rc = capture_multi(rs))) return rc;
+            GX_CUDA(h, cudaGraphLaunch(h->graph_multi[rs], h->stream));
+            h->launches += h->graph_multi_kernels[rs];
+            h->lambda_pending = thermo;
+            s += kTicksPerGraph - 1;
+            continue;
+        }
         if (h->graph_exec[par][rs] && h->graph_key[par][rs] == key) {
             GX_CUDA(h, cudaGraphLaunch(h->graph_exec[par][rs], h->stream));
             h->launches += h->graph_kernels[par][rs];
@@ -899,6 +944,17 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
         h->graph_exec[par][rs] = ex;
         h->graph_key[par][rs] = key;
         h->graph_kernels[par][rs] = h->launches - l0;
+        // the list path's multi-tick graph is captured with the single one, so
+        // that any call that captures (a warm-up) leaves both ready
+        if (use_nl && !(h->graph_multi[rs] && h->graph_multi_key[rs] == key)) {
+            const uint64_t l1 = h->launches;
+            const bool pend1 = h->lambda_pending;
+            h->lambda_pending = pend0;  // as before the single tick's capture
+            int mrc = capture_multi(rs);
+            h->lambda_pending = pend1;
+            h->launches = l1;
+            if (mrc) return mrc;
+        }
         GX_CUDA(h, cudaGraphLaunch(ex, h->stream));  // the captured tick has not run yet: run it now
     }
     if (use_nl) h->sorted = false;  // buf[cur] is ordered by the list grid, not the force grid

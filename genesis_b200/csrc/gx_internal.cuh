@@ -243,6 +243,10 @@ struct gx_handle {
     cudaGraphExec_t graph_exec[2][2] = {};
     uint64_t graph_key[2][2] = {};
     uint64_t graph_kernels[2][2] = {};
+    // list path: kTicksPerGraph ticks captured in one graph, without / with records
+    cudaGraphExec_t graph_multi[2] = {};
+    uint64_t graph_multi_key[2] = {};
+    uint64_t graph_multi_kernels[2] = {};
 
     // stream-ordered timers and the launch counter
     cudaEvent_t timers[16] = {};
