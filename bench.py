@@ -931,7 +931,20 @@ def ours_arm(args, dist):
             he = Handle(cfg, "mixed", dev)
             he.set_state(arr[0], arr[1], u.elem, acc=arr[2], charge=u.charge, mass=u.mass, entity=u.entity)
             he.step(2)
+            he.tick_host(arr[0], arr[1], arr[2])  # the first call allocates its staging
             he.synchronize()
+            dist.barrier()
+            t0 = time.perf_counter()
+            for _ in range(Ke):
+                stt = he.tick_host(arr[0], arr[1], arr[2])
+            he.synchronize()
+            te = time.perf_counter() - t0
+            te = dist.max(te)
+            extras["e2e"] = {"value": dist.world * n * Ke / te, "unit": UNIT,
+                             "h2d_bytes_per_step": 3 * n * 24, "d2h_bytes_per_step": 3 * n * 24 + stt.nbytes,
+                             "steps": Ke, "timing": "host wall clock, pinned host buffers, one gx_tick_host per "
+                             "tick (Position, Velocity, Acceleration in and out, copies overlapped with the tick)"}
+            # the same ticks through the three separate calls a host system could make
             dist.barrier()
             t0 = time.perf_counter()
             for _ in range(Ke):
@@ -939,12 +952,10 @@ def ours_arm(args, dist):
                 stt = he.step(1, stats=True)
                 he.get_state_into(arr[0], arr[1], arr[2])
             he.synchronize()
-            te = time.perf_counter() - t0
-            te = dist.max(te)
-            extras["e2e"] = {"value": dist.world * n * Ke / te, "unit": UNIT,
-                             "h2d_bytes_per_step": 3 * n * 24, "d2h_bytes_per_step": 3 * n * 24 + stt.nbytes,
-                             "steps": Ke, "timing": "host wall clock, pinned host buffers, "
-                             "gx_set_dynamic + gx_step(1) + gx_get_state every tick"}
+            t3 = dist.max(time.perf_counter() - t0)
+            extras["e2e_three_calls"] = {"value": dist.world * n * Ke / t3, "unit": UNIT, "steps": Ke,
+                                         "timing": "host wall clock, pinned host buffers, gx_set_dynamic + "
+                                         "gx_step(1) + gx_get_state every tick (no overlap)"}
             he.close()
         except Exception as e:  # noqa: BLE001
             extras["e2e_error"] = repr(e)

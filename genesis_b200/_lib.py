@@ -70,7 +70,7 @@ EXPORTS = (
     "gx_set_list_skin", "gx_list_rebuilds", "gx_list_stats", "gx_batch_set_mode", "gx_batch_get_mode", "gx_batch_autotune", "gx_batch_set_list_skin", "gx_batch_list_rebuilds", "gx_batch_list_stats",
     "gx_get_list_config", "gx_set_list_threads", "gx_set_list_stash", "gx_set_list_brick", "gx_set_list_block", "gx_get_list_shape", "gx_set_pass_timing", "gx_pass_ms", "gx_bond_observe", "gx_bond_tracker_reset", "gx_get_bonds",
     "gx_bond_components", "gx_collisions", "gx_collision_count", "gx_xyz_frame", "gx_snapshot_world",
-    "gx_set_step_async",
+    "gx_set_step_async", "gx_tick_host",
 )
 
 _lib = None
@@ -115,6 +115,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
         "gx_profile_enable": (C.c_int, [vp, C.c_int]),
         "gx_profile_read": (C.c_int, [vp, C.POINTER(C.c_char_p), u64p, dp, C.c_int, C.c_int]),
         "gx_set_dynamic": (C.c_int, [vp, dp, dp, dp]),
+        "gx_tick_host": (C.c_int, [vp, dp, dp, dp, C.POINTER(GxTickStats)]),
         "gx_timer_mark": (C.c_int, [vp, C.c_int]),
         "gx_timer_elapsed": (C.c_int, [vp, C.c_int, C.c_int, dp]),
         "gx_launch_count": (C.c_uint64, [vp]),
@@ -378,6 +379,21 @@ class Handle:
         """Per-tick sync of the dynamic columns from host arrays (slot order)."""
         a = [None if x is None else np.ascontiguousarray(x, dtype=np.float64) for x in (pos, vel, acc)]
         self._check(self.lib.gx_set_dynamic(self.h, *(_ptr(x, C.c_double) for x in a)))
+
+    def tick_host(self, pos, vel, acc, stats: bool = True):
+        """One tick against host columns (float64 (n, 3), slot order), updated
+        in place: gx_set_dynamic + gx_step(1) + gx_get_state in one call with
+        the copies overlapped (pinned arrays give the overlap)."""
+        for x in (pos, vel, acc):
+            if not (isinstance(x, np.ndarray) and x.dtype == np.float64 and x.flags.c_contiguous
+                    and x.shape == (self.n, 3)):
+                raise ValueError("tick_host needs C-contiguous float64 (n, 3) arrays")
+        rec = (GxTickStats * 1)() if stats else None
+        self._check(self.lib.gx_tick_host(self.h, _ptr(pos, C.c_double), _ptr(vel, C.c_double),
+                                          _ptr(acc, C.c_double), rec))
+        if not stats:
+            return None
+        return np.frombuffer(rec, dtype=TICK_DTYPE, count=1).copy()
 
     def get_state_into(self, pos=None, vel=None, acc=None):
         """gx_get_state into caller-owned (e.g. pinned) float64 (n, 3) arrays."""

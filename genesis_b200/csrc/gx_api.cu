@@ -510,6 +510,13 @@ void gx_destroy(gx_handle* h) {
     snapshot_free(h);
     for (cudaEvent_t e : h->pass_ev)
         if (e) cudaEventDestroy(e);
+    if (h->io_stream) {
+        cudaStreamSynchronize(h->io_stream);
+        cudaStreamDestroy(h->io_stream);
+    }
+    for (cudaEvent_t e : h->io_ev)
+        if (e) cudaEventDestroy(e);
+    cudaFree(h->io_stage);
     if (h->herr) cudaFreeHost(h->herr);
     free_buf(h->buf[0]);
     free_buf(h->buf[1]);
@@ -764,7 +771,10 @@ int gx_stats(gx_handle* h, double* kinetic, double* speed_sum) {
     return GX_OK;
 }
 
-int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
+namespace {
+// gx_step's body.  With `defer` (gx_tick_host) the ticks are only queued:
+// the record stays on the device and nothing waits for the stream.
+int step_impl(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph, bool defer) {
     int rc = require_state(h);
     if (rc) return rc;
     if (nsteps < 0) return GX_ERR_ARG;
@@ -959,6 +969,8 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
     }
     if (use_nl) h->sorted = false;  // buf[cur] is ordered by the list grid, not the force grid
     h->nl_fresh = nsteps > 0 ? (use_nl && h->nl_valid) : fresh0;
+    h->last_tick_nl = use_nl;
+    if (defer) return GX_OK;
     if (drec) {
         GX_CUDA(h, cudaMemcpyAsync(stats, drec, (size_t)nsteps * sizeof(gx_tick_stats), cudaMemcpyDeviceToHost,
                                    h->stream));
@@ -976,6 +988,11 @@ int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
     uint32_t e = 0;
     GX_CUDA(h, cudaMemcpy(&e, h->derr, sizeof e, cudaMemcpyDeviceToHost));
     return step_error(h, e);
+}
+}  // namespace
+
+int gx_step(gx_handle* h, int nsteps, gx_tick_stats* stats, int use_graph) {
+    return step_impl(h, nsteps, stats, use_graph, false);
 }
 
 int gx_collisions(gx_handle* h, uint64_t* collisions) {
@@ -1251,6 +1268,110 @@ int gx_set_dynamic(gx_handle* h, const double* pos, const double* vel, const dou
     GX_CUDA(h, cudaStreamSynchronize(h->stream));
     GX_CUDA(h, cudaGetLastError());
     return GX_OK;
+}
+
+// One tick against host columns: gx_set_dynamic, gx_step(h, 1, stats, 1)
+// and gx_get_state in one call, with the same results, and with the copies
+// overlapped.  The columns cross PCIe on a stream of their own: each one is
+// scattered to the sorted order as soon as it lands, and on the list path
+// the positions go back while the pair pass runs (a list tick records
+// io_ev[3] once they are final); velocities and accelerations follow the
+// tick.
+int gx_tick_host(gx_handle* h, double* pos, double* vel, double* acc, gx_tick_stats* stats) {
+    int rc = require_state(h);
+    if (rc) return rc;
+    if (!pos || !vel || !acc) return set_err(h, GX_ERR_ARG, "gx_tick_host needs the position, velocity and "
+                                                            "acceleration columns");
+    if ((rc = settle_step_errors(h))) return rc;
+    if (!h->io_stream) {
+        GX_CUDA(h, cudaStreamCreateWithFlags(&h->io_stream, cudaStreamNonBlocking));
+        for (cudaEvent_t& e : h->io_ev) GX_CUDA(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    if (!h->io_events) {
+        h->io_events = true;
+        invalidate_graphs(h);  // the captured list ticks gain the positions-final event
+    }
+    if (h->io_cap < h->cap) {
+        GX_CUDA(h, cudaStreamSynchronize(h->io_stream));
+        cudaFree(h->io_stage);
+        h->io_stage = nullptr;
+        h->io_cap = 0;
+        GX_CUDA(h, cudaMalloc(&h->io_stage, 9 * h->cap * sizeof(double)));
+        h->io_cap = h->cap;
+    }
+    const uint32_t n = (uint32_t)h->n;
+    const size_t bytes = 3 * (size_t)n * sizeof(double);
+    double* st[3] = {h->io_stage, h->io_stage + 3 * h->io_cap, h->io_stage + 6 * h->io_cap};
+    cudaStream_t ms = h->stream, io = h->io_stream;
+    // From the first queued copy on, a failure waits for both streams before
+    // it returns, so that no queued work still reads the caller's columns.
+    auto fail = [&](int r) -> int {
+        h->stream = ms;
+        cudaStreamSynchronize(io);
+        cudaStreamSynchronize(ms);
+        return r;
+    };
+#define GX_IO(call)                                                  \
+    do {                                                             \
+        cudaError_t e_ = (call);                                     \
+        if (e_ != cudaSuccess) return fail(cuda_err(h, e_, #call));  \
+    } while (0)
+    if (h->lambda_pending) {  // the host columns replace v: the pending scale is void
+        GX_LAUNCH(h, k_fill_d, 1, 32, h->dscal, 1, 1.0);
+        h->lambda_pending = false;
+    }
+    {
+        StateBuf& b = h->buf[h->cur];
+        const double* ins[3] = {pos, vel, acc};
+        double* dsts[3][3] = {{b.x, b.y, b.z}, {b.vx, b.vy, b.vz}, {b.ax, b.ay, b.az}};
+        for (int k = 0; k < 3; ++k) {
+            if (!n) break;
+            GX_IO(cudaMemcpyAsync(st[k], ins[k], bytes, cudaMemcpyHostToDevice, io));
+            GX_IO(cudaEventRecord(h->io_ev[k], io));
+            GX_IO(cudaStreamWaitEvent(ms, h->io_ev[k], 0));
+            GX_LAUNCH(h, k_aos_to_sorted, nblk(n, 256), 256, st[k], h->pos_of_slot, dsts[k][0], dsts[k][1],
+                      dsts[k][2], n);
+        }
+        h->sorted = false;
+        h->nl_fresh = false;
+    }
+    if ((rc = step_impl(h, 1, stats, 1, true))) return fail(rc);
+    if (n) {
+        StateBuf& b = h->buf[h->cur];
+        if (h->last_tick_nl) {  // positions final at io_ev[3]: gathered and copied beside the pair pass
+            GX_IO(cudaStreamWaitEvent(io, h->io_ev[3], 0));
+            h->stream = io;
+            GX_LAUNCH(h, k_soa_to_aos, nblk(n, 256), 256, b.x, b.y, b.z, b.slot, st[0], n);
+            h->stream = ms;
+        } else {
+            GX_LAUNCH(h, k_soa_to_aos, nblk(n, 256), 256, b.x, b.y, b.z, b.slot, st[0], n);
+            GX_IO(cudaEventRecord(h->io_ev[0], ms));
+            GX_IO(cudaStreamWaitEvent(io, h->io_ev[0], 0));
+        }
+        GX_IO(cudaGetLastError());
+        GX_IO(cudaMemcpyAsync(pos, st[0], bytes, cudaMemcpyDeviceToHost, io));
+        if ((rc = commit_lambda(h))) return fail(rc);
+        double* srcs[2][3] = {{b.vx, b.vy, b.vz}, {b.ax, b.ay, b.az}};
+        double* outs[2] = {vel, acc};
+        for (int k = 0; k < 2; ++k) {
+            GX_LAUNCH(h, k_soa_to_aos, nblk(n, 256), 256, srcs[k][0], srcs[k][1], srcs[k][2], b.slot, st[k + 1], n);
+            GX_IO(cudaEventRecord(h->io_ev[k + 1], ms));
+            GX_IO(cudaStreamWaitEvent(io, h->io_ev[k + 1], 0));
+            GX_IO(cudaMemcpyAsync(outs[k], st[k + 1], bytes, cudaMemcpyDeviceToHost, io));
+        }
+    }
+    GX_IO(cudaGetLastError());
+    GX_IO(cudaStreamSynchronize(io));
+    GX_IO(cudaStreamSynchronize(ms));
+    if (stats) {
+        size_t rows = h->cap / 64 + kRedCap;
+        GX_IO(cudaMemcpy(stats, h->red + 4 * rows, sizeof(gx_tick_stats), cudaMemcpyDeviceToHost));
+    }
+#undef GX_IO
+    h->step_errs_pending = false;
+    uint32_t e = 0;
+    GX_CUDA(h, cudaMemcpy(&e, h->derr, sizeof e, cudaMemcpyDeviceToHost));
+    return step_error(h, e);
 }
 
 int gx_synchronize(gx_handle* h) {

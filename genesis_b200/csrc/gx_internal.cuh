@@ -232,6 +232,17 @@ struct gx_handle {
     uint32_t* bonds = nullptr;
     size_t nbonds = 0, bonds_cap = 0;
 
+    // gx_tick_host: the column copies run on their own stream beside the tick.
+    // io_ev[0..2] order each staged column against its use; io_ev[3] is
+    // recorded by every list tick (captured ones too) once the positions are
+    // final, so that they can be copied out while the pair pass runs.
+    cudaStream_t io_stream = nullptr;
+    cudaEvent_t io_ev[4] = {};
+    bool io_events = false;
+    double* io_stage = nullptr;  // three AoS columns of 3 * io_cap doubles
+    size_t io_cap = 0;
+    bool last_tick_nl = false;   // the last gx_step tick ran on the neighbour-list path
+
     // profiling
     bool pass_timing = false;      // events around the pair pass, in captured ticks too
     cudaEvent_t pass_ev[2] = {};

@@ -1425,6 +1425,11 @@ int nl_tick(gx_handle* h, const double* lambda, double* kpart, double* spart, in
     if (rc) return rc;
     GX_LAUNCH(h, k_nl_end, 1, 1, s->flag, h->p.enable_boundaries ? 1 : 0, h->dcount);
     prof_end(h, "nl_rebuild");
+    // Positions and the slot map are final here (the pair pass, the spring,
+    // the collision pass and the finish write only forces and velocities).
+    if (h->io_events)
+        GX_CUDA(h, cudaEventRecordWithFlags(h->io_ev[3], h->stream,
+                                            cond ? cudaEventRecordExternal : cudaEventRecordDefault));
     const bool halfl = s->half == 1;
     const bool f64 = h->precision != GX_MIXED;
     LawF32 L = make_law32(h);

@@ -372,6 +372,18 @@ int gx_xyz_frame(gx_handle* h, uint64_t tick, char* out, size_t cap, size_t* len
  * resident atoms without touching the static columns (AtomType, Mass,
  * Charge, EntityId).  Any pointer may be NULL (column unchanged). */
 int gx_set_dynamic(gx_handle* h, const double* pos, const double* vel, const double* acc);
+/* One Universe::tick (src/universe/mod.rs:141-159) of the force schedule
+ * against host ECS columns: reads Position, Velocity and Acceleration (slot
+ * order, AoS f64, all three required), runs the tick and writes the three
+ * columns back in place -- the same results as gx_set_dynamic +
+ * gx_step(h, 1, stats, 1) + gx_get_state, in one call.  The copies run on a
+ * stream of their own and overlap the tick: each column is scattered to the
+ * device order as it lands, and on the neighbour-list path the positions go
+ * back while the pair pass runs.  Page-locked (pinned) columns give the
+ * overlap; pageable ones are correct but copy synchronously.  stats may be
+ * NULL, else it receives the tick's record.  Waits for the tick and
+ * reports its pair-pass errors like gx_step. */
+int gx_tick_host(gx_handle* h, double* pos, double* vel, double* acc, gx_tick_stats* stats);
 
 /* ---- batched replicas (temperature sweep) ------------------------------ */
 
