@@ -529,7 +529,33 @@ def adjoint_leg(dev: int) -> dict:
             "max_rel_err_vs_fd": {"potential": err(np.r_[gsV, geV], fd["potential"]),
                                   "gr": err(np.r_[gsG, geG], fd["gr"])},
             "fd_step": "central, 1e-5 x parameter", "loss_values": {"potential": lv, "gr": lg},
-            "timing": "host wall clock around the synchronous C-ABI calls"}
+            "timing": "host wall clock around the synchronous C-ABI calls",
+            "mixed_forward": mixed_adjoint(acfg, au, spec, target, fd, err, dev)}
+
+
+def mixed_adjoint(acfg, au, spec, target, fd, err, dev: int) -> dict:
+    """The C5 form: the forward in the mixed method (FP32 pair law,
+    fixed-point force sums), the FP64 adjoint on that trajectory, against the
+    central differences of the FP64 forward."""
+    import numpy as np
+
+    from genesis_b200 import adjoint as adj
+    from genesis_b200._lib import Handle
+
+    with Handle(acfg, "mixed", dev) as hm:
+        hm.set_universe(au)
+        hm.adjoint_forward(spec.nsteps, **spec.kwargs())  # warm-up
+        t0 = time.perf_counter()
+        V, g = hm.adjoint_forward(spec.nsteps, **spec.kwargs())
+        t1 = time.perf_counter()
+        gsV, geV = hm.adjoint_backward(dl_dpotential=adj.potential_loss(V)[1])
+        t2 = time.perf_counter()
+        gsG, geG = hm.adjoint_backward(dl_dgr=adj.gr_loss(g, target)[1])
+    return {"precision": "FP32 pair law + 64-bit fixed-point force sums forward, FP64 adjoint",
+            "forward_ms": (t1 - t0) * 1e3, "gradient_ms": (t2 - t0) * 1e3,
+            "max_rel_err_vs_fd": {"potential": err(np.r_[gsV, geV], fd["potential"]),
+                                  "gr": err(np.r_[gsG, geG], fd["gr"])},
+            "fd": "the FP64 forward's central differences above"}
 
 
 def ionic_leg(dev: int, cpu: bool, steps: int | None = None, cpu_budget_s: float = 10.0, variant: int = -1) -> dict:

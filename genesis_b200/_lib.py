@@ -461,9 +461,10 @@ class Handle:
     # -- adjoint --------------------------------------------------------------
     def adjoint_forward(self, nsteps: int, checkpoint_every: int = 20, gr_bins: int = 0, gr_every: int = 1,
                         gr_rmax: float = 1.0, gr_width: float = 0.1, gr_support: float = 6.0):
-        """FP64 trajectory of ``nsteps`` NVE ticks from the current state
-        (left unchanged); returns (V per tick, time-averaged Gaussian-kernel
-        g(r) or None)."""
+        """Trajectory of ``nsteps`` NVE ticks from the current state (left
+        unchanged): FP64 on an "fp64" handle, the mixed method (FP32 pair law,
+        fixed-point force sums, FP64 state) on a "mixed" one; returns (V per
+        tick, time-averaged Gaussian-kernel g(r) or None)."""
         spec = GxAdjointSpec(nsteps, checkpoint_every, gr_bins, gr_every, gr_rmax, gr_width, gr_support)
         V = np.zeros(nsteps)
         g = np.zeros(gr_bins) if gr_bins > 0 else None

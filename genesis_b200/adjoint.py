@@ -57,9 +57,10 @@ def with_params(cfg, sigma=None, epsilon_k=None):
     return c
 
 
-def forward(cfg, universe, spec: AdjointSpec, device: int = 0):
-    """(V per tick, time-averaged g) of the FP64 trajectory."""
-    with Handle(cfg, "fp64", device) as h:
+def forward(cfg, universe, spec: AdjointSpec, device: int = 0, precision: str = "fp64"):
+    """(V per tick, time-averaged g) of the trajectory: FP64, or the mixed
+    method (FP32 pair law, fixed-point force sums) with ``precision="mixed"``."""
+    with Handle(cfg, precision, device) as h:
         h.set_universe(universe)
         return h.adjoint_forward(spec.nsteps, **spec.kwargs())
 
@@ -80,11 +81,13 @@ def gr_target(cfg, universe, spec: AdjointSpec, device: int = 0) -> np.ndarray:
     return forward(c, universe, spec, device)[1]
 
 
-def gradients(cfg, universe, spec: AdjointSpec, target=None, device: int = 0):
+def gradients(cfg, universe, spec: AdjointSpec, target=None, device: int = 0, precision: str = "fp64"):
     """Losses and adjoint gradients.  Returns a dict with
-    ``potential`` (<V>, dsigma[10], deps[10]) and, with a target, ``gr``."""
+    ``potential`` (<V>, dsigma[10], deps[10]) and, with a target, ``gr``.
+    ``precision="mixed"`` runs the forward in the mixed method (FP32 pair
+    law, fixed-point force sums); the adjoint is FP64 either way."""
     out = {}
-    with Handle(cfg, "fp64", device) as h:
+    with Handle(cfg, precision, device) as h:
         h.set_universe(universe)
         V, g = h.adjoint_forward(spec.nsteps, **spec.kwargs())
         lv, cv = potential_loss(V)

@@ -8,8 +8,13 @@
 //
 // Forward.  The trajectory is recomputed in slot order (atoms never move
 // between arrays; a per-tick counting sort gives the cell list as an index),
-// in FP64 with the reference's per-pair arithmetic (pair_f64).  A checkpoint
-// of (x, v, a) is kept every K ticks.
+// in FP64 with the reference's per-pair arithmetic (pair_f64).  On a handle
+// of mixed precision the forward is the mixed method instead: the FP32 pair
+// law of the list passes (pair_f32) on the FP64 minimum-image displacement
+// rounded to FP32, the per-atom force summed in 2^-32 fixed point, and FP64
+// positions, velocities and observables; the backward below stays FP64,
+// linearised on that trajectory.  A checkpoint of (x, v, a) is kept every K
+// ticks.
 //
 // Backward.  Per segment: restore the checkpoint, recompute the segment's
 // positions, then walk the ticks backwards.  With adjoints (Lx, Lv, La) of
@@ -37,6 +42,7 @@
 #include <vector>
 
 #include "gx_law64.cuh"
+#include "gx_pair_f32.cuh"
 
 namespace gx {
 namespace {
@@ -185,13 +191,19 @@ __device__ __forceinline__ double lane_sum(double v) {
     for (int o = kAdjLanes / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, kAdjLanes);
     return v;
 }
+// Integer partials: any order gives the same sum.
+__device__ __forceinline__ long long lane_sum_ll(long long v) {
+#pragma unroll
+    for (int o = kAdjLanes / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, kAdjLanes);
+    return v;
+}
 
 // ---------------------------------------------------------------------------
 // Kernels (slot order unless noted).
 
 // Handle state (cell-sorted) -> slot order.
 __global__ void k_adj_import(StateBuf b, uint32_t n, Vec3Field x, Vec3Field v, Vec3Field a, uint8_t* elem,
-                             double* charge, double* mass, double* inv_mass) {
+                             double* charge, double* mass, double* inv_mass, uint8_t* kind) {
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     uint32_t s = b.slot[p];
@@ -208,6 +220,7 @@ __global__ void k_adj_import(StateBuf b, uint32_t n, Vec3Field x, Vec3Field v, V
     charge[s] = b.charge[p];
     mass[s] = b.mass[p];
     inv_mass[s] = b.inv_mass[p];
+    kind[s] = b.kind[p];
 }
 
 // First kick, drift, wrap (integrate.rs:39-43, 62-66; boundary.rs:28-34) and
@@ -244,12 +257,13 @@ __global__ void k_adj_stage(uint32_t n, const uint32_t* __restrict__ perm, const
                             Vec3Field x, const uint8_t* __restrict__ elem, const double* __restrict__ charge,
                             const double* __restrict__ mass, const double* __restrict__ inv_mass, Vec3Field xs,
                             uint8_t* es, double* qs, double* ms, uint32_t* ks, Vec3Field Lv, Vec3Field La,
-                            double half_dt, Vec3Field ws) {
+                            double half_dt, Vec3Field ws, const uint8_t* __restrict__ kind, uint8_t* kinds) {
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     uint32_t i = perm[p];
     for (int k = 0; k < 3; ++k) xs.c(k, p) = x.c(k, i);
     es[p] = elem[i];
+    if (kinds) kinds[p] = kind[i];
     qs[p] = charge[i];
     ms[p] = mass[i];
     ks[p] = key[i];
@@ -265,13 +279,18 @@ __global__ void k_adj_stage(uint32_t n, const uint32_t* __restrict__ perm, const
 // combines their accelerations; the potential and the smoothed histogram
 // take each pair-list entry once (canonical half-shell visits, or j > p
 // within a cell).  One histogram per warp in shared memory, integer counts.
-template <bool OBS, bool GR>
+// F32: the mixed method's pair law (pair_f32 on the FP64 displacement
+// rounded to FP32, the kinds' FP32 pair table) with the force summed in
+// 2^-32 fixed point and a = F 2^-32 / m as the list path's finish takes it;
+// the potential sums the FP32 pair energies in FP64.
+template <bool OBS, bool GR, bool F32>
 __global__ void __launch_bounds__(kAdjThreads)
     k_adj_force(GridGeom g, uint32_t n, LawF64 L, const double* __restrict__ psig, const double* __restrict__ peps,
                 const uint32_t* __restrict__ start, const uint32_t* __restrict__ ks, Vec3Field xs,
                 const uint8_t* __restrict__ es, const double* __restrict__ qs, const double* __restrict__ ms,
                 const uint32_t* __restrict__ perm, const double* __restrict__ inv_mass, Vec3Field v, Vec3Field a,
-                double half_dt, double* __restrict__ vpart, GrSpec gs, double* __restrict__ hpart) {
+                double half_dt, double* __restrict__ vpart, GrSpec gs, double* __restrict__ hpart, LawF32 L32,
+                const PairF* __restrict__ tabf, const uint8_t* __restrict__ kinds, uint32_t* __restrict__ err) {
     constexpr int kWarps = kAdjThreads / 32;
     __shared__ double shd[kWarps];
     __shared__ unsigned long long hist[GR ? kWarps : 1][GR ? kAdjMaxBins : 1];
@@ -284,11 +303,13 @@ __global__ void __launch_bounds__(kAdjThreads)
     const int lane = (int)(t % kAdjLanes);
     double V = 0.0;
     double ax = 0.0, ay = 0.0, az = 0.0;
+    long long fx = 0, fy = 0, fz = 0;
     if (p < n) {
         uint32_t c = ks[p], cx, cy, cz;
         decode(g, c, cx, cy, cz);
         double xi = xs.c(0, p), yi = xs.c(1, p), zi = xs.c(2, p);
         int ti = es[p];
+        const int kti = F32 ? (int)kinds[p] * L32.nkinds : 0;
         double qi = qs[p], mi = ms[p];
         double inv_mi = inv_mass[perm[p]];
         for (int k = lane - 1; k < g.nfull; k += kAdjLanes) {
@@ -305,9 +326,21 @@ __global__ void __launch_bounds__(kAdjThreads)
                 double d = xsqrt(d2);
                 if (d <= kEpsF64) continue;
                 bool count = (k < 0) ? (q > p) : half;
-                int tj = es[q];
-                double fmag, Vij = 0.0;
-                pair_f64(L, d, psig[ti * kNElem + tj], peps[ti * kNElem + tj], qi, qs[q], mi, ms[q], fmag, Vij);
+                double fmag = 0.0, Vij = 0.0;
+                if (F32) {
+                    const float fdx = (float)dx, fdy = (float)dy, fdz = (float)dz;
+                    float fs, vf;
+                    pair_f32(L32, tabf[kti + kinds[q]], dist2(fdx, fdy, fdz), fs, vf);
+                    long long qx, qy, qz;
+                    quant3(fmul(fdx, fs), fmul(fdy, fs), fmul(fdz, fs), qx, qy, qz, err);
+                    fx += qx;
+                    fy += qy;
+                    fz += qz;
+                    Vij = (double)vf;
+                } else {
+                    int tj = es[q];
+                    pair_f64(L, d, psig[ti * kNElem + tj], peps[ti * kNElem + tj], qi, qs[q], mi, ms[q], fmag, Vij);
+                }
                 if (OBS && count) V = xadd(V, Vij);
                 if (GR && count) {
                     int k0 = (int)ceil((d - gs.reach) / gs.dr - 0.5), k1 = (int)floor((d + gs.reach) / gs.dr - 0.5);
@@ -320,7 +353,7 @@ __global__ void __launch_bounds__(kAdjThreads)
                         atomicAdd(&wh[bb], (unsigned long long)llrint(G * kHistScale));
                     }
                 }
-                if (fmag != 0.0) {
+                if (!F32 && fmag != 0.0) {
                     double inv = xdiv(1.0, d);
                     ax = xadd(ax, xmul(xmul(xmul(dx, inv), fmag), inv_mi));
                     ay = xadd(ay, xmul(xmul(xmul(dy, inv), fmag), inv_mi));
@@ -330,9 +363,21 @@ __global__ void __launch_bounds__(kAdjThreads)
         }
     }
     // every lane of an atom is in the same warp and takes part
-    ax = lane_sum(ax);
-    ay = lane_sum(ay);
-    az = lane_sum(az);
+    if (F32) {
+        fx = lane_sum_ll(fx);
+        fy = lane_sum_ll(fy);
+        fz = lane_sum_ll(fz);
+        if (p < n) {
+            const double im = inv_mass[perm[p]];
+            ax = xmul(xmul(__ll2double_rn(fx), kFixInv), im);
+            ay = xmul(xmul(__ll2double_rn(fy), kFixInv), im);
+            az = xmul(xmul(__ll2double_rn(fz), kFixInv), im);
+        }
+    } else {
+        ax = lane_sum(ax);
+        ay = lane_sum(ay);
+        az = lane_sum(az);
+    }
     if (p < n && lane == 0) {
         uint32_t i = perm[p];
         a.c(0, i) = ax;
@@ -489,6 +534,8 @@ struct AdjBuffers {
     int cap_T = 0, cap_ck = 0, cap_K = 0, cap_bins = 0;
     double gr_rmax = 0, gr_width = 0, gr_support = 0;
     bool ready = false;
+    bool f32 = false;  // the forward in the mixed method (a handle of mixed precision)
+    uint8_t *kind = nullptr, *kinds = nullptr;  // kind per slot, per sorted position (F32 forward)
     double *S = nullptr, *Ladj = nullptr, *P = nullptr, *ck = nullptr, *seg = nullptr;
     double *xs = nullptr, *ws = nullptr, *qs = nullptr, *ms = nullptr;
     double *charge = nullptr, *mass = nullptr, *inv_mass = nullptr;
@@ -547,6 +594,8 @@ int adj_alloc(gx_handle* h, AdjBuffers* A, size_t n, int T, int K, int bins) {
     rc |= get((void**)&A->inv_mass, cap * sizeof(double));
     rc |= get((void**)&A->elem, cap);
     rc |= get((void**)&A->es, cap);
+    rc |= get((void**)&A->kind, cap);
+    rc |= get((void**)&A->kinds, cap);
     rc |= get((void**)&A->key, cap * sizeof(uint32_t));
     rc |= get((void**)&A->perm, cap * sizeof(uint32_t));
     rc |= get((void**)&A->ks, cap * sizeof(uint32_t));
@@ -600,16 +649,19 @@ int adj_tick(gx_handle* h, AdjBuffers* A, int t, bool obs, double* xsave, bool w
     if (rc) return rc;
     Vec3Field xs = field(A->xs, cap), none = field(nullptr, cap);
     GX_LAUNCH(h, k_adj_stage, nblk(n, 256), 256, n, A->perm, A->key, x, A->elem, A->charge, A->mass, A->inv_mass,
-              xs, A->es, A->qs, A->ms, A->ks, none, none, half_dt, none);
+              xs, A->es, A->qs, A->ms, A->ks, none, none, half_dt, none, A->kind, A->f32 ? A->kinds : nullptr);
     LawF64 L = make_law64(h);
     const double* psig = A->tab;
     const double* peps = A->tab + kNElem * kNElem;
     GrSpec gs = gr_spec(A);
     unsigned nb = nblk((size_t)n * kAdjLanes, kAdjThreads);
     bool gr = obs && A->bins > 0 && (t % A->every) == 0;
-    auto kern = !obs ? k_adj_force<false, false> : (gr ? k_adj_force<true, true> : k_adj_force<true, false>);
+    auto kern = A->f32 ? (!obs ? k_adj_force<false, false, true>
+                               : (gr ? k_adj_force<true, true, true> : k_adj_force<true, false, true>))
+                       : (!obs ? k_adj_force<false, false, false>
+                               : (gr ? k_adj_force<true, true, false> : k_adj_force<true, false, false>));
     GX_LAUNCH(h, kern, nb, kAdjThreads, g, n, L, psig, peps, A->cl.start, A->ks, xs, A->es, A->qs, A->ms, A->perm,
-              A->inv_mass, v, a, half_dt, A->vpart, gs, A->hpart);
+              A->inv_mass, v, a, half_dt, A->vpart, gs, A->hpart, make_law32(h), h->d_pairf, A->kinds, h->derr);
     if (obs) {
         launch_finalize_sum(h, A->vpart, (int)nb, A->dV + (t - 1));
         if (gr) {
@@ -635,6 +687,10 @@ int check_err(gx_handle* h) {
     if (e & kErrNonFinite) {
         cudaMemsetAsync(h->derr, 0, sizeof(uint32_t), h->stream);
         return set_err(h, GX_ERR_NONFINITE, "non-finite position in the adjoint trajectory");
+    }
+    if (e & kErrSaturation) {  // the fixed-point force of the mixed forward
+        cudaMemsetAsync(h->derr, 0, sizeof(uint32_t), h->stream);
+        return set_err(h, GX_ERR_SATURATION, "fixed-point force saturated in the adjoint trajectory");
     }
     return GX_OK;
 }
@@ -664,6 +720,8 @@ int gx_adjoint_forward(gx_handle* h, const gx_adjoint_spec* spec, double* potent
     for (int e = 0; e < kNElem; ++e)
         if (!(h->p.epsilon_k[e] > 0.0)) return set_err(h, GX_ERR_UNSUPPORTED, "the adjoint needs every epsilon_k > 0");
     if (h->n >= (1u << 31)) return set_err(h, GX_ERR_CAPACITY, "too many atoms");
+    if (h->precision == GX_MIXED && h->nkinds > kMaxKinds)
+        return set_err(h, GX_ERR_UNSUPPORTED, "the mixed forward supports at most 16 distinct (element, charge) kinds");
     // NVE only, so no Berendsen scale can be pending on the handle's velocities.
     if (!h->adj) h->adj = new AdjBuffers();
     AdjBuffers* A = static_cast<AdjBuffers*>(h->adj);
@@ -680,6 +738,7 @@ int gx_adjoint_forward(gx_handle* h, const gx_adjoint_spec* spec, double* potent
     A->gr_support = spec->gr_support;
     A->samples = 0;
     A->n = h->n;
+    A->f32 = h->precision == GX_MIXED;
     const uint32_t n = (uint32_t)h->n;
     const size_t cap = A->cap;
     // pair table, epsilon_k
@@ -690,7 +749,7 @@ int gx_adjoint_forward(gx_handle* h, const gx_adjoint_spec* spec, double* potent
     GX_CUDA(h, cudaMemcpyAsync(A->tab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     StateBuf& b = h->buf[h->cur];
     GX_LAUNCH(h, k_adj_import, nblk(n, 256), 256, b, n, field(A->S, cap), field(A->S + 3 * cap, cap),
-              field(A->S + 6 * cap, cap), A->elem, A->charge, A->mass, A->inv_mass);
+              field(A->S + 6 * cap, cap), A->elem, A->charge, A->mass, A->inv_mass, A->kind);
     GX_CUDA(h, cudaMemcpyAsync(A->ck, A->S, 9 * cap * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
     if (A->bins > 0) GX_CUDA(h, cudaMemsetAsync(A->hacc, 0, A->bins * sizeof(double), h->stream));
     for (int t = 1; t <= T; ++t) {
@@ -756,7 +815,7 @@ int gx_adjoint_backward(gx_handle* h, const double* dl_dpotential, const double*
             GX_LAUNCH(h, k_adj_keys, nblk(n, 256), 256, g, n, xt, A->key);
             if ((rc = counting_sort(h, A->cl, g.ncell, A->key, n, A->perm))) return rc;
             GX_LAUNCH(h, k_adj_stage, nblk(n, 256), 256, n, A->perm, A->key, xt, A->elem, A->charge, A->mass,
-                      A->inv_mass, xs, A->es, A->qs, A->ms, A->ks, Lv, La, half_dt, ws);
+                      A->inv_mass, xs, A->es, A->qs, A->ms, A->ks, Lv, La, half_dt, ws, A->kind, nullptr);
             bool gr = has_gr && (t % A->every) == 0;
             auto kern = gr ? k_adj_back<true> : k_adj_back<false>;
             GX_LAUNCH(h, kern, nb, kAdjThreads, g, n, L, psig, peps, epsk, A->cl.start, A->ks, xs, ws, A->es, A->qs,

@@ -463,8 +463,12 @@ int gx_batch_list_stats(gx_batch* b, uint64_t* entries, uint64_t* overflowed_slo
  *          r_k = (k + 1/2) gr_rmax / gr_bins,  w = gr_width,
  *          c_k = L_x L_y L_z / (N (N - 1) / 2 * 4 pi r_k^2 * sqrt(2 pi) w).
  * The ticks are the reference's (src/universe/mod.rs:356-369: kick, drift,
- * wrap, forces, kick) in FP64 with its per-pair arithmetic, whatever the
- * handle's precision.  gx_adjoint_forward keeps a checkpoint of (x, v, a)
+ * wrap, forces, kick): on a GX_FP64 handle in FP64 with its per-pair
+ * arithmetic; on a GX_MIXED handle in the mixed method (the FP32 pair law on
+ * the FP64 displacement rounded to FP32, forces summed in 2^-32 fixed point,
+ * FP64 positions, velocities and observables), at most 16 kinds.  The
+ * adjoint is FP64 in both, linearised on the forward's trajectory.
+ * gx_adjoint_forward keeps a checkpoint of (x, v, a)
  * every checkpoint_every ticks; gx_adjoint_backward recomputes each segment
  * from its checkpoint and runs the adjoint of the velocity-Verlet step and
  * of the force pass backwards through it.  The cutoffs (LJ, Coulomb,

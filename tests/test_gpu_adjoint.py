@@ -172,13 +172,61 @@ def test_c5_forward_matches_plain_fp64_steps(c5_case):
     assert np.max(np.abs(V - st["potential"]) / np.abs(st["potential"])) <= 1e-10
 
 
-def test_c5_gradients_match_finite_differences(c5_case):
+@pytest.fixture(scope="module")
+def c5_fd(c5_case):
+    cfg, u, spec, target = c5_case
+    return A.fd_gradients(cfg, u, spec, target, rel_step=1e-5)
+
+
+def test_c5_gradients_match_finite_differences(c5_case, c5_fd):
     cfg, u, spec, target = c5_case
     ad = A.gradients(cfg, u, spec, target)
-    fd = A.fd_gradients(cfg, u, spec, target, rel_step=1e-5)
     for key in ("potential", "gr"):
         g = np.r_[ad[key][1], ad[key][2]]
-        assert _close(g, fd[key], 1e-4, 1e-6), (key, g, fd[key])
+        assert _close(g, c5_fd[key], 1e-4, 1e-6), (key, g, c5_fd[key])
+
+
+def test_c5_mixed_forward_gradients_match_finite_differences(c5_case, c5_fd):
+    """The C5 form: the forward in the mixed method (FP32 pair law,
+    fixed-point force sums), the adjoint in FP64 on that trajectory, against
+    central differences of the plain FP64 forward, 1e-4 relative."""
+    cfg, u, spec, target = c5_case
+    ad = A.gradients(cfg, u, spec, target, precision="mixed")
+    for key in ("potential", "gr"):
+        g = np.r_[ad[key][1], ad[key][2]]
+        assert _close(g, c5_fd[key], 1e-4, 1e-6), (key, g, c5_fd[key])
+
+
+def test_c5_mixed_forward_follows_mixed_steps(c5_case):
+    """V_t of the mixed forward against the FP64 forward (the trajectories
+    part only by the FP32 pair law's rounding) and against mixed gx_step
+    records (whose pair law runs on cell-frame FP32 displacements)."""
+    from genesis_b200._lib import Handle
+    cfg, u, spec, _ = c5_case
+    Vm, gm = A.forward(cfg, u, spec, precision="mixed")
+    V64, g64 = A.forward(cfg, u, spec)
+    with Handle(cfg, "mixed") as h:
+        h.set_universe(u)
+        st = h.step(spec.nsteps)
+    assert np.max(np.abs(Vm - V64) / np.abs(V64)) <= 1e-5
+    assert np.max(np.abs(Vm - st["potential"]) / np.abs(st["potential"])) <= 1e-5
+    assert np.max(np.abs(gm - g64)) <= 1e-4 * np.max(np.abs(g64))
+
+
+def test_mixed_forward_is_deterministic_and_checkpoint_invariant(gpu):
+    cfg, u = _small(coul=True)
+    T = 24
+    out = []
+    for K in (1, 5, 24):
+        from genesis_b200._lib import Handle
+        with Handle(cfg, "mixed") as h:
+            h.set_universe(u)
+            V, g = h.adjoint_forward(T, checkpoint_every=K, **GR)
+            gs, ge = h.adjoint_backward(dl_dpotential=np.full(T, 1.0 / T))
+        out.append((V, g, gs, ge))
+    for o in out[1:]:
+        for x, y in zip(out[0], o):
+            assert np.array_equal(x, y)
 
 
 def test_c5_gradients_match_dual_oracle(c5_case, orc):
