@@ -40,7 +40,7 @@ def _columns(u, pinned):
     return out
 
 
-def _run_pair(cfg, u, precision, variant, ticks, pinned, move=None):
+def _run_pair(cfg, u, precision, variant, ticks, pinned, move=None, bonds=None):
     from genesis_b200._lib import Handle
     keep = _columns(u, pinned)  # torch tensors stay alive while their arrays are used
     cols = [c.numpy() if hasattr(c, "numpy") else c for c in keep]
@@ -49,6 +49,8 @@ def _run_pair(cfg, u, precision, variant, ticks, pinned, move=None):
     for h in (ha, hb):
         h.set_kernel_variant(variant)
         h.set_universe(u)
+        if bonds is not None:
+            h.set_bonds(bonds)
     rec_a, rec_b = [], []
     for t in range(ticks):
         if move is not None and t == move:  # the host moves one atom by a box quarter
@@ -100,6 +102,21 @@ def test_host_moves_between_ticks(gpu):
         assert np.array_equal(x, y)
     assert np.array_equal(ra, rb)
     assert na == nb
+
+
+def test_spring_and_collisions_on_the_list_path(gpu):
+    # the spring and the collision pass run after the positions-final event:
+    # they write forces and velocities only
+    cfg, u = _lattice(12, temperature=300.0)
+    cfg.enable_bond_interaction = True
+    cfg.enable_collisions = True
+    cfg.particle_radius = 1.3  # contact 2.6, below the lattice spacing: neighbours touch
+    bonds = np.array([[2 * k, 2 * k + 1] for k in range(60)], dtype=np.uint32)
+    cols, ref, ra, rb, na, nb = _run_pair(cfg, u, "mixed", 6, 12, True, bonds=bonds)
+    for x, y in zip(cols, ref):
+        assert np.array_equal(x, y)
+    assert np.array_equal(ra, rb)
+    assert np.any(ra["bond_energy"] != 0.0)
 
 
 def test_tick_host_then_step_then_tick_host(gpu):
