@@ -331,14 +331,14 @@ __global__ void __launch_bounds__(kBnThreads) k_bn_force(const BnGeo* __restrict
                 for (int k = 0; k < 4; ++k) {
                     const float4 sh = sh_tab[w[k] >> 27];
                     const uint32_t q = w[k] & kBnIdxMask;
-                    nl_pair(L, st, ki, pi, pj[k], sh.x, sh.y, sh.z, ENERGY && q > s, a, err, F, q, fstride);
+                    nl_pair(L, st, ki, pi, pj[k], sh.x, sh.y, sh.z, ENERGY, a, err, F, q, fstride);  // half list: q > s
                 }
             }
             for (; e < m; ++e) {
                 const uint32_t w = __ldg(lp + (size_t)e * stride);
                 const float4 sh = sh_tab[w >> 27];
                 const uint32_t q = w & kBnIdxMask;
-                nl_pair(L, st, ki, pi, __ldg(pos4 + q), sh.x, sh.y, sh.z, ENERGY && q > s, a, err, F, q, fstride);
+                nl_pair(L, st, ki, pi, __ldg(pos4 + q), sh.x, sh.y, sh.z, ENERGY, a, err, F, q, fstride);  // half list: q > s
             }
         } else {  // overflowed list: the later slots of the home-grid cells
             const BnGeo& G = geo[r];
@@ -374,7 +374,7 @@ __global__ void __launch_bounds__(kBnThreads) k_bn_force(const BnGeo* __restrict
         }
     } else if (r != 0xFFFFFFFFu) {
         atomicAdd(&racc[2 * r], (unsigned long long)a.vq);
-        atomicAdd(&racc[2 * r + 1], a.np);
+        atomicAdd(&racc[2 * r + 1], (unsigned long long)a.np);
     }
 }
 

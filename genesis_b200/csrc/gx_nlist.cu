@@ -466,15 +466,16 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force(GridGeom g, const float
                 for (int k = 0; k < 4; ++k) {
                     float4 sh = s_shift[w[k] >> 27];
                     uint32_t q = w[k] & kIdxMask;
-                    nl_pair(L, st, ki, pi, pj[k], sh.x, sh.y, sh.z, ENERGY && q > p, a, err, HALF ? F : nullptr, q, fstride);
+                    nl_pair(L, st, ki, pi, pj[k], sh.x, sh.y, sh.z, ENERGY && (HALF || q > p), a, err, HALF ? F : nullptr, q,
+                            fstride);
                 }
             }
             for (; e < m; ++e) {
                 uint32_t w = __ldg(lp + (size_t)e * stride);
                 float4 sh = s_shift[w >> 27];
                 uint32_t q = w & kIdxMask;
-                nl_pair(L, st, ki, pi, __ldg(pos4 + q), sh.x, sh.y, sh.z, ENERGY && q > p, a, err, HALF ? F : nullptr, q,
-                        fstride);
+                nl_pair(L, st, ki, pi, __ldg(pos4 + q), sh.x, sh.y, sh.z, ENERGY && (HALF || q > p), a, err,
+                        HALF ? F : nullptr, q, fstride);
             }
         } else {  // overflowed list: scan the home-grid cells directly
             uint32_t cx, cy, cz;
@@ -553,14 +554,17 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force_tpp(GridGeom g, const f
                 float4 p0 = __ldg(pos4 + (w0 & kIdxMask)), p1 = __ldg(pos4 + (w1 & kIdxMask));
                 float4 s0 = s_shift[w0 >> 27], s1 = s_shift[w1 >> 27];
                 uint32_t q0 = w0 & kIdxMask, q1 = w1 & kIdxMask;
-                nl_pair(L, st, ki, pi, p0, s0.x, s0.y, s0.z, ENERGY && q0 > p, a, err, HALF ? F : nullptr, q0, fstride);
-                nl_pair(L, st, ki, pi, p1, s1.x, s1.y, s1.z, ENERGY && q1 > p, a, err, HALF ? F : nullptr, q1, fstride);
+                nl_pair(L, st, ki, pi, p0, s0.x, s0.y, s0.z, ENERGY && (HALF || q0 > p), a, err, HALF ? F : nullptr, q0,
+                        fstride);
+                nl_pair(L, st, ki, pi, p1, s1.x, s1.y, s1.z, ENERGY && (HALF || q1 > p), a, err, HALF ? F : nullptr, q1,
+                        fstride);
             }
             if (e < m) {
                 uint32_t w = __ldg(lp + (size_t)e * stride);
                 float4 sh = s_shift[w >> 27];
                 uint32_t q = w & kIdxMask;
-                nl_pair(L, st, ki, pi, __ldg(pos4 + q), sh.x, sh.y, sh.z, ENERGY && q > p, a, err, HALF ? F : nullptr,
+                nl_pair(L, st, ki, pi, __ldg(pos4 + q), sh.x, sh.y, sh.z, ENERGY && (HALF || q > p), a, err,
+                        HALF ? F : nullptr,
                         q, fstride);
             }
         } else {  // overflowed list: the group splits the 27 home-grid cells
@@ -923,7 +927,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force_brick(GridGeom g, const
                 for (int u = 0; u < 4; ++u) {
                     const float4 sh = s_shift[w[u] >> 27];
                     const uint32_t q = w[u] & kIdxMask;
-                    nl_pair(L, st, ki, pi, pj[u], sh.x, sh.y, sh.z, ENERGY && q > p, a, err, F, q, fstride);
+                    nl_pair(L, st, ki, pi, pj[u], sh.x, sh.y, sh.z, ENERGY, a, err, F, q, fstride);  // half list: q > p
                 }
             }
             for (; e < m; ++e) {
@@ -931,7 +935,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force_brick(GridGeom g, const
                 const uint32_t q = w & kIdxMask;
                 const float4 pj = brick_pos(S, staged, w, pos4);
                 const float4 sh = s_shift[w >> 27];
-                nl_pair(L, st, ki, pi, pj, sh.x, sh.y, sh.z, ENERGY && q > p, a, err, F, q, fstride);
+                nl_pair(L, st, ki, pi, pj, sh.x, sh.y, sh.z, ENERGY, a, err, F, q, fstride);  // half list: q > p
             }
         } else {  // overflowed list: scan the home-grid cells directly
             uint32_t cx, ccy, ccz;

@@ -142,7 +142,7 @@ void launch_force_mixed_tiled(gx_handle* h, const GridGeom& g, const float4* pos
 // end q (half lists), and with `once` the potential and pair count.
 struct PairAcc {
     long long fx = 0, fy = 0, fz = 0, vq = 0;
-    unsigned long long np = 0;
+    unsigned int np = 0;  // in-cutoff pairs of one thread (widened when summed)
 };
 
 // far != null: also subtract the pair force from the far end q (HALF lists).
@@ -155,14 +155,22 @@ __device__ __forceinline__ void nl_pair(const LawF32& L, const PairF* st, int ki
     float fs, v;
     pair_f32(L, st[ki * L.nkinds + __float_as_int(pj.w)], d2, fs, v);
     long long qx, qy, qz;
-    quant3(fmul(dx, fs), fmul(dy, fs), fmul(dz, fs), qx, qy, qz, err);
-    a.fx += qx;
-    a.fy += qy;
-    a.fz += qz;
     if (far) {
-        atomicAdd((unsigned long long*)&far[q], (unsigned long long)(-qx));
-        atomicAdd((unsigned long long*)&far[fstride + q], (unsigned long long)(-qy));
-        atomicAdd((unsigned long long*)&far[2 * fstride + q], (unsigned long long)(-qz));
+        // The far end's share quantised directly: the conversion rounds to
+        // nearest even, which is symmetric in sign, so these are exactly
+        // -quant(f) (flags included), and this end subtracts them.
+        quant3(-fmul(dx, fs), -fmul(dy, fs), -fmul(dz, fs), qx, qy, qz, err);
+        a.fx -= qx;
+        a.fy -= qy;
+        a.fz -= qz;
+        atomicAdd((unsigned long long*)&far[q], (unsigned long long)qx);
+        atomicAdd((unsigned long long*)&far[fstride + q], (unsigned long long)qy);
+        atomicAdd((unsigned long long*)&far[2 * fstride + q], (unsigned long long)qz);
+    } else {
+        quant3(fmul(dx, fs), fmul(dy, fs), fmul(dz, fs), qx, qy, qz, err);
+        a.fx += qx;
+        a.fy += qy;
+        a.fz += qz;
     }
     if (once) {
         a.vq += quant(v, err);
