@@ -564,8 +564,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_force_tpp(GridGeom g, const f
                 float4 sh = s_shift[w >> 27];
                 uint32_t q = w & kIdxMask;
                 nl_pair(L, st, ki, pi, __ldg(pos4 + q), sh.x, sh.y, sh.z, ENERGY && (HALF || q > p), a, err,
-                        HALF ? F : nullptr,
-                        q, fstride);
+                        HALF ? F : nullptr, q, fstride);
             }
         } else {  // overflowed list: the group splits the 27 home-grid cells
             uint32_t cx, cy, cz;
