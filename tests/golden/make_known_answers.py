@@ -90,6 +90,8 @@ CASES = [
      "atoms": 512, "world": [24.0, 24.0, 24.0], "t0": 20.0, "target": 180.0, "tau": 10.0, "ticks": 2500, "tol": 10.0},
     {"id": "fixed_bond_nve", "cite": "src/systems/forces.rs:453-538", "check": "r_eq * 0.5 + 0.15",
      "world": [32.0, 32.0, 32.0], "stretch": 0.15, "relax": 100, "window": 100, "gap": 1500, "energy_rel": 1e-3},
+    {"id": "quench_bonds_appear", "cite": "src/systems/forces.rs:433-451", "check": "u.run_ticks(6000);",
+     "atoms": 216, "world": [24.0, 24.0, 24.0], "t0": 300.0, "target": 80.0, "ticks": 6000},
 ]
 
 

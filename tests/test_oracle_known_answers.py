@@ -368,3 +368,23 @@ def test_threaded_forces_match_sequential(orc):
     assert n1 == n4
     assert np.array_equal(a1, a4)  # per-atom sums run in pair-list order on every split
     assert abs(v1 - v4) <= 1e-12 * abs(v1)
+
+
+def test_quench_bonds_appear(orc):
+    """A cold quench of a 6^3 lattice jams it: persistent pairs appear within
+    6,000 ticks (bond observation every tick, Berendsen to 80 K)."""
+    c = CASES["quench_bonds_appear"]
+    cfg = W.C1.config()
+    cfg.size = tuple(c["world"])
+    cfg.enable_thermostat = True
+    cfg.thermostat_temperature = c["target"]
+    n_side = round(c["atoms"] ** (1.0 / 3.0))
+    u = synth.lattice(n_side, c["world"][0] / n_side, 0.02, c["t0"], 0.01, 0)
+    assert u.n == c["atoms"]
+    tracker = orc.BondTracker(cfg)
+    pos, vel, acc = u.pos, u.vel, None
+    for tick in range(1, c["ticks"] + 1):
+        pos, vel, acc, _ = orc.ticks(cfg, pos, vel, acc, u.elem, u.charge, u.mass, 1)
+        bound = orc.bound_pairs(pos, u.elem, None, cfg.size, cfg.bond_k_bind, cfg.sigma)
+        st, _ = tracker.observe(bound, u.elem, tick)
+    assert st["bonded_pairs"] > 0
