@@ -74,6 +74,25 @@ bond_k_bind = 1.4
     assert c.thermostat_temperature == 80.0 and c.enable_thermostat and c.bond_k_bind == 1.4
 
 
+def test_config_partial_affinity_override_stays_partial():
+    # affinity_table_parses_and_roundtrips (config/mod.rs:536-573): O sets only
+    # its charge, so its sigma and epsilon stay the built-in ones
+    c = G.from_toml(BASE + "gravity_constant = 6.674e-11\n[physics.elements]\n"
+                    "Na = { sigma = 2.2, epsilon_k = 130.0, charge = 1.0 }\nO = { charge = -2.0 }\n"
+                    "[systems]\nenable_electrostatics = true\n")
+    o, na = E.by_name("O"), E.by_name("Na")
+    assert c.charge[o] == -2.0
+    assert c.sigma[o] == E.SIGMA[o] and c.epsilon_k[o] == E.EPSILON_K[o]
+    assert (c.sigma[na], c.epsilon_k[na], c.charge[na]) == (2.2, 130.0, 1.0)
+
+
+def test_config_unknown_affinity_symbol_is_named_in_the_error():
+    # affinity_table_with_unknown_symbol_is_rejected (config/mod.rs:575-605)
+    with pytest.raises(G.ConfigError, match="Faux"):
+        G.from_toml(BASE + "gravity_constant = 6.674e-11\n[physics.elements]\nFaux = { charge = -2.0 }\n"
+                    "[systems]\nenable_electrostatics = true\n")
+
+
 def test_element_names():
     assert E.by_name("Na") == 5 and E.by_name("Sodium") == 5 and E.by_name("sodium") == 5
     assert E.by_name("Xx") is None
